@@ -1,0 +1,332 @@
+"""ctypes view of the CPU oracle (test infrastructure only).
+
+Loads oracle/liboracle.so (the plain-C restatement, femoracle.c) and, when it has
+been built, oracle/_ref/libshipsim_ref.so (the reference's own sources compiled by
+oracle/Makefile, behind ref_shim.cpp).  Both expose the C interface of femoracle.h,
+under the prefixes ``or_`` and ``ref_``.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this module; the
+product path (sinking-simulator_b200/) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libshipsim_ref.so")
+
+MAT_LEN = 14
+POINT_LEN = 15
+INCR_LEN = 9
+FORMS_LEN = 1507
+SHELL_STATE_LEN = 129
+
+f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Tet32(C.Structure):
+    _fields_ = [("nodes", C.c_size_t), ("tets", C.c_size_t),
+                ("position", C.POINTER(C.c_float)), ("velocity", C.POINTER(C.c_float)),
+                ("mass", C.POINTER(C.c_float)), ("fixed", C.POINTER(C.c_uint32)),
+                ("index", C.POINTER(C.c_uint32)), ("rest_inv", C.POINTER(C.c_float)),
+                ("rest_volume", C.POINTER(C.c_float)), ("tet_force", C.POINTER(C.c_float)),
+                ("adj_offset", C.POINTER(C.c_uint32)), ("adj_entry", C.POINTER(C.c_uint32))]
+
+
+class Tet64(C.Structure):
+    _fields_ = [("nodes", C.c_size_t), ("tets", C.c_size_t),
+                ("position", C.POINTER(C.c_double)), ("velocity", C.POINTER(C.c_double)),
+                ("mass", C.POINTER(C.c_double)), ("fixed", C.POINTER(C.c_uint32)),
+                ("index", C.POINTER(C.c_uint32)), ("rest_inv", C.POINTER(C.c_double)),
+                ("rest_volume", C.POINTER(C.c_double)), ("tet_force", C.POINTER(C.c_double)),
+                ("adj_offset", C.POINTER(C.c_uint32)), ("adj_entry", C.POINTER(C.c_uint32)),
+                ("plastic", C.POINTER(C.c_double)), ("stress", C.POINTER(C.c_double)),
+                ("fext", C.POINTER(C.c_double)), ("energy", C.c_double * 5), ("step", C.c_long)]
+
+
+class Tet64Params(C.Structure):
+    _fields_ = [("E", C.c_double), ("nu", C.c_double), ("rho", C.c_double),
+                ("yield_", C.c_double), ("hardening", C.c_double), ("dt", C.c_double),
+                ("gravity", C.c_double), ("damping", C.c_double), ("ramp_steps", C.c_int),
+                ("polar_fixed", C.c_int)]
+
+
+class Shell(C.Structure):
+    _fields_ = [("nodes", C.c_size_t), ("elements", C.c_size_t),
+                ("rest", C.POINTER(C.c_double)), ("position", C.POINTER(C.c_double)),
+                ("velocity", C.POINTER(C.c_double)), ("mass", C.POINTER(C.c_double)),
+                ("pinned", C.POINTER(C.c_uint8)), ("index", C.POINTER(C.c_uint32)),
+                ("forms", C.POINTER(C.c_double)), ("state", C.POINTER(C.c_double)),
+                ("element_force", C.POINTER(C.c_double)), ("stress", C.POINTER(C.c_double)),
+                ("gauss_volume", C.POINTER(C.c_double)), ("adj_offset", C.POINTER(C.c_uint32)),
+                ("adj_entry", C.POINTER(C.c_uint32)), ("fext", C.POINTER(C.c_double)),
+                ("energy", C.c_double * 5), ("step", C.c_long)]
+
+
+class ShellParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("damping", C.c_double), ("rise_time", C.c_double)]
+
+
+def build_port() -> str:
+    """Compile liboracle.so with oracle/Makefile if it is missing (gcc is in the image)."""
+    if not os.path.exists(PORT_SO):
+        subprocess.run(["make", "-C", HERE, "port"], check=True, capture_output=True)
+    return PORT_SO
+
+
+def have_ref() -> bool:
+    return os.path.exists(REF_SO)
+
+
+class Oracle:
+    """One implementation of femoracle.h: prefix 'or_' (restatement) or 'ref_'."""
+
+    def __init__(self, which: str = "port"):
+        if which == "port":
+            self.lib = C.CDLL(build_port())
+            self.p = "or_"
+        elif which == "ref":
+            if not have_ref():
+                raise FileNotFoundError(REF_SO)
+            self.lib = C.CDLL(REF_SO)
+            self.p = "ref_"
+        else:
+            raise ValueError(which)
+        self.which = which
+        L = self.lib
+        g = self._fn
+        g("plastic_update", C.c_int, [f64p, C.c_double, f64p, f64p, f64p, C.c_void_p, f64p])
+        g("box_tet_sizes", None, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)])
+        g("box_tet_mesh", None, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, f32p, u32p])
+        g("tet32_rest_state", None, [C.POINTER(Tet32), C.c_float, C.c_float, C.c_float])
+        g("tet32_forces", None, [C.POINTER(Tet32), C.c_size_t, C.c_float, C.c_float, f32p])
+        g("tet32_step", None, [C.POINTER(Tet32), C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                               C.c_float, C.c_int])
+        g("tet32_critical_dt", C.c_float, [C.POINTER(Tet32), C.c_float, C.c_float, C.c_float, C.c_float])
+        g("tet64_rest_state", None, [C.POINTER(Tet64), C.c_double])
+        g("tet64_step", None, [C.POINTER(Tet64), C.POINTER(Tet64Params), C.c_int])
+        g("shell_forms", C.c_int, [f64p, C.c_int, f64p])
+        g("shell_mass", None, [f64p, C.c_double, f64p])
+        g("shell_gauss_volumes", None, [f64p, f64p])
+        g("shell_init_state", None, [f64p, f64p, f64p])
+        g("shell_plastic_update", C.c_int, [f64p, f64p, f64p, f64p, f64p, f64p, f64p, f64p])
+        g("shell_rotation", None, [f64p, f64p, f64p])
+        g("shell_stiffness", None, [f64p, C.c_double, C.c_double, C.c_int, f64p])
+        g("shell_critical_dt", C.c_double, [f64p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double])
+        g("plate_sizes", None, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)])
+        g("plate_mesh", None, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, f64p, u32p])
+        g("plate_pressure_load", None, [f64p, u32p, C.c_size_t, C.c_size_t, C.c_double, f64p])
+        g("shell_setup", None, [C.POINTER(Shell), f64p, C.c_double])
+        g("shell_step", None, [C.POINTER(Shell), f64p, C.POINTER(ShellParams), C.c_int])
+        g("shell_energy", None, [C.POINTER(Shell), f64p])
+        if which == "port":
+            g("tet64_critical_dt", C.c_double, [C.POINTER(Tet64), C.c_double, C.c_double, C.c_double,
+                                                C.c_double])
+        else:
+            g("shell_time_parallel", C.c_double, [C.POINTER(Shell), f64p, C.POINTER(ShellParams), C.c_int,
+                                                  C.c_int])
+            g("default_workers", C.c_uint, [])
+
+    def _fn(self, name, res, args):
+        f = getattr(self.lib, self.p + name)
+        f.restype = res
+        f.argtypes = args
+        setattr(self, name, f)
+
+
+def material(E=210e9, nu=0.3, yield_=235e6, hardening=1e9, kinematic=0.0, swift=None,
+             failure=None) -> np.ndarray:
+    """Flat point-law material (femoracle.h).  failure: (uniform, fracture) or None = never."""
+    m = np.zeros(MAT_LEN)
+    m[0], m[1], m[2], m[3], m[4] = E, nu, yield_, hardening, kinematic
+    if swift is not None:
+        m[5] = 1.0
+        m[6], m[7], m[8] = swift
+    if failure is None:
+        m[9], m[10] = np.inf, np.inf
+    else:
+        m[9], m[10] = failure
+    m[11], m[12], m[13] = 1.5, 1.0 / 3.0, -1.0 / 3.0
+    return m
+
+
+class TetMesh32:
+    """A fem::TetMesh in numpy arrays, bound to an or_tet32 struct."""
+
+    def __init__(self, o: Oracle, position, index):
+        self.o = o
+        self.position = np.array(position, np.float32).reshape(-1)
+        self.index = np.array(index, np.uint32).reshape(-1)
+        n = self.position.size // 3
+        t = self.index.size // 4
+        self.nodes, self.tets = n, t
+        self.velocity = np.zeros(3 * n, np.float32)
+        self.mass = np.zeros(n, np.float32)
+        self.fixed = np.zeros(n, np.uint32)
+        self.rest_inv = np.zeros(9 * t, np.float32)
+        self.rest_volume = np.zeros(t, np.float32)
+        self.tet_force = np.zeros(12 * t, np.float32)
+        self.adj_offset = np.zeros(n + 1, np.uint32)
+        self.adj_entry = np.zeros(4 * t, np.uint32)
+
+    def struct(self) -> Tet32:
+        s = Tet32()
+        s.nodes, s.tets = self.nodes, self.tets
+        for name, ct in (("position", C.c_float), ("velocity", C.c_float), ("mass", C.c_float),
+                         ("fixed", C.c_uint32), ("index", C.c_uint32), ("rest_inv", C.c_float),
+                         ("rest_volume", C.c_float), ("tet_force", C.c_float),
+                         ("adj_offset", C.c_uint32), ("adj_entry", C.c_uint32)):
+            setattr(s, name, _ptr(getattr(self, name), ct))
+        return s
+
+    def rest_state(self, E, nu, rho):
+        s = self.struct()
+        fixed = self.fixed.copy()
+        self.o.tet32_rest_state(C.byref(s), E, nu, rho)
+        self.fixed[:] = fixed
+
+    def step(self, E, nu, rho, dt, gravity, damping, steps):
+        s = self.struct()
+        self.o.tet32_step(C.byref(s), E, nu, rho, dt, gravity, damping, steps)
+
+    def copy(self):
+        c = TetMesh32.__new__(TetMesh32)
+        c.__dict__.update({k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
+        return c
+
+
+def box_tet_mesh(o: Oracle, lx, ly, lz, nx, ny, nz):
+    n, t = C.c_size_t(), C.c_size_t()
+    o.box_tet_sizes(nx, ny, nz, C.byref(n), C.byref(t))
+    pos = np.zeros(3 * n.value, np.float32)
+    idx = np.zeros(4 * t.value, np.uint32)
+    o.box_tet_mesh(lx, ly, lz, nx, ny, nz, pos, idx)
+    return pos, idx
+
+
+class TetMesh64:
+    """O-tet64 state (double, J2) bound to an or_tet64 struct."""
+
+    def __init__(self, o: Oracle, position32, index, fixed, fext=None, rho=7850.0):
+        self.o = o
+        self.position = np.ascontiguousarray(position32, np.float32).astype(np.float64).reshape(-1)
+        self.index = np.array(index, np.uint32).reshape(-1)
+        n = self.position.size // 3
+        t = self.index.size // 4
+        self.nodes, self.tets = n, t
+        self.velocity = np.zeros(3 * n)
+        self.mass = np.zeros(n)
+        self.fixed = np.ascontiguousarray(fixed, np.uint32)
+        self.rest_inv = np.zeros(9 * t)
+        self.rest_volume = np.zeros(t)
+        self.tet_force = np.zeros(12 * t)
+        self.adj_offset = np.zeros(n + 1, np.uint32)
+        self.adj_entry = np.zeros(4 * t, np.uint32)
+        self.plastic = np.zeros(7 * t)
+        self.stress = np.zeros(6 * t)
+        self.fext = None if fext is None else np.ascontiguousarray(fext, np.float64).reshape(-1)
+        self.energy = np.zeros(5)
+        self.steps = 0
+        self._s = self._make()
+        o.tet64_rest_state(C.byref(self._s), rho)
+
+    def _make(self) -> Tet64:
+        s = Tet64()
+        s.nodes, s.tets = self.nodes, self.tets
+        for name, ct in (("position", C.c_double), ("velocity", C.c_double), ("mass", C.c_double),
+                         ("fixed", C.c_uint32), ("index", C.c_uint32), ("rest_inv", C.c_double),
+                         ("rest_volume", C.c_double), ("tet_force", C.c_double),
+                         ("adj_offset", C.c_uint32), ("adj_entry", C.c_uint32),
+                         ("plastic", C.c_double), ("stress", C.c_double), ("fext", C.c_double)):
+            setattr(s, name, _ptr(getattr(self, name), ct))
+        s.step = 0
+        return s
+
+    def step(self, params: Tet64Params, steps: int):
+        self.o.tet64_step(C.byref(self._s), C.byref(params), steps)
+        self.energy[:] = list(self._s.energy)
+        self.steps = self._s.step
+
+
+def tet64_params(E=210e9, nu=0.3, rho=7850.0, yield_=235e6, hardening=1e9, dt=1e-7, gravity=0.0,
+                 damping=1.0, ramp_steps=0, polar_fixed=0) -> Tet64Params:
+    return Tet64Params(E, nu, rho, yield_, hardening, dt, gravity, damping, ramp_steps, polar_fixed)
+
+
+def plate_mesh(o: Oracle, lx, ly, t, nx, ny, nz=1):
+    n, e = C.c_size_t(), C.c_size_t()
+    o.plate_sizes(nx, ny, nz, C.byref(n), C.byref(e))
+    pos = np.zeros(3 * n.value)
+    idx = np.zeros(8 * e.value, np.uint32)
+    o.plate_mesh(lx, ly, t, nx, ny, nz, pos, idx)
+    return pos, idx
+
+
+class ShellModel:
+    """The composed explicit shell step (or_shell)."""
+
+    def __init__(self, o: Oracle, rest, index, pinned, mat, density=7850.0, fext=None, position=None):
+        self.o = o
+        self.mat = np.ascontiguousarray(mat, np.float64)
+        self.rest = np.ascontiguousarray(rest, np.float64).reshape(-1)
+        self.position = self.rest.copy() if position is None else np.ascontiguousarray(position, np.float64).reshape(-1).copy()
+        self.index = np.array(index, np.uint32).reshape(-1)
+        n = self.rest.size // 3
+        e = self.index.size // 8
+        self.nodes, self.elements = n, e
+        self.velocity = np.zeros(3 * n)
+        self.mass = np.zeros(n)
+        self.pinned = np.ascontiguousarray(pinned, np.uint8).reshape(-1)
+        self.forms = np.zeros(FORMS_LEN * e)
+        self.state = np.zeros(SHELL_STATE_LEN * e)
+        self.element_force = np.zeros(24 * e)
+        self.stress = np.zeros(48 * e)
+        self.gauss_volume = np.zeros(8 * e)
+        self.adj_offset = np.zeros(n + 1, np.uint32)
+        self.adj_entry = np.zeros(8 * e, np.uint32)
+        self.fext = None if fext is None else np.ascontiguousarray(fext, np.float64).reshape(-1)
+        self._s = Shell()
+        s = self._s
+        s.nodes, s.elements = n, e
+        for name, ct in (("rest", C.c_double), ("position", C.c_double), ("velocity", C.c_double),
+                         ("mass", C.c_double), ("pinned", C.c_uint8), ("index", C.c_uint32),
+                         ("forms", C.c_double), ("state", C.c_double), ("element_force", C.c_double),
+                         ("stress", C.c_double), ("gauss_volume", C.c_double),
+                         ("adj_offset", C.c_uint32), ("adj_entry", C.c_uint32), ("fext", C.c_double)):
+            setattr(s, name, _ptr(getattr(self, name), ct))
+        s.step = 0
+        o.shell_setup(C.byref(s), self.mat, density)
+
+    @property
+    def energy(self):
+        return np.array(list(self._s.energy))
+
+    @property
+    def steps(self):
+        return self._s.step
+
+    def step(self, dt, steps, damping=1.0, rise_time=0.0):
+        p = ShellParams(dt, damping, rise_time)
+        self.o.shell_step(C.byref(self._s), self.mat, C.byref(p), steps)
+
+    def compute_energy(self):
+        self.o.shell_energy(C.byref(self._s), self.mat)
+        return self.energy
+
+    def time_parallel(self, dt, steps, workers=0, rise_time=0.0):
+        p = ShellParams(dt, 1.0, rise_time)
+        return self.o.shell_time_parallel(C.byref(self._s), self.mat, C.byref(p), steps, workers)
