@@ -1,0 +1,121 @@
+/*
+ * femstep.h -- C ABI of the B200 explicit structural FEM step.
+ *
+ * One shared library, libfemstep.so, built for sm_100a.  Plain C types only: host
+ * pointers and sizes in, status codes out.  Every entry point below names the
+ * reference interface it replaces (paths relative to the solarbaron/sinking-simulator
+ * source tree).
+ *
+ * Status codes: 0 is success.  FEMSTEP_SKIP means "no usable CUDA device": callers
+ * degrade exactly as the reference's Vulkan back-ends do when there is no device
+ * (engine/gpu/fem_gpu.hpp:21-22, engine/gpu/zone_gpu.hpp:186-202).  Every other
+ * non-zero code is an error whose text is available from the *_error function of the
+ * handle, or femstep_last_error() when no handle was made.
+ *
+ * Threading: a handle is used from one host thread at a time, like the reference's
+ * solvers.  Handles are independent; each owns its device memory and stream.
+ */
+#ifndef FEMSTEP_H
+#define FEMSTEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEMSTEP_OK 0
+#define FEMSTEP_SKIP 1      /* no CUDA device */
+#define FEMSTEP_EINVAL 2    /* a size, index or adjacency that does not describe a mesh */
+#define FEMSTEP_ENOMEM 3    /* device or host allocation failed / over the memory budget */
+#define FEMSTEP_ECUDA 4     /* a CUDA call failed */
+#define FEMSTEP_ESTATE 5    /* call out of order (e.g. run before upload) */
+#define FEMSTEP_ETIMEOUT 6  /* a bounded device-side wait gave up */
+
+/* Text of the last error raised on this thread by a call that has no handle yet. */
+const char *femstep_last_error(void);
+/* Name of CUDA device 0, or FEMSTEP_SKIP.  Mirrors gpu::FemGpuSolver::deviceName
+   (engine/gpu/fem_gpu.hpp:37). */
+int femstep_device_name(char *buffer, size_t length);
+
+/* =====================================================================================
+ * Linear-tet step.  Replaces gpu::FemGpuSolver (engine/gpu/fem_gpu.hpp:17-45) and
+ * extends it to the J2 tet.
+ * ===================================================================================== */
+
+typedef enum {
+    /* Co-rotational linear-elastic tet in float, arithmetic of fem::tetForces /
+       fem::stepCpu (engine/sim/fem.cpp:73-117, 187-215): bit-identical to the
+       reference CPU step.  Uses the caller's mass / restInv / restVolume. */
+    FEMSTEP_TET_REF32 = 0,
+    /* J2 tet (linear isotropic hardening), FP32, displacement state, no compensation. */
+    FEMSTEP_TET_J2_F32 = 1,
+    /* J2 tet, FP32 with Kahan-compensated displacement and plastic strain. */
+    FEMSTEP_TET_J2_F32K = 2,
+    /* J2 tet in FP64: fem.cpp's kinematics with plasticity::update
+       (engine/sim/plasticity.cpp:319-505) at the single point; bit-identical to the
+       FP64 CPU composition of those two. */
+    FEMSTEP_TET_J2_F64 = 3
+} femstep_tet_mode;
+
+/* The reference's sim::fem::TetMesh (engine/sim/fem.hpp:38-68), as raw arrays. */
+typedef struct {
+    size_t nodes, tets;
+    const float *position;          /* 3N, fem.hpp:40 */
+    const float *velocity;          /* 3N, fem.hpp:41; NULL = at rest */
+    const float *mass;              /* N,  fem.hpp:42 (REF32; J2 modes lump it from density) */
+    const uint32_t *fixed;          /* N,  fem.hpp:43; non-zero pins the node; NULL = none */
+    const uint32_t *index;          /* 4T, fem.hpp:46 */
+    const float *rest_inv;          /* 9T, fem.hpp:47 (REF32) */
+    const float *rest_volume;       /* T,  fem.hpp:48 (REF32) */
+    const uint32_t *adjacency_offset; /* N+1, fem.hpp:56 */
+    const uint32_t *adjacency_entry;  /* 4T,  fem.hpp:57, entry = tet*4 + corner */
+    const double *external_force;   /* 3N full-amplitude nodal load, NULL = none (J2 modes) */
+    double density;                 /* kg/m^3, J2 modes: rest state is formed from it */
+} femstep_tet_mesh;
+
+typedef struct {
+    double youngs_modulus, poisson_ratio;   /* fem.hpp:24-27 Material */
+    double yield_strength, hardening_modulus; /* J2 modes: plasticity.hpp:115-118 linear curve */
+    double dt, gravity, damping;            /* FemGpuSolver::run arguments (fem_gpu.hpp:31) */
+    int ramp_steps;                         /* external load factor min((step+1)/ramp, 1); 0 = full */
+} femstep_tet_params;
+
+typedef struct femstep_tet femstep_tet;
+
+/* gpu::FemGpuSolver::initialise (fem_gpu.hpp:23, fem_gpu.cpp:183): validate and upload. */
+int femstep_tet_create(const femstep_tet_mesh *mesh, int mode, femstep_tet **out);
+/* gpu::FemGpuSolver::run (fem_gpu.hpp:31, fem_gpu.cpp:374): `substeps` steps on the
+   device, returns the device-measured milliseconds in *gpu_ms (may be NULL). */
+int femstep_tet_run(femstep_tet *solver, int substeps, const femstep_tet_params *params, double *gpu_ms);
+/* gpu::FemGpuSolver::readback (fem_gpu.hpp:35, fem_gpu.cpp:424): positions and
+   velocities back into the caller's 3N float arrays (either may be NULL). */
+int femstep_tet_readback(femstep_tet *solver, float *position, float *velocity);
+/* The same in double (exact for J2_F64; the FP32 modes add rest + displacement in double). */
+int femstep_tet_readback_f64(femstep_tet *solver, double *position, double *velocity);
+/* Per-tet plastic state, 7 doubles each: plastic strain [xx,yy,zz,xy,yz,zx]
+   (engineering shears, plasticity.hpp:74-88) and equivalent plastic strain. */
+int femstep_tet_plastic(femstep_tet *solver, double *plastic);
+/* Energy account reduced on the device in FP64 and fixed order:
+   [0] external work  [1] plastic dissipation  [2] strain energy (last force pass)
+   [3] kinetic  [4] gravity work.  Zeros for REF32, which keeps no account. */
+int femstep_tet_energy(femstep_tet *solver, double out[5]);
+/* Critical time step by the FP64 element eigenvalue bound, on the device:
+   safety * 2 / sqrt(max_e omega_e^2), omega_e^2 = (4/rho) lambda_max(B^T C B).
+   Replaces the edge heuristic fem::criticalTimestep (fem.cpp:183-185) with a bound. */
+int femstep_tet_critical_dt(femstep_tet *solver, double youngs, double poisson, double density,
+                            double safety, double *dt);
+/* Per-kernel device time: runs `steps` steps with CUDA events around each launch and
+   writes the mean milliseconds of [0] the element kernel and [1] the node kernel.
+   The same arithmetic as femstep_tet_run; used by the benchmark's roofline. */
+int femstep_tet_profile(femstep_tet *solver, int steps, const femstep_tet_params *params, double out[2]);
+/* Number of kernel launches the last femstep_tet_run issued. */
+long long femstep_tet_launches(const femstep_tet *solver);
+const char *femstep_tet_error(const femstep_tet *solver);
+void femstep_tet_destroy(femstep_tet *solver);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -140,6 +140,8 @@ class Oracle:
             g("shell_time_parallel", C.c_double, [C.POINTER(Shell), f64p, C.POINTER(ShellParams), C.c_int,
                                                   C.c_int])
             g("default_workers", C.c_uint, [])
+            g("tet64_time_parallel", C.c_double, [C.POINTER(Tet64), C.POINTER(Tet64Params), C.c_int, C.c_int])
+            g("tet32_time", C.c_double, [C.POINTER(Tet32), C.c_float, C.c_float, C.c_float, C.c_float, C.c_int])
 
     def _fn(self, name, res, args):
         f = getattr(self.lib, self.p + name)

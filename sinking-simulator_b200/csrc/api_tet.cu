@@ -1,0 +1,526 @@
+// api_tet.cu -- host side of the tet step behind the C ABI (include/femstep.h).
+//
+// Replaces gpu::FemGpuSolver (engine/gpu/fem_gpu.{hpp,cpp}): the same three calls
+// (initialise -> femstep_tet_create, run -> femstep_tet_run, readback ->
+// femstep_tet_readback) with the same ownership (the handle owns its device copy, the
+// caller keeps the host mesh) and the same error convention (a status plus text;
+// no device is a skip, not an abort).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/femstep.h"
+#include "common.cuh"
+#include "host_util.hpp"
+#include "tet.hpp"
+
+using fs::TetDevice;
+using fs::TetParams;
+
+struct femstep_tet {
+    int mode = 0;
+    size_t nodes = 0, tets = 0;
+    cudaStream_t stream = nullptr;
+    fs::DeviceArena arena;
+    TetDevice<float> d32;
+    TetDevice<double> d64;
+    std::vector<float> rest;          // FP32 J2 modes: rest positions for readback
+    std::vector<double> rest_inv64;   // J2 modes: Dm^-1 in double (critical dt)
+    int eblocks = 0, nblocks = 0;
+    double* d_out = nullptr;          // 8 doubles of reduction output
+    double* d_scratch = nullptr;      // per-block maxima for the critical step
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    TetParams graph_params{};
+    long long launches = 0;
+    std::string error;
+};
+
+namespace {
+
+int fail(femstep_tet* s, int code, const std::string& what) {
+    if (s) s->error = what;
+    fs::set_last_error(what);
+    return code;
+}
+
+// computeRestState (engine/sim/fem.cpp:119-158) in double from the float positions:
+// Dm^-1 (column-major, singular guard), |det|/6, lumped rho V / 4 per corner.
+void rest_state64(const femstep_tet_mesh& m, std::vector<double>& inv, std::vector<double>& vol,
+                  std::vector<double>& mass) {
+    const size_t T = m.tets;
+    inv.assign(T * 9, 0.0);
+    vol.assign(T, 0.0);
+    mass.assign(m.nodes, 0.0);
+    for (size_t t = 0; t < T; ++t) {
+        const uint32_t* idx = &m.index[t * 4];
+        double a[9];  // column-major
+        for (int c = 0; c < 3; ++c)
+            for (int r = 0; r < 3; ++r)
+                a[c * 3 + r] = (double)m.position[(size_t)idx[c + 1] * 3 + r] - (double)m.position[(size_t)idx[0] * 3 + r];
+#define A(r, c) a[(c) * 3 + (r)]
+        const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
+                           A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                           A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+        const double volume = det / 6.0;
+        vol[t] = std::fabs(volume);
+        const double id = std::fabs(det) > 1e-300 ? 1.0 / det : 0.0;
+        double* r = &inv[t * 9];
+#define R(rr, cc) r[(cc) * 3 + (rr)]
+        R(0, 0) = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) * id;
+        R(0, 1) = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * id;
+        R(0, 2) = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * id;
+        R(1, 0) = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) * id;
+        R(1, 1) = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * id;
+        R(1, 2) = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * id;
+        R(2, 0) = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) * id;
+        R(2, 1) = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * id;
+        R(2, 2) = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * id;
+#undef R
+#undef A
+        const double quarter = m.density * vol[t] * 0.25;
+        for (int c = 0; c < 4; ++c) mass[idx[c]] += quarter;
+    }
+}
+
+template <typename T>
+std::vector<T> soa(const T* aos, size_t count, int width) {
+    std::vector<T> out((size_t)width * count);
+    for (size_t i = 0; i < count; ++i)
+        for (int k = 0; k < width; ++k) out[(size_t)k * count + i] = aos[i * width + k];
+    return out;
+}
+
+int check(femstep_tet* s, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return FEMSTEP_OK;
+    return fail(s, e == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+TetParams make_params(const femstep_tet* s, const femstep_tet_params& p) {
+    TetParams q{};
+    if (s->mode == FEMSTEP_TET_REF32) {
+        // fem::Material::lameLambda / lameMu (fem.hpp:29-33), in float arithmetic.
+        const float E = (float)p.youngs_modulus, nu = (float)p.poisson_ratio;
+        q.lambda = (double)(E * nu / ((1.0f + nu) * (1.0f - 2.0f * nu)));
+        q.mu = (double)(E / (2.0f * (1.0f + nu)));
+    } else {
+        const double E = p.youngs_modulus, nu = p.poisson_ratio;
+        q.lambda = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
+        q.mu = E / (2.0 * (1.0 + nu));
+        q.bulk = E / (3.0 * (1.0 - 2.0 * nu));
+    }
+    q.yield = p.yield_strength;
+    q.hardening = p.hardening_modulus;
+    q.dt = p.dt;
+    q.gravity = p.gravity;
+    q.damping = p.damping;
+    q.ramp = p.ramp_steps;
+    return q;
+}
+
+void launch_step(femstep_tet* s, const TetParams& q, int parts = fs::kWholeStep) {
+    switch (s->mode) {
+        case FEMSTEP_TET_REF32: fs::launch_ref32_step(s->d32, q, s->stream, parts); break;
+        case FEMSTEP_TET_J2_F32: fs::launch_f32_step(s->d32, q, false, s->stream, parts); break;
+        case FEMSTEP_TET_J2_F32K: fs::launch_f32_step(s->d32, q, true, s->stream, parts); break;
+        default: fs::launch_f64_step(s->d64, q, s->stream, parts); break;
+    }
+}
+
+constexpr int kGraphSteps = 32;
+
+}  // namespace
+
+extern "C" {
+
+int femstep_tet_create(const femstep_tet_mesh* mesh, int mode, femstep_tet** out) {
+    if (out) *out = nullptr;
+    if (!mesh || !out) return fail(nullptr, FEMSTEP_EINVAL, "null mesh or output handle");
+    if (mode < FEMSTEP_TET_REF32 || mode > FEMSTEP_TET_J2_F64) return fail(nullptr, FEMSTEP_EINVAL, "unknown mode");
+    const femstep_tet_mesh& m = *mesh;
+    const size_t N = m.nodes, T = m.tets;
+    if (N == 0 || T == 0) return fail(nullptr, FEMSTEP_EINVAL, "empty mesh");
+    if (N >= 0xffffffffu || T * 4 >= 0xffffffffu) return fail(nullptr, FEMSTEP_EINVAL, "mesh too large for 32-bit ids");
+    if (!m.position || !m.index) return fail(nullptr, FEMSTEP_EINVAL, "position and index are required");
+    for (size_t i = 0; i < T * 4; ++i)
+        if (m.index[i] >= N) return fail(nullptr, FEMSTEP_EINVAL, "tet index out of range");
+    if (mode == FEMSTEP_TET_REF32 && (!m.mass || !m.rest_inv || !m.rest_volume))
+        return fail(nullptr, FEMSTEP_EINVAL, "REF32 needs the caller's mass, rest_inv and rest_volume");
+    if (mode != FEMSTEP_TET_REF32 && !(m.density > 0.0))
+        return fail(nullptr, FEMSTEP_EINVAL, "J2 modes need a positive density");
+
+    // CSR: the caller's (validated), or built by counting sort as fem.cpp:147-157.
+    std::vector<uint32_t> offset, entry;
+    if (m.adjacency_offset && m.adjacency_entry) {
+        offset.assign(m.adjacency_offset, m.adjacency_offset + N + 1);
+        entry.assign(m.adjacency_entry, m.adjacency_entry + T * 4);
+        if (offset[0] != 0 || offset[N] != T * 4) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets do not span 4T entries");
+        for (size_t n = 0; n < N; ++n)
+            if (offset[n + 1] < offset[n]) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets decrease");
+    } else {
+        fs::build_csr(N, T, 4, m.index, offset, entry);
+    }
+    std::vector<uint32_t> slot(T * 4, 0xffffffffu);
+    for (size_t n = 0; n < N; ++n)
+        for (uint32_t k = offset[n]; k < offset[n + 1]; ++k) {
+            const uint32_t e = entry[k];
+            if (e >= T * 4 || m.index[e] != n || slot[e] != 0xffffffffu)
+                return fail(nullptr, FEMSTEP_EINVAL, "adjacency is not the node-to-corner map of this mesh");
+            slot[e] = k;
+        }
+    // The mesh is checked before the device, so a bad mesh is reported as such on any
+    // machine; a good one on a machine with no GPU is a skip.
+    const int dev = fs::device_status();
+    if (dev != FEMSTEP_OK) return dev;
+
+    femstep_tet* s = new femstep_tet();
+    s->mode = mode;
+    s->nodes = N;
+    s->tets = T;
+    s->eblocks = fs::blocks_for((long long)T, fs::kBlock);
+    s->nblocks = fs::blocks_for((long long)N, fs::kBlock);
+    int rc = check(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    if (rc == FEMSTEP_OK) rc = check(s, cudaEventCreate(&s->ev0), "event");
+    if (rc == FEMSTEP_OK) rc = check(s, cudaEventCreate(&s->ev1), "event");
+    if (rc != FEMSTEP_OK) {
+        femstep_tet_destroy(s);
+        return rc;
+    }
+    fs::DeviceArena& A = s->arena;
+    std::vector<uint8_t> fixed(N, 0);
+    if (m.fixed)
+        for (size_t n = 0; n < N; ++n) fixed[n] = m.fixed[n] ? 1 : 0;
+
+    std::vector<double> inv64, vol64, mass64;
+    if (mode != FEMSTEP_TET_REF32) rest_state64(m, inv64, vol64, mass64);
+
+    auto common = [&](auto& d) {
+        d.nodes = (long long)N;
+        d.tets = (long long)T;
+        d.index = (const uint4*)A.upload(m.index, T * 4);
+        d.slot = (const uint4*)A.upload(slot.data(), T * 4);
+        d.fixed = A.upload(fixed.data(), N);
+        d.offset = A.upload(offset.data(), N + 1);
+        d.counter = A.zeros<long long>(2);
+        d.e_diss = A.zeros<double>(s->eblocks);
+        d.e_strain = A.zeros<double>(s->eblocks);
+        d.n_work = A.zeros<double>(s->nblocks);
+        d.n_kin = A.zeros<double>(s->nblocks);
+        d.n_grav = A.zeros<double>(s->nblocks);
+    };
+
+    if (mode == FEMSTEP_TET_J2_F64) {
+        TetDevice<double>& d = s->d64;
+        common(d);
+        std::vector<double> pos(N * 3), vel(N * 3, 0.0);
+        for (size_t i = 0; i < N * 3; ++i) pos[i] = m.position[i];
+        if (m.velocity)
+            for (size_t i = 0; i < N * 3; ++i) vel[i] = m.velocity[i];
+        d.position = A.upload(pos.data(), N * 3);
+        d.velocity = A.upload(vel.data(), N * 3);
+        d.mass = A.upload(mass64.data(), N);
+        const std::vector<double> inv_soa = soa(inv64.data(), T, 9);
+        d.rest_inv = A.upload(inv_soa.data(), T * 9);
+        d.rest_vol = A.upload(vol64.data(), T);
+        d.plastic = A.zeros<double>(T * 7);
+        if (m.external_force) d.ext = A.upload(m.external_force, N * 3);
+        d.slots = A.zeros<double>(T * 4 * 3 + 2);
+    } else {
+        TetDevice<float>& d = s->d32;
+        common(d);
+        std::vector<float> vel(N * 3, 0.0f);
+        if (m.velocity) std::memcpy(vel.data(), m.velocity, sizeof(float) * N * 3);
+        d.velocity = A.upload(vel.data(), N * 3);
+        d.slots = A.zeros<float>(T * 4 * 3 + 4);
+        if (mode == FEMSTEP_TET_REF32) {
+            d.position = A.upload(m.position, N * 3);
+            d.mass = A.upload(m.mass, N);
+            const std::vector<float> inv_soa = soa(m.rest_inv, T, 9);
+            d.rest_inv = A.upload(inv_soa.data(), T * 9);
+            d.rest_vol = A.upload(m.rest_volume, T);
+        } else {
+            s->rest.assign(m.position, m.position + N * 3);
+            d.rest = A.upload(m.position, N * 3);
+            d.disp = A.zeros<float>(N * 3);
+            if (mode == FEMSTEP_TET_J2_F32K) d.disp_c = A.zeros<float>(N * 3);
+            std::vector<float> mass(N), inv_mass(N), inv(T * 9), vol(T);
+            for (size_t n = 0; n < N; ++n) {
+                mass[n] = (float)mass64[n];
+                inv_mass[n] = mass64[n] > 0.0 ? (float)(1.0 / mass64[n]) : 0.0f;
+            }
+            for (size_t i = 0; i < T * 9; ++i) inv[i] = (float)inv64[i];
+            for (size_t t = 0; t < T; ++t) vol[t] = (float)vol64[t];
+            d.mass = A.upload(mass.data(), N);
+            d.inv_mass = A.upload(inv_mass.data(), N);
+            const std::vector<float> inv_soa = soa(inv.data(), T, 9);
+            d.rest_inv = A.upload(inv_soa.data(), T * 9);
+            d.rest_vol = A.upload(vol.data(), T);
+            d.plastic = A.zeros<float>(T * 7);
+            if (mode == FEMSTEP_TET_J2_F32K) d.plastic_c = A.zeros<float>(T * 7);
+            if (m.external_force) {
+                std::vector<float> ext(N * 3);
+                for (size_t i = 0; i < N * 3; ++i) ext[i] = (float)m.external_force[i];
+                d.ext = A.upload(ext.data(), N * 3);
+            }
+        }
+    }
+    if (mode != FEMSTEP_TET_REF32) s->rest_inv64 = std::move(inv64);
+    s->d_out = A.zeros<double>(8);
+    if (!A.ok()) {
+        const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;
+        fail(s, code, std::string("device upload failed: ") + cudaGetErrorString(A.status()));
+        femstep_tet_destroy(s);
+        return code;
+    }
+    *out = s;
+    return FEMSTEP_OK;
+}
+
+int femstep_tet_run(femstep_tet* s, int substeps, const femstep_tet_params* params, double* gpu_ms) {
+    if (!s || !params) return fail(s, FEMSTEP_EINVAL, "null solver or params");
+    if (substeps < 0) return fail(s, FEMSTEP_EINVAL, "negative step count");
+    if (!(params->dt > 0.0) || !std::isfinite(params->dt)) return fail(s, FEMSTEP_EINVAL, "dt must be positive");
+    const TetParams q = make_params(s, *params);
+    s->launches = 0;
+    int rc = check(s, cudaEventRecord(s->ev0, s->stream), "event record");
+    if (rc) return rc;
+    // Whole chunks replay one captured graph of kGraphSteps steps; the rest launch
+    // directly.  The graph bakes the parameters in, so it is rebuilt when they change.
+    int left = substeps;
+    if (left >= kGraphSteps) {
+        if (!s->graph || std::memcmp(&s->graph_params, &q, sizeof(q)) != 0) {
+            if (s->graph) cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+            cudaGraph_t g = nullptr;
+            rc = check(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "capture");
+            if (rc) return rc;
+            for (int i = 0; i < kGraphSteps; ++i) launch_step(s, q);
+            rc = check(s, cudaStreamEndCapture(s->stream, &g), "capture end");
+            if (rc) return rc;
+            rc = check(s, cudaGraphInstantiate(&s->graph, g, 0), "graph instantiate");
+            cudaGraphDestroy(g);
+            if (rc) return rc;
+            s->graph_params = q;
+        }
+        while (left >= kGraphSteps) {
+            rc = check(s, cudaGraphLaunch(s->graph, s->stream), "graph launch");
+            if (rc) return rc;
+            left -= kGraphSteps;
+            s->launches += 2 * kGraphSteps;
+        }
+    }
+    for (; left > 0; --left) {
+        launch_step(s, q);
+        s->launches += 2;
+    }
+    rc = check(s, cudaGetLastError(), "kernel launch");
+    if (rc) return rc;
+    rc = check(s, cudaEventRecord(s->ev1, s->stream), "event record");
+    if (rc) return rc;
+    rc = check(s, cudaEventSynchronize(s->ev1), "step");
+    if (rc) return rc;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    if (gpu_ms) *gpu_ms = ms;
+    return FEMSTEP_OK;
+}
+
+int femstep_tet_readback(femstep_tet* s, float* position, float* velocity) {
+    if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
+    const size_t n3 = s->nodes * 3;
+    int rc = FEMSTEP_OK;
+    if (s->mode == FEMSTEP_TET_J2_F64) {
+        std::vector<double> p, v;
+        rc = femstep_tet_readback_f64(s, position ? (p.resize(n3), p.data()) : nullptr,
+                                      velocity ? (v.resize(n3), v.data()) : nullptr);
+        if (rc) return rc;
+        if (position)
+            for (size_t i = 0; i < n3; ++i) position[i] = (float)p[i];
+        if (velocity)
+            for (size_t i = 0; i < n3; ++i) velocity[i] = (float)v[i];
+        return FEMSTEP_OK;
+    }
+    if (position) {
+        if (s->mode == FEMSTEP_TET_REF32) {
+            rc = check(s, cudaMemcpy(position, s->d32.position, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+        } else {
+            std::vector<float> u(n3);
+            rc = check(s, cudaMemcpy(u.data(), s->d32.disp, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = s->rest[i] + u[i];
+        }
+        if (rc) return rc;
+    }
+    if (velocity)
+        rc = check(s, cudaMemcpy(velocity, s->d32.velocity, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+    return rc;
+}
+
+int femstep_tet_readback_f64(femstep_tet* s, double* position, double* velocity) {
+    if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
+    const size_t n3 = s->nodes * 3;
+    int rc = FEMSTEP_OK;
+    if (s->mode == FEMSTEP_TET_J2_F64) {
+        if (position)
+            rc = check(s, cudaMemcpy(position, s->d64.position, n3 * sizeof(double), cudaMemcpyDeviceToHost), "readback");
+        if (!rc && velocity)
+            rc = check(s, cudaMemcpy(velocity, s->d64.velocity, n3 * sizeof(double), cudaMemcpyDeviceToHost), "readback");
+        return rc;
+    }
+    std::vector<float> p(n3), v(n3);
+    if (position) {
+        if (s->mode == FEMSTEP_TET_REF32) {
+            rc = check(s, cudaMemcpy(p.data(), s->d32.position, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = p[i];
+        } else {
+            rc = check(s, cudaMemcpy(p.data(), s->d32.disp, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = (double)s->rest[i] + (double)p[i];
+        }
+        if (rc) return rc;
+    }
+    if (velocity) {
+        rc = check(s, cudaMemcpy(v.data(), s->d32.velocity, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+        for (size_t i = 0; i < n3 && !rc; ++i) velocity[i] = v[i];
+    }
+    return rc;
+}
+
+int femstep_tet_plastic(femstep_tet* s, double* plastic) {
+    if (!s || !plastic) return fail(s, FEMSTEP_EINVAL, "null argument");
+    const size_t T = s->tets;
+    if (s->mode == FEMSTEP_TET_REF32) {
+        std::memset(plastic, 0, sizeof(double) * T * 7);
+        return FEMSTEP_OK;
+    }
+    if (s->mode == FEMSTEP_TET_J2_F64) {
+        std::vector<double> a(T * 7);
+        const int rc = check(s, cudaMemcpy(a.data(), s->d64.plastic, a.size() * sizeof(double), cudaMemcpyDeviceToHost), "readback");
+        if (rc) return rc;
+        for (size_t t = 0; t < T; ++t)
+            for (int k = 0; k < 7; ++k) plastic[t * 7 + k] = a[(size_t)k * T + t];
+        return FEMSTEP_OK;
+    }
+    std::vector<float> a(T * 7);
+    const int rc = check(s, cudaMemcpy(a.data(), s->d32.plastic, a.size() * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+    if (rc) return rc;
+    for (size_t t = 0; t < T; ++t)
+        for (int k = 0; k < 7; ++k) plastic[t * 7 + k] = a[(size_t)k * T + t];
+    return FEMSTEP_OK;
+}
+
+int femstep_tet_energy(femstep_tet* s, double out[5]) {
+    if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    for (int i = 0; i < 5; ++i) out[i] = 0.0;
+    if (s->mode == FEMSTEP_TET_REF32) return FEMSTEP_OK;
+    const bool f64 = s->mode == FEMSTEP_TET_J2_F64;
+    const double* arrays[5] = {f64 ? s->d64.n_work : s->d32.n_work, f64 ? s->d64.e_diss : s->d32.e_diss,
+                               f64 ? s->d64.e_strain : s->d32.e_strain, f64 ? s->d64.n_kin : s->d32.n_kin,
+                               f64 ? s->d64.n_grav : s->d32.n_grav};
+    const long long counts[5] = {s->nblocks, s->eblocks, s->eblocks, s->nblocks, s->nblocks};
+    for (int i = 0; i < 5; ++i) fs::launch_reduce_sum(arrays[i], counts[i], s->d_out + i, s->stream);
+    int rc = check(s, cudaGetLastError(), "reduce");
+    if (rc) return rc;
+    rc = check(s, cudaMemcpyAsync(out, s->d_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
+    if (rc) return rc;
+    return check(s, cudaStreamSynchronize(s->stream), "reduce");
+}
+
+int femstep_tet_critical_dt(femstep_tet* s, double youngs, double poisson, double density, double safety,
+                            double* dt) {
+    if (!s || !dt) return fail(s, FEMSTEP_EINVAL, "null argument");
+    if (!(density > 0.0)) return fail(s, FEMSTEP_EINVAL, "density must be positive");
+    const size_t T = s->tets;
+    const double* inv = nullptr;
+    double* tmp = nullptr;
+    int rc = FEMSTEP_OK;
+    if (s->mode == FEMSTEP_TET_J2_F64) {
+        inv = s->d64.rest_inv;
+    } else {
+        std::vector<double> host(T * 9);
+        if (s->mode == FEMSTEP_TET_REF32) {
+            std::vector<float> f(T * 9);
+            rc = check(s, cudaMemcpy(f.data(), s->d32.rest_inv, f.size() * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+            if (rc) return rc;
+            for (size_t i = 0; i < f.size(); ++i) host[i] = f[i];  // already SoA
+        } else {
+            const std::vector<double> a = soa(s->rest_inv64.data(), T, 9);
+            host = a;
+        }
+        rc = check(s, cudaMalloc(&tmp, host.size() * sizeof(double)), "alloc");
+        if (rc) return rc;
+        rc = check(s, cudaMemcpy(tmp, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
+        if (rc) {
+            cudaFree(tmp);
+            return rc;
+        }
+        inv = tmp;
+    }
+    double* block_max = nullptr;
+    rc = check(s, cudaMalloc(&block_max, sizeof(double) * s->eblocks), "alloc");
+    if (!rc) {
+        fs::launch_tet_omega2((long long)T, inv, youngs, poisson, density, block_max, s->eblocks, s->stream);
+        fs::launch_reduce_max(block_max, s->eblocks, s->d_out + 7, s->stream);
+        double w2 = 0.0;
+        rc = check(s, cudaMemcpyAsync(&w2, s->d_out + 7, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
+        if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "critical dt");
+        *dt = w2 > 0.0 ? safety * 2.0 / std::sqrt(w2) : 0.0;
+    }
+    cudaFree(block_max);
+    if (tmp) cudaFree(tmp);
+    return rc;
+}
+
+int femstep_tet_profile(femstep_tet* s, int steps, const femstep_tet_params* params, double out[2]) {
+    if (!s || !params || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    if (steps <= 0) return fail(s, FEMSTEP_EINVAL, "steps must be positive");
+    const TetParams q = make_params(s, *params);
+    std::vector<cudaEvent_t> ev(3 * (size_t)steps, nullptr);
+    int rc = FEMSTEP_OK;
+    for (auto& e : ev)
+        if (!rc) rc = check(s, cudaEventCreate(&e), "event");
+    for (int i = 0; i < steps && !rc; ++i) {
+        cudaEventRecord(ev[3 * i], s->stream);
+        launch_step(s, q, fs::kElementPart);
+        cudaEventRecord(ev[3 * i + 1], s->stream);
+        launch_step(s, q, fs::kNodePart);
+        cudaEventRecord(ev[3 * i + 2], s->stream);
+    }
+    if (!rc) rc = check(s, cudaGetLastError(), "kernel launch");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "profile");
+    double e_ms = 0.0, n_ms = 0.0;
+    for (int i = 0; i < steps && !rc; ++i) {
+        float a = 0.0f, b = 0.0f;
+        cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
+        cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]);
+        e_ms += a;
+        n_ms += b;
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    out[0] = e_ms / steps;
+    out[1] = n_ms / steps;
+    return rc;
+}
+
+long long femstep_tet_launches(const femstep_tet* s) { return s ? s->launches : 0; }
+
+const char* femstep_tet_error(const femstep_tet* s) { return s ? s->error.c_str() : fs::last_error(); }
+
+void femstep_tet_destroy(femstep_tet* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->arena.release();
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+}  // extern "C"

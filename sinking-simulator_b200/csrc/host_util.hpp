@@ -1,0 +1,77 @@
+// host_util.hpp -- host helpers shared by the C-ABI implementations.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace fs {
+
+// Thread-local text of the last failure raised before a handle existed.
+void set_last_error(const std::string& what);
+const char* last_error();
+
+// FEMSTEP_OK when a CUDA device is usable, FEMSTEP_SKIP (with the reason recorded)
+// when there is none -- the reference's "degrade, not abort" (fem_gpu.hpp:21-22).
+int device_status();
+
+// Every device allocation a handle makes, freed together.  Upload failures are sticky
+// so a constructor can do all its uploads and check once.
+class DeviceArena {
+public:
+    template <typename T>
+    T* alloc(size_t count) {
+        if (status_ != cudaSuccess) return nullptr;
+        void* p = nullptr;
+        const size_t bytes = count ? count * sizeof(T) : sizeof(T);
+        status_ = cudaMalloc(&p, bytes);
+        if (status_ != cudaSuccess) return nullptr;
+        ptrs_.push_back(p);
+        bytes_ += bytes;
+        return static_cast<T*>(p);
+    }
+    template <typename T>
+    T* upload(const T* host, size_t count) {
+        T* d = alloc<T>(count);
+        if (d && count) status_ = cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice);
+        return d;
+    }
+    template <typename T>
+    T* zeros(size_t count) {
+        T* d = alloc<T>(count);
+        if (d) status_ = cudaMemset(d, 0, (count ? count : 1) * sizeof(T));
+        return d;
+    }
+    bool ok() const { return status_ == cudaSuccess; }
+    cudaError_t status() const { return status_; }
+    size_t bytes() const { return bytes_; }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+        bytes_ = 0;
+    }
+
+private:
+    std::vector<void*> ptrs_;
+    size_t bytes_ = 0;
+    cudaError_t status_ = cudaSuccess;
+};
+
+// Node -> incident corner CSR by counting sort, the construction of
+// engine/sim/fem.cpp:147-157 and engine/sim/zone.cpp:739-754.
+inline void build_csr(size_t nodes, size_t elements, int corners, const uint32_t* index,
+                      std::vector<uint32_t>& offset, std::vector<uint32_t>& entry) {
+    offset.assign(nodes + 1, 0u);
+    for (size_t e = 0; e < elements; ++e)
+        for (int c = 0; c < corners; ++c) ++offset[index[e * corners + c] + 1];
+    for (size_t n = 0; n < nodes; ++n) offset[n + 1] += offset[n];
+    entry.assign(elements * corners, 0u);
+    std::vector<uint32_t> cursor(offset.begin(), offset.end() - 1);
+    for (size_t e = 0; e < elements; ++e)
+        for (int c = 0; c < corners; ++c)
+            entry[cursor[index[e * corners + c]]++] = (uint32_t)e * (uint32_t)corners + (uint32_t)c;
+}
+
+}  // namespace fs

@@ -1,0 +1,125 @@
+"""Tet step on the GPU, through the C ABI, against the oracle.
+
+REF32 and J2_F64 must be bit-identical to their CPU counterparts; the FP32 modes are
+held to the north-star tolerance against the FP64 oracle (1e-5 relative displacement,
+0.5 % energy-balance drift).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def cantilever(fem, nx=40, ny=4, nz=4, load=20e3):
+    """1.0 x 0.1 x 0.1 m, 6 Kuhn tets per cell, clamped at x = 0,
+    tip load spread equally over the x = 1 face nodes in -z."""
+    pos, idx = fem.box_tet_mesh(1.0, 0.1, 0.1, nx, ny, nz)
+    fixed = (pos[0::3] < 1e-6).astype(np.uint32)
+    tip = pos[0::3] > 1.0 - 1e-6
+    fext = np.zeros(pos.size)
+    fext[2::3][tip] = -load / tip.sum()
+    return pos, idx, fixed, fext
+
+
+def test_ref32_bit_identical_to_reference_step(fem, port):
+    """The fem_spike GPU-vs-CPU case (tools/fem_spike/main.cpp:143-222), where the
+    reference accepts 1e-4 after one step: here the GPU matches bit for bit."""
+    g = np.load(os.path.join(GOLDEN, "tet32_spike.npz"))
+    s = fem.TetSolver(g["start"], g["index"], mode="ref32", mass=g["mass"], fixed=g["fixed"],
+                      rest_inv=g["rest_inv"], rest_volume=g["rest_volume"], adjacency_offset=g["adj_offset"],
+                      adjacency_entry=g["adj_entry"])
+    dt = float(g["dt"])
+    done = 0
+    for target in (1, 10, 100):
+        s.run(target - done, youngs=210e9, poisson=0.3, dt=dt, gravity=9.80665, damping=1.0)
+        done = target
+        p, v = s.readback()
+        assert np.array_equal(p, g[f"position_{target}"]), target
+        assert np.array_equal(v, g[f"velocity_{target}"]), target
+    # and on to 1000 steps against the restatement (graph-captured chunks)
+    m = O.TetMesh32(port, g["start"], g["index"])
+    m.fixed[:] = g["fixed"]
+    for name in ("mass", "rest_inv", "rest_volume", "adj_offset", "adj_entry"):
+        getattr(m, name)[:] = g[name]
+    m.step(210e9, 0.3, 7850.0, dt, 9.80665, 1.0, 1000)
+    s.run(900, youngs=210e9, poisson=0.3, dt=dt, gravity=9.80665, damping=1.0)
+    p, v = s.readback()
+    assert np.array_equal(p, m.position) and np.array_equal(v, m.velocity)
+
+
+def test_f64_bit_identical_to_oracle(fem):
+    g = np.load(os.path.join(GOLDEN, "tet64_cantilever.npz"))
+    pos, idx, fixed, fext = cantilever(fem)
+    s = fem.TetSolver(pos, idx, mode="f64", fixed=fixed, external_force=fext, density=7850.0)
+    assert s.critical_dt(210e9, 0.3, 7850.0, 0.9) == float(g["dt"])
+    s.run(int(g["steps"]), dt=float(g["dt"]), ramp_steps=2000)
+    p, v = s.readback64()
+    assert np.array_equal(p, g["position"])
+    assert np.array_equal(v, g["velocity"])
+    assert np.array_equal(s.plastic().reshape(-1), g["plastic"])
+    e = s.energy()
+    assert np.allclose(e[:4], g["energy"][:4], rtol=1e-12, atol=1e-18)
+
+
+def _rel_disp_error(p, ref, rest):
+    u, ur = p - rest, ref - rest
+    return np.abs(u - ur).max() / np.abs(ur).max()
+
+
+@pytest.mark.parametrize("mode,tol", [("f32k", 1e-5), ("f32", 1e-3)])
+def test_f32_against_fp64_oracle(fem, port, mode, tol):
+    """2000 ramped steps of config 0 (scaled load so the root yields)."""
+    pos, idx, fixed, fext = cantilever(fem, load=60e3)
+    ref = O.TetMesh64(port, pos, idx, fixed, fext)
+    dt = port.tet64_critical_dt(C.byref(ref._s), 210e9, 0.3, 7850.0, 0.9)
+    params = O.tet64_params(dt=dt, ramp_steps=2000)
+    ref.step(params, 2000)
+    s = fem.TetSolver(pos, idx, mode=mode, fixed=fixed, external_force=fext, density=7850.0)
+    s.run(2000, dt=dt, ramp_steps=2000)
+    p, _ = s.readback64()
+    rest = pos.astype(np.float64)
+    err = _rel_disp_error(p, ref.position, rest)
+    yielded = (ref.plastic.reshape(-1, 7)[:, 6] > 0).mean()
+    assert yielded > 0.0, "the case must exercise plasticity"
+    assert err < tol, (mode, err)
+    e, er = s.energy(), ref.energy
+    # energy account against the oracle's, and its own balance
+    assert abs(e[0] - er[0]) / er[0] < 5e-3
+    drift = abs(e[0] - (e[1] + e[2] + e[3])) / e[0]
+    drift_ref = abs(er[0] - (er[1] + er[2] + er[3])) / er[0]
+    assert abs(drift - drift_ref) < 5e-3
+
+
+def test_graph_replay_is_bit_identical_to_single_launches(fem):
+    pos, idx, fixed, fext = cantilever(fem, nx=20, ny=2, nz=2)
+    a = fem.TetSolver(pos, idx, mode="f32k", fixed=fixed, external_force=fext, density=7850.0)
+    b = fem.TetSolver(pos, idx, mode="f32k", fixed=fixed, external_force=fext, density=7850.0)
+    dt = a.critical_dt()
+    a.run(96, dt=dt, ramp_steps=200)
+    for _ in range(96):
+        b.run(1, dt=dt, ramp_steps=200)
+    pa, va = a.readback()
+    pb, vb = b.readback()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert np.array_equal(a.energy(), b.energy())
+    assert a.launches == 2 * 96 and b.launches == 2
+
+
+def test_rest_stays_at_rest(fem):
+    """A patch at rest with no load stays at rest (tests/test_zone.cpp:483), in every mode."""
+    pos, idx, fixed, _ = cantilever(fem, nx=8, ny=2, nz=2)
+    for mode in ("f32", "f32k", "f64"):
+        s = fem.TetSolver(pos, idx, mode=mode, fixed=fixed, density=7850.0)
+        s.run(200, dt=s.critical_dt())
+        p, v = s.readback64()
+        # FP32 modes carry the displacement gradient, which is exactly zero at rest;
+        # FP64 carries F = Ds Dm^-1, whose rounding residue (~1e-16) may move a node
+        # by far less than a femtometre.
+        tol = 0.0 if mode != "f64" else 1e-15
+        assert np.abs(p - pos).max() <= tol and np.abs(v).max() <= tol * 1e3, mode
