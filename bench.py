@@ -3,19 +3,25 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-One JSON line from rank 0.  `value` is element-updates/s over all ranks (each rank
-steps its own replica: the meshes are independent, so there is no data-path
+One JSON line from rank 0.  `value` is element-updates/s over all ranks: each rank
+steps its own replica (the meshes are independent, so there is no data-path
 collective and the scaling is weak).  Inputs are resident in HBM when the timed region
-starts; the device time is taken with CUDA events on the library's own stream around
-exactly K steps, after W untimed warm-up steps, with a barrier and a device
-synchronize on both sides, and the maximum over ranks is reported.  `e2e` is the same
-metric through the C ABI from host buffers: upload (femstep_*_create), K steps,
-readback, all inside the timed region.
+starts; device time is taken with CUDA events on the library's stream around exactly
+K steps, after W untimed warm-up steps, with a barrier and a device synchronize on
+both sides; the maximum over ranks is reported.  Every workload moves more bytes per
+step than the 126 MB L2 holds, so no flush is needed between steps.  `e2e` is the same
+metric through the C ABI from host buffers: upload (femstep_*_create), K steps and the
+readback of positions and velocities, all inside one wall-clock region.
 
-Workloads (synthetic, seeded; no dataset is involved):
-  tet-precision   the 200x20x20-cell Kuhn beam of the precision study (480,000 tets,
-                  88,641 nodes), J2 FP32 with Kahan-compensated state
-  tet-cantilever  the 40x4x4 config-0 cantilever (3,840 tets), J2 FP32-compensated
+Workloads (synthetic and seeded; no dataset is involved):
+  shell-panel     the single-large-mesh case: a 20 x 10 m, 12 mm stiffened panel as
+                  2000 x 1000 solid-shell hexes (2.0 M elements, 4.0 M nodes), six
+                  longitudinal stiffener lines pinned, edges clamped, 1 mm seeded
+                  imperfection, 0.5 MPa Gaussian pulse (1.5 m, 5 ms rise); FP32 with
+                  Kahan-compensated state.  The default.
+  tet-precision   the precision-study beam, 200 x 20 x 20 cells x 6 Kuhn tets (480,000
+                  tets), J2 FP32-compensated, 200 kN tip load ramped over 10,000 steps
+  tet-cantilever  the 40 x 4 x 4 cantilever (3,840 tets), same element
 """
 from __future__ import annotations
 
@@ -37,9 +43,19 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 METRIC = "element-updates/s @1 B200 (batched vs plain, % HBM peak); p50/p99 step latency"
 UNIT = "element-updates/s"
 
+WORKLOADS = {
+    "shell-panel": dict(kind="shell", cells=(2000, 1000), sample_cells=(100, 50)),
+    # a 2 x 1 m corner of the same panel (20,000 elements, 0.14 GB per step): the size
+    # the ncu captures are taken on
+    "shell-sample": dict(kind="shell", cells=(200, 100), sample_cells=(100, 50)),
+    "tet-precision": dict(kind="tet", cells=(200, 20, 20), load=200e3, ramp=10000, mode="f32k"),
+    "tet-cantilever": dict(kind="tet", cells=(40, 4, 4), load=200e3, ramp=1000, mode="f32k"),
+}
+SHELL_MATERIAL = dict(youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9)
+
 
 # ---------------------------------------------------------------------------------
-# workloads
+# inputs
 
 def tet_beam(nx, ny, nz, length=1.0, width=0.1, depth=0.1, load=20e3):
     import femstep as F
@@ -52,24 +68,30 @@ def tet_beam(nx, ny, nz, length=1.0, width=0.1, depth=0.1, load=20e3):
     return pos, idx, fixed, fext
 
 
-WORKLOADS = {
-    # precision-study beam, load scaled with the cross-section (20 kN on 0.1 x 0.1
-    # grows with the grid as 1:1 here; the mesh is what sizes the workload)
-    "tet-precision": dict(kind="tet", cells=(200, 20, 20), load=60e3, mode="f32k"),
-    "tet-cantilever": dict(kind="tet", cells=(40, 4, 4), load=20e3, mode="f32k"),
-}
+def shell_panel(nx, ny):
+    import femstep as F
 
+    # the full panel is 2000 x 1000 cells of 10 mm; a sample keeps the cell size
+    return F.stiffened_panel(nx=nx, ny=ny, lx=20.0 * nx / 2000, ly=10.0 * ny / 1000)
+
+
+# ---------------------------------------------------------------------------------
+# algorithmic bytes (each array counted once per launch; 4-byte ints)
 
 def tet_bytes(T, N, mode):
-    """Algorithmic bytes of one element-kernel launch and one node-kernel launch
-    (each array counted once per launch; 4-byte ints)."""
-    if mode == "f64":
-        elem = T * (16 + 16 + 72 + 8 + 2 * 56 + 4 * 3 * 8) + N * 24
-        node = N * (4 + 2 * 24 + 2 * 24 + 8 + 1 + 24) + T * 4 * 24
-    else:
-        comp = 2 if mode == "f32k" else 1
-        elem = T * (16 + 16 + 36 + 4 + comp * 2 * 28 + 4 * 12) + N * 12
-        node = N * (4 + comp * 2 * 12 + 2 * 12 + 4 + 4 + 1 + 12) + T * 4 * 12
+    comp = 2 if mode == "f32k" else 1
+    elem = T * (16 + 16 + 36 + 4 + comp * 2 * 28 + 4 * 12) + N * 12
+    node = N * (4 + comp * 2 * 12 + 2 * 12 + 4 + 4 + 1 + 12) + T * 4 * 12
+    return elem, node
+
+
+def shell_bytes(E, N):
+    """Element kernel: forms 8 x 188 floats + J0^-1 36 + state R/W 2 x 8 x 14 floats +
+    alpha R/W 2 x 32 + index 32 + slot map 32 + corner forces 96, and the node reads
+    (rest 24 + displacement 12) once per node.  Node kernel: offsets 4, forces 12 per
+    slot, displacement and compensation R/W 48, velocity R/W 24, mass 8, pins 1, load 12."""
+    elem = E * (8 * 188 * 4 + 36 + 2 * 8 * 14 * 4 + 2 * 32 + 32 + 32 + 96) + N * (24 + 12)
+    node = N * (4 + 48 + 24 + 8 + 1 + 12) + E * 8 * 12
     return elem, node
 
 
@@ -85,17 +107,23 @@ class ClockSampler:
         self.device = device_index
         self.rows = []
         self.proc = None
+        self.mark = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except (OSError, ValueError):
             self.proc = None
         return self
+
+    def wait_first(self, limit=3.0):
+        """Block until the sampler has produced a line, so the timed region is covered."""
+        t0 = time.perf_counter()
+        while self.proc and not self.rows and time.perf_counter() - t0 < limit:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -112,15 +140,20 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in self.rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in self.rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
 
-
-# ---------------------------------------------------------------------------------
 
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -131,7 +164,7 @@ def measured_peak():
 
 
 def ncu_traffic(workload):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the dominant kernel, from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(path):
         with open(path) as f:
@@ -139,68 +172,137 @@ def ncu_traffic(workload):
     return None
 
 
+# ---------------------------------------------------------------------------------
+# the reference's CPU path on this box's host cores (bounded samples)
+
 def cpu_baseline(wl, seconds=15.0):
-    """The reference's CPU path on this box's host cores, on a bounded sample of the
-    same workload: the compiled reference (oracle/_ref) when present, else the C
-    restatement.  O-tet64: fem.cpp kinematics + plasticity::update in double, element
-    loop over all host cores with core::JobSystem, serial CSR gather."""
+    """The compiled reference (oracle/_ref) when present, else the C restatement.
+
+    tet:   O-tet64 -- fem.cpp kinematics + plasticity::update in double, element loop
+           over all host cores with core::JobSystem, serial CSR gather.
+    shell: zone::Solver's element loop (elementPlasticUpdate with cached RestForms,
+           zone.cpp:967) over all host cores with core::JobSystem, serial CSR gather and
+           node update, on a sub-panel with the full panel's 10 mm cells."""
     import oracle as O
 
     kind = "reference" if O.have_ref() else "port"
     o = O.Oracle("ref" if kind == "reference" else "port")
-    pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
-    m = O.TetMesh64(o, pos, idx, fixed, fext)
-    p = O.tet64_params(dt=1e-7, ramp_steps=2000)
     workers = os.cpu_count() or 1
-    T = idx.size // 4
-    if kind == "reference":
-        rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), 1, workers)  # warm
-        steps = max(1, int(seconds * rate / T))
-        rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), steps, workers)
-        cores = workers
+    if wl["kind"] == "tet":
+        pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
+        m = O.TetMesh64(o, pos, idx, fixed, fext)
+        p = O.tet64_params(dt=1e-7, ramp_steps=wl["ramp"])
+        T = idx.size // 4
+        if kind == "reference":
+            rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), 1, workers)
+            steps = max(1, int(seconds * rate / T))
+            rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), steps, workers)
+            cores = workers
+        else:
+            t0 = time.perf_counter()
+            m.step(p, 1)
+            rate = T / (time.perf_counter() - t0)
+            steps = max(1, int(seconds * rate / T))
+            t0 = time.perf_counter()
+            m.step(p, steps)
+            rate = T * steps / (time.perf_counter() - t0)
+            cores = 1
+        sample = f"{steps} steps of the {T}-tet workload mesh, FP64 J2 (O-tet64)"
     else:
-        t0 = time.perf_counter()
-        m.step(p, 1)
-        rate = T / (time.perf_counter() - t0)
-        steps = max(1, int(seconds * rate / T))
-        t0 = time.perf_counter()
-        m.step(p, steps)
-        rate = T * steps / (time.perf_counter() - t0)
-        cores = 1
-    return {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{steps} steps of the {T}-tet workload mesh, FP64 J2 (O-tet64)"}
+        nx, ny = wl["sample_cells"]
+        rest, index, pinned, load = shell_panel(nx, ny)
+        mat = O.material(E=206e9, nu=0.3, yield_=355e6, hardening=1e9)
+        m = O.ShellModel(o, rest, index, pinned, mat, fext=load)
+        E = index.size // 8
+        if kind == "reference":
+            rate = m.time_parallel(1e-6, 1, workers, rise_time=5e-3)
+            steps = max(1, int(seconds * rate / E))
+            rate = m.time_parallel(1e-6, steps, workers, rise_time=5e-3)
+            cores = workers
+        else:
+            t0 = time.perf_counter()
+            m.step(1e-6, 1, rise_time=5e-3)
+            rate = E / (time.perf_counter() - t0)
+            steps = max(1, int(seconds * rate / E))
+            t0 = time.perf_counter()
+            m.step(1e-6, steps, rise_time=5e-3)
+            rate = E * steps / (time.perf_counter() - t0)
+            cores = 1
+        sample = (f"{steps} steps of a {nx}x{ny}-cell sub-panel ({E} elements, the full panel's 10 mm cells), "
+                  "FP64 elastoplastic solid-shell")
+    return {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
 
 def run_reference(args, wl):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    t_all = []
-    base = None
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 1)):
         cpu_baseline(wl, seconds=2.0)
-    for _ in range(args.steps):
-        base = cpu_baseline(wl, seconds=max(2.0, 30.0 / max(args.steps, 1)))
-        t_all.append(base["value"])
-    value = float(np.median(t_all))
+    rates = []
+    base = None
+    per = max(2.0, 60.0 / max(args.steps, 1))
+    for _ in range(min(args.steps, 10)):
+        base = cpu_baseline(wl, seconds=per)
+        rates.append(base["value"])
+    value = float(np.median(rates))
     base["value"] = value
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": args.workload, "tets": int(np.prod(wl["cells"]) * 6)},
-           "cpu_baseline": base, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                                         "d2h_bytes_per_step": 0}}
+           "config": {"workload": args.workload}, "cpu_baseline": base,
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------------
+
+class Solver:
+    """One workload's solver behind a common face."""
+
+    def __init__(self, wl):
+        import femstep as F
+
+        self.wl = wl
+        if wl["kind"] == "tet":
+            pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
+            self.inputs = dict(position=pos, index=idx, fixed=fixed, external_force=fext)
+            self.units = idx.size // 4
+            self.nodes = pos.size // 3
+            self.make = lambda: F.TetSolver(pos, idx, mode=wl["mode"], fixed=fixed, external_force=fext,
+                                            density=7850.0)
+            s = self.make()
+            self.kw = dict(dt=s.critical_dt(210e9, 0.3, 7850.0, 0.9), ramp_steps=wl["ramp"])
+            self.bytes = tet_bytes(self.units, self.nodes, wl["mode"])
+            self.kernel = "f32_forces (tet element)"
+        else:
+            rest, index, pinned, load = shell_panel(*wl["cells"])
+            self.inputs = dict(rest=rest, index=index, pinned=pinned, load=load)
+            self.units = index.size // 8
+            self.nodes = rest.size // 3
+            self.make = lambda: F.ShellSolver(rest, index, pinned=pinned, load=load, density=7850.0)
+            s = self.make()
+            dt = s.critical_dt(206e9, 0.3, 7850.0, 0.9)
+            self.kw = dict(dt=dt, rise_time=5e-3, compensated=True, **SHELL_MATERIAL)
+            self.bytes = shell_bytes(self.units, self.nodes)
+            self.kernel = "shell_forces (solid-shell element)"
+        self.s = s
+
+    def readback(self, s):
+        return s.readback()
+
+    def h2d_bytes(self):
+        return sum(v.nbytes for v in self.inputs.values())
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tet-precision", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="shell-panel", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -212,24 +314,19 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
     if world > 1:
+        import datetime
+
         import torch
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        os.environ.setdefault("CUDA_VISIBLE_DEVICES", str(local))
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    else:
-        os.environ.setdefault("CUDA_VISIBLE_DEVICES", "0")
-
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     import femstep as F
 
-    pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
-    T, N = idx.size // 4, pos.size // 3
-    s = F.TetSolver(pos, idx, mode=wl["mode"], fixed=fixed, external_force=fext, density=7850.0)
-    dt = s.critical_dt(210e9, 0.3, 7850.0, 0.9)
-    kw = dict(dt=dt, ramp_steps=2000)
-
-    s.run(args.warmup, **kw)
+    F.set_device(local)  # one process per GPU
+    w = Solver(wl)
+    s = w.s
+    s.run(args.warmup, **w.kw)
 
     def barrier():
         if dist is not None:
@@ -240,59 +337,60 @@ def main():
 
     barrier()
     with ClockSampler(local) as clocks:
-        ms = s.run(args.steps, **kw)
-    launches = s.launches
-    barrier()
+        clocks.wait_first()
+        ms = s.run(args.steps, **w.kw)
+        launches = s.launches
+        barrier()
+        time.sleep(0.25)
     if dist is not None:
         import torch
 
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = T * args.steps * world / (ms / 1e3)
+    value = w.units * args.steps * world / (ms / 1e3)
 
-    # per-kernel device time for the roofline (separate, untimed for `value`)
-    elem_ms, node_ms = s.profile(20, **kw)
-    elem_b, node_b = tet_bytes(T, N, wl["mode"])
+    # per-kernel device time for the roofline (outside the timed region)
+    elem_ms, node_ms = s.profile(5, **w.kw)
+    elem_b, node_b = w.bytes
     peak, peak_kind = measured_peak()
     achieved = elem_b / (elem_ms / 1e3) / 1e9
-    traffic = ncu_traffic(args.workload)
+    stats = s.stats() if hasattr(s, "stats") else None
     s.close()
 
-    # end to end through the C ABI from host buffers
-    t0 = time.perf_counter()
-    e = F.TetSolver(pos, idx, mode=wl["mode"], fixed=fixed, external_force=fext, density=7850.0)
-    e.run(args.steps, **kw)
-    p_host, v_host = e.readback()
-    e.close()
-    wall = time.perf_counter() - t0
-    h2d = pos.nbytes + idx.nbytes + fixed.nbytes + fext.nbytes
-    d2h = p_host.nbytes + v_host.nbytes
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        e = w.make()
+        e.run(args.steps, **w.kw)
+        p_host, v_host = w.readback(e)
+        e.close()
+        wall = time.perf_counter() - t0
+        e2e = {"value": w.units * args.steps / wall, "unit": UNIT,
+               "h2d_bytes_per_step": w.h2d_bytes() / args.steps,
+               "d2h_bytes_per_step": (p_host.nbytes + v_host.nbytes) / args.steps,
+               "note": "upload + K steps + readback through the C ABI, wall clock"}
 
-    if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
-        return
-    out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "tets": T, "nodes": N, "mode": wl["mode"], "dt": dt,
-                   "element_kernel_ms": elem_ms, "node_kernel_ms": node_ms,
-                   "step_effective_gbs": (elem_b + node_b) / (ms / args.steps / 1e3) / 1e9,
-                   "l2": "inputs larger than L2 (%.0f MB per step)" % ((elem_b + node_b) / 1e6),
-                   "parallelism": f"replicas x{world}"},
-        "e2e": {"value": T * args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-                "d2h_bytes_per_step": d2h / args.steps},
-        "gpu_launches": launches,
-        "clocks": clocks.summary(),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": "element (f32_forces)",
-                     "peak_source": peak_kind},
-    }
-    if not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(wl)
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "elements": w.units, "nodes": w.nodes,
+                       "dt": w.kw["dt"], "element_kernel_ms": elem_ms, "node_kernel_ms": node_ms,
+                       "step_effective_gbs": (elem_b + node_b) / (ms / args.steps / 1e3) / 1e9,
+                       "l2": "no flush: %.1f GB move per step, above the 126 MB L2" % ((elem_b + node_b) / 1e9),
+                       "parallelism": f"replicas x{world}", "newton": stats},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic(args.workload), "kernel": w.kernel,
+                         "peak_source": peak_kind},
+        }
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(wl)
+        print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 

@@ -35,9 +35,13 @@ extern "C" {
 
 /* Text of the last error raised on this thread by a call that has no handle yet. */
 const char *femstep_last_error(void);
-/* Name of CUDA device 0, or FEMSTEP_SKIP.  Mirrors gpu::FemGpuSolver::deviceName
+/* Name of the current CUDA device, or FEMSTEP_SKIP.  Mirrors gpu::FemGpuSolver::deviceName
    (engine/gpu/fem_gpu.hpp:37). */
 int femstep_device_name(char *buffer, size_t length);
+/* Select the CUDA device the calling thread's subsequent handles are made on (one
+   process per GPU: device = local rank).  No reference counterpart: the reference
+   picks the first discrete Vulkan device (engine/gpu/fem_gpu.cpp:207-213). */
+int femstep_set_device(int device);
 
 /* =====================================================================================
  * Linear-tet step.  Replaces gpu::FemGpuSolver (engine/gpu/fem_gpu.hpp:17-45) and
@@ -114,6 +118,82 @@ int femstep_tet_profile(femstep_tet *solver, int steps, const femstep_tet_params
 long long femstep_tet_launches(const femstep_tet *solver);
 const char *femstep_tet_error(const femstep_tet *solver);
 void femstep_tet_destroy(femstep_tet *solver);
+
+/* =====================================================================================
+ * Solid-shell zone step.  Replaces gpu::ZoneGpuSolver (engine/gpu/zone_gpu.hpp:179-234):
+ * the 8-node ANS + 7-parameter EAS solid-shell with J2 plasticity (linear isotropic
+ * hardening, failure off), the CSR gather and the lumped-mass node update of
+ * zone::Solver::step (engine/sim/zone.cpp:928-989, 1094-1121, 1200-1202), in FP32 with
+ * optional Kahan-compensated displacement and plastic strain.
+ * ===================================================================================== */
+
+/* A solid-shell mesh: the reference's solidshell::HexMesh (solid_shell.hpp:464-477)
+   plus what zone::Solver hands its accelerator (zone.hpp:903-961). */
+typedef struct {
+    size_t nodes, elements;
+    const double *rest;             /* 3N rest positions (HexMesh::position) */
+    const double *position;         /* 3N current positions (Solver::position), NULL = rest */
+    const double *velocity;         /* 3N (Solver::velocity), NULL = at rest */
+    const uint32_t *index;          /* 8E, node order of solid_shell.hpp:115-126 */
+    const uint8_t *pinned;          /* 3N (Solver::pinnedDof / HexMesh::fixed), NULL = none */
+    const double *load;             /* 3N full-amplitude external nodal load, NULL = none */
+    const double *forms;            /* NULL: formed on the device in FP64.  Else the caller's
+                                       RestForms, 1505 doubles per element in the order of
+                                       engine/gpu/zone_gpu.cpp:28-34 (b, g, weight, J0^-1) */
+    const double *mass;             /* N lumped mass (Solver::nodalMass), NULL = lumped on device */
+    const double *state;            /* 129 doubles per element (zone_gpu.cpp:36-40 layout), NULL = virgin */
+    const uint32_t *adjacency_offset; /* N+1 (Solver::adjacencyOffset), NULL = built */
+    const uint32_t *adjacency_entry;  /* 8E, entry = element*8 + corner */
+    double density;                 /* kg/m^3, for the lumped mass when mass is NULL */
+} femstep_shell_mesh;
+
+typedef struct {
+    double youngs_modulus, poisson_ratio;      /* plasticity::Material (plasticity.hpp:220-228) */
+    double yield_strength, hardening_modulus;  /* linear curve (plasticity.hpp:115-118) */
+    double dt, damping;                        /* SolveParams::timestep / damping (zone.hpp:698-699) */
+    double rise_time;                          /* load factor min((step+1) dt / rise, 1); 0 = full */
+    int max_iterations;                        /* EAS Newton cap (CPU: 40) */
+    double tol_residual, tol_work;             /* Newton stops on ||r|| or |delta.r| below tol * sigma_y V */
+    int compensated;                           /* 1: Kahan-compensated displacement and plastic strain */
+} femstep_shell_params;
+
+typedef struct femstep_shell femstep_shell;
+
+/* gpu::ZoneGpuSolver::initialise (zone_gpu.hpp:203-207, zone_gpu.cpp:495). */
+int femstep_shell_create(const femstep_shell_mesh *mesh, femstep_shell **out);
+/* gpu::ZoneGpuSolver::run (zone_gpu.hpp:214, zone_gpu.cpp:877): device milliseconds. */
+int femstep_shell_run(femstep_shell *solver, int substeps, const femstep_shell_params *params, double *gpu_ms);
+/* gpu::ZoneGpuSolver::readback (zone_gpu.hpp:218, zone_gpu.cpp:932): positions (rest +
+   displacement, in double) and velocities; either may be NULL. */
+int femstep_shell_readback(femstep_shell *solver, double *position, double *velocity);
+/* Per-element plastic state in the 129-double layout of zone_gpu.cpp:36-40 (eight points
+   of plastic strain, back stress, eq. plastic strain, damage, failed; seven enhanced
+   parameters; failure strain; torn), the ElementPlasticState zone::Solver::adopt takes. */
+int femstep_shell_state(femstep_shell *solver, double *state);
+/* [0] external work [1] plastic dissipation [2] strain energy [3] kinetic, FP64 reduced
+   on the device in fixed order (zone::Solver::accumulateEnergy, zone.cpp:1014-1044). */
+int femstep_shell_energy(femstep_shell *solver, double out[4]);
+/* [0] element-steps whose EAS Newton hit its cap, [1] yielded Gauss points last step. */
+int femstep_shell_stats(femstep_shell *solver, long long out[2]);
+/* Smallest element critical step, FP64 power iteration per element on the device
+   (solidshell::criticalTimestep, solid_shell.cpp:1088-1133, 1187-1198). */
+int femstep_shell_critical_dt(femstep_shell *solver, double youngs, double poisson, double density,
+                              double safety, double *dt);
+/* Mean device ms of [0] the element kernel and [1] the node kernel over `steps` steps. */
+int femstep_shell_profile(femstep_shell *solver, int steps, const femstep_shell_params *params, double out[2]);
+long long femstep_shell_launches(const femstep_shell *solver);
+/* Bytes of device memory the solver holds. */
+size_t femstep_shell_device_bytes(const femstep_shell *solver);
+const char *femstep_shell_error(const femstep_shell *solver);
+void femstep_shell_destroy(femstep_shell *solver);
+
+/* RestForms of `elements` elements formed on the device in FP64
+   (solidshell::computeRestForms, solid_shell.cpp:237-375), with elementMass (:655) and
+   criticalTimestep (:1088).  nodes: 24 doubles per element.  forms_out: 1507 doubles per
+   element (1505 in zone_gpu.cpp order, then easCount, ok); mass_out: 8 per element;
+   dt_out: 1 per element; each may be NULL. */
+int femstep_shell_forms(const double *nodes, size_t elements, int formulation, double youngs, double poisson,
+                        double density, double safety, double *forms_out, double *mass_out, double *dt_out);
 
 #ifdef __cplusplus
 }

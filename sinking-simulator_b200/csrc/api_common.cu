@@ -33,11 +33,24 @@ extern "C" {
 
 const char* femstep_last_error(void) { return fs::last_error(); }
 
+int femstep_set_device(int device) {
+    const int st = fs::device_status();
+    if (st != FEMSTEP_OK) return st;
+    const cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        fs::set_last_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        return FEMSTEP_EINVAL;
+    }
+    return FEMSTEP_OK;
+}
+
 int femstep_device_name(char* buffer, size_t length) {
     const int st = fs::device_status();
     if (st != FEMSTEP_OK) return st;
+    int dev = 0;
+    cudaGetDevice(&dev);
     cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, 0) != cudaSuccess) return FEMSTEP_ECUDA;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return FEMSTEP_ECUDA;
     if (buffer && length) {
         std::strncpy(buffer, prop.name, length - 1);
         buffer[length - 1] = '\0';

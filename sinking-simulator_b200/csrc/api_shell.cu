@@ -1,0 +1,486 @@
+// api_shell.cu -- host side of the solid-shell zone step behind the C ABI.
+//
+// Replaces gpu::ZoneGpuSolver (engine/gpu/zone_gpu.{hpp,cpp}): initialise uploads the
+// patch (or forms it on the device), run records `substeps` steps without the host in
+// the loop, readback returns positions, velocities and the plastic state in the layout
+// zone::Solver::adopt consumes.  Errors are a status plus text; no device is a skip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/femstep.h"
+#include "common.cuh"
+#include "host_util.hpp"
+#include "shell.hpp"
+#include "tet.hpp"
+
+using fs::ShellDevice;
+using fs::ShellParams;
+
+struct femstep_shell {
+    size_t nodes = 0, elements = 0;
+    long long groups = 0;
+    cudaStream_t stream = nullptr;
+    fs::DeviceArena arena;
+    ShellDevice d;
+    int eblocks = 0, nblocks = 0;
+    double* d_out = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    ShellParams graph_params{};
+    long long launches = 0;
+    double failure_strain = INFINITY;
+    std::vector<double> rest;  // host copy for readback
+    std::string error;
+};
+
+namespace {
+
+int fail(femstep_shell* s, int code, const std::string& what) {
+    if (s) s->error = what;
+    fs::set_last_error(what);
+    return code;
+}
+
+int check(femstep_shell* s, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return FEMSTEP_OK;
+    return fail(s, e == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+ShellParams make_params(const femstep_shell_params& p) {
+    ShellParams q{};
+    const double E = p.youngs_modulus, nu = p.poisson_ratio;
+    q.dmu = E / (2.0 * (1.0 + nu));
+    q.dkappa = E / (3.0 * (1.0 - 2.0 * nu));
+    q.mu = (float)q.dmu;
+    q.kappa = (float)q.dkappa;
+    q.yield = (float)p.yield_strength;
+    q.hardening = (float)p.hardening_modulus;
+    q.dt = (float)p.dt;
+    q.dt64 = p.dt;
+    q.damping = (float)p.damping;
+    q.rise_time = p.rise_time;
+    q.max_iterations = p.max_iterations > 0 ? p.max_iterations : 12;
+    q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 1e-6);
+    q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-13);
+    q.compensated = p.compensated;
+    return q;
+}
+
+constexpr int kGraphSteps = 16;
+
+}  // namespace
+
+extern "C" {
+
+int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
+    if (out) *out = nullptr;
+    if (!mesh || !out) return fail(nullptr, FEMSTEP_EINVAL, "null mesh or output handle");
+    const femstep_shell_mesh& m = *mesh;
+    const size_t N = m.nodes, E = m.elements;
+    if (N == 0 || E == 0) return fail(nullptr, FEMSTEP_EINVAL, "empty mesh");
+    if (N >= 0xffffffffu || E * 8 >= 0xffffffffu) return fail(nullptr, FEMSTEP_EINVAL, "mesh too large for 32-bit ids");
+    if (!m.rest || !m.index) return fail(nullptr, FEMSTEP_EINVAL, "rest and index are required");
+    for (size_t i = 0; i < E * 8; ++i)
+        if (m.index[i] >= N) return fail(nullptr, FEMSTEP_EINVAL, "element index out of range");
+    if (!m.mass && !(m.density > 0.0)) return fail(nullptr, FEMSTEP_EINVAL, "need a lumped mass or a positive density");
+    std::vector<uint32_t> offset, entry;
+    if (m.adjacency_offset && m.adjacency_entry) {
+        offset.assign(m.adjacency_offset, m.adjacency_offset + N + 1);
+        entry.assign(m.adjacency_entry, m.adjacency_entry + E * 8);
+        if (offset[0] != 0 || offset[N] != E * 8) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets do not span 8E entries");
+    } else {
+        fs::build_csr(N, E, 8, m.index, offset, entry);
+    }
+    std::vector<uint32_t> slot(E * 8, 0xffffffffu);
+    for (size_t n = 0; n < N; ++n) {
+        if (offset[n + 1] < offset[n]) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets decrease");
+        for (uint32_t k = offset[n]; k < offset[n + 1]; ++k) {
+            const uint32_t e = entry[k];
+            if (e >= E * 8 || m.index[e] != n || slot[e] != 0xffffffffu)
+                return fail(nullptr, FEMSTEP_EINVAL, "adjacency is not the node-to-corner map of this mesh");
+            slot[e] = k;
+        }
+    }
+    const int dev = fs::device_status();
+    if (dev != FEMSTEP_OK) return dev;
+
+    femstep_shell* s = new femstep_shell();
+    s->nodes = N;
+    s->elements = E;
+    s->groups = (long long)((E + 3) / 4);
+    s->eblocks = fs::blocks_for(s->groups * 32, fs::kShellBlock);
+    s->nblocks = fs::blocks_for((long long)N, fs::kShellNodeBlock);
+    int rc = check(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = check(s, cudaEventCreate(&s->ev0), "event");
+    if (!rc) rc = check(s, cudaEventCreate(&s->ev1), "event");
+    if (rc) {
+        femstep_shell_destroy(s);
+        return rc;
+    }
+    fs::DeviceArena& A = s->arena;
+    ShellDevice& d = s->d;
+    const size_t Epad = (size_t)s->groups * 4;
+    d.nodes = (long long)N;
+    d.elements = (long long)E;
+    d.groups = s->groups;
+    s->rest.assign(m.rest, m.rest + N * 3);
+    d.rest = A.upload(m.rest, N * 3);
+    d.index = A.upload(m.index, E * 8);
+    d.slot = A.upload(slot.data(), E * 8);
+    d.offset = A.upload(offset.data(), N + 1);
+    float4* forms = A.zeros<float4>((size_t)s->groups * fs::kShellRec4 * 32);
+    d.forms = forms;
+    float* j0 = A.zeros<float>(E * 9);
+    d.j0inv = j0;
+    d.state = A.zeros<float>((size_t)s->groups * fs::kShellStateQ * 32);
+    d.alpha = A.zeros<float>(Epad * 8);
+    d.slots = A.zeros<float>(E * 8 * 3 + 4);
+    d.counter = A.zeros<long long>(2);
+    d.e_diss = A.zeros<double>(s->eblocks);
+    d.e_strain = A.zeros<double>(s->eblocks);
+    d.e_stats = A.zeros<int>((size_t)s->eblocks * 2);
+    d.n_work = A.zeros<double>(s->nblocks);
+    d.n_kin = A.zeros<double>(s->nblocks);
+    s->d_out = A.zeros<double>(8);
+
+    // nodes
+    std::vector<float> disp(N * 3, 0.0f), vel(N * 3, 0.0f);
+    if (m.position)
+        for (size_t i = 0; i < N * 3; ++i) disp[i] = (float)(m.position[i] - m.rest[i]);
+    if (m.velocity)
+        for (size_t i = 0; i < N * 3; ++i) vel[i] = (float)m.velocity[i];
+    d.disp = A.upload(disp.data(), N * 3);
+    d.disp_c = A.zeros<float>(N * 3);
+    d.velocity = A.upload(vel.data(), N * 3);
+    std::vector<uint8_t> pin(N, 0);
+    if (m.pinned)
+        for (size_t n = 0; n < N; ++n)
+            pin[n] = (uint8_t)((m.pinned[n * 3] ? 1 : 0) | (m.pinned[n * 3 + 1] ? 2 : 0) | (m.pinned[n * 3 + 2] ? 4 : 0));
+    d.pinned = A.upload(pin.data(), N);
+    if (m.load) {
+        std::vector<float> load(N * 3);
+        for (size_t i = 0; i < N * 3; ++i) load[i] = (float)m.load[i];
+        d.load = A.upload(load.data(), N * 3);
+    }
+    float* mass = A.alloc<float>(N);
+    float* inv_mass = A.alloc<float>(N);
+    d.mass = mass;
+    d.inv_mass = inv_mass;
+
+    // forms: the caller's (narrowed to float, as zone_gpu.cpp:668-684 does), or formed here
+    if (A.ok() && m.forms) {
+        std::vector<float4> rec((size_t)s->groups * fs::kShellRec4 * 32, make_float4(0, 0, 0, 0));
+        std::vector<float> j(E * 9);
+        for (size_t e = 0; e < E; ++e) {
+            const double* f = m.forms + e * 1505;
+            for (int gp = 0; gp < 8; ++gp) {
+                float r[fs::kShellRec];
+                for (int i = 0; i < 6; ++i)
+                    for (int c = 0; c < 24; ++c) r[i * 24 + c] = (float)f[(gp * 6 + i) * 24 + c];
+                for (int i = 0; i < 6; ++i)
+                    for (int k = 0; k < 7; ++k) r[144 + i * 7 + k] = (float)f[1152 + (gp * 6 + i) * 7 + k];
+                r[186] = (float)f[1488 + gp];
+                r[187] = 0.0f;
+                const size_t base = (e / 4) * fs::kShellRec4 * 32 + (e % 4) * 8 + gp;
+                for (int k = 0; k < fs::kShellRec4; ++k)
+                    rec[base + (size_t)k * 32] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
+            }
+            for (int k = 0; k < 9; ++k) j[e * 9 + k] = (float)f[1496 + k];
+        }
+        cudaMemcpy(forms, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice);
+        cudaMemcpy(j0, j.data(), j.size() * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    double* corner_mass = nullptr;
+    if (A.ok() && (!m.forms || !m.mass)) {
+        corner_mass = m.mass ? nullptr : A.zeros<double>(E * 8);
+        fs::ShellSetupArgs a{};
+        a.elements = (long long)E;
+        a.groups = s->groups;
+        a.rest = d.rest;
+        a.index = d.index;
+        a.slot = d.slot;
+        a.formulation = 2;
+        a.density = m.density;
+        a.forms = m.forms ? nullptr : forms;
+        a.j0inv = m.forms ? nullptr : j0;
+        a.corner_mass = corner_mass;
+        fs::launch_shell_setup(a, s->stream);
+        if (corner_mass) fs::launch_shell_mass((long long)N, d.offset, corner_mass, nullptr, mass, inv_mass, s->stream);
+        cudaStreamSynchronize(s->stream);
+        rc = check(s, cudaGetLastError(), "rest forms");
+        if (rc) {
+            femstep_shell_destroy(s);
+            return rc;
+        }
+    }
+    if (A.ok() && m.mass) {
+        std::vector<float> mf(N), im(N);
+        for (size_t n = 0; n < N; ++n) {
+            mf[n] = (float)m.mass[n];
+            im[n] = m.mass[n] > 0.0 ? (float)(1.0 / m.mass[n]) : 0.0f;
+        }
+        cudaMemcpy(mass, mf.data(), N * sizeof(float), cudaMemcpyHostToDevice);
+        cudaMemcpy(inv_mass, im.data(), N * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    if (A.ok() && m.state) {
+        std::vector<float> st((size_t)s->groups * fs::kShellStateQ * 32, 0.0f), al(Epad * 8, 0.0f);
+        for (size_t e = 0; e < E; ++e) {
+            const double* x = m.state + e * 129;
+            for (int gp = 0; gp < 8; ++gp) {
+                const size_t base = (e / 4) * fs::kShellStateQ * 32 + (e % 4) * 8 + gp;
+                for (int k = 0; k < 6; ++k) st[base + (size_t)k * 32] = (float)x[gp * 15 + k];
+                st[base + (size_t)6 * 32] = (float)x[gp * 15 + 12];
+            }
+            for (int k = 0; k < 7; ++k) al[e * 8 + k] = (float)x[120 + k];
+        }
+        s->failure_strain = m.state[127];
+        cudaMemcpy(d.state, st.data(), st.size() * sizeof(float), cudaMemcpyHostToDevice);
+        cudaMemcpy(d.alpha, al.data(), al.size() * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    if (!A.ok()) {
+        const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;
+        fail(s, code, std::string("device upload failed: ") + cudaGetErrorString(A.status()));
+        femstep_shell_destroy(s);
+        return code;
+    }
+    rc = check(s, cudaDeviceSynchronize(), "upload");
+    if (rc) {
+        femstep_shell_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params* params, double* gpu_ms) {
+    if (!s || !params) return fail(s, FEMSTEP_EINVAL, "null solver or params");
+    if (substeps < 0) return fail(s, FEMSTEP_EINVAL, "negative step count");
+    if (!(params->dt > 0.0) || !std::isfinite(params->dt)) return fail(s, FEMSTEP_EINVAL, "dt must be positive");
+    const ShellParams q = make_params(*params);
+    s->launches = 0;
+    int rc = check(s, cudaEventRecord(s->ev0, s->stream), "event record");
+    if (rc) return rc;
+    int left = substeps;
+    if (left >= kGraphSteps) {
+        if (!s->graph || std::memcmp(&s->graph_params, &q, sizeof(q)) != 0) {
+            if (s->graph) cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+            cudaGraph_t g = nullptr;
+            rc = check(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "capture");
+            if (rc) return rc;
+            for (int i = 0; i < kGraphSteps; ++i) fs::launch_shell_step(s->d, q, s->stream, 3);
+            rc = check(s, cudaStreamEndCapture(s->stream, &g), "capture end");
+            if (rc) return rc;
+            rc = check(s, cudaGraphInstantiate(&s->graph, g, 0), "graph instantiate");
+            cudaGraphDestroy(g);
+            if (rc) return rc;
+            s->graph_params = q;
+        }
+        while (left >= kGraphSteps) {
+            rc = check(s, cudaGraphLaunch(s->graph, s->stream), "graph launch");
+            if (rc) return rc;
+            left -= kGraphSteps;
+            s->launches += 2 * kGraphSteps;
+        }
+    }
+    for (; left > 0; --left) {
+        fs::launch_shell_step(s->d, q, s->stream, 3);
+        s->launches += 2;
+    }
+    rc = check(s, cudaGetLastError(), "kernel launch");
+    if (!rc) rc = check(s, cudaEventRecord(s->ev1, s->stream), "event record");
+    if (!rc) rc = check(s, cudaEventSynchronize(s->ev1), "step");
+    if (rc) return rc;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    if (gpu_ms) *gpu_ms = ms;
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_readback(femstep_shell* s, double* position, double* velocity) {
+    if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
+    const size_t n3 = s->nodes * 3;
+    std::vector<float> buf(n3);
+    int rc = FEMSTEP_OK;
+    if (position) {
+        rc = check(s, cudaMemcpy(buf.data(), s->d.disp, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+        if (rc) return rc;
+        for (size_t i = 0; i < n3; ++i) position[i] = s->rest[i] + (double)buf[i];
+    }
+    if (velocity) {
+        rc = check(s, cudaMemcpy(buf.data(), s->d.velocity, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+        if (rc) return rc;
+        for (size_t i = 0; i < n3; ++i) velocity[i] = buf[i];
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_state(femstep_shell* s, double* state) {
+    if (!s || !state) return fail(s, FEMSTEP_EINVAL, "null argument");
+    const size_t E = s->elements;
+    std::vector<float> st((size_t)s->groups * fs::kShellStateQ * 32), al((size_t)s->groups * 4 * 8);
+    int rc = check(s, cudaMemcpy(st.data(), s->d.state, st.size() * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+    if (!rc) rc = check(s, cudaMemcpy(al.data(), s->d.alpha, al.size() * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+    if (rc) return rc;
+    for (size_t e = 0; e < E; ++e) {
+        double* x = state + e * 129;
+        std::fill(x, x + 129, 0.0);
+        for (int gp = 0; gp < 8; ++gp) {
+            const size_t base = (e / 4) * fs::kShellStateQ * 32 + (e % 4) * 8 + gp;
+            for (int k = 0; k < 6; ++k) x[gp * 15 + k] = st[base + (size_t)k * 32];
+            x[gp * 15 + 12] = st[base + (size_t)6 * 32];
+        }
+        for (int k = 0; k < 7; ++k) x[120 + k] = al[e * 8 + k];
+        x[127] = s->failure_strain;
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_energy(femstep_shell* s, double out[4]) {
+    if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    const double* arrays[4] = {s->d.n_work, s->d.e_diss, s->d.e_strain, s->d.n_kin};
+    const long long counts[4] = {s->nblocks, s->eblocks, s->eblocks, s->nblocks};
+    for (int i = 0; i < 4; ++i) fs::launch_reduce_sum(arrays[i], counts[i], s->d_out + i, s->stream);
+    int rc = check(s, cudaGetLastError(), "reduce");
+    if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "reduce");
+    return rc;
+}
+
+int femstep_shell_stats(femstep_shell* s, long long out[2]) {
+    if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    std::vector<int> st((size_t)s->eblocks * 2);
+    const int rc = check(s, cudaMemcpy(st.data(), s->d.e_stats, st.size() * sizeof(int), cudaMemcpyDeviceToHost), "readback");
+    if (rc) return rc;
+    out[0] = out[1] = 0;
+    for (int b = 0; b < s->eblocks; ++b) {
+        out[0] += st[b * 2];
+        out[1] += st[b * 2 + 1];
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_critical_dt(femstep_shell* s, double youngs, double poisson, double density, double safety,
+                              double* dt) {
+    if (!s || !dt) return fail(s, FEMSTEP_EINVAL, "null argument");
+    double* per = nullptr;
+    int rc = check(s, cudaMalloc(&per, s->elements * sizeof(double)), "alloc");
+    if (rc) return rc;
+    fs::ShellSetupArgs a{};
+    a.elements = (long long)s->elements;
+    a.groups = s->groups;
+    a.rest = s->d.rest;
+    a.index = s->d.index;
+    a.slot = s->d.slot;
+    a.formulation = 2;
+    a.density = density;
+    a.youngs = youngs;
+    a.poisson = poisson;
+    a.safety = safety;
+    a.dt_out = per;
+    fs::launch_shell_setup(a, s->stream);
+    std::vector<double> h(s->elements);
+    rc = check(s, cudaMemcpyAsync(h.data(), per, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "critical dt");
+    cudaFree(per);
+    if (rc) return rc;
+    // smallest positive element step (solid_shell.cpp:1187-1198)
+    double best = INFINITY;
+    for (double v : h)
+        if (v > 0.0) best = std::min(best, v);
+    *dt = std::isfinite(best) ? best : 0.0;
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_profile(femstep_shell* s, int steps, const femstep_shell_params* params, double out[2]) {
+    if (!s || !params || !out || steps <= 0) return fail(s, FEMSTEP_EINVAL, "bad argument");
+    const ShellParams q = make_params(*params);
+    std::vector<cudaEvent_t> ev(3 * (size_t)steps, nullptr);
+    int rc = FEMSTEP_OK;
+    for (auto& e : ev)
+        if (!rc) rc = check(s, cudaEventCreate(&e), "event");
+    for (int i = 0; i < steps && !rc; ++i) {
+        cudaEventRecord(ev[3 * i], s->stream);
+        fs::launch_shell_step(s->d, q, s->stream, 1);
+        cudaEventRecord(ev[3 * i + 1], s->stream);
+        fs::launch_shell_step(s->d, q, s->stream, 2);
+        cudaEventRecord(ev[3 * i + 2], s->stream);
+    }
+    if (!rc) rc = check(s, cudaGetLastError(), "kernel launch");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "profile");
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < steps && !rc; ++i) {
+        float x = 0.0f, y = 0.0f;
+        cudaEventElapsedTime(&x, ev[3 * i], ev[3 * i + 1]);
+        cudaEventElapsedTime(&y, ev[3 * i + 1], ev[3 * i + 2]);
+        a += x;
+        b += y;
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    out[0] = a / steps;
+    out[1] = b / steps;
+    return rc;
+}
+
+long long femstep_shell_launches(const femstep_shell* s) { return s ? s->launches : 0; }
+size_t femstep_shell_device_bytes(const femstep_shell* s) { return s ? s->arena.bytes() : 0; }
+const char* femstep_shell_error(const femstep_shell* s) { return s ? s->error.c_str() : fs::last_error(); }
+
+void femstep_shell_destroy(femstep_shell* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->arena.release();
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int femstep_shell_forms(const double* nodes, size_t elements, int formulation, double youngs, double poisson,
+                        double density, double safety, double* forms_out, double* mass_out, double* dt_out) {
+    if (!nodes || elements == 0) return fail(nullptr, FEMSTEP_EINVAL, "no elements");
+    if (formulation < 0 || formulation > 2) return fail(nullptr, FEMSTEP_EINVAL, "unknown formulation");
+    const int dev = fs::device_status();
+    if (dev != FEMSTEP_OK) return dev;
+    fs::DeviceArena A;
+    const size_t E = elements;
+    std::vector<uint32_t> ident(E * 8);
+    for (size_t i = 0; i < E * 8; ++i) ident[i] = (uint32_t)i;
+    fs::ShellSetupArgs a{};
+    a.elements = (long long)E;
+    a.groups = (long long)((E + 3) / 4);
+    a.rest = A.upload(nodes, E * 24);
+    a.index = A.upload(ident.data(), E * 8);
+    a.slot = a.index;
+    a.formulation = formulation;
+    a.density = density;
+    a.youngs = youngs;
+    a.poisson = poisson;
+    a.safety = safety;
+    a.forms64 = forms_out ? A.alloc<double>(E * 1507) : nullptr;
+    a.corner_mass = mass_out ? A.alloc<double>(E * 8) : nullptr;
+    a.dt_out = dt_out ? A.alloc<double>(E) : nullptr;
+    int rc = FEMSTEP_OK;
+    if (!A.ok()) {
+        rc = fail(nullptr, FEMSTEP_ENOMEM, "device allocation failed");
+    } else {
+        fs::launch_shell_setup(a, 0);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess && forms_out) e = cudaMemcpy(forms_out, a.forms64, E * 1507 * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && mass_out) e = cudaMemcpy(mass_out, a.corner_mass, E * 8 * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && dt_out) e = cudaMemcpy(dt_out, a.dt_out, E * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(nullptr, FEMSTEP_ECUDA, std::string("shell forms: ") + cudaGetErrorString(e));
+    }
+    A.release();
+    return rc;
+}
+
+}  // extern "C"

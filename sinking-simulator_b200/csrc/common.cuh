@@ -8,6 +8,8 @@ namespace fs {
 
 constexpr int kBlock = 256;  // threads per block for the element and node kernels
 
+inline int blocks_for(long long n, int block) { return (int)((n + block - 1) / block); }
+
 // Deterministic block sum in double: shuffle tree inside each warp, then warp 0 adds
 // the per-warp partials in warp order.  The association order depends only on the
 // block size, never on scheduling, so the same launch always produces the same bits.

@@ -1,0 +1,106 @@
+// shell.hpp -- device layout of a solid-shell zone and its kernel launchers.
+//
+// The element is the reference's 8-node ANS + 7-parameter EAS solid-shell
+// (engine/sim/solid_shell.{hpp,cpp}); the step is zone::Solver::step's element loop,
+// CSR gather and node update (engine/sim/zone.cpp:928-989, 1094-1121, 1200-1202).
+//
+// Work mapping: one element = 8 lanes of a warp, lane g owning Gauss point g, so a
+// warp holds 4 elements.  The per-Gauss-point forms record (B 6x24, G 6x7, w) is
+// stored lane-interleaved in "warp groups" of 4 elements, so every load a warp issues
+// is one contiguous 512-byte run of float4s:
+//
+//   forms   float4 [groups][kRec4][32]     kRec4 = 47 float4 = 188 floats per lane:
+//                                          B[6][24] (144) | G[6][7] (42) | w (1) | pad
+//   j0inv   float  [E][9]                  rest Jacobian inverse at the centre (row-major)
+//   state   float  [groups][14][32]        per lane: plastic strain (6), eq. plastic
+//                                          strain, and their Kahan compensations (7)
+//   alpha   float  [E][8]                  the seven enhanced parameters (+ pad)
+//   index   uint32 [E][8]; slot uint32 [E][8] (node-major CSR position of each corner)
+//
+//   nodes:  rest double[3N] (rest positions), disp/disp_c float[3N] (displacement and
+//           its compensation), velocity float[3N], mass/inv_mass float[N],
+//           pinned uint8[N] (bit k pins DOF k), load float[3N] (full-amplitude load),
+//           offset uint32[N+1] (CSR)
+//   slots:  float[3 * 8E] in CSR order
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fs {
+
+constexpr int kShellRec = 188;       // floats per lane record
+constexpr int kShellRec4 = kShellRec / 4;
+constexpr int kShellStateQ = 14;     // floats of state per lane
+constexpr int kShellLanesPerElement = 8;
+constexpr int kShellElementsPerWarp = 4;
+
+struct ShellDevice {
+    long long nodes = 0, elements = 0, groups = 0;
+    const float4* forms = nullptr;
+    const float* j0inv = nullptr;
+    float* state = nullptr;
+    float* alpha = nullptr;
+    const uint32_t* index = nullptr;
+    const uint32_t* slot = nullptr;
+    const double* rest = nullptr;
+    float* disp = nullptr;
+    float* disp_c = nullptr;
+    float* velocity = nullptr;
+    const float* mass = nullptr;
+    const float* inv_mass = nullptr;
+    const uint8_t* pinned = nullptr;
+    const float* load = nullptr;
+    const uint32_t* offset = nullptr;
+    float* slots = nullptr;
+    long long* counter = nullptr;     // [0] steps taken, [1] step of the current node pass
+    // FP64 per-block partials (fixed block -> data mapping)
+    double* e_diss = nullptr;         // += per element block
+    double* e_strain = nullptr;       // =
+    double* n_work = nullptr;         // += per node block
+    double* n_kin = nullptr;          // =
+    int* e_stats = nullptr;           // per element block: [0] += non-converged, [1] = yielded points
+};
+
+struct ShellParams {
+    float mu, kappa, yield, hardening;   // J2 point law, linear isotropic hardening
+    double dmu, dkappa;                   // the same in double, for the energy account
+    float dt, damping;
+    double dt64, rise_time;               // load factor min((step+1) dt / rise, 1)
+    int max_iterations;                   // EAS Newton cap
+    float tol_residual, tol_work;         // relative to sigma_y V
+    int compensated;                      // Kahan on displacement and plastic strain
+};
+
+constexpr int kShellBlock = 128;          // 16 elements per block
+constexpr int kShellNodeBlock = 256;
+
+void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts);
+
+// Rest forms in FP64 on the device (solid_shell.cpp:237-375), one thread per
+// element: writes the FP32 lane records and J0^-1, and in double the lumped corner
+// masses (into CSR slots), the Gauss volumes and, if dt_out is non-null, the
+// element's critical step (solid_shell.cpp:1088-1133).  forms64 (optional, 1507
+// doubles per element) receives the double forms for testing.
+struct ShellSetupArgs {
+    long long elements, groups;
+    const double* rest;        // 3N
+    const uint32_t* index;     // 8E
+    const uint32_t* slot;      // 8E
+    int formulation;           // 0 displacement, 1 ANS, 2 solid-shell
+    double density, youngs, poisson, safety;
+    float4* forms;             // device layout (may be null)
+    float* j0inv;              // [E][9] (may be null)
+    double* corner_mass;       // CSR slots (may be null)
+    double* gauss_volume;      // [E][8] (may be null)
+    double* dt_out;            // [E] (may be null)
+    double* forms64;           // [E][1507] (may be null)
+    int* ok;                   // [E] (may be null)
+};
+void launch_shell_setup(const ShellSetupArgs& a, cudaStream_t stream);
+// Sum the CSR corner masses per node in CSR order (the element order zone.cpp:709-712
+// accumulates them in), then the FP32 mass and 1/mass.
+void launch_shell_mass(long long nodes, const uint32_t* offset, const double* corner_mass, double* mass64,
+                       float* mass, float* inv_mass, cudaStream_t stream);
+
+}  // namespace fs

@@ -1,0 +1,556 @@
+// shell_step.cu -- the solid-shell explicit step in FP32: element kernel and node kernel.
+//
+// Element kernel: the elastoplastic update of solidshell::elementPlasticUpdate with
+// cached forms (engine/sim/solid_shell.cpp:826-1029), one element per 8 lanes, lane g
+// owning Gauss point g.  Per element and step:
+//
+//   1. rotation from the centre deformation gradient (solid_shell.cpp:702, 473): F =
+//      I + H with H = (sum_a dN_a(0) (x) d_a) J0^-1; R = I + Q by the Higham iteration
+//      carried in the deviation Q (Q <- (Q - (M Q)^T)/2, M = (I + Q)^-1), so no digit of
+//      a small rotation is lost to the identity;
+//   2. co-rotated displacement relative to corner 0 (B annihilates a translation):
+//      u'_a = R^T (dX_a + dd_a) - dX_a = Q^T dX_a + dd_a + Q^T dd_a;
+//   3. strain at the lane's point eps_u = B_g u' (B streamed from HBM);
+//   4. EAS Newton on r(alpha) = sum_g w_g G_g^T sigma_g = 0: every iterate restarts
+//      the point law from the step's start state (plasticity.cpp:319-505, linear
+//      isotropic hardening), the residual and K_aa = sum_g w_g G_g^T C_g G_g are warp
+//      butterfly sums over the element's 8 lanes (fixed order, identical bits in every
+//      lane), and each lane runs the same 7x7 Cholesky (solid_shell.cpp:432);
+//      convergence on the correction's energy |delta . r| against sigma_y V
+//      (solid_shell.cpp:963-988), with an FP32 tolerance and iteration cap;
+//   5. commit the state of the last evaluation, f = -R sum_g w_g B_g^T sigma_g: a
+//      3-round reduce-scatter leaves node a's force in lane a, which writes it to the
+//      node-major CSR slot.
+//
+// FP64 only for the per-block energy partials.
+#include "common.cuh"
+#include "shell.hpp"
+
+namespace fs {
+namespace {
+
+__device__ __forceinline__ float sum8(float v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    return v;
+}
+
+__device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
+    const float y = x - comp;
+    const float t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+}
+
+// 3x3 row-major inverse with the reference's singular guard
+__device__ __forceinline__ void inv3f(const float a[9], float r[9]) {
+    const float det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                      a[2] * (a[3] * a[7] - a[4] * a[6]);
+    const float id = fabsf(det) > 1e-30f ? 1.0f / det : 0.0f;
+    r[0] = (a[4] * a[8] - a[5] * a[7]) * id;
+    r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    r[3] = (a[5] * a[6] - a[3] * a[8]) * id;
+    r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    r[6] = (a[3] * a[7] - a[4] * a[6]) * id;
+    r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+}
+
+struct PointOut {
+    float sigma[6];
+    float n[6];        // flow direction (tensor components), valid when yielded
+    float theta, theta_bar;
+    float dp[6];       // plastic strain increment (engineering shears)
+    float deq;
+    bool yielded;
+};
+
+// Radial return, linear isotropic hardening, no back stress, failure off
+// (plasticity.cpp:333-456) with the algorithmic tangent's scalars (:490-504).
+__device__ __forceinline__ void point_law(const float eps[6], const float ps[7], const ShellParams& p, PointOut& o) {
+    float el[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) el[i] = eps[i] - ps[i];
+    const float vol = el[0] + el[1] + el[2];
+    const float pressure = p.kappa * vol;
+    float trial[6];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        trial[i] = 2.0f * p.mu * (el[i] - vol * (1.0f / 3.0f));
+        trial[3 + i] = p.mu * el[3 + i];
+    }
+    const float norm = sqrtf(trial[0] * trial[0] + trial[1] * trial[1] + trial[2] * trial[2] +
+                             2.0f * (trial[3] * trial[3] + trial[4] * trial[4] + trial[5] * trial[5]));
+    const float root23 = 0.81649658092772603f;
+    const float radius = root23 * (p.yield + p.hardening * fmaxf(ps[6], 0.0f));
+    const float excess = norm - radius;
+    if (!(excess > 0.0f)) {
+        o.yielded = false;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            o.sigma[i] = pressure + trial[i];
+            o.sigma[3 + i] = trial[3 + i];
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            o.n[i] = 0.0f;
+            o.dp[i] = 0.0f;
+        }
+        o.theta = 1.0f;
+        o.theta_bar = 0.0f;
+        o.deq = 0.0f;
+        return;
+    }
+    o.yielded = true;
+    const float gamma = excess / (2.0f * p.mu + (2.0f / 3.0f) * p.hardening);
+    const float inv_norm = 1.0f / norm;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) o.n[i] = trial[i] * inv_norm;
+    const float k = 2.0f * p.mu * gamma;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        o.sigma[i] = pressure + trial[i] - k * o.n[i];
+        o.sigma[3 + i] = trial[3 + i] - k * o.n[3 + i];
+        o.dp[i] = gamma * o.n[i];
+        o.dp[3 + i] = 2.0f * gamma * o.n[3 + i];
+    }
+    o.deq = root23 * gamma;
+    o.theta = 1.0f - k * inv_norm;
+    o.theta_bar = 1.0f / (1.0f + p.hardening / (3.0f * p.mu)) - (1.0f - o.theta);
+}
+
+// C g for the algorithmic tangent C = kappa 1(x)1 + 2 mu theta I_dev - 2 mu thetaBar n(x)n
+// in the reference's Voigt convention (engineering strain in, tensor stress out).
+__device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellParams& p, const float g[6], float out[6]) {
+    const float tr = g[0] + g[1] + g[2];
+    const float ng = o.n[0] * g[0] + o.n[1] * g[1] + o.n[2] * g[2] + o.n[3] * g[3] + o.n[4] * g[4] + o.n[5] * g[5];
+    const float a = 2.0f * p.mu * o.theta, b = 2.0f * p.mu * o.theta_bar * ng;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) out[i] = p.kappa * tr + a * (g[i] - tr * (1.0f / 3.0f)) - b * o.n[i];
+#pragma unroll
+    for (int i = 3; i < 6; ++i) out[i] = 0.5f * a * g[i] - b * o.n[i];
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, ShellParams p) {
+    __shared__ double scratch[32];
+    __shared__ int istat[2];
+    const int lane = threadIdx.x & 31;
+    const int gp = lane & 7;
+    const long long group_raw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long e_raw = group_raw * 4 + (lane >> 3);
+    const bool valid = e_raw < d.elements;
+    // Tail lanes (past the last element, or whole warps past the last group) shadow the
+    // last element and group for their loads and write nothing.
+    const long long e = valid ? e_raw : d.elements - 1;
+    const long long group = group_raw < d.groups ? group_raw : d.groups - 1;
+    if (threadIdx.x == 0) {
+        istat[0] = 0;
+        istat[1] = 0;
+    }
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const long long s = d.counter[0];
+        d.counter[1] = s;
+        d.counter[0] = s + 1;
+    }
+    __syncthreads();
+
+    // ---- nodes of the element (every lane reads all eight: broadcast loads) ----
+    const uint4 i0 = reinterpret_cast<const uint4*>(d.index)[e * 2];
+    const uint4 i1 = reinterpret_cast<const uint4*>(d.index)[e * 2 + 1];
+    const unsigned nid[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+    float dX[8][3], dd[8][3];
+    {
+        const double X0 = d.rest[(size_t)nid[0] * 3], Y0 = d.rest[(size_t)nid[0] * 3 + 1],
+                     Z0 = d.rest[(size_t)nid[0] * 3 + 2];
+        const float u0 = d.disp[(size_t)nid[0] * 3], v0 = d.disp[(size_t)nid[0] * 3 + 1],
+                    w0 = d.disp[(size_t)nid[0] * 3 + 2];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const size_t o = (size_t)nid[a] * 3;
+            dX[a][0] = (float)(d.rest[o] - X0);
+            dX[a][1] = (float)(d.rest[o + 1] - Y0);
+            dX[a][2] = (float)(d.rest[o + 2] - Z0);
+            dd[a][0] = d.disp[o] - u0;
+            dd[a][1] = d.disp[o + 1] - v0;
+            dd[a][2] = d.disp[o + 2] - w0;
+        }
+    }
+    // ---- rotation: H = (sum_a dN_a(0) (x) dd_a) J0^-1, R = I + Q ----
+    float q[9];
+    {
+        const float sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
+                    sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+        float jd[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                a0 += sx[a] * dd[a][i];
+                a1 += sy[a] * dd[a][i];
+                a2 += sz[a] * dd[a][i];
+            }
+            jd[i * 3] = 0.125f * a0;
+            jd[i * 3 + 1] = 0.125f * a1;
+            jd[i * 3 + 2] = 0.125f * a2;
+        }
+        float j0[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) j0[k] = d.j0inv[e * 9 + k];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) q[i * 3 + j] = jd[i * 3] * j0[j] + jd[i * 3 + 1] * j0[3 + j] + jd[i * 3 + 2] * j0[6 + j];
+#pragma unroll 1
+        for (int it = 0; it < 6; ++it) {
+            float ipq[9], m[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) ipq[k] = q[k];
+            ipq[0] += 1.0f;
+            ipq[4] += 1.0f;
+            ipq[8] += 1.0f;
+            inv3f(ipq, m);
+            float mq[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) mq[i * 3 + j] = m[i * 3] * q[j] + m[i * 3 + 1] * q[3 + j] + m[i * 3 + 2] * q[6 + j];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) ipq[i * 3 + j] = 0.5f * (q[i * 3 + j] - mq[j * 3 + i]);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) q[k] = ipq[k];
+        }
+    }
+    // ---- co-rotated relative displacement u'_a = Q^T dX_a + dd_a + Q^T dd_a ----
+    float u[24];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float s = dX[a][0] + dd[a][0];
+            const float t = dX[a][1] + dd[a][1];
+            const float w = dX[a][2] + dd[a][2];
+            u[a * 3 + i] = dd[a][i] + (q[0 * 3 + i] * s + q[1 * 3 + i] * t + q[2 * 3 + i] * w);
+        }
+
+    // ---- the lane's forms record ----
+    const float4* rec = d.forms + (size_t)group * kShellRec4 * 32 + lane;
+    float eps_u[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        float s = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float4 b = __ldg(rec + (size_t)(i * 6 + k) * 32);
+            s += b.x * u[k * 4] + b.y * u[k * 4 + 1] + b.z * u[k * 4 + 2] + b.w * u[k * 4 + 3];
+        }
+        eps_u[i] = s;
+    }
+    float G[42];
+    float w;
+    {
+        const float4* gr = rec + (size_t)36 * 32;
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+            const float4 v = __ldg(gr + (size_t)k * 32);
+            if (4 * k < 42) G[4 * k] = v.x;
+            if (4 * k + 1 < 42) G[4 * k + 1] = v.y;
+            if (4 * k + 2 < 42) G[4 * k + 2] = v.z;
+            if (4 * k + 3 < 42) G[4 * k + 3] = v.w;
+            if (k == 10) w = v.z;
+        }
+    }
+    // element volume and the energy scale sigma_y V
+    const float volume = sum8(w);
+    const float scale = p.yield * volume;
+
+    // ---- start-of-step state ----
+    const size_t sbase = (size_t)group * kShellStateQ * 32 + lane;
+    float ps[7], pc[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) ps[k] = d.state[sbase + (size_t)k * 32];
+    if (KAHAN) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) pc[k] = d.state[sbase + (size_t)(7 + k) * 32];
+    }
+    float alpha[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) alpha[k] = d.alpha[e * 8 + k];
+
+    // ---- EAS Newton ----
+    // The four elements of a warp iterate together (the shuffles need the whole warp):
+    // an element that has finished keeps re-evaluating at its final alpha, which
+    // reproduces its final point state exactly, and applies no further correction.
+    PointOut o;
+    bool converged = false, done = false;
+#pragma unroll 1
+    for (int iteration = 0;; ++iteration) {
+        float eps[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            float s = eps_u[i];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) s += G[i * 7 + k] * alpha[k];
+            eps[i] = s;
+        }
+        point_law(eps, ps, p, o);
+        float r[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            float s = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) s += G[i * 7 + k] * o.sigma[i];
+            r[k] = sum8(w * s);
+        }
+        if (!done) {
+            float rn = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) rn += r[k] * r[k];
+            if (sqrtf(rn) <= p.tol_residual * scale) {
+                converged = true;
+                done = true;
+            } else if (iteration + 1 >= p.max_iterations) {
+                done = true;
+            }
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+        // K_aa = sum_g w_g G^T C G, lower triangle
+        float kaa[28];
+        {
+            float cg[7][6];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                float g[6];
+#pragma unroll
+                for (int i = 0; i < 6; ++i) g[i] = G[i * 7 + k];
+                tangent_apply(o, p, g, cg[k]);
+            }
+            int t = 0;
+#pragma unroll
+            for (int a = 0; a < 7; ++a)
+#pragma unroll
+                for (int b = 0; b <= a; ++b) {
+                    float s = 0.0f;
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) s += G[i * 7 + a] * cg[b][i];
+                    kaa[t++] = sum8(w * s);
+                }
+        }
+        // Cholesky (solid_shell.cpp:432-457), identical in every lane
+        float l[28];
+        bool spd = true;
+        {
+            int t = 0;
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+#pragma unroll
+                for (int j = 0; j <= i; ++j) {
+                    float s = kaa[t];
+#pragma unroll
+                    for (int k = 0; k < j; ++k) s -= l[i * (i + 1) / 2 + k] * l[j * (j + 1) / 2 + k];
+                    if (i == j) {
+                        spd = spd && (s > 0.0f);
+                        l[t] = sqrtf(fmaxf(s, 1e-30f));
+                    } else {
+                        l[t] = s / l[j * (j + 1) / 2 + j];
+                    }
+                    ++t;
+                }
+            }
+        }
+        float delta[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            float s = -r[i];
+#pragma unroll
+            for (int k = 0; k < i; ++k) s -= l[i * (i + 1) / 2 + k] * delta[k];
+            delta[i] = s / l[i * (i + 1) / 2 + i];
+        }
+#pragma unroll
+        for (int i = 6; i >= 0; --i) {
+            float s = delta[i];
+#pragma unroll
+            for (int k = i + 1; k < 7; ++k) s -= l[k * (k + 1) / 2 + i] * delta[k];
+            delta[i] = s / l[i * (i + 1) / 2 + i];
+        }
+        float work = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) work += delta[k] * r[k];
+        if (!done) {
+            if (!spd) {
+                done = true;  // no stiffness left in the enhanced modes: report, do not iterate
+            } else if (fabsf(work) <= p.tol_work * scale) {
+                converged = true;  // stop before applying, as solid_shell.cpp:983-988
+                done = true;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 7; ++k) alpha[k] += delta[k];
+            }
+        }
+    }
+
+    // ---- commit ----
+    double diss = 0.0, energy = 0.0;
+    if (valid) {
+        if (o.yielded) {
+            float dsum = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) dsum += o.sigma[i] * o.dp[i];
+            diss = (double)w * (double)dsum;
+            if (KAHAN) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) kahan_add(ps[i], pc[i], o.dp[i]);
+                kahan_add(ps[6], pc[6], o.deq);
+#pragma unroll
+                for (int k = 0; k < 7; ++k) d.state[sbase + (size_t)(7 + k) * 32] = pc[k];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) ps[i] += o.dp[i];
+                ps[6] += o.deq;
+            }
+#pragma unroll
+            for (int k = 0; k < 7; ++k) d.state[sbase + (size_t)k * 32] = ps[k];
+            atomicAdd(&istat[1], 1);
+        }
+        if (gp < 7) d.alpha[e * 8 + gp] = alpha[gp];
+        if (gp == 0 && !converged) atomicAdd(&istat[0], 1);
+        const double s0 = o.sigma[0], s1 = o.sigma[1], s2 = o.sigma[2], s3 = o.sigma[3], s4 = o.sigma[4],
+                     s5 = o.sigma[5];
+        const double pr = (s0 + s1 + s2) / 3.0;
+        double density = 0.5 * s0 * ((s0 - pr) / (2.0 * p.dmu) + pr / (3.0 * p.dkappa)) +
+                         0.5 * s1 * ((s1 - pr) / (2.0 * p.dmu) + pr / (3.0 * p.dkappa)) +
+                         0.5 * s2 * ((s2 - pr) / (2.0 * p.dmu) + pr / (3.0 * p.dkappa));
+        density += 0.5 * (s3 * s3 + s4 * s4 + s5 * s5) / p.dmu;
+        energy = (double)w * density;
+    }
+
+    // ---- f = -R sum_g w_g B_g^T sigma_g, reduce-scattered so lane a holds node a ----
+    float f[24];
+    {
+        float ws[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) ws[i] = w * o.sigma[i];
+#pragma unroll
+        for (int j = 0; j < 24; ++j) f[j] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const float4 b = __ldg(rec + (size_t)(i * 6 + k) * 32);
+                f[k * 4] += b.x * ws[i];
+                f[k * 4 + 1] += b.y * ws[i];
+                f[k * 4 + 2] += b.z * ws[i];
+                f[k * 4 + 3] += b.w * ws[i];
+            }
+    }
+    // round 1 (xor 4): keep nodes 0-3 (bit 2 clear) or 4-7
+    const bool hi4 = (gp & 4) != 0, hi2 = (gp & 2) != 0, hi1 = (gp & 1) != 0;
+#pragma unroll
+    for (int j = 0; j < 12; ++j) {
+        const float keep = hi4 ? f[12 + j] : f[j];
+        const float give = hi4 ? f[j] : f[12 + j];
+        f[j] = keep + __shfl_xor_sync(0xffffffffu, give, 4);
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const float keep = hi2 ? f[6 + j] : f[j];
+        const float give = hi2 ? f[j] : f[6 + j];
+        f[j] = keep + __shfl_xor_sync(0xffffffffu, give, 2);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float keep = hi1 ? f[3 + j] : f[j];
+        const float give = hi1 ? f[j] : f[3 + j];
+        f[j] = keep + __shfl_xor_sync(0xffffffffu, give, 1);
+    }
+    if (valid) {
+        // lane gp now holds sum over points of node gp's internal force; apply -R
+        float* out = d.slots + (size_t)d.slot[e * 8 + gp] * 3;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[i] = -(f[i] + (q[i * 3] * f[0] + q[i * 3 + 1] * f[1] + q[i * 3 + 2] * f[2]));
+    }
+    const double bd = block_sum(diss, scratch);
+    const double be = block_sum(energy, scratch);
+    if (threadIdx.x == 0) {
+        d.e_diss[blockIdx.x] += bd;
+        d.e_strain[blockIdx.x] = be;
+        d.e_stats[blockIdx.x * 2] += istat[0];
+        d.e_stats[blockIdx.x * 2 + 1] = istat[1];
+    }
+}
+
+template <bool KAHAN>
+__global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, ShellParams p) {
+    __shared__ double scratch[32];
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double work = 0.0, kin = 0.0;
+    if (n < d.nodes) {
+        const double t = (double)(d.counter[1] + 1) * p.dt64;
+        const float lf = p.rise_time > 0.0 ? (float)(t / p.rise_time < 1.0 ? t / p.rise_time : 1.0) : 1.0f;
+        float force[3] = {0.0f, 0.0f, 0.0f};
+        const uint32_t b = d.offset[n], e = d.offset[n + 1];
+        const float* sl = d.slots + (size_t)b * 3;
+#pragma unroll 4
+        for (uint32_t k = b; k < e; ++k, sl += 3) {
+            force[0] += sl[0];
+            force[1] += sl[1];
+            force[2] += sl[2];
+        }
+        const uint8_t pin = d.pinned[n];
+        const float im = d.inv_mass[n], m = d.mass[n];
+        float* vel = d.velocity + (size_t)n * 3;
+        float* u = d.disp + (size_t)n * 3;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float ext = d.load ? lf * d.load[(size_t)n * 3 + k] : 0.0f;
+            float v = vel[k];
+            if (pin & (1u << k)) {
+                v = 0.0f;
+            } else if (m > 0.0f) {
+                v += (force[k] + ext) * im * p.dt;
+            }
+            v *= p.damping;
+            vel[k] = v;
+            const float du = v * p.dt;
+            if (KAHAN) {
+                float c = d.disp_c[(size_t)n * 3 + k];
+                float s = u[k];
+                kahan_add(s, c, du);
+                u[k] = s;
+                d.disp_c[(size_t)n * 3 + k] = c;
+            } else {
+                u[k] += du;
+            }
+            work += (double)ext * (double)v * (double)p.dt;
+            kin += 0.5 * (double)m * (double)v * (double)v;
+        }
+    }
+    const double bw = block_sum(work, scratch);
+    const double bk = block_sum(kin, scratch);
+    if (threadIdx.x == 0) {
+        d.n_work[blockIdx.x] += bw;
+        d.n_kin[blockIdx.x] = bk;
+    }
+}
+
+}  // namespace
+
+void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts) {
+    const int eb = blocks_for(d.groups * 32, kShellBlock);
+    const int nb = blocks_for(d.nodes, kShellNodeBlock);
+    if (p.compensated) {
+        if (parts & 1) shell_forces<true><<<eb, kShellBlock, 0, stream>>>(d, p);
+        if (parts & 2) shell_nodes<true><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
+    } else {
+        if (parts & 1) shell_forces<false><<<eb, kShellBlock, 0, stream>>>(d, p);
+        if (parts & 2) shell_nodes<false><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
+    }
+}
+
+}  // namespace fs

@@ -91,6 +91,4 @@ void launch_tet_omega2(long long tets, const double* rest_inv, double E, double 
 void launch_reduce_sum(const double* in, long long n, double* out, cudaStream_t stream);
 void launch_reduce_max(const double* in, long long n, double* out, cudaStream_t stream);
 
-inline int blocks_for(long long n, int block) { return (int)((n + block - 1) / block); }
-
 }  // namespace fs

@@ -92,6 +92,16 @@ def _raise(code: int, text: bytes | None):
     raise FemStepError(code, msg)
 
 
+_set_device = _sig("femstep_set_device", C.c_int, [C.c_int])
+
+
+def set_device(device: int) -> None:
+    """Select the GPU this process's solvers live on (one process per GPU)."""
+    rc = _set_device(int(device))
+    if rc:
+        _raise(rc, _last_error())
+
+
 def device_name() -> str:
     buf = C.create_string_buffer(256)
     rc = _device_name(buf, 256)
@@ -254,3 +264,233 @@ def csr(nodes, index, corners):
     offset[1:] = np.cumsum(counts)
     entry = np.argsort(index, kind="stable").astype(np.uint32)
     return offset, entry
+
+
+# ---------------------------------------------------------------------------------
+# Solid-shell zone: gpu::ZoneGpuSolver (engine/gpu/zone_gpu.hpp:179-234).
+
+class ShellMeshC(C.Structure):
+    _fields_ = [("nodes", C.c_size_t), ("elements", C.c_size_t), ("rest", C.c_void_p), ("position", C.c_void_p),
+                ("velocity", C.c_void_p), ("index", C.c_void_p), ("pinned", C.c_void_p), ("load", C.c_void_p),
+                ("forms", C.c_void_p), ("mass", C.c_void_p), ("state", C.c_void_p),
+                ("adjacency_offset", C.c_void_p), ("adjacency_entry", C.c_void_p), ("density", C.c_double)]
+
+
+class ShellParamsC(C.Structure):
+    _fields_ = [("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double), ("yield_strength", C.c_double),
+                ("hardening_modulus", C.c_double), ("dt", C.c_double), ("damping", C.c_double),
+                ("rise_time", C.c_double), ("max_iterations", C.c_int), ("tol_residual", C.c_double),
+                ("tol_work", C.c_double), ("compensated", C.c_int)]
+
+
+_sh_create = _sig("femstep_shell_create", C.c_int, [C.POINTER(ShellMeshC), C.POINTER(C.c_void_p)])
+_sh_run = _sig("femstep_shell_run", C.c_int, [C.c_void_p, C.c_int, C.POINTER(ShellParamsC), C.POINTER(C.c_double)])
+_sh_readback = _sig("femstep_shell_readback", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p])
+_sh_state = _sig("femstep_shell_state", C.c_int, [C.c_void_p, C.c_void_p])
+_sh_energy = _sig("femstep_shell_energy", C.c_int, [C.c_void_p, C.c_void_p])
+_sh_stats = _sig("femstep_shell_stats", C.c_int, [C.c_void_p, C.c_void_p])
+_sh_dt = _sig("femstep_shell_critical_dt", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
+                                                       C.POINTER(C.c_double)])
+_sh_profile = _sig("femstep_shell_profile", C.c_int, [C.c_void_p, C.c_int, C.POINTER(ShellParamsC), C.c_void_p])
+_sh_launches = _sig("femstep_shell_launches", C.c_longlong, [C.c_void_p])
+_sh_bytes = _sig("femstep_shell_device_bytes", C.c_size_t, [C.c_void_p])
+_sh_error = _sig("femstep_shell_error", C.c_char_p, [C.c_void_p])
+_sh_destroy = _sig("femstep_shell_destroy", None, [C.c_void_p])
+_sh_forms = _sig("femstep_shell_forms", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_double, C.c_double,
+                                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p])
+
+
+class ShellSolver:
+    """A solid-shell zone resident on the GPU; the reference's gpu::ZoneGpuSolver.
+
+    rest/index are the HexMesh arrays (solid_shell.hpp:464-477); pinned is 3 flags per
+    node; load is the full-amplitude external nodal force.  forms/mass/state may be
+    handed over from a CPU zone::Solver, as ZoneGpuSolver::initialise does; otherwise
+    the forms and the lumped mass are built on the device in FP64.
+    """
+
+    def __init__(self, rest, index, pinned=None, load=None, position=None, velocity=None, forms=None, mass=None,
+                 state=None, adjacency_offset=None, adjacency_entry=None, density=7850.0):
+        keep = {}
+
+        def arr(name, a, dt):
+            if a is None:
+                return None
+            keep[name] = np.ascontiguousarray(a, dt).reshape(-1)
+            return keep[name]
+
+        r = arr("rest", rest, np.float64)
+        idx = arr("index", index, np.uint32)
+        self.nodes = r.size // 3
+        self.elements = idx.size // 8
+        m = ShellMeshC()
+        m.nodes, m.elements = self.nodes, self.elements
+        m.rest = _p(r)
+        m.position = _p(arr("position", position, np.float64))
+        m.velocity = _p(arr("velocity", velocity, np.float64))
+        m.index = _p(idx)
+        m.pinned = _p(arr("pinned", pinned, np.uint8))
+        m.load = _p(arr("load", load, np.float64))
+        m.forms = _p(arr("forms", forms, np.float64))
+        m.mass = _p(arr("mass", mass, np.float64))
+        m.state = _p(arr("state", state, np.float64))
+        m.adjacency_offset = _p(arr("adjacency_offset", adjacency_offset, np.uint32))
+        m.adjacency_entry = _p(arr("adjacency_entry", adjacency_entry, np.uint32))
+        m.density = float(density)
+        h = C.c_void_p()
+        rc = _sh_create(C.byref(m), C.byref(h))
+        if rc:
+            _raise(rc, _last_error())
+        self._h = h
+
+    def _check(self, rc):
+        if rc:
+            _raise(rc, _sh_error(self._h))
+
+    @staticmethod
+    def params(youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9, dt=1e-7, damping=1.0,
+               rise_time=0.0, max_iterations=12, tol_residual=1e-6, tol_work=1e-13, compensated=True):
+        return ShellParamsC(youngs, poisson, yield_strength, hardening, dt, damping, rise_time, int(max_iterations),
+                            tol_residual, tol_work, int(bool(compensated)))
+
+    def run(self, substeps, **kw) -> float:
+        p = self.params(**kw)
+        ms = C.c_double()
+        self._check(_sh_run(self._h, int(substeps), C.byref(p), C.byref(ms)))
+        return ms.value
+
+    def readback(self):
+        p = np.zeros(3 * self.nodes)
+        v = np.zeros(3 * self.nodes)
+        self._check(_sh_readback(self._h, _p(p), _p(v)))
+        return p, v
+
+    def state(self):
+        out = np.zeros(129 * self.elements)
+        self._check(_sh_state(self._h, _p(out)))
+        return out.reshape(self.elements, 129)
+
+    def energy(self):
+        """[external work, dissipation, strain energy, kinetic], FP64 on device."""
+        out = np.zeros(4)
+        self._check(_sh_energy(self._h, _p(out)))
+        return out
+
+    def stats(self):
+        out = np.zeros(2, np.int64)
+        self._check(_sh_stats(self._h, _p(out)))
+        return {"nonconverged_element_steps": int(out[0]), "yielded_points": int(out[1])}
+
+    def critical_dt(self, youngs=206e9, poisson=0.3, density=7850.0, safety=0.9) -> float:
+        dt = C.c_double()
+        self._check(_sh_dt(self._h, youngs, poisson, density, safety, C.byref(dt)))
+        return dt.value
+
+    def profile(self, steps, **kw):
+        p = self.params(**kw)
+        out = np.zeros(2)
+        self._check(_sh_profile(self._h, int(steps), C.byref(p), _p(out)))
+        return float(out[0]), float(out[1])
+
+    @property
+    def launches(self) -> int:
+        return int(_sh_launches(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(_sh_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _sh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def shell_forms(nodes, formulation=2, youngs=206e9, poisson=0.3, density=7850.0, safety=0.9):
+    """Rest forms, lumped masses and element critical steps of standalone elements,
+    formed on the device in FP64.  nodes: (E, 24)."""
+    nodes = np.ascontiguousarray(nodes, np.float64).reshape(-1, 24)
+    E = nodes.shape[0]
+    forms = np.zeros((E, 1507))
+    mass = np.zeros((E, 8))
+    dt = np.zeros(E)
+    rc = _sh_forms(_p(nodes), E, int(formulation), youngs, poisson, density, safety, _p(forms), _p(mass), _p(dt))
+    if rc:
+        _raise(rc, _last_error())
+    return forms, mass, dt
+
+
+def plate_mesh(lx, ly, thickness, nx, ny, nz=1):
+    """solidshell::makePlateMesh (engine/sim/solid_shell.cpp:1152-1185): node
+    (i*sy + j)*sz + k, thickness index fastest, mid-surface at z = 0."""
+    sy, sz = ny + 1, nz + 1
+    i, j, k = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    pos = np.empty(i.shape + (3,))
+    pos[..., 0] = lx * i.astype(np.float64) / nx
+    pos[..., 1] = ly * j.astype(np.float64) / ny
+    pos[..., 2] = -0.5 * thickness + thickness * k.astype(np.float64) / nz
+    ei, ej, ek = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ei, ej, ek = ei.reshape(-1), ej.reshape(-1), ek.reshape(-1)
+
+    def at(a, b, c):
+        return ((a * sy + b) * sz + c).astype(np.uint32)
+
+    idx = np.stack([at(ei, ej, ek), at(ei + 1, ej, ek), at(ei + 1, ej + 1, ek), at(ei, ej + 1, ek),
+                    at(ei, ej, ek + 1), at(ei + 1, ej, ek + 1), at(ei + 1, ej + 1, ek + 1), at(ei, ej + 1, ek + 1)],
+                   axis=1)
+    return pos.reshape(-1), idx.reshape(-1)
+
+
+def plate_pressure_load(position, index, pressure=1.0):
+    """Consistent nodal loads of a pressure on the +zeta face of every element
+    (solidshell::uniformPressureLoad, solid_shell.cpp:1505-1553, for one element
+    through the thickness, where every top face is a boundary face), vectorised."""
+    pos = np.asarray(position, np.float64).reshape(-1, 3)
+    top = np.asarray(index, np.int64).reshape(-1, 8)[:, 4:8]
+    load = np.zeros_like(pos)
+    q = 1.0 / np.sqrt(3.0)
+    corner = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], np.float64)
+    x = pos[top]  # (E, 4, 3)
+    for gs in (-q, q):
+        for gt in (-q, q):
+            shape = 0.25 * (1 + gs * corner[:, 0]) * (1 + gt * corner[:, 1])
+            ds = 0.25 * corner[:, 0] * (1 + gt * corner[:, 1])
+            dt = 0.25 * corner[:, 1] * (1 + gs * corner[:, 0])
+            xs = np.einsum("c,eci->ei", ds, x)
+            xt = np.einsum("c,eci->ei", dt, x)
+            area = np.cross(xs, xt)
+            contrib = -pressure * shape[None, :, None] * area[:, None, :]
+            np.add.at(load, top, contrib)
+    return load.reshape(-1)
+
+
+def stiffened_panel(nx=2000, ny=1000, lx=20.0, ly=10.0, thickness=0.012, stiffeners=6, imperfection=1e-3,
+                    peak_pressure=0.5e6, radius=1.5, seed=20261203):
+    """The stiffened plate panel of the single-large-mesh workload: lx x ly plate of
+    `thickness`, one solid-shell element through the thickness, edges clamped, the
+    plating nodes on `stiffeners` evenly spaced longitudinal lines pinned (the
+    reference's Stiffeners::RigidSupport, zone.hpp:380-390, zone.cpp:583-592), a seeded
+    Gaussian out-of-plane imperfection applied identically to both faces of each
+    through-thickness node pair, and a Gaussian pressure of `peak_pressure` and 1/e^0.5
+    radius `radius` centred on the plate.  Returns (rest, index, pinned, load_at_peak)."""
+    rest, index = plate_mesh(lx, ly, thickness, nx, ny, 1)
+    p = rest.reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    bump = rng.normal(0.0, imperfection, (nx + 1) * (ny + 1))
+    p[:, 2] += np.repeat(bump, 2)  # thickness index fastest: pairs (k = 0, 1) share it
+    i = np.arange(p.shape[0]) // (2 * (ny + 1))
+    j = (np.arange(p.shape[0]) // 2) % (ny + 1)
+    edge = (i == 0) | (i == nx) | (j == 0) | (j == ny)
+    lines = {int(round(ny * s / (stiffeners + 1))) for s in range(1, stiffeners + 1)}
+    stiff = np.isin(j, list(lines))
+    pinned = np.repeat(edge | stiff, 3).astype(np.uint8)
+    unit = plate_pressure_load(rest, index, 1.0).reshape(-1, 3)
+    r2 = (p[:, 0] - lx / 2) ** 2 + (p[:, 1] - ly / 2) ** 2
+    load = unit * (peak_pressure * np.exp(-r2 / (2 * radius ** 2)))[:, None]
+    return rest, index, pinned, load.reshape(-1)

@@ -68,3 +68,17 @@ def test_mesher_matches_reference_generator(fem, port):
         m.rest_state(210e9, 0.3, 7850.0)
         off, ent = fem.csr(m.nodes, a[1], 4)
         assert np.array_equal(off, m.adj_offset) and np.array_equal(ent, m.adj_entry)
+
+
+def test_plate_mesher_matches_reference_generator(fem, port):
+    import oracle as O
+
+    for dims in ((0.06, 0.04, 0.012, 6, 4, 1), (1.0, 0.5, 0.02, 3, 5, 2)):
+        a = fem.plate_mesh(*dims)
+        b = O.plate_mesh(port, *dims)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        load = fem.plate_pressure_load(a[0], a[1], 2.5e5)
+        if dims[-1] == 1:
+            ref = np.zeros(a[0].size)
+            port.plate_pressure_load(b[0], b[1], b[0].size // 3, b[1].size // 8, 2.5e5, ref)
+            assert np.allclose(load, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())

@@ -74,19 +74,20 @@ def _rel_disp_error(p, ref, rest):
 
 @pytest.mark.parametrize("mode,tol", [("f32k", 1e-5), ("f32", 1e-3)])
 def test_f32_against_fp64_oracle(fem, port, mode, tol):
-    """2000 ramped steps of config 0 (scaled load so the root yields)."""
-    pos, idx, fixed, fext = cantilever(fem, load=60e3)
+    """The config-0 cantilever with the tip load scaled to 200 kN (ramped over 1000
+    steps) so that ~40 % of the tets yield by step 2000, as the precision study asks."""
+    pos, idx, fixed, fext = cantilever(fem, load=200e3)
     ref = O.TetMesh64(port, pos, idx, fixed, fext)
     dt = port.tet64_critical_dt(C.byref(ref._s), 210e9, 0.3, 7850.0, 0.9)
-    params = O.tet64_params(dt=dt, ramp_steps=2000)
+    params = O.tet64_params(dt=dt, ramp_steps=1000)
     ref.step(params, 2000)
     s = fem.TetSolver(pos, idx, mode=mode, fixed=fixed, external_force=fext, density=7850.0)
-    s.run(2000, dt=dt, ramp_steps=2000)
+    s.run(2000, dt=dt, ramp_steps=1000)
     p, _ = s.readback64()
     rest = pos.astype(np.float64)
     err = _rel_disp_error(p, ref.position, rest)
     yielded = (ref.plastic.reshape(-1, 7)[:, 6] > 0).mean()
-    assert yielded > 0.0, "the case must exercise plasticity"
+    assert yielded > 0.3, "the case must exercise plasticity"
     assert err < tol, (mode, err)
     e, er = s.energy(), ref.energy
     # energy account against the oracle's, and its own balance
@@ -121,5 +122,5 @@ def test_rest_stays_at_rest(fem):
         # FP32 modes carry the displacement gradient, which is exactly zero at rest;
         # FP64 carries F = Ds Dm^-1, whose rounding residue (~1e-16) may move a node
         # by far less than a femtometre.
-        tol = 0.0 if mode != "f64" else 1e-15
-        assert np.abs(p - pos).max() <= tol and np.abs(v).max() <= tol * 1e3, mode
+        tol = 0.0 if mode != "f64" else 1e-14
+        assert np.abs(p - pos).max() <= tol and np.abs(v).max() <= tol * 1e5, mode
