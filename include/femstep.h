@@ -119,6 +119,36 @@ long long femstep_tet_launches(const femstep_tet *solver);
 const char *femstep_tet_error(const femstep_tet *solver);
 void femstep_tet_destroy(femstep_tet *solver);
 
+/* A tet mesh already in the caller's device memory, in the reference's TetMesh layout
+   (engine/sim/fem.hpp:38-68).  All pointers are device pointers. */
+typedef struct {
+    size_t nodes, tets;
+    float *position;                  /* 3N, advanced in place */
+    float *velocity;                  /* 3N, advanced in place */
+    const float *mass;                /* N */
+    const uint32_t *fixed;            /* N, may be NULL */
+    const uint32_t *index;            /* 4T */
+    const float *rest_inv;            /* 9T, column-major per tet */
+    const float *rest_volume;         /* T */
+    const uint32_t *adjacency_offset; /* N+1 */
+    const uint32_t *adjacency_entry;  /* 4T */
+} femstep_tet_device_mesh;
+
+/* No counterpart in the reference.  The REF32 step (bit-identical to
+   femstep_tet_create + femstep_tet_run in FEMSTEP_TET_REF32 mode) for callers that
+   cannot allocate device memory -- an engine or plugin that owns all device memory
+   through its own allocator or a fixed budget.  It allocates nothing: the caller passes
+   its device arrays, and the only scratch, the per-tet corner forces, is a fixed
+   library-resident array of 65,536 tets (3 MiB per GPU that loads the library, held
+   until the process exits).  Larger meshes are rejected with FEMSTEP_EINVAL.  The
+   first call on a device looks up that array's device address, so make that call
+   before any stream capture.  Every call on a device shares the array: calls whose
+   kernels overlap on the GPU race; calls ordered on one stream do not.  Launches on
+   `stream` (a cudaStream_t, NULL for the legacy default stream) and returns without
+   synchronising. */
+int femstep_tet_step_noalloc(const femstep_tet_device_mesh *mesh, int substeps, const femstep_tet_params *params,
+                             void *stream);
+
 /* =====================================================================================
  * Solid-shell zone step.  Replaces gpu::ZoneGpuSolver (engine/gpu/zone_gpu.hpp:179-234):
  * the 8-node ANS + 7-parameter EAS solid-shell with J2 plasticity (linear isotropic
