@@ -28,6 +28,9 @@ struct femstep_shell {
     fs::DeviceArena arena;
     ShellDevice d;
     int eblocks = 0, nblocks = 0;
+    long long ewarps = 0;             // element-kernel warps = per-warp partial entries
+    float* kaa_factor = nullptr;      // [E][32] elastic K_aa factor, for factor_E / factor_nu
+    double factor_E = 0.0, factor_nu = 0.0;
     double* d_out = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -66,13 +69,30 @@ ShellParams make_params(const femstep_shell_params& p) {
     q.damping = (float)p.damping;
     q.rise_time = p.rise_time;
     q.max_iterations = p.max_iterations > 0 ? p.max_iterations : 12;
-    q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 1e-6);
+    q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 5e-5);
     q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-13);
     q.compensated = p.compensated;
     return q;
 }
 
 constexpr int kGraphSteps = 16;
+
+// The elastic K_aa factor depends on the material: formed before the first run and
+// again whenever E or nu change.
+int ensure_factor(femstep_shell* s, const femstep_shell_params& p) {
+    if (s->d.kaa_factor && s->factor_E == p.youngs_modulus && s->factor_nu == p.poisson_ratio) return FEMSTEP_OK;
+    fs::launch_shell_elastic_factor(s->d, p.youngs_modulus, p.poisson_ratio, s->kaa_factor, s->stream);
+    const int rc = check(s, cudaGetLastError(), "elastic factor");
+    if (rc) return rc;
+    s->d.kaa_factor = s->kaa_factor;
+    s->factor_E = p.youngs_modulus;
+    s->factor_nu = p.poisson_ratio;
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return FEMSTEP_OK;
+}
 
 }  // namespace
 
@@ -115,6 +135,7 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     s->elements = E;
     s->groups = (long long)((E + 3) / 4);
     s->eblocks = fs::blocks_for(s->groups * 32, fs::kShellBlock);
+    s->ewarps = (long long)s->eblocks * (fs::kShellBlock / 32);
     s->nblocks = fs::blocks_for((long long)N, fs::kShellNodeBlock);
     int rc = check(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
     if (!rc) rc = check(s, cudaEventCreate(&s->ev0), "event");
@@ -142,9 +163,10 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.alpha = A.zeros<float>(Epad * 8);
     d.slots = A.zeros<float>(E * 8 * 3 + 4);
     d.counter = A.zeros<long long>(2);
-    d.e_diss = A.zeros<double>(s->eblocks);
-    d.e_strain = A.zeros<double>(s->eblocks);
-    d.e_stats = A.zeros<int>((size_t)s->eblocks * 2);
+    d.e_diss = A.zeros<double>(s->ewarps);
+    d.e_strain = A.zeros<double>(s->ewarps);
+    d.e_stats = A.zeros<int>((size_t)s->ewarps * 2);
+    s->kaa_factor = A.zeros<float>(E * 32);
     d.n_work = A.zeros<double>(s->nblocks);
     d.n_kin = A.zeros<double>(s->nblocks);
     s->d_out = A.zeros<double>(8);
@@ -264,7 +286,9 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
     if (!(params->dt > 0.0) || !std::isfinite(params->dt)) return fail(s, FEMSTEP_EINVAL, "dt must be positive");
     const ShellParams q = make_params(*params);
     s->launches = 0;
-    int rc = check(s, cudaEventRecord(s->ev0, s->stream), "event record");
+    int rc = ensure_factor(s, *params);
+    if (rc) return rc;
+    rc = check(s, cudaEventRecord(s->ev0, s->stream), "event record");
     if (rc) return rc;
     int left = substeps;
     if (left >= kGraphSteps) {
@@ -345,7 +369,7 @@ int femstep_shell_state(femstep_shell* s, double* state) {
 int femstep_shell_energy(femstep_shell* s, double out[4]) {
     if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
     const double* arrays[4] = {s->d.n_work, s->d.e_diss, s->d.e_strain, s->d.n_kin};
-    const long long counts[4] = {s->nblocks, s->eblocks, s->eblocks, s->nblocks};
+    const long long counts[4] = {s->nblocks, s->ewarps, s->ewarps, s->nblocks};
     for (int i = 0; i < 4; ++i) fs::launch_reduce_sum(arrays[i], counts[i], s->d_out + i, s->stream);
     int rc = check(s, cudaGetLastError(), "reduce");
     if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
@@ -355,11 +379,11 @@ int femstep_shell_energy(femstep_shell* s, double out[4]) {
 
 int femstep_shell_stats(femstep_shell* s, long long out[2]) {
     if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
-    std::vector<int> st((size_t)s->eblocks * 2);
+    std::vector<int> st((size_t)s->ewarps * 2);
     const int rc = check(s, cudaMemcpy(st.data(), s->d.e_stats, st.size() * sizeof(int), cudaMemcpyDeviceToHost), "readback");
     if (rc) return rc;
     out[0] = out[1] = 0;
-    for (int b = 0; b < s->eblocks; ++b) {
+    for (long long b = 0; b < s->ewarps; ++b) {
         out[0] += st[b * 2];
         out[1] += st[b * 2 + 1];
     }
@@ -402,7 +426,7 @@ int femstep_shell_profile(femstep_shell* s, int steps, const femstep_shell_param
     if (!s || !params || !out || steps <= 0) return fail(s, FEMSTEP_EINVAL, "bad argument");
     const ShellParams q = make_params(*params);
     std::vector<cudaEvent_t> ev(3 * (size_t)steps, nullptr);
-    int rc = FEMSTEP_OK;
+    int rc = ensure_factor(s, *params);
     for (auto& e : ev)
         if (!rc) rc = check(s, cudaEventCreate(&e), "event");
     for (int i = 0; i < steps && !rc; ++i) {

@@ -53,13 +53,15 @@ struct ShellDevice {
     const float* load = nullptr;
     const uint32_t* offset = nullptr;
     float* slots = nullptr;
+    const float* kaa_factor = nullptr; // [E][32]: Cholesky factor of the elastic K_aa (may be null)
     long long* counter = nullptr;     // [0] steps taken, [1] step of the current node pass
-    // FP64 per-block partials (fixed block -> data mapping)
-    double* e_diss = nullptr;         // += per element block
+    // FP64 partials with a fixed mapping: one entry per warp of the element kernel
+    // (a warp = a group of 4 elements), one per block of the node kernel
+    double* e_diss = nullptr;         // += per element warp
     double* e_strain = nullptr;       // =
     double* n_work = nullptr;         // += per node block
     double* n_kin = nullptr;          // =
-    int* e_stats = nullptr;           // per element block: [0] += non-converged, [1] = yielded points
+    int* e_stats = nullptr;           // per element warp: [0] += non-converged, [1] = yielded points
 };
 
 struct ShellParams {
@@ -76,6 +78,9 @@ constexpr int kShellBlock = 128;          // 16 elements per block
 constexpr int kShellNodeBlock = 256;
 
 void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts);
+// Factor of the elastic K_aa per element for this material (into `out`, [E][32]).
+void launch_shell_elastic_factor(const ShellDevice& d, double youngs, double poisson, float* out,
+                                 cudaStream_t stream);
 
 // Rest forms in FP64 on the device (solid_shell.cpp:237-375), one thread per
 // element: writes the FP32 lane records and J0^-1, and in double the lumped corner

@@ -134,10 +134,14 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
     for (int i = 3; i < 6; ++i) out[i] = 0.5f * a * g[i] - b * o.n[i];
 }
 
+// Blocks per SM the register budget is sized for: 3 (168 registers, 12 warps per SM)
+// measured 1.32x faster than 2 (177 registers, 8 warps) on the 2 M-element panel.
+#ifndef FEMSTEP_SHELL_MINB
+#define FEMSTEP_SHELL_MINB 3
+#endif
+
 template <bool KAHAN>
-__global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, ShellParams p) {
-    __shared__ double scratch[32];
-    __shared__ int istat[2];
+__global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(ShellDevice d, ShellParams p) {
     const int lane = threadIdx.x & 31;
     const int gp = lane & 7;
     const long long group_raw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -147,16 +151,11 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
     // last element and group for their loads and write nothing.
     const long long e = valid ? e_raw : d.elements - 1;
     const long long group = group_raw < d.groups ? group_raw : d.groups - 1;
-    if (threadIdx.x == 0) {
-        istat[0] = 0;
-        istat[1] = 0;
-    }
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const long long s = d.counter[0];
         d.counter[1] = s;
         d.counter[0] = s + 1;
     }
-    __syncthreads();
 
     // ---- nodes of the element (every lane reads all eight: broadcast loads) ----
     const uint4 i0 = reinterpret_cast<const uint4*>(d.index)[e * 2];
@@ -205,6 +204,9 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) q[i * 3 + j] = jd[i * 3] * j0[j] + jd[i * 3 + 1] * j0[3 + j] + jd[i * 3 + 2] * j0[6 + j];
+        // Higham iteration to convergence in FP32 (the CPU runs it to 1e-16 in double,
+        // solid_shell.cpp:473-487): stop once a step moves Q by less than FP32 can see
+        // against |Q|, at most six iterations.
 #pragma unroll 1
         for (int it = 0; it < 6; ++it) {
             float ipq[9], m[9];
@@ -223,8 +225,14 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) ipq[i * 3 + j] = 0.5f * (q[i * 3 + j] - mq[j * 3 + i]);
+            float step = 0.0f, size = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 9; ++k) q[k] = ipq[k];
+            for (int k = 0; k < 9; ++k) {
+                step = fmaxf(step, fabsf(ipq[k] - q[k]));
+                size = fmaxf(size, fabsf(ipq[k]));
+                q[k] = ipq[k];
+            }
+            if (step <= 1e-7f * size) break;
         }
     }
     // ---- co-rotated relative displacement u'_a = Q^T dX_a + dd_a + Q^T dd_a ----
@@ -282,6 +290,8 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
     float alpha[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) alpha[k] = d.alpha[e * 8 + k];
+    // the elastic K_aa factor of this element is usable (formed, and positive definite)
+    const bool have_factor = d.kaa_factor != nullptr && __ldg(d.kaa_factor + e * 32) > 0.0f;
 
     // ---- EAS Newton ----
     // The four elements of a warp iterate together (the shuffles need the whole warp):
@@ -320,6 +330,15 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
             }
         }
         if (__all_sync(0xffffffffu, done)) break;
+        // An element whose eight points are all elastic at this iterate has the
+        // elastic K_aa, whose Cholesky factor is formed once per material
+        // (shell_elastic_factor).  The warp builds K_aa itself only when one of its
+        // elements has a yielded point; the shuffles need the whole warp.
+        const unsigned yielded_mask = __ballot_sync(0xffffffffu, o.yielded);
+        const bool elastic_element = have_factor && ((yielded_mask >> (lane & 24)) & 0xffu) == 0u;
+        float l[28];
+        bool spd = true;
+        if (__any_sync(0xffffffffu, !elastic_element)) {
         // K_aa = sum_g w_g G^T C G, lower triangle
         float kaa[28];
         {
@@ -343,8 +362,6 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
                 }
         }
         // Cholesky (solid_shell.cpp:432-457), identical in every lane
-        float l[28];
-        bool spd = true;
         {
             int t = 0;
 #pragma unroll
@@ -363,6 +380,19 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
                     ++t;
                 }
             }
+        }
+        }
+        if (elastic_element) {
+            const float4* lf = reinterpret_cast<const float4*>(d.kaa_factor + e * 32);
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                const float4 v = __ldg(lf + k);
+                l[4 * k] = v.x;
+                l[4 * k + 1] = v.y;
+                l[4 * k + 2] = v.z;
+                l[4 * k + 3] = v.w;
+            }
+            spd = true;
         }
         float delta[7];
 #pragma unroll
@@ -416,10 +446,8 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
             }
 #pragma unroll
             for (int k = 0; k < 7; ++k) d.state[sbase + (size_t)k * 32] = ps[k];
-            atomicAdd(&istat[1], 1);
         }
         if (gp < 7) d.alpha[e * 8 + gp] = alpha[gp];
-        if (gp == 0 && !converged) atomicAdd(&istat[0], 1);
         const double s0 = o.sigma[0], s1 = o.sigma[1], s2 = o.sigma[2], s3 = o.sigma[3], s4 = o.sigma[4],
                      s5 = o.sigma[5];
         const double pr = (s0 + s1 + s2) / 3.0;
@@ -475,13 +503,20 @@ __global__ void __launch_bounds__(kShellBlock) shell_forces(ShellDevice d, Shell
 #pragma unroll
         for (int i = 0; i < 3; ++i) out[i] = -(f[i] + (q[i * 3] * f[0] + q[i * 3 + 1] * f[1] + q[i * 3 + 2] * f[2]));
     }
-    const double bd = block_sum(diss, scratch);
-    const double be = block_sum(energy, scratch);
-    if (threadIdx.x == 0) {
-        d.e_diss[blockIdx.x] += bd;
-        d.e_strain[blockIdx.x] = be;
-        d.e_stats[blockIdx.x * 2] += istat[0];
-        d.e_stats[blockIdx.x * 2 + 1] = istat[1];
+    // per-warp partials in fixed shuffle order: no block barrier, so a warp whose
+    // elements converge early does not wait for the slowest warp of its block
+    const unsigned nonconv = __ballot_sync(0xffffffffu, valid && gp == 0 && !converged);
+    const unsigned ypts = __ballot_sync(0xffffffffu, valid && o.yielded);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        diss += __shfl_xor_sync(0xffffffffu, diss, off);
+        energy += __shfl_xor_sync(0xffffffffu, energy, off);
+    }
+    if (lane == 0) {
+        d.e_diss[group_raw] += diss;
+        d.e_strain[group_raw] = energy;
+        d.e_stats[group_raw * 2] += __popc(nonconv);
+        d.e_stats[group_raw * 2 + 1] = __popc(ypts);
     }
 }
 
@@ -539,7 +574,71 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
     }
 }
 
+// The elastic K_aa = sum_g w_g G_g^T C G_g of every element, from the FP32 forms the
+// step uses, accumulated in double, and its Cholesky factor (packed lower triangle,
+// 28 of 32 floats per element).  A zero first entry marks an element whose elastic
+// K_aa is not positive definite; the step then forms K_aa itself.
+__global__ void shell_elastic_factor(ShellDevice d, double lambda, double mu, float* out) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d.elements) return;
+    const float4* base = d.forms + (size_t)(e / 4) * kShellRec4 * 32 + (e % 4) * 8;
+    double kaa[7][7];
+    for (int a = 0; a < 7; ++a)
+        for (int b = 0; b < 7; ++b) kaa[a][b] = 0.0;
+    for (int gp = 0; gp < 8; ++gp) {
+        float g[44];
+        for (int k = 0; k < 11; ++k) {
+            const float4 v = base[(size_t)(36 + k) * 32 + gp];
+            g[4 * k] = v.x;
+            g[4 * k + 1] = v.y;
+            g[4 * k + 2] = v.z;
+            g[4 * k + 3] = v.w;
+        }
+        const double w = g[42];
+        for (int b = 0; b < 7; ++b) {
+            double col[6], cg[6];
+            for (int i = 0; i < 6; ++i) col[i] = g[i * 7 + b];
+            const double tr = col[0] + col[1] + col[2];
+            for (int i = 0; i < 3; ++i) cg[i] = lambda * tr + 2.0 * mu * col[i];
+            for (int i = 3; i < 6; ++i) cg[i] = mu * col[i];
+            for (int a = 0; a < 7; ++a) {
+                double s = 0.0;
+                for (int i = 0; i < 6; ++i) s += (double)g[i * 7 + a] * cg[i];
+                kaa[a][b] += w * s;
+            }
+        }
+    }
+    float l[32];
+    double ld[28];
+    bool spd = true;
+    int t = 0;
+    for (int i = 0; i < 7; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double s = kaa[i][j];
+            for (int k = 0; k < j; ++k) s -= ld[i * (i + 1) / 2 + k] * ld[j * (j + 1) / 2 + k];
+            if (i == j) {
+                spd = spd && s > 0.0;
+                ld[t] = sqrt(s > 0.0 ? s : 1e-300);
+            } else {
+                ld[t] = s / ld[j * (j + 1) / 2 + j];
+            }
+            ++t;
+        }
+    for (int k = 0; k < 28; ++k) l[k] = (float)ld[k];
+    l[28] = l[29] = l[30] = l[31] = 0.0f;
+    if (!spd) l[0] = 0.0f;
+    float4* o = reinterpret_cast<float4*>(out + e * 32);
+    for (int k = 0; k < 8; ++k) o[k] = make_float4(l[4 * k], l[4 * k + 1], l[4 * k + 2], l[4 * k + 3]);
+}
+
 }  // namespace
+
+void launch_shell_elastic_factor(const ShellDevice& d, double youngs, double poisson, float* out,
+                                 cudaStream_t stream) {
+    const double lambda = youngs * poisson / ((1.0 + poisson) * (1.0 - 2.0 * poisson));
+    const double mu = youngs / (2.0 * (1.0 + poisson));
+    shell_elastic_factor<<<blocks_for(d.elements, 128), 128, 0, stream>>>(d, lambda, mu, out);
+}
 
 void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts) {
     const int eb = blocks_for(d.groups * 32, kShellBlock);

@@ -349,7 +349,7 @@ class ShellSolver:
 
     @staticmethod
     def params(youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9, dt=1e-7, damping=1.0,
-               rise_time=0.0, max_iterations=12, tol_residual=1e-6, tol_work=1e-13, compensated=True):
+               rise_time=0.0, max_iterations=12, tol_residual=5e-5, tol_work=1e-13, compensated=True):
         return ShellParamsC(youngs, poisson, yield_strength, hardening, dt, damping, rise_time, int(max_iterations),
                             tol_residual, tol_work, int(bool(compensated)))
 
