@@ -150,6 +150,88 @@ int femstep_tet_step_noalloc(const femstep_tet_device_mesh *mesh, int substeps, 
                              void *stream);
 
 /* =====================================================================================
+ * Pool of many tet meshes: the batched and the served step.  No reference
+ * counterpart: the reference solves one mesh at a time (fem::stepCpu,
+ * engine/sim/fem.cpp:187; gpu::FemGpuSolver::run, engine/gpu/fem_gpu.cpp:374).  Every
+ * mesh keeps its own material, load, time step and step count; the arithmetic per
+ * mesh is the J2_F32K tet step's (its displacement, velocity and plastic state are
+ * bit-identical to a femstep_tet handle in FEMSTEP_TET_J2_F32K mode given the same
+ * dt), and a mesh's result does not depend on what else is in the pool.
+ *
+ * Every pool call is ordered on the pool's one stream, so admit / release may be
+ * called while a chunk from femstep_pool_run_async is still running: their device
+ * work lands behind it.  Admission does its host work while the GPU runs.
+ * ===================================================================================== */
+
+typedef struct {
+    size_t nodes, tets;
+    const float *position;            /* 3N (TetMesh::position) */
+    const uint32_t *index;            /* 4T, mesh-local node ids */
+    const uint32_t *fixed;            /* N, may be NULL */
+    const double *external_force;     /* 3N full-amplitude load, may be NULL */
+    double density, youngs_modulus, poisson_ratio, yield_strength, hardening_modulus;
+    double dt;                        /* 0: 0.9 x the FP64 element eigenvalue bound, on the GPU */
+    double gravity, damping;          /* damping 0 means 1 (none) */
+    int ramp_steps;                   /* load factor min((step+1)/ramp, 1); 0 = full */
+} femstep_pool_mesh;
+
+typedef struct femstep_pool femstep_pool;
+
+#define FEMSTEP_POOL_AUTO 0        /* the pool's schedule (set by autotune or set_schedule) */
+#define FEMSTEP_POOL_GRAPH 1       /* two launches per step, replayed from a CUDA graph */
+#define FEMSTEP_POOL_PERSISTENT 2  /* one cooperative launch per chunk, grid barriers */
+
+/* A pool holding up to `tet_capacity` tets and `node_capacity` nodes (each mesh also
+   takes one spare node slot) of at most `max_meshes` meshes; tile = threads per block
+   (128, 256 or 512; 0 = 256).  Device memory: femstep_pool_bytes_per_tet() per tet and
+   femstep_pool_bytes_per_node() per node of capacity, all allocated here.
+   tet_capacity <= 1e9 (slot ids are 32-bit). */
+int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshes, int tile, femstep_pool **out);
+size_t femstep_pool_bytes_per_tet(void);
+size_t femstep_pool_bytes_per_node(void);
+/* Admit a mesh that will take `steps` steps (at rest, zero plastic strain).
+   FEMSTEP_ENOMEM when it does not fit in the free space now: the caller keeps it
+   queued and retries after a release. */
+int femstep_pool_admit(femstep_pool *pool, const femstep_pool_mesh *mesh, long long steps, int *id);
+/* Free a mesh's space.  Its device state is frozen behind any queued work. */
+int femstep_pool_release(femstep_pool *pool, int id);
+/* Queue one chunk: every admitted mesh that has steps left advances by up to `steps`
+   steps (meshes that reach their count stop there).  Returns without waiting. */
+int femstep_pool_run_async(femstep_pool *pool, int steps, int mode);
+/* Wait for the queued chunk; its device milliseconds (CUDA events). */
+int femstep_pool_wait(femstep_pool *pool, double *gpu_ms);
+/* run_async + wait. */
+int femstep_pool_run(femstep_pool *pool, int steps, int mode, double *gpu_ms);
+/* Ids of the meshes whose step count was reached by the last chunk that was waited
+   for (up to `capacity` of them; *count = how many there are). */
+int femstep_pool_finished(femstep_pool *pool, int *ids, int capacity, int *count);
+/* Steps taken and requested of one mesh (waits for queued work). */
+int femstep_pool_status(femstep_pool *pool, int id, long long *steps_done, long long *steps_target);
+/* Positions (rest + displacement) and velocities of one mesh, 3N doubles each. */
+int femstep_pool_readback(femstep_pool *pool, int id, double *position, double *velocity);
+/* Plastic strain of one mesh, 7 per tet (6 engineering components, equivalent). */
+int femstep_pool_plastic(femstep_pool *pool, int id, double *plastic);
+/* [0] external work (load and gravity) [1] dissipation [2] strain energy [3] kinetic
+   of one mesh, reduced on the GPU in FP64 in a fixed order. */
+int femstep_pool_energy(femstep_pool *pool, int id, double out[4]);
+/* The time step a mesh runs with (its own, or the bound computed at admission). */
+int femstep_pool_dt(femstep_pool *pool, int id, double *dt);
+/* The autotuner: times every tile size in {128, 256, 512} with both schedules for
+   `steps` steps on the pool as it is, restores the pool's state after each trial (so
+   tuning does not change any result), keeps the fastest, and reports it. */
+int femstep_pool_autotune(femstep_pool *pool, int steps, int *tile, int *mode, double *ms_per_step);
+/* Set the schedule by hand (tile 128 / 256 / 512; GRAPH or PERSISTENT). */
+int femstep_pool_set_schedule(femstep_pool *pool, int tile, int mode);
+/* Mean device milliseconds per launch of [0] the element pass and [1] the node pass,
+   over `steps` steps taken one launch at a time (the steps count as taken). */
+int femstep_pool_profile(femstep_pool *pool, int steps, double out[2]);
+/* [0] tets in use [1] nodes in use [2] meshes admitted [3] tile [4] mode [5] kernel
+   launches of the last chunk [6] device bytes held [7] pinned staging buffers */
+int femstep_pool_info(femstep_pool *pool, long long out[8]);
+const char *femstep_pool_error(const femstep_pool *pool);
+void femstep_pool_destroy(femstep_pool *pool);
+
+/* =====================================================================================
  * Solid-shell zone step.  Replaces gpu::ZoneGpuSolver (engine/gpu/zone_gpu.hpp:179-234):
  * the 8-node ANS + 7-parameter EAS solid-shell with J2 plasticity (linear isotropic
  * hardening, failure off), the CSR gather and the lumped-mass node update of

@@ -1,6 +1,7 @@
 // api_common.cu -- error text and device discovery shared by every entry point.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -25,6 +26,42 @@ int device_status() {
         return FEMSTEP_SKIP;
     }
     return FEMSTEP_OK;
+}
+
+void tet_rest_state64(size_t nodes, size_t tets, const float* position, const uint32_t* index, double density,
+                      std::vector<double>& inv, std::vector<double>& vol, std::vector<double>& mass) {
+    inv.assign(tets * 9, 0.0);
+    vol.assign(tets, 0.0);
+    mass.assign(nodes, 0.0);
+    for (size_t t = 0; t < tets; ++t) {
+        const uint32_t* idx = &index[t * 4];
+        double a[9];  // column-major
+        for (int c = 0; c < 3; ++c)
+            for (int r = 0; r < 3; ++r)
+                a[c * 3 + r] = (double)position[(size_t)idx[c + 1] * 3 + r] - (double)position[(size_t)idx[0] * 3 + r];
+#define A(r, c) a[(c) * 3 + (r)]
+        const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
+                           A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                           A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+        const double volume = det / 6.0;
+        vol[t] = std::fabs(volume);
+        const double id = std::fabs(det) > 1e-300 ? 1.0 / det : 0.0;
+        double* r = &inv[t * 9];
+#define R(rr, cc) r[(cc) * 3 + (rr)]
+        R(0, 0) = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) * id;
+        R(0, 1) = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * id;
+        R(0, 2) = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * id;
+        R(1, 0) = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) * id;
+        R(1, 1) = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * id;
+        R(1, 2) = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * id;
+        R(2, 0) = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) * id;
+        R(2, 1) = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * id;
+        R(2, 2) = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * id;
+#undef R
+#undef A
+        const double quarter = density * vol[t] * 0.25;
+        for (int c = 0; c < 4; ++c) mass[idx[c]] += quarter;
+    }
 }
 
 }  // namespace fs

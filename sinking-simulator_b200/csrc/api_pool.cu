@@ -1,0 +1,856 @@
+// api_pool.cu -- host side of the multi-mesh pool (pool.hpp) behind the C ABI.
+//
+// The pool is the engine of both the batched and the served workloads: meshes are
+// admitted into free ranges of the pool's arrays against its capacity, stepped
+// together (each with its own material, load, time step and step count), read back
+// and released.  Admission that does not fit returns FEMSTEP_ENOMEM, so a serving
+// loop keeps the request queued and admits it as soon as a release frees room; the
+// requests already on the GPU keep running meanwhile (continuous batching).
+//
+// Everything the pool does on the device goes through its one stream, in call order.
+// That makes every call safe while a chunk is still running: an admission's uploads,
+// a release's freeze and a new work list all land behind the chunk.  Admission does
+// its host work (rest state, CSR, slot map) while the GPU runs and hands the bytes to
+// the stream from pinned staging buffers, so it never waits for the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/femstep.h"
+#include "common.cuh"
+#include "host_util.hpp"
+#include "pool.hpp"
+#include "tet.hpp"
+
+using fs::PoolDevice;
+using fs::PoolMesh;
+using fs::PoolTile;
+
+namespace {
+
+// First-fit allocator over [0, capacity) with coalescing on release.
+class RangeAllocator {
+public:
+    void reset(long long capacity) {
+        free_.clear();
+        if (capacity > 0) free_[0] = capacity;
+    }
+    long long take(long long n) {
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= n) {
+                const long long at = it->first, left = it->second - n;
+                free_.erase(it);
+                if (left > 0) free_[at + n] = left;
+                return at;
+            }
+        return -1;
+    }
+    void give(long long at, long long n) {
+        auto next = free_.lower_bound(at);
+        if (next != free_.end() && at + n == next->first) {
+            n += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == at) {
+                prev->second += n;
+                return;
+            }
+        }
+        free_[at] = n;
+    }
+
+private:
+    std::map<long long, long long> free_;  // start -> length
+};
+
+// Pinned host buffers for uploads queued behind device work.  A buffer is reused once
+// the event recorded after its copies has completed.
+class Staging {
+public:
+    struct Buf {
+        char* host = nullptr;
+        size_t cap = 0, used = 0;
+        cudaEvent_t done = nullptr;
+        bool pending = false;
+    };
+    // A buffer of at least `bytes`, not in use by any queued copy.
+    Buf* get(size_t bytes, cudaError_t& err) {
+        err = cudaSuccess;
+        Buf* best = nullptr;
+        for (Buf& b : bufs_) {
+            if (b.pending) {
+                if (cudaEventQuery(b.done) != cudaSuccess) continue;
+                b.pending = false;
+            }
+            if (b.cap >= bytes && (!best || b.cap < best->cap)) best = &b;
+        }
+        if (!best) {
+            Buf b;
+            b.cap = std::max<size_t>(bytes, size_t(4) << 20);
+            err = cudaHostAlloc(&b.host, b.cap, cudaHostAllocDefault);
+            if (err != cudaSuccess) return nullptr;
+            err = cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
+            if (err != cudaSuccess) {
+                cudaFreeHost(b.host);
+                return nullptr;
+            }
+            bufs_.push_back(b);
+            best = &bufs_.back();
+        }
+        best->used = 0;
+        return best;
+    }
+    // Reserve `bytes` (256-aligned) inside `b`.
+    static char* take(Buf* b, size_t bytes) {
+        char* p = b->host + b->used;
+        b->used += (bytes + 255) & ~size_t(255);
+        return p;
+    }
+    static void submit(Buf* b, cudaStream_t s) {
+        cudaEventRecord(b->done, s);
+        b->pending = true;
+    }
+    void release() {
+        for (Buf& b : bufs_) {
+            if (b.done) cudaEventDestroy(b.done);
+            if (b.host) cudaFreeHost(b.host);
+        }
+        bufs_.clear();
+    }
+    size_t count() const { return bufs_.size(); }
+
+private:
+    std::deque<Buf> bufs_;  // a deque, so a Buf* stays valid as buffers are added
+};
+
+struct HostMesh {
+    bool used = false;
+    long long t0 = 0, T = 0, n0 = 0, N = 0;  // pool ranges (N + 1 node slots held)
+    long long e_part = 0, n_part = 0, e_tiles = 0, n_tiles = 0;  // partial slots (tile 128)
+    long long target = 0, serial = 0;
+    std::vector<float> rest;                  // 3N rest positions, for readback
+};
+
+constexpr int kMinTile = 128;
+constexpr int kGraphSteps = 16;
+
+}  // namespace
+
+struct femstep_pool {
+    long long tet_cap = 0, node_cap = 0, part_cap = 0;
+    int max_meshes = 0;
+    long long next_serial = 1;
+    int tile = 256;
+    int mode = FEMSTEP_POOL_GRAPH;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    fs::DeviceArena arena;
+    PoolDevice d;
+    RangeAllocator tets, nodes, parts;
+    std::vector<HostMesh> meshes;
+    Staging staging;
+    bool dirty = true;  // work lists need rebuilding
+    PoolTile* d_etiles = nullptr;
+    PoolTile* d_ntiles = nullptr;
+    int* d_active = nullptr;
+    double* d_block_max = nullptr;  // critical-dt scratch
+    cudaGraphExec_t graph = nullptr;
+    long long launches = 0;
+    bool in_flight = false;
+    bool broken = false;
+    double* d_out = nullptr;
+    PoolMesh* h_meshes = nullptr;  // pinned mirror of the mesh table, refreshed per chunk
+    int* h_error = nullptr;        // pinned mirror of the barrier error flag
+    std::string error;
+};
+
+namespace {
+
+int fail(femstep_pool* p, int code, const std::string& what) {
+    if (p) p->error = what;
+    fs::set_last_error(what);
+    return code;
+}
+
+int check(femstep_pool* p, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return FEMSTEP_OK;
+    return fail(p, e == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+bool valid_id(const femstep_pool* p, int id) { return p && id >= 0 && id < p->max_meshes && p->meshes[id].used; }
+
+void drop_graph(femstep_pool* p) {
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+}
+
+// Rebuild the tile lists of the admitted meshes (tiles never straddle meshes) and
+// queue their upload; the lists' device buffers are sized for the pool's capacity.
+int rebuild(femstep_pool* p) {
+    if (!p->dirty) return FEMSTEP_OK;
+    std::vector<PoolTile> et, nt;
+    std::vector<int> active;
+    const int T = p->tile;
+    for (int id = 0; id < (int)p->meshes.size(); ++id) {
+        const HostMesh& m = p->meshes[id];
+        if (!m.used) continue;
+        active.push_back(id);
+        for (long long k = 0, b = 0; b < m.T; ++k, b += T)
+            et.push_back(PoolTile{id, (int)(m.e_part + k), m.t0 + b, m.t0 + std::min(m.T, b + T)});
+        for (long long k = 0, b = 0; b < m.N; ++k, b += T)
+            nt.push_back(PoolTile{id, (int)(m.n_part + k), m.n0 + b, m.n0 + std::min(m.N, b + T)});
+    }
+    if ((long long)et.size() > p->part_cap || (long long)nt.size() > p->part_cap)
+        return fail(p, FEMSTEP_ESTATE, "work list above its capacity");
+    const size_t be = et.size() * sizeof(PoolTile), bn = nt.size() * sizeof(PoolTile),
+                 ba = active.size() * sizeof(int);
+    cudaError_t err;
+    Staging::Buf* buf = p->staging.get(be + bn + ba + 3 * 256, err);
+    if (!buf) return check(p, err, "pinned staging");
+    auto put = [&](void* dst, const void* src, size_t bytes) {
+        if (!bytes) return;
+        char* h = Staging::take(buf, bytes);
+        std::memcpy(h, src, bytes);
+        cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, p->stream);
+    };
+    put(p->d_etiles, et.data(), be);
+    put(p->d_ntiles, nt.data(), bn);
+    put(p->d_active, active.data(), ba);
+    Staging::submit(buf, p->stream);
+    p->d.etiles = p->d_etiles;
+    p->d.ntiles = p->d_ntiles;
+    p->d.n_etiles = (int)et.size();
+    p->d.n_ntiles = (int)nt.size();
+    p->d.active = p->d_active;
+    p->d.n_active = (int)active.size();
+    p->dirty = false;
+    drop_graph(p);
+    return check(p, cudaGetLastError(), "work list upload");
+}
+
+int launch_chunk(femstep_pool* p, int steps, int mode) {
+    if (steps <= 0 || p->d.n_etiles == 0) return FEMSTEP_OK;
+    if (mode == FEMSTEP_POOL_PERSISTENT) {
+        const int blocks = std::min(fs::pool_persistent_max_blocks(p->tile), p->d.n_etiles);
+        if (blocks <= 0) return fail(p, FEMSTEP_ECUDA, "no co-resident blocks for the persistent launch");
+        const int rc = check(p, fs::launch_pool_persistent(p->d, p->tile, steps, blocks, p->stream),
+                             "persistent launch");
+        p->launches += 2;
+        return rc;
+    }
+    int left = steps;
+    if (left >= kGraphSteps) {
+        if (!p->graph) {
+            cudaGraph_t g = nullptr;
+            int rc = check(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "capture");
+            if (rc) return rc;
+            fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream);
+            rc = check(p, cudaStreamEndCapture(p->stream, &g), "capture end");
+            if (rc) return rc;
+            rc = check(p, cudaGraphInstantiate(&p->graph, g, 0), "graph instantiate");
+            cudaGraphDestroy(g);
+            if (rc) return rc;
+        }
+        for (; left >= kGraphSteps; left -= kGraphSteps) {
+            const int rc = check(p, cudaGraphLaunch(p->graph, p->stream), "graph launch");
+            if (rc) return rc;
+            p->launches += 2 * kGraphSteps + 1;
+        }
+    }
+    if (left > 0) {
+        fs::launch_pool_steps(p->d, p->tile, left, p->stream);
+        p->launches += 2 * left + 1;
+    }
+    return check(p, cudaGetLastError(), "kernel launch");
+}
+
+// Everything a step changes, over the used prefix of the pool: the state a trial run
+// is rolled back to.
+struct Snapshot {
+    std::vector<std::pair<void*, size_t>> spans;
+    char* buf = nullptr;
+};
+
+int snapshot(femstep_pool* p, Snapshot& s, bool restore) {
+    long long tmax = 0, nmax = 0, pmax = 0;
+    for (const HostMesh& m : p->meshes)
+        if (m.used) {
+            tmax = std::max(tmax, m.t0 + m.T);
+            nmax = std::max(nmax, m.n0 + m.N + 1);
+            pmax = std::max(pmax, std::max(m.e_part + m.e_tiles, m.n_part + m.n_tiles));
+        }
+    if (!restore) {
+        s.spans.clear();
+        for (int k = 0; k < 7; ++k) {
+            s.spans.push_back({p->d.plastic + (size_t)k * p->tet_cap, (size_t)tmax * 4});
+            s.spans.push_back({p->d.plastic_c + (size_t)k * p->tet_cap, (size_t)tmax * 4});
+        }
+        s.spans.push_back({p->d.disp, (size_t)nmax * 12});
+        s.spans.push_back({p->d.disp_c, (size_t)nmax * 12});
+        s.spans.push_back({p->d.velocity, (size_t)nmax * 12});
+        s.spans.push_back({p->d.meshes, (size_t)p->max_meshes * sizeof(PoolMesh)});
+        s.spans.push_back({p->d.e_diss, (size_t)pmax * 8});
+        s.spans.push_back({p->d.e_strain, (size_t)pmax * 8});
+        s.spans.push_back({p->d.n_work, (size_t)pmax * 8});
+        s.spans.push_back({p->d.n_kin, (size_t)pmax * 8});
+        size_t total = 0;
+        for (auto& sp : s.spans) total += sp.second;
+        const int rc = check(p, cudaMalloc(&s.buf, total ? total : 1), "snapshot");
+        if (rc) return rc;
+    }
+    size_t off = 0;
+    for (auto& sp : s.spans) {
+        if (restore)
+            cudaMemcpyAsync(sp.first, s.buf + off, sp.second, cudaMemcpyDeviceToDevice, p->stream);
+        else
+            cudaMemcpyAsync(s.buf + off, sp.first, sp.second, cudaMemcpyDeviceToDevice, p->stream);
+        off += sp.second;
+    }
+    return check(p, cudaStreamSynchronize(p->stream), "snapshot copy");
+}
+
+int wait_chunk(femstep_pool* p, double* gpu_ms) {
+    if (gpu_ms) *gpu_ms = 0.0;
+    if (!p->in_flight) return FEMSTEP_OK;
+    p->in_flight = false;
+    int rc = check(p, cudaEventSynchronize(p->ev1), "pool step");
+    if (rc) return rc;
+    if (*p->h_error) {
+        p->broken = true;
+        return fail(p, FEMSTEP_ETIMEOUT, "a grid barrier of the persistent launch gave up waiting");
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+    if (gpu_ms) *gpu_ms = ms;
+    return FEMSTEP_OK;
+}
+
+int refresh_mirror(femstep_pool* p) {
+    return check(p, cudaMemcpyAsync(p->h_meshes, p->d.meshes, sizeof(PoolMesh) * p->max_meshes,
+                                    cudaMemcpyDeviceToHost, p->stream), "mesh table");
+}
+
+}  // namespace
+
+extern "C" {
+
+int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshes, int tile, femstep_pool** out) {
+    if (out) *out = nullptr;
+    if (!out || tet_capacity == 0 || node_capacity == 0 || max_meshes <= 0)
+        return fail(nullptr, FEMSTEP_EINVAL, "empty pool");
+    if (tet_capacity > 1000000000ull) return fail(nullptr, FEMSTEP_EINVAL, "tet capacity above 1e9 (32-bit slot ids)");
+    if (node_capacity > 2000000000ull) return fail(nullptr, FEMSTEP_EINVAL, "node capacity above 2e9");
+    if (tile == 0) tile = 256;
+    if (tile != 128 && tile != 256 && tile != 512) return fail(nullptr, FEMSTEP_EINVAL, "tile must be 128, 256 or 512");
+    const int dev = fs::device_status();
+    if (dev != FEMSTEP_OK) return dev;
+    femstep_pool* p = new femstep_pool();
+    p->tet_cap = (long long)tet_capacity;
+    p->node_cap = (long long)node_capacity;
+    p->max_meshes = max_meshes;
+    p->tile = tile;
+    // partial slots: every mesh reserves ceil(T/128) + ceil(N/128) (the smallest tile)
+    p->part_cap = (long long)(tet_capacity + node_capacity) / kMinTile + 2LL * max_meshes;
+    int rc = check(p, cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
+    if (!rc) rc = check(p, cudaEventCreate(&p->ev0), "event");
+    if (!rc) rc = check(p, cudaEventCreate(&p->ev1), "event");
+    if (!rc) rc = check(p, cudaHostAlloc(&p->h_meshes, sizeof(PoolMesh) * max_meshes, cudaHostAllocDefault), "pinned");
+    if (!rc) rc = check(p, cudaHostAlloc(&p->h_error, sizeof(int), cudaHostAllocDefault), "pinned");
+    if (rc) {
+        femstep_pool_destroy(p);
+        return rc;
+    }
+    std::memset(p->h_meshes, 0, sizeof(PoolMesh) * max_meshes);
+    *p->h_error = 0;
+    fs::DeviceArena& A = p->arena;
+    PoolDevice& d = p->d;
+    const size_t Tc = tet_capacity, Nc = node_capacity;
+    d.tet_cap = (long long)Tc;
+    d.node_cap = (long long)Nc;
+    d.index = A.zeros<uint4>(Tc);
+    d.slot = A.zeros<uint4>(Tc);
+    d.rest_inv = A.alloc<float>(Tc * 9);
+    d.rest_vol = A.alloc<float>(Tc);
+    d.plastic = A.alloc<float>(Tc * 7);
+    d.plastic_c = A.alloc<float>(Tc * 7);
+    d.slots = A.alloc<float>(Tc * 12 + 4);
+    d.offset = A.zeros<uint32_t>(Nc);
+    d.disp = A.alloc<float>(Nc * 3);
+    d.disp_c = A.alloc<float>(Nc * 3);
+    d.velocity = A.alloc<float>(Nc * 3);
+    d.mass = A.alloc<float>(Nc);
+    d.inv_mass = A.alloc<float>(Nc);
+    d.fixed = A.zeros<uint8_t>(Nc);
+    d.ext = A.zeros<float>(Nc * 3);
+    d.meshes = A.zeros<PoolMesh>(max_meshes);
+    d.e_diss = A.zeros<double>(p->part_cap);
+    d.e_strain = A.zeros<double>(p->part_cap);
+    d.n_work = A.zeros<double>(p->part_cap);
+    d.n_kin = A.zeros<double>(p->part_cap);
+    d.barrier = A.zeros<unsigned int>(2);
+    d.error = A.zeros<int>(1);
+    p->d_etiles = A.alloc<PoolTile>(p->part_cap);
+    p->d_ntiles = A.alloc<PoolTile>(p->part_cap);
+    p->d_active = A.zeros<int>(max_meshes);
+    p->d_block_max = A.zeros<double>(Tc / fs::kBlock + 1);
+    p->d_out = A.zeros<double>(8);
+    if (!A.ok()) {
+        const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;
+        fail(p, code, std::string("pool allocation failed: ") + cudaGetErrorString(A.status()));
+        femstep_pool_destroy(p);
+        return code;
+    }
+    p->tets.reset(p->tet_cap);
+    p->nodes.reset(p->node_cap);
+    p->parts.reset(p->part_cap);
+    p->meshes.resize(max_meshes);
+    *out = p;
+    return FEMSTEP_OK;
+}
+
+size_t femstep_pool_bytes_per_tet(void) { return 16 + 16 + 36 + 4 + 28 + 28 + 48; }
+size_t femstep_pool_bytes_per_node(void) { return 4 + 12 + 12 + 12 + 4 + 4 + 1 + 12; }
+
+int femstep_pool_admit(femstep_pool* p, const femstep_pool_mesh* mesh, long long steps, int* id) {
+    if (!p || !mesh || !id) return fail(p, FEMSTEP_EINVAL, "null argument");
+    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
+    const femstep_pool_mesh& m = *mesh;
+    const long long N = (long long)m.nodes, T = (long long)m.tets;
+    if (N == 0 || T == 0 || !m.position || !m.index) return fail(p, FEMSTEP_EINVAL, "empty mesh");
+    if (steps < 0) return fail(p, FEMSTEP_EINVAL, "negative step count");
+    if (!(m.density > 0.0)) return fail(p, FEMSTEP_EINVAL, "density must be positive");
+    if (!(m.youngs_modulus > 0.0) || !(m.poisson_ratio > -1.0 && m.poisson_ratio < 0.5))
+        return fail(p, FEMSTEP_EINVAL, "elastic constants out of range");
+    for (long long i = 0; i < T * 4; ++i)
+        if (m.index[i] >= (uint32_t)N) return fail(p, FEMSTEP_EINVAL, "tet index out of range");
+    int slot_id = -1;
+    for (int k = 0; k < p->max_meshes; ++k)
+        if (!p->meshes[k].used) {
+            slot_id = k;
+            break;
+        }
+    if (slot_id < 0) return fail(p, FEMSTEP_ENOMEM, "mesh table full");
+    const long long e_tiles = (T + kMinTile - 1) / kMinTile, n_tiles = (N + kMinTile - 1) / kMinTile;
+    const long long t0 = p->tets.take(T);
+    if (t0 < 0) return fail(p, FEMSTEP_ENOMEM, "no room for the tets now");
+    const long long n0 = p->nodes.take(N + 1);
+    if (n0 < 0) {
+        p->tets.give(t0, T);
+        return fail(p, FEMSTEP_ENOMEM, "no room for the nodes now");
+    }
+    const long long part0 = p->parts.take(e_tiles + n_tiles);
+    auto undo = [&]() {
+        p->tets.give(t0, T);
+        p->nodes.give(n0, N + 1);
+        if (part0 >= 0) p->parts.give(part0, e_tiles + n_tiles);
+    };
+    if (part0 < 0) {
+        undo();
+        return fail(p, FEMSTEP_ENOMEM, "no room for the energy partials now");
+    }
+    // host-side forms (while the GPU runs whatever is queued): FP64 rest state, CSR in
+    // the reference's order, slot map
+    std::vector<double> inv64, vol64, mass64;
+    fs::tet_rest_state64((size_t)N, (size_t)T, m.position, m.index, m.density, inv64, vol64, mass64);
+    double vmax = 0.0;
+    for (double v : vol64) vmax = std::max(vmax, v);
+    if (!(vmax > 0.0)) {
+        undo();
+        return fail(p, FEMSTEP_EINVAL, "every tet is degenerate");
+    }
+    std::vector<uint32_t> off, entry;
+    fs::build_csr((size_t)N, (size_t)T, 4, m.index, off, entry);
+
+    const size_t bytes = (size_t)T * (16 + 16 + 36 + 4) + (size_t)(N + 1) * (4 + 4 + 4 + 1 + 12) + sizeof(PoolMesh) +
+                         16 * 256;
+    cudaError_t err;
+    Staging::Buf* buf = p->staging.get(bytes, err);
+    if (!buf) {
+        undo();
+        return check(p, err, "pinned staging");
+    }
+    PoolDevice& d = p->d;
+    cudaStream_t st = p->stream;
+    auto stage = [&](size_t n) { return Staging::take(buf, n); };
+    auto send = [&](void* dst, const void* h, size_t n) { cudaMemcpyAsync(dst, h, n, cudaMemcpyHostToDevice, st); };
+
+    const long long s0 = 4 * t0;
+    uint4* idx4 = (uint4*)stage(T * sizeof(uint4));
+    uint4* slot4 = (uint4*)stage(T * sizeof(uint4));
+    {
+        std::vector<uint32_t> sl(T * 4);
+        for (long long n = 0; n < N; ++n)
+            for (uint32_t k = off[n]; k < off[n + 1]; ++k) sl[entry[k]] = (uint32_t)(s0 + k);
+        for (long long t = 0; t < T; ++t) {
+            idx4[t] = make_uint4((uint32_t)(n0 + m.index[t * 4]), (uint32_t)(n0 + m.index[t * 4 + 1]),
+                                 (uint32_t)(n0 + m.index[t * 4 + 2]), (uint32_t)(n0 + m.index[t * 4 + 3]));
+            slot4[t] = make_uint4(sl[t * 4], sl[t * 4 + 1], sl[t * 4 + 2], sl[t * 4 + 3]);
+        }
+    }
+    send(d.index + t0, idx4, T * sizeof(uint4));
+    send(d.slot + t0, slot4, T * sizeof(uint4));
+    float* inv = (float*)stage((size_t)T * 9 * 4);
+    for (int k = 0; k < 9; ++k) {
+        float* col = inv + (size_t)k * T;
+        for (long long t = 0; t < T; ++t) col[t] = (float)inv64[t * 9 + k];
+        send(d.rest_inv + (size_t)k * p->tet_cap + t0, col, T * 4);
+    }
+    float* vol = (float*)stage(T * 4);
+    for (long long t = 0; t < T; ++t) vol[t] = (float)vol64[t];
+    send(d.rest_vol + t0, vol, T * 4);
+    for (int k = 0; k < 7; ++k) {
+        cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+        cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+    }
+    uint32_t* offs = (uint32_t*)stage((N + 1) * 4);
+    for (long long n = 0; n <= N; ++n) offs[n] = (uint32_t)(s0 + off[n]);
+    send(d.offset + n0, offs, (N + 1) * 4);
+    float* mass = (float*)stage((N + 1) * 4);
+    float* imass = (float*)stage((N + 1) * 4);
+    uint8_t* fixed = (uint8_t*)stage(N + 1);
+    float* ext = (float*)stage((N + 1) * 12);
+    for (long long n = 0; n < N; ++n) {
+        mass[n] = (float)mass64[n];
+        imass[n] = mass64[n] > 0.0 ? (float)(1.0 / mass64[n]) : 0.0f;
+        fixed[n] = m.fixed && m.fixed[n] ? 1 : 0;
+        for (int k = 0; k < 3; ++k) ext[n * 3 + k] = m.external_force ? (float)m.external_force[n * 3 + k] : 0.0f;
+    }
+    mass[N] = imass[N] = 0.0f;
+    fixed[N] = 1;
+    ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
+    send(d.mass + n0, mass, (N + 1) * 4);
+    send(d.inv_mass + n0, imass, (N + 1) * 4);
+    send(d.fixed + n0, fixed, N + 1);
+    send(d.ext + n0 * 3, ext, (N + 1) * 12);
+    cudaMemsetAsync(d.disp + n0 * 3, 0, (N + 1) * 12, st);
+    cudaMemsetAsync(d.disp_c + n0 * 3, 0, (N + 1) * 12, st);
+    cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
+    cudaMemsetAsync(d.e_diss + part0, 0, e_tiles * 8, st);
+    cudaMemsetAsync(d.e_strain + part0, 0, e_tiles * 8, st);
+    cudaMemsetAsync(d.n_work + part0 + e_tiles, 0, n_tiles * 8, st);
+    cudaMemsetAsync(d.n_kin + part0 + e_tiles, 0, n_tiles * 8, st);
+    PoolMesh* pm = (PoolMesh*)stage(sizeof(PoolMesh));
+    std::memset(pm, 0, sizeof(PoolMesh));
+    const double E = m.youngs_modulus, nu = m.poisson_ratio;
+    pm->dmu = E / (2.0 * (1.0 + nu));
+    pm->dkappa = E / (3.0 * (1.0 - 2.0 * nu));
+    pm->mu = (float)pm->dmu;
+    pm->kappa = (float)pm->dkappa;
+    pm->yield = (float)m.yield_strength;
+    pm->hardening = (float)m.hardening_modulus;
+    pm->dt64 = m.dt > 0.0 ? m.dt : 0.0;
+    pm->dt = (float)pm->dt64;
+    pm->gravity = (float)m.gravity;
+    pm->damping = (float)(m.damping > 0.0 ? m.damping : 1.0);
+    pm->ramp = m.ramp_steps;
+    pm->step = 0;
+    pm->target = steps;
+    pm->e_part = part0;
+    pm->n_part = part0 + e_tiles;
+    pm->serial = p->next_serial;
+    send(d.meshes + slot_id, pm, sizeof(PoolMesh));
+    // no step given: 0.9 x the FP64 element eigenvalue bound of the uploaded FP32 Dm^-1,
+    // computed and stored on the device behind the uploads
+    if (!(m.dt > 0.0))
+        fs::launch_pool_dt(d, slot_id, t0, T, E, nu, m.density, 0.9, p->d_block_max, p->d_out + 7, st);
+    Staging::submit(buf, st);
+    const int rc = check(p, cudaGetLastError(), "admit upload");
+    if (rc) {
+        undo();
+        return rc;
+    }
+    HostMesh& h = p->meshes[slot_id];
+    h.used = true;
+    h.t0 = t0;
+    h.T = T;
+    h.n0 = n0;
+    h.N = N;
+    h.e_part = part0;
+    h.n_part = part0 + e_tiles;
+    h.e_tiles = e_tiles;
+    h.n_tiles = n_tiles;
+    h.target = steps;
+    h.serial = p->next_serial++;
+    h.rest.assign(m.position, m.position + N * 3);
+    p->dirty = true;
+    *id = slot_id;
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_release(femstep_pool* p, int id) {
+    if (!valid_id(p, id)) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    HostMesh& h = p->meshes[id];
+    // freeze it behind any queued work, so no work list can touch the ranges again
+    cudaMemsetAsync(p->d.meshes + id, 0, sizeof(PoolMesh), p->stream);
+    p->tets.give(h.t0, h.T);
+    p->nodes.give(h.n0, h.N + 1);
+    p->parts.give(h.e_part, h.e_tiles + h.n_tiles);
+    h = HostMesh{};
+    p->dirty = true;
+    return check(p, cudaGetLastError(), "release");
+}
+
+int femstep_pool_run_async(femstep_pool* p, int steps, int mode) {
+    if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
+    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
+    if (steps < 0) return fail(p, FEMSTEP_EINVAL, "negative step count");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is already running: wait for it first");
+    if (mode == FEMSTEP_POOL_AUTO) mode = p->mode;
+    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT) return fail(p, FEMSTEP_EINVAL, "bad mode");
+    int rc = rebuild(p);
+    if (rc) return rc;
+    p->launches = 0;
+    rc = check(p, cudaEventRecord(p->ev0, p->stream), "event");
+    if (!rc) rc = launch_chunk(p, steps, mode);
+    if (!rc) rc = refresh_mirror(p);
+    if (!rc) rc = check(p, cudaMemcpyAsync(p->h_error, p->d.error, sizeof(int), cudaMemcpyDeviceToHost, p->stream),
+                        "error flag");
+    if (!rc) rc = check(p, cudaEventRecord(p->ev1, p->stream), "event");
+    if (rc) return rc;
+    p->in_flight = true;
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_wait(femstep_pool* p, double* gpu_ms) {
+    if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
+    return wait_chunk(p, gpu_ms);
+}
+
+int femstep_pool_run(femstep_pool* p, int steps, int mode, double* gpu_ms) {
+    const int rc = femstep_pool_run_async(p, steps, mode);
+    if (rc) return rc;
+    return wait_chunk(p, gpu_ms);
+}
+
+int femstep_pool_finished(femstep_pool* p, int* ids, int capacity, int* count) {
+    if (!p || !count || (capacity > 0 && !ids)) return fail(p, FEMSTEP_EINVAL, "null argument");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
+    int n = 0;
+    for (int id = 0; id < p->max_meshes; ++id) {
+        const HostMesh& h = p->meshes[id];
+        if (!h.used) continue;
+        // the mirror is as of the last chunk: a record of an earlier tenant of this id,
+        // or none yet, carries another serial
+        const PoolMesh& r = p->h_meshes[id];
+        if (r.serial == h.serial && r.step >= r.target) {
+            if (n < capacity) ids[n] = id;
+            ++n;
+        }
+    }
+    *count = n;
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_status(femstep_pool* p, int id, long long* steps_done, long long* steps_target) {
+    if (!valid_id(p, id)) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    std::vector<PoolMesh> r(1);
+    int rc = check(p, cudaMemcpyAsync(r.data(), p->d.meshes + id, sizeof(PoolMesh), cudaMemcpyDeviceToHost,
+                                      p->stream), "status");
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "status");
+    if (!rc) {
+        if (steps_done) *steps_done = r[0].step;
+        if (steps_target) *steps_target = r[0].target;
+    }
+    return rc;
+}
+
+int femstep_pool_readback(femstep_pool* p, int id, double* position, double* velocity) {
+    if (!valid_id(p, id)) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    const HostMesh& h = p->meshes[id];
+    std::vector<float> u(h.N * 3), v(h.N * 3);
+    int rc = check(p, cudaMemcpyAsync(u.data(), p->d.disp + h.n0 * 3, u.size() * 4, cudaMemcpyDeviceToHost, p->stream),
+                   "readback");
+    if (!rc)
+        rc = check(p, cudaMemcpyAsync(v.data(), p->d.velocity + h.n0 * 3, v.size() * 4, cudaMemcpyDeviceToHost,
+                                      p->stream), "readback");
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "readback");
+    if (rc) return rc;
+    if (position)
+        for (size_t i = 0; i < u.size(); ++i) position[i] = (double)h.rest[i] + (double)u[i];
+    if (velocity)
+        for (size_t i = 0; i < v.size(); ++i) velocity[i] = v[i];
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_plastic(femstep_pool* p, int id, double* plastic) {
+    if (!valid_id(p, id) || !plastic) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    const HostMesh& h = p->meshes[id];
+    std::vector<float> buf((size_t)h.T * 7);
+    int rc = FEMSTEP_OK;
+    for (int k = 0; k < 7 && !rc; ++k)
+        rc = check(p, cudaMemcpyAsync(buf.data() + (size_t)k * h.T, p->d.plastic + (size_t)k * p->tet_cap + h.t0,
+                                      h.T * 4, cudaMemcpyDeviceToHost, p->stream), "readback");
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "readback");
+    if (rc) return rc;
+    for (long long t = 0; t < h.T; ++t)
+        for (int k = 0; k < 7; ++k) plastic[t * 7 + k] = buf[(size_t)k * h.T + t];
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_energy(femstep_pool* p, int id, double out[4]) {
+    if (!valid_id(p, id) || !out) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    const HostMesh& h = p->meshes[id];
+    // accumulated terms: every slot the mesh holds (a slot no tiling touched is 0);
+    // instantaneous terms: the slots of the current tiling
+    const long long et = (h.T + p->tile - 1) / p->tile, nt = (h.N + p->tile - 1) / p->tile;
+    fs::launch_reduce_sum(p->d.n_work + h.n_part, h.n_tiles, p->d_out + 0, p->stream);
+    fs::launch_reduce_sum(p->d.e_diss + h.e_part, h.e_tiles, p->d_out + 1, p->stream);
+    fs::launch_reduce_sum(p->d.e_strain + h.e_part, et, p->d_out + 2, p->stream);
+    fs::launch_reduce_sum(p->d.n_kin + h.n_part, nt, p->d_out + 3, p->stream);
+    std::vector<double> tmp(4);
+    int rc = check(p, cudaGetLastError(), "reduce");
+    if (!rc) rc = check(p, cudaMemcpyAsync(tmp.data(), p->d_out, 32, cudaMemcpyDeviceToHost, p->stream), "readback");
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "reduce");
+    if (!rc) std::memcpy(out, tmp.data(), 32);
+    return rc;
+}
+
+int femstep_pool_dt(femstep_pool* p, int id, double* dt) {
+    if (!valid_id(p, id) || !dt) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    std::vector<PoolMesh> r(1);
+    int rc = check(p, cudaMemcpyAsync(r.data(), p->d.meshes + id, sizeof(PoolMesh), cudaMemcpyDeviceToHost, p->stream),
+                   "dt");
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "dt");
+    if (!rc) *dt = r[0].dt64;
+    return rc;
+}
+
+int femstep_pool_autotune(femstep_pool* p, int steps, int* tile_out, int* mode_out, double* ms_out) {
+    if (!p || steps <= 0) return fail(p, FEMSTEP_EINVAL, "bad argument");
+    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
+    Snapshot snap;
+    int rc = snapshot(p, snap, false);
+    if (rc) return rc;
+    const int tiles[3] = {128, 256, 512};
+    const int modes[2] = {FEMSTEP_POOL_GRAPH, FEMSTEP_POOL_PERSISTENT};
+    const int tile0 = p->tile, mode0 = p->mode;
+    double best = INFINITY;
+    int best_tile = tile0, best_mode = mode0;
+    for (int ti = 0; ti < 3 && !rc; ++ti)
+        for (int mi = 0; mi < 2 && !rc; ++mi) {
+            p->tile = tiles[ti];
+            p->dirty = true;
+            double ms = 0.0;
+            rc = femstep_pool_run(p, steps, modes[mi], &ms);  // warm (graph build, caches)
+            if (!rc) rc = snapshot(p, snap, true);
+            if (!rc) rc = femstep_pool_run(p, steps, modes[mi], &ms);
+            if (!rc) rc = snapshot(p, snap, true);
+            if (!rc && ms < best) {
+                best = ms;
+                best_tile = tiles[ti];
+                best_mode = modes[mi];
+            }
+        }
+    cudaFree(snap.buf);
+    p->tile = best_tile;
+    p->mode = best_mode;
+    p->dirty = true;
+    if (rc) return rc;
+    // the instantaneous partials of the other tilings are stale: zero them
+    cudaMemsetAsync(p->d.e_strain, 0, (size_t)p->part_cap * 8, p->stream);
+    cudaMemsetAsync(p->d.n_kin, 0, (size_t)p->part_cap * 8, p->stream);
+    // the mirror of the mesh table as the restored state has it
+    rc = refresh_mirror(p);
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "autotune");
+    if (tile_out) *tile_out = best_tile;
+    if (mode_out) *mode_out = best_mode;
+    if (ms_out) *ms_out = best / steps;
+    return rc;
+}
+
+int femstep_pool_set_schedule(femstep_pool* p, int tile, int mode) {
+    if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
+    if (tile != 128 && tile != 256 && tile != 512) return fail(p, FEMSTEP_EINVAL, "tile must be 128, 256 or 512");
+    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT) return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (tile != p->tile) {
+        // the instantaneous partials of the old tiling are stale
+        cudaMemsetAsync(p->d.e_strain, 0, (size_t)p->part_cap * 8, p->stream);
+        cudaMemsetAsync(p->d.n_kin, 0, (size_t)p->part_cap * 8, p->stream);
+        p->dirty = true;
+    }
+    p->tile = tile;
+    p->mode = mode;
+    return check(p, cudaGetLastError(), "schedule");
+}
+
+int femstep_pool_profile(femstep_pool* p, int steps, double out[2]) {
+    if (!p || !out || steps <= 0) return fail(p, FEMSTEP_EINVAL, "bad argument");
+    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
+    int rc = rebuild(p);
+    if (rc) return rc;
+    cudaEvent_t ev[3];
+    for (auto& e : ev) cudaEventCreate(&e);
+    double te = 0.0, tn = 0.0;
+    for (int s = 0; s < steps && !rc; ++s) {
+        cudaEventRecord(ev[0], p->stream);
+        fs::launch_pool_element_pass(p->d, p->tile, s, p->stream);
+        cudaEventRecord(ev[1], p->stream);
+        fs::launch_pool_node_pass(p->d, p->tile, s, p->stream);
+        cudaEventRecord(ev[2], p->stream);
+        rc = check(p, cudaEventSynchronize(ev[2]), "profile");
+        float a = 0.0f, b = 0.0f;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        te += a;
+        tn += b;
+    }
+    if (!rc) {
+        fs::launch_pool_advance(p->d, steps, p->stream);
+        rc = refresh_mirror(p);
+        if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "profile");
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    out[0] = te / steps;
+    out[1] = tn / steps;
+    return rc;
+}
+
+int femstep_pool_info(femstep_pool* p, long long out[8]) {
+    if (!p || !out) return fail(p, FEMSTEP_EINVAL, "null argument");
+    long long t = 0, n = 0, k = 0;
+    for (const HostMesh& m : p->meshes)
+        if (m.used) {
+            t += m.T;
+            n += m.N;
+            ++k;
+        }
+    out[0] = t;
+    out[1] = n;
+    out[2] = k;
+    out[3] = p->tile;
+    out[4] = p->mode;
+    out[5] = p->launches;
+    out[6] = (long long)p->arena.bytes();
+    out[7] = (long long)p->staging.count();
+    return FEMSTEP_OK;
+}
+
+const char* femstep_pool_error(const femstep_pool* p) { return p ? p->error.c_str() : fs::last_error(); }
+
+void femstep_pool_destroy(femstep_pool* p) {
+    if (!p) return;
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    drop_graph(p);
+    p->arena.release();
+    p->staging.release();
+    if (p->h_meshes) cudaFreeHost(p->h_meshes);
+    if (p->h_error) cudaFreeHost(p->h_error);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    delete p;
+}
+
+}  // extern "C"

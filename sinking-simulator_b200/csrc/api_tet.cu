@@ -49,43 +49,9 @@ int fail(femstep_tet* s, int code, const std::string& what) {
     return code;
 }
 
-// computeRestState (engine/sim/fem.cpp:119-158) in double from the float positions:
-// Dm^-1 (column-major, singular guard), |det|/6, lumped rho V / 4 per corner.
 void rest_state64(const femstep_tet_mesh& m, std::vector<double>& inv, std::vector<double>& vol,
                   std::vector<double>& mass) {
-    const size_t T = m.tets;
-    inv.assign(T * 9, 0.0);
-    vol.assign(T, 0.0);
-    mass.assign(m.nodes, 0.0);
-    for (size_t t = 0; t < T; ++t) {
-        const uint32_t* idx = &m.index[t * 4];
-        double a[9];  // column-major
-        for (int c = 0; c < 3; ++c)
-            for (int r = 0; r < 3; ++r)
-                a[c * 3 + r] = (double)m.position[(size_t)idx[c + 1] * 3 + r] - (double)m.position[(size_t)idx[0] * 3 + r];
-#define A(r, c) a[(c) * 3 + (r)]
-        const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
-                           A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
-                           A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
-        const double volume = det / 6.0;
-        vol[t] = std::fabs(volume);
-        const double id = std::fabs(det) > 1e-300 ? 1.0 / det : 0.0;
-        double* r = &inv[t * 9];
-#define R(rr, cc) r[(cc) * 3 + (rr)]
-        R(0, 0) = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) * id;
-        R(0, 1) = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * id;
-        R(0, 2) = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * id;
-        R(1, 0) = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) * id;
-        R(1, 1) = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * id;
-        R(1, 2) = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * id;
-        R(2, 0) = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) * id;
-        R(2, 1) = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * id;
-        R(2, 2) = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * id;
-#undef R
-#undef A
-        const double quarter = m.density * vol[t] * 0.25;
-        for (int c = 0; c < 4; ++c) mass[idx[c]] += quarter;
-    }
+    fs::tet_rest_state64(m.nodes, m.tets, m.position, m.index, m.density, inv, vol, mass);
 }
 
 template <typename T>

@@ -59,6 +59,12 @@ private:
     cudaError_t status_ = cudaSuccess;
 };
 
+// computeRestState (engine/sim/fem.cpp:119-158) in double from float positions:
+// Dm^-1 (column-major, singular guard), |det|/6, lumped rho V / 4 per corner.  The
+// FP64 tet step's rest state, bit-identical to the FP64 oracle's.
+void tet_rest_state64(size_t nodes, size_t tets, const float* position, const uint32_t* index, double density,
+                      std::vector<double>& inv, std::vector<double>& vol, std::vector<double>& mass);
+
 // Node -> incident corner CSR by counting sort, the construction of
 // engine/sim/fem.cpp:147-157 and engine/sim/zone.cpp:739-754.
 inline void build_csr(size_t nodes, size_t elements, int corners, const uint32_t* index,

@@ -1,0 +1,190 @@
+// pool.cu -- kernels of the multi-mesh pool (pool.hpp): the batched and served step.
+//
+// Every block works on one tile: a run of one mesh's tets (or nodes).  The mesh's
+// parameters come from its record; a mesh whose step count is reached is frozen
+// (its tiles do nothing) until the host retires it.  The energy partial of a tile goes
+// to the slot its mesh was given at admission, so nothing in a mesh's result depends
+// on what else is in the pool.
+#include "common.cuh"
+#include "pool.hpp"
+#include "tet.hpp"
+
+namespace fs {
+namespace {
+
+__device__ __forceinline__ J2f mesh_material(const PoolMesh& m) {
+    return J2f{m.mu, m.kappa, m.yield, m.hardening, m.dmu, m.dkappa};
+}
+
+__device__ __forceinline__ TetElementRefs element_refs(const PoolDevice& d) {
+    return TetElementRefs{d.index, d.slot, d.rest_inv, d.rest_vol, d.plastic, d.plastic_c, d.disp, d.slots,
+                          d.tet_cap};
+}
+
+__device__ __forceinline__ TetNodeRefs node_refs(const PoolDevice& d) {
+    return TetNodeRefs{d.offset, d.slots, d.fixed, d.mass, d.inv_mass, d.ext, d.velocity, d.disp, d.disp_c};
+}
+
+// One element tile at sub-step `sub` of the chunk (all threads of the block call it).
+// CG: data other blocks wrote earlier in the same launch is read through L2.
+template <bool CG>
+__device__ __forceinline__ void element_tile(const PoolDevice& d, int tile, int sub, double* scratch) {
+    const PoolTile tl = d.etiles[tile];
+    const PoolMesh& m = d.meshes[tl.mesh];
+    const bool live = m.step + sub < m.target;
+    double diss = 0.0, energy = 0.0;
+    const long long t = tl.begin + threadIdx.x;
+    if (live && t < tl.end) tet_element_f32<true, CG>(element_refs(d), t, mesh_material(m), diss, energy);
+    const double bd = block_sum(diss, scratch);
+    const double be = block_sum(energy, scratch);
+    if (live && threadIdx.x == 0) {
+        d.e_diss[tl.part] += bd;
+        d.e_strain[tl.part] = be;
+    }
+}
+
+template <bool CG>
+__device__ __forceinline__ void node_tile(const PoolDevice& d, int tile, int sub, double* scratch) {
+    const PoolTile tl = d.ntiles[tile];
+    const PoolMesh& m = d.meshes[tl.mesh];
+    const long long step = m.step + sub;
+    const bool live = step < m.target;
+    double work = 0.0, kin = 0.0, gwork = 0.0;
+    const long long n = tl.begin + threadIdx.x;
+    if (live && n < tl.end) {
+        const float lf = (float)ramp_factor(step, m.ramp);
+        tet_node_f32<true, CG>(node_refs(d), n, lf, m.dt, m.gravity, m.damping, work, kin, gwork);
+    }
+    const double bw = block_sum(work + gwork, scratch);
+    const double bk = block_sum(kin, scratch);
+    if (live && threadIdx.x == 0) {
+        d.n_work[tl.part] += bw;
+        d.n_kin[tl.part] = bk;
+    }
+}
+
+__global__ void __launch_bounds__(512) pool_elements(PoolDevice d, int sub) {
+    __shared__ double scratch[32];
+    element_tile<false>(d, blockIdx.x, sub, scratch);
+}
+
+__global__ void __launch_bounds__(512) pool_nodes(PoolDevice d, int sub) {
+    __shared__ double scratch[32];
+    node_tile<false>(d, blockIdx.x, sub, scratch);
+}
+
+// Every active mesh advances by the steps it took in the chunk.
+__global__ void pool_advance(PoolDevice d, int steps) {
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < d.n_active; i += blockDim.x * gridDim.x) {
+        PoolMesh* m = d.meshes + d.active[i];
+        if (m->step < m->target) {
+            const long long next = m->step + steps;
+            m->step = next < m->target ? next : m->target;
+        }
+    }
+}
+
+// Grid-wide barrier for the persistent launch, bounded: a block that waits longer
+// than ~0.5 s sets the error flag and goes on, and every later barrier then gives up
+// at once, so the launch always ends.  The launch is cooperative, so all blocks are
+// co-resident and the wait is never expected to run out.
+__device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int nblocks, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = bar + 1;
+        const unsigned int g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*gen == g) {
+                if (*(volatile int*)err != 0 || ++spins > (1ull << 24)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int*)err == 0;
+}
+
+__global__ void __launch_bounds__(512) pool_persistent(PoolDevice d, int steps) {
+    __shared__ double scratch[32];
+    for (int s = 0; s < steps; ++s) {
+        for (int tile = blockIdx.x; tile < d.n_etiles; tile += gridDim.x) element_tile<true>(d, tile, s, scratch);
+        if (!grid_sync(d.barrier, gridDim.x, d.error)) return;
+        for (int tile = blockIdx.x; tile < d.n_ntiles; tile += gridDim.x) node_tile<true>(d, tile, s, scratch);
+        if (!grid_sync(d.barrier, gridDim.x, d.error)) return;
+    }
+}
+
+__global__ void pool_set_dt(PoolMesh* meshes, int id, const double* w2, double safety) {
+    const double v = w2[0];
+    const double dt = v > 0.0 ? safety * 2.0 / sqrt(v) : 0.0;
+    meshes[id].dt64 = dt;
+    meshes[id].dt = (float)dt;
+}
+
+}  // namespace
+
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream) {
+    if (d.n_etiles == 0 || steps <= 0) return;
+    for (int s = 0; s < steps; ++s) {
+        pool_elements<<<d.n_etiles, tile, 0, stream>>>(d, s);
+        pool_nodes<<<d.n_ntiles, tile, 0, stream>>>(d, s);
+    }
+    pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
+}
+
+void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream) {
+    if (d.n_etiles) pool_elements<<<d.n_etiles, tile, 0, stream>>>(d, sub);
+}
+
+void launch_pool_node_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream) {
+    if (d.n_ntiles) pool_nodes<<<d.n_ntiles, tile, 0, stream>>>(d, sub);
+}
+
+void launch_pool_advance(const PoolDevice& d, int steps, cudaStream_t stream) {
+    if (d.n_active) pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
+}
+
+int pool_persistent_max_blocks(int tile) {
+    int per_sm = 0, sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pool_persistent, tile, 0);
+    return per_sm * sms;
+}
+
+cudaError_t launch_pool_persistent(const PoolDevice& d, int tile, int steps, int blocks, cudaStream_t stream) {
+    if (d.n_etiles == 0 || steps <= 0) return cudaSuccess;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(tile);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, pool_persistent, d, steps);
+    if (e != cudaSuccess) return e;
+    pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
+    return cudaGetLastError();
+}
+
+void launch_pool_dt(const PoolDevice& d, int id, long long t0, long long T, double E, double nu, double rho,
+                    double safety, double* block_max, double* w2, cudaStream_t stream) {
+    const int blocks = blocks_for(T, kBlock);
+    launch_tet_omega2_f32(T, d.rest_inv + t0, d.tet_cap, E, nu, rho, block_max, blocks, stream);
+    launch_reduce_max(block_max, blocks, w2, stream);
+    pool_set_dt<<<1, 1, 0, stream>>>(d.meshes, id, w2, safety);
+}
+
+}  // namespace fs

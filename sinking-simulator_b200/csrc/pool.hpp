@@ -1,0 +1,100 @@
+// pool.hpp -- a resident pool of many independent J2 tet meshes, stepped together.
+//
+// The batched and the served workloads (many meshes of uneven size, each with its own
+// material, load, time step and step count) share one device pool:
+//
+//   * tets and nodes of every admitted mesh live in contiguous ranges of pool-wide
+//     structure-of-arrays (the same per-tet / per-node layout as the single mesh,
+//     tet.hpp), allocated first-fit against the pool's capacity;
+//   * the work is a list of tiles, each a run of up to `tile` tets (or nodes) of ONE
+//     mesh, so a block never mixes meshes and each mesh's arithmetic -- including
+//     the fixed-order energy partial of each of its own tiles -- is the same whatever
+//     else is in the pool;
+//   * a chunk of `steps` steps is an element pass and a node pass per step, then one
+//     advance of every mesh's step counter by the steps it took.  During a chunk the
+//     counters are read only: sub-step s of a mesh at step k is step k + s, live while
+//     k + s < target.  The passes run either as two launches per step (replayed from
+//     a captured CUDA graph) or inside one persistent launch with two bounded grid
+//     barriers per step.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tet_f32.cuh"
+
+namespace fs {
+
+struct PoolMesh {           // device-side per-mesh record
+    float mu, kappa, yield, hardening;
+    double dmu, dkappa;
+    float dt, gravity, damping;
+    int ramp;               // load ramp in steps
+    long long step;         // steps taken
+    long long target;       // steps requested; the mesh is frozen once step == target
+    long long e_part, n_part;  // first energy-partial slot of its element / node tiles
+    double dt64;            // the time step before rounding to float
+    long long serial;       // admission number: tells a record from an earlier tenant's
+};
+
+struct PoolTile {           // a run of one mesh's tets or nodes
+    int mesh;
+    int part;               // energy-partial slot
+    long long begin, end;   // pool indices
+};
+
+struct PoolDevice {
+    long long tet_cap = 0, node_cap = 0;
+    // tets (SoA, stride tet_cap)
+    uint4* index = nullptr;
+    uint4* slot = nullptr;
+    float* rest_inv = nullptr;
+    float* rest_vol = nullptr;
+    float* plastic = nullptr;
+    float* plastic_c = nullptr;
+    float* slots = nullptr;        // 12 per tet capacity
+    // nodes
+    uint32_t* offset = nullptr;    // [node_cap]: CSR begin of each node; every mesh holds
+                                   // one spare node slot after its last node for the end
+    float* disp = nullptr;
+    float* disp_c = nullptr;
+    float* velocity = nullptr;
+    float* mass = nullptr;
+    float* inv_mass = nullptr;
+    uint8_t* fixed = nullptr;
+    float* ext = nullptr;
+    // meshes and work
+    PoolMesh* meshes = nullptr;
+    const PoolTile* etiles = nullptr;
+    const PoolTile* ntiles = nullptr;
+    int n_etiles = 0, n_ntiles = 0;
+    const int* active = nullptr;   // ids of the meshes in the work lists
+    int n_active = 0;
+    // FP64 energy partials, per tile slot (fixed per mesh for its lifetime):
+    // dissipation (+=), strain energy (=), external work incl. gravity (+=), kinetic (=)
+    double* e_diss = nullptr;
+    double* e_strain = nullptr;
+    double* n_work = nullptr;
+    double* n_kin = nullptr;
+    unsigned int* barrier = nullptr;  // [0] arrivals, [1] generation
+    int* error = nullptr;             // set by a grid barrier that gave up waiting
+};
+
+// Two launches per step (element, node), `steps` times, then the advance, on `stream`.
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream);
+// The passes one at a time (per-kernel timing): element or node pass of sub-step
+// `sub`, and the advance by `steps`.
+void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream);
+void launch_pool_node_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream);
+void launch_pool_advance(const PoolDevice& d, int steps, cudaStream_t stream);
+// One persistent cooperative launch for `steps` steps on `blocks` co-resident blocks,
+// then the advance.
+cudaError_t launch_pool_persistent(const PoolDevice& d, int tile, int steps, int blocks, cudaStream_t stream);
+int pool_persistent_max_blocks(int tile);
+// meshes[id].dt = safety * 2 / sqrt(max omega^2) of the mesh's tets [t0, t0 + T),
+// from the pool's FP32 Dm^-1; 0 when the bound is not positive.  `block_max` holds
+// ceil(T / 256) doubles and `w2` one double of scratch.
+void launch_pool_dt(const PoolDevice& d, int id, long long t0, long long T, double E, double nu, double rho,
+                    double safety, double* block_max, double* w2, cudaStream_t stream);
+
+}  // namespace fs

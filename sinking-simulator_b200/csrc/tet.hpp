@@ -87,6 +87,10 @@ void launch_f32_step(const TetDevice<float>& d, const TetParams& p, bool compens
 // FP64 element eigenvalue bound: omega^2 per tet, reduced to the maximum on device.
 void launch_tet_omega2(long long tets, const double* rest_inv, double E, double nu, double rho,
                        double* per_block_max, int blocks, cudaStream_t stream);
+// The same bound from an FP32 Dm^-1 (SoA with stride `stride`, `rest_inv` pointing at
+// the first tet), promoted to double: the matrix the FP32 element kernels use.
+void launch_tet_omega2_f32(long long tets, const float* rest_inv, long long stride, double E, double nu, double rho,
+                           double* per_block_max, int blocks, cudaStream_t stream);
 // Fixed-order FP64 sum / max of `n` doubles into out[0] (one block).
 void launch_reduce_sum(const double* in, long long n, double* out, cudaStream_t stream);
 void launch_reduce_max(const double* in, long long n, double* out, cudaStream_t stream);

@@ -373,8 +373,11 @@ __global__ void __launch_bounds__(kBlock) f64_nodes(TetDevice<double> d, TetPara
 // (4/rho) lambda_max(B^T C B) by power iteration, as solid_shell.cpp:1088-1133 does
 // for the hex (Rayleigh quotient, at most 400 iterations, relative 1e-10, the same
 // start vector).  max over elements bounds the assembled problem.
-__global__ void __launch_bounds__(kBlock) tet_omega2(long long tets, const double* rest_inv, double lambda,
-                                                     double mu, double rho, double* block_max) {
+// Dm^-1 may be the FP64 array (single-mesh J2 step) or a pool's FP32 array, read
+// from `first` with SoA stride `stride` and promoted to double.
+template <typename In>
+__global__ void __launch_bounds__(kBlock) tet_omega2(long long tets, const In* rest_inv, long long stride,
+                                                     double lambda, double mu, double rho, double* block_max) {
     __shared__ double smax[kBlock];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double w2 = 0.0;
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(kBlock) tet_omega2(long long tets, const doubl
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) g[c + 1][a] = rest_inv[(size_t)(a * 3 + c) * tets + t];
+            for (int a = 0; a < 3; ++a) g[c + 1][a] = (double)rest_inv[(size_t)(a * 3 + c) * stride + t];
 #pragma unroll
         for (int a = 0; a < 3; ++a) g[0][a] = -(g[1][a] + g[2][a] + g[3][a]);
         double v[12];
@@ -489,7 +492,14 @@ void launch_tet_omega2(long long tets, const double* rest_inv, double E, double 
                        double* per_block_max, int blocks, cudaStream_t stream) {
     const double lambda = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     const double mu = E / (2.0 * (1.0 + nu));
-    tet_omega2<<<blocks, kBlock, 0, stream>>>(tets, rest_inv, lambda, mu, rho, per_block_max);
+    tet_omega2<double><<<blocks, kBlock, 0, stream>>>(tets, rest_inv, tets, lambda, mu, rho, per_block_max);
+}
+
+void launch_tet_omega2_f32(long long tets, const float* rest_inv, long long stride, double E, double nu, double rho,
+                           double* per_block_max, int blocks, cudaStream_t stream) {
+    const double lambda = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double mu = E / (2.0 * (1.0 + nu));
+    tet_omega2<float><<<blocks, kBlock, 0, stream>>>(tets, rest_inv, stride, lambda, mu, rho, per_block_max);
 }
 
 void launch_reduce_sum(const double* in, long long n, double* out, cudaStream_t stream) {

@@ -1,38 +1,17 @@
-// tet_fast.cu -- the FP32 J2 tet step, plain and Kahan-compensated.
+// tet_fast.cu -- the single-mesh FP32 J2 tet step, plain and Kahan-compensated.
 //
-// Same element and node update as the FP64 step in tet_exact.cu (fem.cpp's
-// co-rotational tet, plasticity::update's radial return, fem.cpp's node loop with a
-// ramped external load), re-formulated so that FP32 keeps the digits that matter:
-//
-//   * nodes carry the displacement u = x - X (rest X fixed), not the position, so a
-//     step's increment v dt ~ 1e-7 m is added to a number of size |u| ~ 1e-3 m rather
-//     than |x| ~ 1 m.  The compensated mode adds it with Kahan summation;
-//   * the element works on the displacement gradient H = Du Dm^-1 and the rotation's
-//     deviation from identity Q = R - I, never on F = I + H and R themselves, so the
-//     strain R^T F - I = H + Q^T + Q^T H is formed from small terms with no
-//     cancellation.  The Higham iteration R <- (R + R^-T)/2 is carried in Q:
-//     Q <- (Q - (M Q)^T)/2 with M = (I + Q)^-1 (fem.cpp:62-69, four iterations);
-//   * the plastic strain is accumulated with Kahan compensation in the compensated
-//     mode.
-//
-// FP64 appears only in the per-block energy partials (dissipation, strain energy,
-// external work, kinetic), which the host reduces on the device in fixed order.
+// The element and node updates are in tet_f32.cuh (shared with the batched pool);
+// this file maps them one thread per tet / per node and keeps the energy account as
+// FP64 per-block partials, which the host reduces on the device in fixed order.
 #include "common.cuh"
 #include "tet.hpp"
+#include "tet_f32.cuh"
 
 namespace fs {
 namespace {
 
-__device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
-    const float y = x - comp;
-    const float t = sum + y;
-    comp = (t - sum) - y;
-    sum = t;
-}
-
 template <bool KAHAN>
-__global__ void __launch_bounds__(kBlock) f32_forces(TetDevice<float> d, float mu, float kappa, float yield,
-                                                     float hardening, float dmu, float dkappa) {
+__global__ void __launch_bounds__(kBlock) f32_forces(TetDevice<float> d, J2f m) {
     __shared__ double scratch[32];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -42,153 +21,9 @@ __global__ void __launch_bounds__(kBlock) f32_forces(TetDevice<float> d, float m
     }
     double diss = 0.0, energy = 0.0;
     if (t < d.tets) {
-        const uint4 idx = d.index[t];
-        const unsigned nid[4] = {idx.x, idx.y, idx.z, idx.w};
-        const float* u = d.disp;
-        float u0[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) u0[a] = u[(size_t)nid[0] * 3 + a];
-        M3<float> du, dm_inv;
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) du(a, c) = u[(size_t)nid[c + 1] * 3 + a] - u0[a];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) dm_inv.m[k] = d.rest_inv[(size_t)k * d.tets + t];
-        const M3<float> h = mul(du, dm_inv);  // displacement gradient
-        // rotation deviation Q = R - I by the Higham iteration on F = I + H
-        M3<float> q = h;
-#pragma unroll 1
-        for (int it = 0; it < 4; ++it) {
-            M3<float> ipq = q;
-            ipq(0, 0) += 1.0f;
-            ipq(1, 1) += 1.0f;
-            ipq(2, 2) += 1.0f;
-            const M3<float> mq = mul(inverse(ipq, 1e-30f), q);
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) ipq(i, j) = 0.5f * (q(i, j) - mq(j, i));
-            q = ipq;
-        }
-        const M3<float> qt = transpose(q);
-        const M3<float> qth = mul(qt, h);
-        float strain[6];
-        strain[0] = h(0, 0) + qt(0, 0) + qth(0, 0);
-        strain[1] = h(1, 1) + qt(1, 1) + qth(1, 1);
-        strain[2] = h(2, 2) + qt(2, 2) + qth(2, 2);
-        strain[3] = (h(0, 1) + qt(0, 1) + qth(0, 1)) + (h(1, 0) + qt(1, 0) + qth(1, 0));
-        strain[4] = (h(1, 2) + qt(1, 2) + qth(1, 2)) + (h(2, 1) + qt(2, 1) + qth(2, 1));
-        strain[5] = (h(2, 0) + qt(2, 0) + qth(2, 0)) + (h(0, 2) + qt(0, 2) + qth(0, 2));
-
-        // radial return, linear isotropic hardening (plasticity.cpp:333-456); for a
-        // linear curve the consistency condition is affine in dgamma and its root is
-        // the closed form below, which the CPU's Newton reaches in one step.
-        float ps[7], pc[7];
-#pragma unroll
-        for (int i = 0; i < 7; ++i) ps[i] = d.plastic[(size_t)i * d.tets + t];
-        if (KAHAN) {
-#pragma unroll
-            for (int i = 0; i < 7; ++i) pc[i] = d.plastic_c[(size_t)i * d.tets + t];
-        }
-        float el[6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) el[i] = strain[i] - ps[i];
-        const float vol_strain = el[0] + el[1] + el[2];
-        const float pressure = kappa * vol_strain;
-        float trial[6];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            trial[i] = 2.0f * mu * (el[i] - vol_strain * (1.0f / 3.0f));
-            trial[3 + i] = mu * el[3 + i];
-        }
-        const float norm = sqrtf(trial[0] * trial[0] + trial[1] * trial[1] + trial[2] * trial[2] +
-                                 2.0f * (trial[3] * trial[3] + trial[4] * trial[4] + trial[5] * trial[5]));
-        const float root23 = 0.81649658092772603f;
-        const float radius = root23 * (yield + hardening * fmaxf(ps[6], 0.0f));
-        const float excess = norm - radius;
-        float sv[6];
-        if (excess > 0.0f) {
-            const float gamma = excess / (2.0f * mu + (2.0f / 3.0f) * hardening);
-            const float k = 2.0f * mu * gamma / norm;
-            float dp[6];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const float n = trial[i] / norm;
-                dp[i] = gamma * n;
-                sv[i] = pressure + trial[i] - k * trial[i];
-            }
-#pragma unroll
-            for (int i = 3; i < 6; ++i) {
-                const float n = trial[i] / norm;
-                dp[i] = 2.0f * gamma * n;
-                sv[i] = trial[i] - k * trial[i];
-            }
-            float dsum = 0.0f;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) dsum += sv[i] * dp[i];
-            diss = (double)dsum;
-            const float deq = root23 * gamma;
-            if (KAHAN) {
-#pragma unroll
-                for (int i = 0; i < 6; ++i) kahan_add(ps[i], pc[i], dp[i]);
-                kahan_add(ps[6], pc[6], deq);
-#pragma unroll
-                for (int i = 0; i < 7; ++i) d.plastic_c[(size_t)i * d.tets + t] = pc[i];
-            } else {
-#pragma unroll
-                for (int i = 0; i < 6; ++i) ps[i] += dp[i];
-                ps[6] += deq;
-            }
-#pragma unroll
-            for (int i = 0; i < 7; ++i) d.plastic[(size_t)i * d.tets + t] = ps[i];
-        } else {
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                sv[i] = pressure + trial[i];
-                sv[3 + i] = trial[3 + i];
-            }
-        }
-        const double vol = (double)d.rest_vol[t];
-        diss *= vol;
-        {
-            const double s0 = sv[0], s1 = sv[1], s2 = sv[2], s3 = sv[3], s4 = sv[4], s5 = sv[5];
-            const double pr = (s0 + s1 + s2) / 3.0;
-            double density = 0.5 * s0 * ((s0 - pr) / (2.0 * dmu) + pr / (3.0 * dkappa)) +
-                             0.5 * s1 * ((s1 - pr) / (2.0 * dmu) + pr / (3.0 * dkappa)) +
-                             0.5 * s2 * ((s2 - pr) / (2.0 * dmu) + pr / (3.0 * dkappa));
-            density += 0.5 * (s3 * s3 + s4 * s4 + s5 * s5) / dmu;
-            energy = vol * density;
-        }
-        // P = R sigma = sigma + Q sigma; nodal forces f_c = -V (P Dm^-T) column c
-        M3<float> sig;
-        sig(0, 0) = sv[0];
-        sig(1, 1) = sv[1];
-        sig(2, 2) = sv[2];
-        sig(0, 1) = sig(1, 0) = sv[3];
-        sig(1, 2) = sig(2, 1) = sv[4];
-        sig(2, 0) = sig(0, 2) = sv[5];
-        const M3<float> qs = mul(q, sig);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) sig.m[k] += qs.m[k];
-        const M3<float> hf = mul(sig, transpose(dm_inv));
-        const float scale = -d.rest_vol[t];
-        const uint4 sl = d.slot[t];
-        const unsigned sid[4] = {sl.x, sl.y, sl.z, sl.w};
-        float f0[3] = {0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            float* out = d.slots + (size_t)sid[c + 1] * 3;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const float v = scale * hf(a, c);
-                out[a] = v;
-                f0[a] -= v;
-            }
-        }
-        float* out0 = d.slots + (size_t)sid[0] * 3;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) out0[a] = f0[a];
+        const TetElementRefs r{d.index, d.slot, d.rest_inv, d.rest_vol, d.plastic, d.plastic_c, d.disp, d.slots,
+                               d.tets};
+        tet_element_f32<KAHAN>(r, t, m, diss, energy);
     }
     const double bd = block_sum(diss, scratch);
     const double be = block_sum(energy, scratch);
@@ -205,50 +40,9 @@ __global__ void __launch_bounds__(kBlock) f32_nodes(TetDevice<float> d, float dt
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double work = 0.0, kin = 0.0, gwork = 0.0;
     if (n < d.nodes) {
-        float* vel = d.velocity + (size_t)n * 3;
-        if (d.fixed[n]) {
-            vel[0] = 0.0f;
-            vel[1] = 0.0f;
-            vel[2] = 0.0f;
-        } else {
-            const float lf = (float)ramp_factor(d.counter[1], ramp);
-            const float m = d.mass[n];
-            float force[3] = {0.0f, 0.0f, -gravity * m};
-            const uint32_t b = d.offset[n], e = d.offset[n + 1];
-            const float* sl = d.slots + (size_t)b * 3;
-#pragma unroll 4
-            for (uint32_t k = b; k < e; ++k, sl += 3) {
-                force[0] += sl[0];
-                force[1] += sl[1];
-                force[2] += sl[2];
-            }
-            float ext[3] = {0.0f, 0.0f, 0.0f};
-            if (d.ext) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) ext[k] = lf * d.ext[(size_t)n * 3 + k];
-            }
-            const float im = d.inv_mass[n];
-            float* u = d.disp + (size_t)n * 3;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float v = vel[k] + (force[k] + ext[k]) * im * dt;
-                v *= damping;
-                vel[k] = v;
-                const float du = v * dt;
-                if (KAHAN) {
-                    float c = d.disp_c[(size_t)n * 3 + k];
-                    float s = u[k];
-                    kahan_add(s, c, du);
-                    u[k] = s;
-                    d.disp_c[(size_t)n * 3 + k] = c;
-                } else {
-                    u[k] += du;
-                }
-                work += (double)ext[k] * (double)v * (double)dt;
-                kin += 0.5 * (double)m * (double)v * (double)v;
-            }
-            gwork = -(double)gravity * (double)m * (double)vel[2] * (double)dt;
-        }
+        const TetNodeRefs r{d.offset, d.slots, d.fixed, d.mass, d.inv_mass, d.ext, d.velocity, d.disp, d.disp_c};
+        const float lf = (float)ramp_factor(d.counter[1], ramp);
+        tet_node_f32<KAHAN>(r, n, lf, dt, gravity, damping, work, kin, gwork);
     }
     const double bw = block_sum(work, scratch);
     const double bk = block_sum(kin, scratch);
@@ -265,16 +59,13 @@ __global__ void __launch_bounds__(kBlock) f32_nodes(TetDevice<float> d, float dt
 void launch_f32_step(const TetDevice<float>& d, const TetParams& p, bool compensated, cudaStream_t stream,
                      int parts) {
     const int eb = blocks_for(d.tets, kBlock), nb = blocks_for(d.nodes, kBlock);
+    const J2f m{(float)p.mu, (float)p.bulk, (float)p.yield, (float)p.hardening, p.mu, p.bulk};
     if (compensated) {
-        if (parts & kElementPart)
-            f32_forces<true><<<eb, kBlock, 0, stream>>>(d, (float)p.mu, (float)p.bulk, (float)p.yield,
-                                                        (float)p.hardening, p.mu, p.bulk);
+        if (parts & kElementPart) f32_forces<true><<<eb, kBlock, 0, stream>>>(d, m);
         if (parts & kNodePart)
             f32_nodes<true><<<nb, kBlock, 0, stream>>>(d, (float)p.dt, (float)p.gravity, (float)p.damping, p.ramp);
     } else {
-        if (parts & kElementPart)
-            f32_forces<false><<<eb, kBlock, 0, stream>>>(d, (float)p.mu, (float)p.bulk, (float)p.yield,
-                                                         (float)p.hardening, p.mu, p.bulk);
+        if (parts & kElementPart) f32_forces<false><<<eb, kBlock, 0, stream>>>(d, m);
         if (parts & kNodePart)
             f32_nodes<false><<<nb, kBlock, 0, stream>>>(d, (float)p.dt, (float)p.gravity, (float)p.damping, p.ramp);
     }

@@ -494,3 +494,183 @@ def stiffened_panel(nx=2000, ny=1000, lx=20.0, ly=10.0, thickness=0.012, stiffen
     r2 = (p[:, 0] - lx / 2) ** 2 + (p[:, 1] - ly / 2) ** 2
     load = unit * (peak_pressure * np.exp(-r2 / (2 * radius ** 2)))[:, None]
     return rest, index, pinned, load.reshape(-1)
+
+
+# ---------------------------------------------------------------------------------
+# Pool of many tet meshes: the batched and the served step (no reference counterpart:
+# the reference steps one mesh at a time, fem.cpp:187).
+
+POOL_AUTO, POOL_GRAPH, POOL_PERSISTENT = 0, 1, 2
+
+
+class PoolMeshC(C.Structure):
+    _fields_ = [("nodes", C.c_size_t), ("tets", C.c_size_t), ("position", C.c_void_p), ("index", C.c_void_p),
+                ("fixed", C.c_void_p), ("external_force", C.c_void_p), ("density", C.c_double),
+                ("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double), ("yield_strength", C.c_double),
+                ("hardening_modulus", C.c_double), ("dt", C.c_double), ("gravity", C.c_double),
+                ("damping", C.c_double), ("ramp_steps", C.c_int)]
+
+
+_pl_create = _sig("femstep_pool_create", C.c_int, [C.c_size_t, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)])
+_pl_bpt = _sig("femstep_pool_bytes_per_tet", C.c_size_t, [])
+_pl_bpn = _sig("femstep_pool_bytes_per_node", C.c_size_t, [])
+_pl_admit = _sig("femstep_pool_admit", C.c_int, [C.c_void_p, C.POINTER(PoolMeshC), C.c_longlong, C.POINTER(C.c_int)])
+_pl_release = _sig("femstep_pool_release", C.c_int, [C.c_void_p, C.c_int])
+_pl_run_async = _sig("femstep_pool_run_async", C.c_int, [C.c_void_p, C.c_int, C.c_int])
+_pl_wait = _sig("femstep_pool_wait", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
+_pl_run = _sig("femstep_pool_run", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)])
+_pl_finished = _sig("femstep_pool_finished", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)])
+_pl_status = _sig("femstep_pool_status", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
+                                                     C.POINTER(C.c_longlong)])
+_pl_readback = _sig("femstep_pool_readback", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p])
+_pl_plastic = _sig("femstep_pool_plastic", C.c_int, [C.c_void_p, C.c_int, C.c_void_p])
+_pl_energy = _sig("femstep_pool_energy", C.c_int, [C.c_void_p, C.c_int, C.c_void_p])
+_pl_dt = _sig("femstep_pool_dt", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)])
+_pl_autotune = _sig("femstep_pool_autotune", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                         C.POINTER(C.c_double)])
+_pl_schedule = _sig("femstep_pool_set_schedule", C.c_int, [C.c_void_p, C.c_int, C.c_int])
+_pl_profile = _sig("femstep_pool_profile", C.c_int, [C.c_void_p, C.c_int, C.c_void_p])
+_pl_info = _sig("femstep_pool_info", C.c_int, [C.c_void_p, C.c_void_p])
+_pl_error = _sig("femstep_pool_error", C.c_char_p, [C.c_void_p])
+_pl_destroy = _sig("femstep_pool_destroy", None, [C.c_void_p])
+
+
+def pool_bytes(tets: int, nodes: int) -> int:
+    """Device bytes a pool of this capacity holds (without the small per-mesh tables)."""
+    return int(_pl_bpt()) * int(tets) + int(_pl_bpn()) * int(nodes)
+
+
+class PoolFull(FemStepError):
+    """The mesh does not fit in the pool's free space now (FEMSTEP_ENOMEM on admit)."""
+
+
+class TetPool:
+    """Many J2 tet meshes resident on one GPU, stepped together (FP32, Kahan-compensated).
+
+    Every mesh has its own material, load, time step and step count.  A mesh's
+    displacement, velocity and plastic state are those of ``TetSolver(mode="f32k")``
+    with the same dt, bit for bit, and do not depend on what else is in the pool.
+    """
+
+    def __init__(self, tet_capacity, node_capacity, max_meshes=1024, tile=256):
+        h = C.c_void_p()
+        rc = _pl_create(int(tet_capacity), int(node_capacity), int(max_meshes), int(tile), C.byref(h))
+        if rc:
+            _raise(rc, _last_error())
+        self._h = h
+        self.max_meshes = int(max_meshes)
+        self.sizes = {}  # id -> (nodes, tets)
+
+    @classmethod
+    def for_budget(cls, budget_bytes, nodes_per_tet=0.25, max_meshes=1024, tile=256):
+        """A pool whose arrays fill `budget_bytes` of device memory, with node capacity
+        `nodes_per_tet` per tet (Kuhn box meshes have fewer than 1/4)."""
+        per = int(_pl_bpt()) + nodes_per_tet * int(_pl_bpn())
+        tets = min(int(budget_bytes // per), 1_000_000_000)
+        return cls(tets, int(tets * nodes_per_tet) + max_meshes + 1, max_meshes=max_meshes, tile=tile)
+
+    def _check(self, rc):
+        if rc:
+            text = _pl_error(self._h)
+            if rc == ENOMEM:
+                raise PoolFull(rc, (text or b"").decode(errors="replace"))
+            _raise(rc, text)
+
+    def admit(self, position, index, steps, fixed=None, external_force=None, density=7850.0, youngs=210e9,
+              poisson=0.3, yield_strength=235e6, hardening=1e9, dt=0.0, gravity=0.0, damping=1.0,
+              ramp_steps=0) -> int:
+        """Admit a mesh for `steps` steps; raises PoolFull when it does not fit now."""
+        pos = np.ascontiguousarray(position, np.float32).reshape(-1)
+        idx = np.ascontiguousarray(index, np.uint32).reshape(-1)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, np.uint32).reshape(-1)
+        fe = None if external_force is None else np.ascontiguousarray(external_force, np.float64).reshape(-1)
+        m = PoolMeshC(pos.size // 3, idx.size // 4, _p(pos), _p(idx), _p(fx), _p(fe), density, youngs, poisson,
+                      yield_strength, hardening, dt, gravity, damping, int(ramp_steps))
+        out = C.c_int()
+        self._check(_pl_admit(self._h, C.byref(m), int(steps), C.byref(out)))
+        self.sizes[out.value] = (pos.size // 3, idx.size // 4)
+        return out.value
+
+    def release(self, mesh_id):
+        self._check(_pl_release(self._h, int(mesh_id)))
+        self.sizes.pop(mesh_id, None)
+
+    def run(self, steps, mode=POOL_AUTO) -> float:
+        ms = C.c_double()
+        self._check(_pl_run(self._h, int(steps), int(mode), C.byref(ms)))
+        return ms.value
+
+    def run_async(self, steps, mode=POOL_AUTO):
+        self._check(_pl_run_async(self._h, int(steps), int(mode)))
+
+    def wait(self) -> float:
+        ms = C.c_double()
+        self._check(_pl_wait(self._h, C.byref(ms)))
+        return ms.value
+
+    def finished(self):
+        ids = np.zeros(self.max_meshes, np.int32)
+        n = C.c_int()
+        self._check(_pl_finished(self._h, _p(ids), self.max_meshes, C.byref(n)))
+        return [int(i) for i in ids[: min(n.value, self.max_meshes)]]
+
+    def status(self, mesh_id):
+        done, target = C.c_longlong(), C.c_longlong()
+        self._check(_pl_status(self._h, int(mesh_id), C.byref(done), C.byref(target)))
+        return done.value, target.value
+
+    def readback(self, mesh_id):
+        n = self.sizes[mesh_id][0]
+        p = np.zeros(3 * n)
+        v = np.zeros(3 * n)
+        self._check(_pl_readback(self._h, int(mesh_id), _p(p), _p(v)))
+        return p, v
+
+    def plastic(self, mesh_id):
+        t = self.sizes[mesh_id][1]
+        out = np.zeros(7 * t)
+        self._check(_pl_plastic(self._h, int(mesh_id), _p(out)))
+        return out.reshape(t, 7)
+
+    def energy(self, mesh_id):
+        """[external work (load + gravity), dissipation, strain energy, kinetic] (FP64)."""
+        out = np.zeros(4)
+        self._check(_pl_energy(self._h, int(mesh_id), _p(out)))
+        return out
+
+    def dt(self, mesh_id) -> float:
+        v = C.c_double()
+        self._check(_pl_dt(self._h, int(mesh_id), C.byref(v)))
+        return v.value
+
+    def autotune(self, steps=32):
+        tile, mode, ms = C.c_int(), C.c_int(), C.c_double()
+        self._check(_pl_autotune(self._h, int(steps), C.byref(tile), C.byref(mode), C.byref(ms)))
+        return {"tile": tile.value, "mode": "graph" if mode.value == POOL_GRAPH else "persistent",
+                "ms_per_step": ms.value}
+
+    def set_schedule(self, tile, mode):
+        self._check(_pl_schedule(self._h, int(tile), int(mode)))
+
+    def profile(self, steps=5):
+        """Mean device milliseconds per launch of (element pass, node pass)."""
+        out = np.zeros(2)
+        self._check(_pl_profile(self._h, int(steps), _p(out)))
+        return float(out[0]), float(out[1])
+
+    def info(self):
+        out = np.zeros(8, np.int64)
+        self._check(_pl_info(self._h, _p(out)))
+        keys = ("tets", "nodes", "meshes", "tile", "mode", "launches", "device_bytes", "staging_buffers")
+        return dict(zip(keys, (int(x) for x in out)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _pl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,208 @@
+"""The multi-mesh pool (batched and served step) on the GPU, through the C ABI.
+
+A pool mesh runs the J2_F32K tet arithmetic: its displacement, velocity and plastic
+state must be bit-identical to a single-mesh FEMSTEP_TET_J2_F32K handle given the same
+time step, whatever else is in the pool, whichever schedule (graph or persistent) and
+tile size runs it, and whenever it was admitted.  Against the FP64 oracle (the
+reference's tet kinematics with plasticity::update, in double) each mesh keeps the
+1e-5 relative displacement and energy within 0.5 %.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def beam(fem, nx, ny, nz, length=1.0, load=100e3, clamp_end=0):
+    pos, idx = fem.box_tet_mesh(length, 0.1, 0.1, nx, ny, nz)
+    x = pos[0::3]
+    fixed = ((x < 1e-6) if clamp_end == 0 else (x > length - 1e-6)).astype(np.uint32)
+    tip = (x > length - 1e-6) if clamp_end == 0 else (x < 1e-6)
+    fext = np.zeros(pos.size)
+    fext[2::3][tip] = -load / tip.sum()
+    return dict(position=pos, index=idx, fixed=fixed, external_force=fext)
+
+
+MATS = [dict(yield_strength=235e6, hardening=1e9), dict(yield_strength=355e6, hardening=0.5e9),
+        dict(yield_strength=300e6, hardening=2e9)]
+
+
+def crit(fem, mesh):
+    """0.9 x the FP64 element bound of the mesh (what the single-mesh handle reports)."""
+    s = fem.TetSolver(mesh["position"], mesh["index"], mode="f32k", fixed=mesh["fixed"], density=7850.0)
+    dt = s.critical_dt(210e9, 0.3, 7850.0, 0.9)
+    s.close()
+    return dt
+
+
+def single(fem, mesh, steps, dt, mat, ramp):
+    s = fem.TetSolver(mesh["position"], mesh["index"], mode="f32k", fixed=mesh["fixed"],
+                      external_force=mesh["external_force"], density=7850.0)
+    s.run(steps, dt=dt, ramp_steps=ramp, **mat)
+    p, v = s.readback64()
+    out = (p, v, s.plastic())
+    s.close()
+    return out
+
+
+def test_pool_mesh_bit_identical_to_single_mesh_step(fem):
+    meshes = [beam(fem, 24, 3, 3, load=300e3), beam(fem, 10, 2, 2, length=0.5, load=200e3, clamp_end=1),
+              beam(fem, 40, 4, 4, load=250e3)]
+    dts = [crit(fem, m) for m in meshes]
+    steps = [1200, 937, 1201]
+    for mode in (fem.POOL_GRAPH, fem.POOL_PERSISTENT):
+        pool = fem.TetPool(200000, 50000, max_meshes=8)
+        ids = [pool.admit(steps=steps[k], dt=dts[k], ramp_steps=400, **MATS[k], **meshes[k]) for k in range(3)]
+        # uneven chunks, more steps than some meshes want
+        for chunk in (17, 100, 5, 200, 900):
+            pool.run(chunk, mode)
+        for k, i in enumerate(ids):
+            assert pool.status(i) == (steps[k], steps[k])
+            p, v = pool.readback(i)
+            pe, ve, ple = single(fem, meshes[k], steps[k], dts[k], MATS[k], 400)
+            assert np.array_equal(p, pe), (mode, k)
+            assert np.array_equal(v, ve), (mode, k)
+            assert np.array_equal(pool.plastic(i), ple), (mode, k)
+            assert (ple[:, 6] > 0).any(), "the case must exercise plasticity"
+        assert sorted(pool.finished()) == sorted(ids)
+        pool.close()
+
+
+def test_result_is_the_same_alone_and_in_the_mix(fem):
+    """A mesh admitted into a busy pool mid-run, next to meshes at other steps, gets the
+    same bits (state and FP64 energy account) as when it runs alone."""
+    a = beam(fem, 30, 3, 3, load=400e3)
+    others = [beam(fem, 16, 2, 2, load=80e3), beam(fem, 50, 4, 4, length=2.0, load=120e3)]
+    alone = fem.TetPool(100000, 30000, max_meshes=4)
+    ia = alone.admit(steps=1500, ramp_steps=500, **MATS[0], **a)  # dt: the device bound
+    alone.run(1500)
+    pa, va = alone.readback(ia)
+    ea = alone.energy(ia)
+    assert (alone.plastic(ia)[:, 6] > 0).mean() > 0.05, "the case must exercise plasticity"
+
+    mix = fem.TetPool(300000, 90000, max_meshes=8)
+    j0 = mix.admit(steps=3000, ramp_steps=300, **MATS[1], **others[0])
+    mix.run(37)
+    j1 = mix.admit(steps=3000, ramp_steps=300, **MATS[2], **others[1])
+    mix.run(50, fem.POOL_PERSISTENT)
+    ib = mix.admit(steps=1500, ramp_steps=500, **MATS[0], **a)  # mid-run
+    assert mix.dt(ib) == alone.dt(ia)
+    for chunk in (3, 64, 200, 133, 1100):
+        mix.run(chunk, fem.POOL_GRAPH if chunk % 2 else fem.POOL_PERSISTENT)
+    assert mix.status(ib)[0] == 1500
+    pb, vb = mix.readback(ib)
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert np.array_equal(ea, mix.energy(ib))
+    assert mix.status(j0)[0] == 37 + 50 + 1500 and mix.status(j1)[0] == 50 + 1500
+
+
+def test_async_admission_behind_a_running_chunk(fem):
+    """admit / release while a chunk is in flight land behind it: the in-flight meshes
+    are unaffected and the new mesh starts from rest at the next chunk."""
+    a, b = beam(fem, 20, 2, 2, load=90e3), beam(fem, 12, 3, 3, load=70e3)
+    da, db = crit(fem, a), crit(fem, b)
+    ref = fem.TetPool(60000, 20000, max_meshes=4)
+    ra = ref.admit(steps=500, dt=da, ramp_steps=100, **MATS[0], **a)
+    ref.run(500)
+    rb = ref.admit(steps=200, dt=db, ramp_steps=100, **MATS[1], **b)
+    ref.run(200)
+    pool = fem.TetPool(60000, 20000, max_meshes=4)
+    ia = pool.admit(steps=500, dt=da, ramp_steps=100, **MATS[0], **a)
+    pool.run_async(250)
+    junk = pool.admit(steps=10, dt=db, **MATS[2], **b)        # admitted while running
+    pool.release(junk)                                        # and dropped again
+    ib = pool.admit(steps=200, dt=db, ramp_steps=100, **MATS[1], **b)
+    pool.wait()
+    assert pool.finished() == []
+    pool.run(250)
+    assert sorted(pool.finished()) == sorted([ia, ib])
+    assert pool.status(ib)[0] == 200
+    assert np.array_equal(pool.readback(ia)[0], ref.readback(ra)[0])
+    assert np.array_equal(pool.readback(ib)[0], ref.readback(rb)[0])
+
+
+def test_tile_sizes_and_autotune_leave_results_unchanged(fem):
+    m = beam(fem, 36, 3, 3, load=170e3)
+    base = None
+    for tile in (128, 256, 512):
+        pool = fem.TetPool(50000, 15000, max_meshes=2, tile=tile)
+        i = pool.admit(steps=300, ramp_steps=150, **MATS[0], **m)
+        pool.run(300)
+        p, v = pool.readback(i)
+        e = pool.energy(i)
+        if base is None:
+            base = (p, v, e)
+        else:
+            assert np.array_equal(p, base[0]) and np.array_equal(v, base[1])
+            assert np.allclose(e, base[2], rtol=1e-12, atol=0.0)
+        pool.close()
+    pool = fem.TetPool(50000, 15000, max_meshes=2)
+    i = pool.admit(steps=300, ramp_steps=150, **MATS[0], **m)
+    pool.run(100)
+    best = pool.autotune(steps=20)
+    assert best["tile"] in (128, 256, 512) and best["ms_per_step"] > 0
+    assert pool.status(i)[0] == 100  # tuning rolled its trial steps back
+    pool.run(200)
+    p, v = pool.readback(i)
+    assert np.array_equal(p, base[0]) and np.array_equal(v, base[1])
+    assert np.allclose(pool.energy(i), base[2], rtol=1e-12, atol=0.0)
+
+
+def test_admission_against_capacity(fem):
+    m = beam(fem, 10, 2, 2)  # 240 tets, 99 nodes
+    pool = fem.TetPool(600, 400, max_meshes=8)
+    i1 = pool.admit(steps=10, dt=1e-7, **m)
+    i2 = pool.admit(steps=10, dt=1e-7, **m)
+    with pytest.raises(fem.PoolFull):
+        pool.admit(steps=10, dt=1e-7, **m)  # 720 tets > 600
+    pool.run(10)
+    assert sorted(pool.finished()) == sorted([i1, i2])
+    pool.release(i1)
+    i3 = pool.admit(steps=5, dt=1e-7, **m)
+    pool.run(5)
+    assert sorted(pool.finished()) == sorted([i2, i3])
+    bad = dict(m)
+    bad["index"] = m["index"].copy()
+    bad["index"][3] = 10_000
+    with pytest.raises(fem.FemStepError) as e:
+        pool.admit(steps=1, **bad)
+    assert e.value.code == fem.EINVAL
+
+
+def test_device_critical_dt_matches_single_mesh_bound(fem):
+    m = beam(fem, 20, 3, 3)
+    pool = fem.TetPool(20000, 5000)
+    i = pool.admit(steps=1, **m)
+    # the pool bounds the FP32 Dm^-1 the kernels use; the single mesh the FP64 one
+    assert abs(pool.dt(i) / crit(fem, m) - 1.0) < 1e-6
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_pool_meshes_against_fp64_oracle(fem, port, k):
+    """Per-mesh materials, 2,000 steps, against O-tet64 (fem.cpp kinematics with the
+    J2 return in double): 1e-5 relative displacement; energy account within 0.5 %."""
+    loads = [200e3, 260e3, 230e3]
+    m = beam(fem, 40, 4, 4, load=loads[k], clamp_end=k % 2)
+    ref = O.TetMesh64(port, m["position"], m["index"], m["fixed"], m["external_force"])
+    dt = port.tet64_critical_dt(C.byref(ref._s), 210e9, 0.3, 7850.0, 0.9)
+    ref.step(O.tet64_params(dt=dt, ramp_steps=1000, yield_=MATS[k]["yield_strength"],
+                            hardening=MATS[k]["hardening"]), 2000)
+    pool = fem.TetPool(100000, 30000, max_meshes=4)
+    pool.admit(steps=2000, dt=dt, **beam(fem, 8, 2, 2))  # a neighbour, so the mesh runs in a mix
+    i = pool.admit(steps=2000, dt=dt, ramp_steps=1000, **MATS[k], **m)
+    pool.run(2000)
+    p, _ = pool.readback(i)
+    rest = m["position"].astype(np.float64)
+    u, ur = p - rest, ref.position - rest
+    err = np.abs(u - ur).max() / np.abs(ur).max()
+    yielded = (ref.plastic.reshape(-1, 7)[:, 6] > 0).mean()
+    assert yielded > 0.2, "the case must exercise plasticity"
+    assert err < 1e-5, err
+    e, er = pool.energy(i), ref.energy
+    assert abs(e[0] - er[0]) / er[0] < 5e-3
+    for j in (1, 2, 3):
+        assert abs(e[j] - er[j]) <= 5e-3 * er[0]
