@@ -22,6 +22,16 @@ Workloads (synthetic and seeded; no dataset is involved):
   tet-precision   the precision-study beam, 200 x 20 x 20 cells x 6 Kuhn tets (480,000
                   tets), J2 FP32-compensated, 200 kN tip load ramped over 10,000 steps
   tet-cantilever  the 40 x 4 x 4 cantilever (3,840 tets), same element
+  tet-batched     256 independent tet beams and plates, tet counts log-uniform in
+                  [2e3, 2e5] (11.0 M tets), yield U[235, 355] MPa, hardening U[0.5, 2]
+                  GPa, a random clamped face, a tip or pressure load of seeded size;
+                  all stepped together in one pool (FP32-compensated), schedule and
+                  tile picked by the autotuner.  Beside it the same meshes one at a
+                  time through the plain single-mesh step (FP64 and FP32-compensated).
+  tet-serving     Poisson arrivals (40/s) of tet meshes of log-uniform size in
+                  [1e3, 5e5] and U[500, 5000] steps, admitted into a pool sized to a
+                  150 GB budget as room frees up, with p50/p99 step latency; the trace
+                  lasts --serve-seconds (default 30 s) of arrivals.
 """
 from __future__ import annotations
 
@@ -50,6 +60,10 @@ WORKLOADS = {
     "shell-sample": dict(kind="shell", cells=(200, 100), sample_cells=(100, 50)),
     "tet-precision": dict(kind="tet", cells=(200, 20, 20), load=200e3, ramp=10000, mode="f32k"),
     "tet-cantilever": dict(kind="tet", cells=(40, 4, 4), load=200e3, ramp=1000, mode="f32k"),
+    "tet-batched": dict(kind="pool", count=256, lo=2e3, hi=2e5),
+    # the first 16 meshes of the batch (1.1 M tets): the size ncu captures are taken on
+    "tet-batched-sample": dict(kind="pool", count=16, lo=2e3, hi=2e5),
+    "tet-serving": dict(kind="serve", rate=40.0, lo=1e3, hi=5e5, budget=150e9),
 }
 SHELL_MATERIAL = dict(youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9)
 
@@ -188,6 +202,36 @@ def cpu_baseline(wl, seconds=15.0):
     kind = "reference" if O.have_ref() else "port"
     o = O.Oracle("ref" if kind == "reference" else "port")
     workers = os.cpu_count() or 1
+    if wl["kind"] in ("pool", "serve"):
+        import workloads as W
+
+        specs = batch_specs(wl)[:6]
+        port = o if kind == "port" else O.Oracle("port")  # the FP64 element bound (set-up, untimed)
+        done, spent, sample = 0.0, 0.0, []
+        for sp in specs:
+            b = W.build(sp)
+            m = O.TetMesh64(o, b.position, b.index, b.fixed, b.external_force)
+            dt = port.tet64_critical_dt(C.byref(m._s), W.YOUNGS, W.POISSON, W.DENSITY, 0.9)
+            p = O.tet64_params(dt=dt, ramp_steps=1000, yield_=sp.yield_strength, hardening=sp.hardening)
+            T = sp.tets
+            budget = seconds / len(specs)
+            if kind == "reference":
+                rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), 1, workers)
+                steps = max(1, int(budget * rate / T))
+                rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), steps, workers)
+                spent += T * steps / rate  # the step loop's own clock (thread start-up excluded)
+            else:
+                t0 = time.perf_counter()
+                m.step(p, 1)
+                steps = max(1, int(budget / max(time.perf_counter() - t0, 1e-9)))
+                t0 = time.perf_counter()
+                m.step(p, steps)
+                spent += time.perf_counter() - t0
+            done += T * steps
+            sample.append(f"{T}x{steps}")
+        return {"value": done / spent, "unit": UNIT, "cores": workers if kind == "reference" else 1, "kind": kind,
+                "sample": "O-tet64 (FP64 J2) on the first %d meshes of the workload, meshes in sequence, tets x "
+                          "steps: %s" % (len(specs), ", ".join(sample))}
     if wl["kind"] == "tet":
         pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
         m = O.TetMesh64(o, pos, idx, fixed, fext)
@@ -255,6 +299,170 @@ def run_reference(args, wl):
 
 
 # ---------------------------------------------------------------------------------
+# the batched and served workloads (a pool of many meshes)
+
+def batch_specs(wl):
+    import workloads as W
+
+    if wl["kind"] == "serve":
+        return W.request_trace(rate=wl["rate"], duration=4.0, lo=wl["lo"], hi=wl["hi"])
+    return W.batch_meshes(count=wl["count"], lo=wl["lo"], hi=wl["hi"], steps=0, ramp_steps=1000)
+
+
+def plain_sequential(F, W, built, steps, mode):
+    """The plain single-mesh step (gpu::FemGpuSolver's shape): one mesh at a time, each
+    in its own handle for `steps` steps.  Device ms summed over the meshes."""
+    total_ms, units = 0.0, 0
+    for b in built:
+        s = F.TetSolver(b.position, b.index, mode=mode, fixed=b.fixed, external_force=b.external_force,
+                        density=W.DENSITY)
+        dt = s.critical_dt(W.YOUNGS, W.POISSON, W.DENSITY, 0.9)
+        kw = dict(dt=dt, ramp_steps=b.spec.ramp_steps, yield_strength=b.spec.yield_strength,
+                  hardening=b.spec.hardening)
+        s.run(3, **kw)  # warm (graph capture)
+        total_ms += s.run(steps, **kw)
+        units += b.spec.tets * steps
+        s.close()
+    return units / (total_ms / 1e3), total_ms
+
+
+def run_pool(args, wl, rank, world, barrier, dist, local):
+    import femstep as F
+    import workloads as W
+
+    specs = batch_specs(wl)
+    built = [W.build(sp) for sp in specs]
+    T = sum(sp.tets for sp in specs)
+    N = sum(sp.nodes for sp in specs)
+    pool = F.TetPool(T, N + len(specs) + 1, max_meshes=len(specs) + 1)
+    t_admit = time.perf_counter()
+    for b in built:
+        pool.admit(steps=10 ** 12, **b.admit_kwargs())
+    pool.run(0)
+    admit_s = time.perf_counter() - t_admit
+    tune = pool.autotune(steps=16)
+    pool.run(args.warmup)
+    barrier()
+    with ClockSampler(local) as clocks:
+        clocks.wait_first()
+        ms = pool.run(args.steps)
+        launches = pool.info()["launches"]
+        barrier()
+        time.sleep(0.25)
+    if dist is not None:
+        import torch
+
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = T * args.steps * world / (ms / 1e3)
+    elem_ms, node_ms = pool.profile(5)
+    eb = sum(tet_bytes(sp.tets, sp.nodes, "f32k")[0] for sp in specs)
+    nb = sum(tet_bytes(sp.tets, sp.nodes, "f32k")[1] for sp in specs)
+    info = pool.info()
+    pool.close()
+
+    # the plain single-mesh step over the same meshes, one at a time
+    plain_steps = max(10, min(args.steps, 50))
+    plain64, _ = plain_sequential(F, W, built, plain_steps, "f64")
+    plain32, _ = plain_sequential(F, W, built, plain_steps, "f32k")
+
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        p2 = F.TetPool(T, N + len(specs) + 1, max_meshes=len(specs) + 1)
+        p2.set_schedule(tune["tile"], F.POOL_GRAPH if tune["mode"] == "graph" else F.POOL_PERSISTENT)
+        ids2 = [p2.admit(steps=args.steps, **b.admit_kwargs()) for b in built]
+        p2.run(args.steps)
+        d2h = 0
+        for i in ids2:
+            pp, vv = p2.readback(i)
+            d2h += pp.nbytes + vv.nbytes
+        p2.close()
+        wall = time.perf_counter() - t0
+        h2d = sum(b.position.nbytes + b.index.nbytes + b.fixed.nbytes + b.external_force.nbytes for b in built)
+        e2e = {"value": T * args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+               "d2h_bytes_per_step": d2h / args.steps,
+               "note": "create the pool, admit every mesh from host arrays (host rest state + upload), K steps, "
+                       "read back every mesh's positions and velocities, through the C ABI, wall clock"}
+    peak, peak_kind = measured_peak()
+    achieved = eb / (elem_ms / 1e3) / 1e9
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "meshes": len(specs), "elements": T, "nodes": N,
+                       "schedule": tune, "element_kernel_ms": elem_ms, "node_kernel_ms": node_ms,
+                       "step_effective_gbs": (eb + nb) / (ms / args.steps / 1e3) / 1e9,
+                       "l2": "no flush: %.2f GB move per step, above the 126 MB L2" % ((eb + nb) / 1e9),
+                       "admit_seconds": admit_s, "device_bytes": info["device_bytes"],
+                       "parallelism": f"replicas x{world}"},
+            "plain": {"f64_elem_upd_per_s": plain64, "f32k_elem_upd_per_s": plain32, "steps": plain_steps,
+                      "batched_over_plain_f64": value / world / plain64,
+                      "batched_over_plain_f32k": value / world / plain32,
+                      "note": "the same meshes one at a time, each through its own single-mesh handle "
+                              "(femstep_tet_run, graph-captured), device time summed"},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": ncu_traffic(args.workload), "kernel": "pool_elements (tet element pass)",
+                         "peak_source": peak_kind},
+        }
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(wl)
+        print(json.dumps(out), flush=True)
+
+
+def run_serving(args, wl, rank, world, barrier, dist, local):
+    import femstep as F
+    import serving as S
+    import workloads as W
+
+    trace = W.request_trace(rate=wl["rate"], duration=args.serve_seconds, lo=wl["lo"], hi=wl["hi"])
+    pool = F.TetPool.for_budget(wl["budget"], nodes_per_tet=0.25, max_meshes=4096)
+    # the schedule, tuned once on a representative mix
+    warm = [pool.admit(steps=10 ** 6, **W.build(sp).admit_kwargs()) for sp in trace[:48]]
+    tune = pool.autotune(steps=16)
+    for i in warm:
+        pool.release(i)
+    reqs = [S.Request(key=k, arrival=sp.arrival, tets=sp.tets, steps=sp.steps,
+                      build=(lambda sp=sp: W.build(sp).admit_kwargs())) for k, sp in enumerate(trace)]
+    barrier()
+    with ClockSampler(local) as clocks:
+        clocks.wait_first()
+        rep = S.Server(pool, chunk=args.serve_chunk, full_error=F.PoolFull).serve(reqs)
+        barrier()
+        time.sleep(0.25)
+    summ = rep.summary()
+    value = summ["elem_upd_per_s"] * world
+    info = pool.info()
+    pool.close()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": rep.chunks,
+            "warmup": args.warmup, "ms_per_step": summ["p50_step_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "arrival_rate": wl["rate"], "seconds": args.serve_seconds,
+                       "budget_bytes": wl["budget"], "pool_device_bytes": info["device_bytes"],
+                       "chunk_steps": args.serve_chunk, "schedule": tune,
+                       "offered_elem_upd_per_s": sum(r.tets * r.steps for r in reqs) / args.serve_seconds,
+                       "l2": "no flush: the resident solves move GBs per step, above the 126 MB L2",
+                       "parallelism": f"replicas x{world}"},
+            "serving": summ,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "the serving loop is end to end: arrivals admitted from host arrays, results read "
+                            "back; value is completed element-updates over the wall clock of the trace"},
+            "gpu_launches": None,
+            "clocks": clocks.summary(),
+        }
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(wl)
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------------
 
 class Solver:
     """One workload's solver behind a common face."""
@@ -303,6 +511,8 @@ def main():
     ap.add_argument("--workload", default="shell-panel", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
+    ap.add_argument("--serve-chunk", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
@@ -324,9 +534,6 @@ def main():
     import femstep as F
 
     F.set_device(local)  # one process per GPU
-    w = Solver(wl)
-    s = w.s
-    s.run(args.warmup, **w.kw)
 
     def barrier():
         if dist is not None:
@@ -335,6 +542,14 @@ def main():
             torch.cuda.synchronize()
             dist.barrier()
 
+    if wl["kind"] in ("pool", "serve"):
+        (run_pool if wl["kind"] == "pool" else run_serving)(args, wl, rank, world, barrier, dist, local)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    w = Solver(wl)
+    s = w.s
+    s.run(args.warmup, **w.kw)
     barrier()
     with ClockSampler(local) as clocks:
         clocks.wait_first()
