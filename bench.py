@@ -364,8 +364,15 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
 
     # the plain single-mesh step over the same meshes, one at a time
     plain_steps = max(10, min(args.steps, 50))
-    plain64, _ = plain_sequential(F, W, built, plain_steps, "f64")
-    plain32, _ = plain_sequential(F, W, built, plain_steps, "f32k")
+    plain = None
+    if not args.no_plain:
+        plain64, _ = plain_sequential(F, W, built, plain_steps, "f64")
+        plain32, _ = plain_sequential(F, W, built, plain_steps, "f32k")
+        plain = {"f64_elem_upd_per_s": plain64, "f32k_elem_upd_per_s": plain32, "steps": plain_steps,
+                 "batched_over_plain_f64": value / world / plain64,
+                 "batched_over_plain_f32k": value / world / plain32,
+                 "note": "the same meshes one at a time, each through its own single-mesh handle "
+                         "(femstep_tet_run, graph-captured), device time summed"}
 
     e2e = None
     if not args.no_e2e:
@@ -398,11 +405,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
                        "l2": "no flush: %.2f GB move per step, above the 126 MB L2" % ((eb + nb) / 1e9),
                        "admit_seconds": admit_s, "device_bytes": info["device_bytes"],
                        "parallelism": f"replicas x{world}"},
-            "plain": {"f64_elem_upd_per_s": plain64, "f32k_elem_upd_per_s": plain32, "steps": plain_steps,
-                      "batched_over_plain_f64": value / world / plain64,
-                      "batched_over_plain_f32k": value / world / plain32,
-                      "note": "the same meshes one at a time, each through its own single-mesh handle "
-                              "(femstep_tet_run, graph-captured), device time summed"},
+            "plain": plain,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
@@ -511,6 +514,7 @@ def main():
     ap.add_argument("--workload", default="shell-panel", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="tet-batched: skip the one-mesh-at-a-time comparison")
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--serve-chunk", type=int, default=64)
     args = ap.parse_args()
