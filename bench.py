@@ -309,6 +309,15 @@ def batch_specs(wl):
     return W.batch_meshes(count=wl["count"], lo=wl["lo"], hi=wl["hi"], steps=0, ramp_steps=1000)
 
 
+def fixed_schedule(F, pool, spec):
+    """`TILE:graph|persistent` set by hand (None: let the autotuner choose)."""
+    if not spec:
+        return None
+    tile, mode = spec.split(":")
+    pool.set_schedule(int(tile), F.POOL_GRAPH if mode == "graph" else F.POOL_PERSISTENT)
+    return {"tile": int(tile), "mode": mode, "ms_per_step": None, "set_by": "--schedule"}
+
+
 def plain_sequential(F, W, built, steps, mode):
     """The plain single-mesh step (gpu::FemGpuSolver's shape): one mesh at a time, each
     in its own handle for `steps` steps.  Device ms summed over the meshes."""
@@ -340,7 +349,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
         pool.admit(steps=10 ** 12, **b.admit_kwargs())
     pool.run(0)
     admit_s = time.perf_counter() - t_admit
-    tune = pool.autotune(steps=16)
+    tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=16)
     pool.run(args.warmup)
     barrier()
     with ClockSampler(local) as clocks:
@@ -427,7 +436,7 @@ def run_serving(args, wl, rank, world, barrier, dist, local):
     pool = F.TetPool.for_budget(wl["budget"], nodes_per_tet=0.25, max_meshes=4096)
     # the schedule, tuned once on a representative mix
     warm = [pool.admit(steps=10 ** 6, **W.build(sp).admit_kwargs()) for sp in trace[:48]]
-    tune = pool.autotune(steps=16)
+    tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=16)
     for i in warm:
         pool.release(i)
     reqs = [S.Request(key=k, arrival=sp.arrival, tets=sp.tets, steps=sp.steps,
@@ -515,6 +524,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="tet-batched: skip the one-mesh-at-a-time comparison")
+    ap.add_argument("--schedule", default=None,
+                    help="pool workloads: TILE:graph|persistent instead of the autotuner (for profiling)")
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--serve-chunk", type=int, default=64)
     args = ap.parse_args()

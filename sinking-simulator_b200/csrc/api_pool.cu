@@ -382,7 +382,7 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
     d.rest_vol = A.alloc<float>(Tc);
     d.plastic = A.alloc<float>(Tc * 7);
     d.plastic_c = A.alloc<float>(Tc * 7);
-    d.slots = A.alloc<float>(Tc * 12 + 4);
+    d.slots = A.alloc<float4>(Tc * 4 + 1);
     d.offset = A.zeros<uint32_t>(Nc);
     d.disp = A.alloc<float>(Nc * 3);
     d.disp_c = A.alloc<float>(Nc * 3);
@@ -417,7 +417,7 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
     return FEMSTEP_OK;
 }
 
-size_t femstep_pool_bytes_per_tet(void) { return 16 + 16 + 36 + 4 + 28 + 28 + 48; }
+size_t femstep_pool_bytes_per_tet(void) { return 16 + 16 + 36 + 4 + 28 + 28 + 64; }
 size_t femstep_pool_bytes_per_node(void) { return 4 + 12 + 12 + 12 + 4 + 4 + 1 + 12; }
 
 int femstep_pool_admit(femstep_pool* p, const femstep_pool_mesh* mesh, long long steps, int* id) {
@@ -541,12 +541,9 @@ int femstep_pool_admit(femstep_pool* p, const femstep_pool_mesh* mesh, long long
     PoolMesh* pm = (PoolMesh*)stage(sizeof(PoolMesh));
     std::memset(pm, 0, sizeof(PoolMesh));
     const double E = m.youngs_modulus, nu = m.poisson_ratio;
-    pm->dmu = E / (2.0 * (1.0 + nu));
-    pm->dkappa = E / (3.0 * (1.0 - 2.0 * nu));
-    pm->mu = (float)pm->dmu;
-    pm->kappa = (float)pm->dkappa;
-    pm->yield = (float)m.yield_strength;
-    pm->hardening = (float)m.hardening_modulus;
+    // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
+    pm->mat = fs::make_j2f(E / (2.0 * (1.0 + nu)), E / (3.0 * (1.0 - 2.0 * nu)), m.yield_strength,
+                           m.hardening_modulus);
     pm->dt64 = m.dt > 0.0 ? m.dt : 0.0;
     pm->dt = (float)pm->dt64;
     pm->gravity = (float)m.gravity;

@@ -204,7 +204,9 @@ int femstep_tet_create(const femstep_tet_mesh* mesh, int mode, femstep_tet** out
         std::vector<float> vel(N * 3, 0.0f);
         if (m.velocity) std::memcpy(vel.data(), m.velocity, sizeof(float) * N * 3);
         d.velocity = A.upload(vel.data(), N * 3);
-        d.slots = A.zeros<float>(T * 4 * 3 + 4);
+        // REF32: three floats per corner (the reference's layout); J2 modes: a padded
+        // float4 per corner, one 16-byte store each
+        d.slots = A.zeros<float>(mode == FEMSTEP_TET_REF32 ? T * 4 * 3 + 4 : T * 4 * 4 + 4);
         if (mode == FEMSTEP_TET_REF32) {
             d.position = A.upload(m.position, N * 3);
             d.mass = A.upload(m.mass, N);

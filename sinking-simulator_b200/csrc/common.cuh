@@ -27,6 +27,32 @@ __device__ __forceinline__ double block_sum(double v, double* scratch /* >= 32 *
     return total;  // valid in thread 0 only
 }
 
+// Two deterministic block sums in one pass (one pair of barriers): the same order as
+// block_sum for each.  scratch >= 64 doubles.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+        scratch[warp] = a;
+        scratch[32 + warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int warps = (blockDim.x + 31) >> 5;
+        double ta = 0.0, tb = 0.0;
+        for (int w = 0; w < warps; ++w) {
+            ta += scratch[w];
+            tb += scratch[32 + w];
+        }
+        a = ta;
+        b = tb;
+    }
+    __syncthreads();
+}
+
 // Column-major 3x3, the layout engine/sim/fem.cpp uses for its M3.
 template <typename T>
 struct M3 {

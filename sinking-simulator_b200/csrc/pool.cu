@@ -12,10 +12,6 @@
 namespace fs {
 namespace {
 
-__device__ __forceinline__ J2f mesh_material(const PoolMesh& m) {
-    return J2f{m.mu, m.kappa, m.yield, m.hardening, m.dmu, m.dkappa};
-}
-
 __device__ __forceinline__ TetElementRefs element_refs(const PoolDevice& d) {
     return TetElementRefs{d.index, d.slot, d.rest_inv, d.rest_vol, d.plastic, d.plastic_c, d.disp, d.slots,
                           d.tet_cap};
@@ -34,12 +30,11 @@ __device__ __forceinline__ void element_tile(const PoolDevice& d, int tile, int 
     const bool live = m.step + sub < m.target;
     double diss = 0.0, energy = 0.0;
     const long long t = tl.begin + threadIdx.x;
-    if (live && t < tl.end) tet_element_f32<true, CG>(element_refs(d), t, mesh_material(m), diss, energy);
-    const double bd = block_sum(diss, scratch);
-    const double be = block_sum(energy, scratch);
+    if (live && t < tl.end) tet_element_f32<true, CG>(element_refs(d), t, m.mat, diss, energy);
+    block_sum2(diss, energy, scratch);  // valid in thread 0
     if (live && threadIdx.x == 0) {
-        d.e_diss[tl.part] += bd;
-        d.e_strain[tl.part] = be;
+        d.e_diss[tl.part] += diss;
+        d.e_strain[tl.part] = energy;
     }
 }
 
@@ -55,21 +50,25 @@ __device__ __forceinline__ void node_tile(const PoolDevice& d, int tile, int sub
         const float lf = (float)ramp_factor(step, m.ramp);
         tet_node_f32<true, CG>(node_refs(d), n, lf, m.dt, m.gravity, m.damping, work, kin, gwork);
     }
-    const double bw = block_sum(work + gwork, scratch);
-    const double bk = block_sum(kin, scratch);
+    work += gwork;
+    block_sum2(work, kin, scratch);  // valid in thread 0
     if (live && threadIdx.x == 0) {
-        d.n_work[tl.part] += bw;
-        d.n_kin[tl.part] = bk;
+        d.n_work[tl.part] += work;
+        d.n_kin[tl.part] = kin;
     }
 }
 
-__global__ void __launch_bounds__(512) pool_elements(PoolDevice d, int sub) {
-    __shared__ double scratch[32];
+// B threads per block (the tile); 1024 / B blocks per SM bound the element pass to 64
+// registers, 32 resident warps per SM whatever the tile.
+template <int B>
+__global__ void __launch_bounds__(B, 1024 / B) pool_elements(PoolDevice d, int sub) {
+    __shared__ double scratch[64];
     element_tile<false>(d, blockIdx.x, sub, scratch);
 }
 
-__global__ void __launch_bounds__(512) pool_nodes(PoolDevice d, int sub) {
-    __shared__ double scratch[32];
+template <int B>
+__global__ void __launch_bounds__(B, 1024 / B) pool_nodes(PoolDevice d, int sub) {
+    __shared__ double scratch[64];
     node_tile<false>(d, blockIdx.x, sub, scratch);
 }
 
@@ -114,8 +113,9 @@ __device__ __forceinline__ bool grid_sync(unsigned int* bar, unsigned int nblock
     return *(volatile int*)err == 0;
 }
 
-__global__ void __launch_bounds__(512) pool_persistent(PoolDevice d, int steps) {
-    __shared__ double scratch[32];
+template <int B>
+__global__ void __launch_bounds__(B, 1024 / B) pool_persistent(PoolDevice d, int steps) {
+    __shared__ double scratch[64];
     for (int s = 0; s < steps; ++s) {
         for (int tile = blockIdx.x; tile < d.n_etiles; tile += gridDim.x) element_tile<true>(d, tile, s, scratch);
         if (!grid_sync(d.barrier, gridDim.x, d.error)) return;
@@ -133,21 +133,31 @@ __global__ void pool_set_dt(PoolMesh* meshes, int id, const double* w2, double s
 
 }  // namespace
 
-void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream) {
-    if (d.n_etiles == 0 || steps <= 0) return;
-    for (int s = 0; s < steps; ++s) {
-        pool_elements<<<d.n_etiles, tile, 0, stream>>>(d, s);
-        pool_nodes<<<d.n_ntiles, tile, 0, stream>>>(d, s);
-    }
-    pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
-}
-
 void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream) {
-    if (d.n_etiles) pool_elements<<<d.n_etiles, tile, 0, stream>>>(d, sub);
+    if (!d.n_etiles) return;
+    switch (tile) {
+        case 128: pool_elements<128><<<d.n_etiles, 128, 0, stream>>>(d, sub); break;
+        case 256: pool_elements<256><<<d.n_etiles, 256, 0, stream>>>(d, sub); break;
+        default: pool_elements<512><<<d.n_etiles, 512, 0, stream>>>(d, sub); break;
+    }
 }
 
 void launch_pool_node_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream) {
-    if (d.n_ntiles) pool_nodes<<<d.n_ntiles, tile, 0, stream>>>(d, sub);
+    if (!d.n_ntiles) return;
+    switch (tile) {
+        case 128: pool_nodes<128><<<d.n_ntiles, 128, 0, stream>>>(d, sub); break;
+        case 256: pool_nodes<256><<<d.n_ntiles, 256, 0, stream>>>(d, sub); break;
+        default: pool_nodes<512><<<d.n_ntiles, 512, 0, stream>>>(d, sub); break;
+    }
+}
+
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream) {
+    if (d.n_etiles == 0 || steps <= 0) return;
+    for (int s = 0; s < steps; ++s) {
+        launch_pool_element_pass(d, tile, s, stream);
+        launch_pool_node_pass(d, tile, s, stream);
+    }
+    pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
 }
 
 void launch_pool_advance(const PoolDevice& d, int steps, cudaStream_t stream) {
@@ -158,7 +168,11 @@ int pool_persistent_max_blocks(int tile) {
     int per_sm = 0, sms = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pool_persistent, tile, 0);
+    switch (tile) {
+        case 128: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pool_persistent<128>, 128, 0); break;
+        case 256: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pool_persistent<256>, 256, 0); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pool_persistent<512>, 512, 0); break;
+    }
     return per_sm * sms;
 }
 
@@ -173,7 +187,12 @@ cudaError_t launch_pool_persistent(const PoolDevice& d, int tile, int steps, int
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, pool_persistent, d, steps);
+    cudaError_t e;
+    switch (tile) {
+        case 128: e = cudaLaunchKernelEx(&cfg, pool_persistent<128>, d, steps); break;
+        case 256: e = cudaLaunchKernelEx(&cfg, pool_persistent<256>, d, steps); break;
+        default: e = cudaLaunchKernelEx(&cfg, pool_persistent<512>, d, steps); break;
+    }
     if (e != cudaSuccess) return e;
     pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
     return cudaGetLastError();

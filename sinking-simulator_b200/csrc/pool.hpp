@@ -26,8 +26,7 @@
 namespace fs {
 
 struct PoolMesh {           // device-side per-mesh record
-    float mu, kappa, yield, hardening;
-    double dmu, dkappa;
+    J2f mat;
     float dt, gravity, damping;
     int ramp;               // load ramp in steps
     long long step;         // steps taken
@@ -52,7 +51,7 @@ struct PoolDevice {
     float* rest_vol = nullptr;
     float* plastic = nullptr;
     float* plastic_c = nullptr;
-    float* slots = nullptr;        // 12 per tet capacity
+    float4* slots = nullptr;       // 4 per tet capacity: (fx, fy, fz, 0) per corner
     // nodes
     uint32_t* offset = nullptr;    // [node_cap]: CSR begin of each node; every mesh holds
                                    // one spare node slot after its last node for the end

@@ -44,10 +44,37 @@ __device__ __forceinline__ M3<float> mul_fma(const M3<float>& a, const M3<float>
     return r;
 }
 
+// (I + Q)^-1 by the adjugate with FMA cofactors, for the Higham step.  A singular
+// matrix (|det| <= tiny) gives zero, as fem.cpp's inverse does.
+__device__ __forceinline__ M3<float> inverse_fma(const M3<float>& a, float tiny) {
+    const float c00 = __fmaf_rn(a(1, 1), a(2, 2), -(a(1, 2) * a(2, 1)));
+    const float c01 = __fmaf_rn(a(1, 2), a(2, 0), -(a(1, 0) * a(2, 2)));
+    const float c02 = __fmaf_rn(a(1, 0), a(2, 1), -(a(1, 1) * a(2, 0)));
+    const float det = __fmaf_rn(a(0, 2), c02, __fmaf_rn(a(0, 1), c01, a(0, 0) * c00));
+    const float id = fabsf(det) > tiny ? 1.0f / det : 0.0f;
+    M3<float> r;
+    r(0, 0) = c00 * id;
+    r(1, 0) = c01 * id;
+    r(2, 0) = c02 * id;
+    r(0, 1) = __fmaf_rn(a(0, 2), a(2, 1), -(a(0, 1) * a(2, 2))) * id;
+    r(1, 1) = __fmaf_rn(a(0, 0), a(2, 2), -(a(0, 2) * a(2, 0))) * id;
+    r(2, 1) = __fmaf_rn(a(0, 1), a(2, 0), -(a(0, 0) * a(2, 1))) * id;
+    r(0, 2) = __fmaf_rn(a(0, 1), a(1, 2), -(a(0, 2) * a(1, 1))) * id;
+    r(1, 2) = __fmaf_rn(a(0, 2), a(1, 0), -(a(0, 0) * a(1, 2))) * id;
+    r(2, 2) = __fmaf_rn(a(0, 0), a(1, 1), -(a(0, 1) * a(1, 0))) * id;
+    return r;
+}
+
 // A global load that bypasses L1 when CG: needed where another SM wrote the data
 // earlier in the same (persistent) launch.
 template <bool CG>
 __device__ __forceinline__ float ldg_coherent(const float* p) {
+    if (CG) return __ldcg(p);
+    return *p;
+}
+
+template <bool CG>
+__device__ __forceinline__ float4 ldg_coherent4(const float4* p) {
     if (CG) return __ldcg(p);
     return *p;
 }
@@ -60,14 +87,20 @@ struct TetElementRefs {
     float* plastic;         // [7][stride]
     float* plastic_c;       // [7][stride] (compensated variant)
     const float* disp;      // [3N]
-    float* slots;           // [3 * 4 * stride]
+    float4* slots;          // [4 * stride]: one (fx, fy, fz, 0) per corner
     long long stride;       // SoA stride (tets, or the pool's tet capacity)
 };
 
 struct J2f {
     float mu, kappa, yield, hardening;
-    double dmu, dkappa;     // for the FP64 strain-energy density
+    // for the FP64 strain-energy density: 1 / (2 mu), 1 / (3 kappa)
+    double inv_2mu, inv_3kappa;
 };
+
+// The material record of the FP32 J2 tet from the FP64 constants.
+__host__ __device__ inline J2f make_j2f(double mu, double kappa, double yield, double hardening) {
+    return J2f{(float)mu, (float)kappa, (float)yield, (float)hardening, 1.0 / (2.0 * mu), 1.0 / (3.0 * kappa)};
+}
 
 // One tet: forces into the node-major slots, plastic state advanced; returns the
 // dissipation and strain energy of the element (FP64, for the energy account).
@@ -96,7 +129,7 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
         ipq(0, 0) += 1.0f;
         ipq(1, 1) += 1.0f;
         ipq(2, 2) += 1.0f;
-        const M3<float> mq = mul_fma(inverse(ipq, 1e-30f), q);
+        const M3<float> mq = mul_fma(inverse_fma(ipq, 1e-30f), q);
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -143,19 +176,18 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
     diss = 0.0;
     if (excess > 0.0f) {
         const float gamma = excess / (2.0f * m.mu + (2.0f / 3.0f) * m.hardening);
-        const float k = 2.0f * m.mu * gamma / norm;
+        const float inv_norm = 1.0f / norm;
+        const float k = 2.0f * m.mu * gamma * inv_norm;
         float dp[6];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const float n = trial[i] / norm;
-            dp[i] = gamma * n;
-            sv[i] = pressure + trial[i] - k * trial[i];
+            dp[i] = gamma * (trial[i] * inv_norm);
+            sv[i] = pressure + __fmaf_rn(-k, trial[i], trial[i]);
         }
 #pragma unroll
         for (int i = 3; i < 6; ++i) {
-            const float n = trial[i] / norm;
-            dp[i] = 2.0f * gamma * n;
-            sv[i] = trial[i] - k * trial[i];
+            dp[i] = 2.0f * gamma * (trial[i] * inv_norm);
+            sv[i] = __fmaf_rn(-k, trial[i], trial[i]);
         }
         float dsum = 0.0f;
 #pragma unroll
@@ -186,12 +218,13 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
     diss *= vol;
     {
         const double s0 = sv[0], s1 = sv[1], s2 = sv[2], s3 = sv[3], s4 = sv[4], s5 = sv[5];
-        const double pr = (s0 + s1 + s2) / 3.0;
-        double density = 0.5 * s0 * ((s0 - pr) / (2.0 * m.dmu) + pr / (3.0 * m.dkappa)) +
-                         0.5 * s1 * ((s1 - pr) / (2.0 * m.dmu) + pr / (3.0 * m.dkappa)) +
-                         0.5 * s2 * ((s2 - pr) / (2.0 * m.dmu) + pr / (3.0 * m.dkappa));
-        density += 0.5 * (s3 * s3 + s4 * s4 + s5 * s5) / m.dmu;
-        energy = vol * density;
+        // 1/2 sigma : C^-1 : sigma = 1/2 [s_dev : s_dev / (2 mu) + p tr(sigma) / (3 kappa)]
+        // with p = tr(sigma) / 3, the engineering shears counted twice
+        const double tr = s0 + s1 + s2;
+        const double pr = tr * (1.0 / 3.0);
+        const double d0 = s0 - pr, d1 = s1 - pr, d2 = s2 - pr;
+        const double dev = d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (s3 * s3 + s4 * s4 + s5 * s5);
+        energy = vol * 0.5 * (dev * m.inv_2mu + pr * tr * m.inv_3kappa);
     }
     // P = R sigma = sigma + Q sigma; nodal forces f_c = -V (P Dm^-T) column c
     M3<float> sig;
@@ -211,22 +244,20 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
     float f0[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float* out = d.slots + (size_t)sid[c + 1] * 3;
+        float v[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float v = scale * hf(a, c);
-            out[a] = v;
-            f0[a] -= v;
+            v[a] = scale * hf(a, c);
+            f0[a] -= v[a];
         }
+        d.slots[sid[c + 1]] = make_float4(v[0], v[1], v[2], 0.0f);  // one 16-byte store
     }
-    float* out0 = d.slots + (size_t)sid[0] * 3;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) out0[a] = f0[a];
+    d.slots[sid[0]] = make_float4(f0[0], f0[1], f0[2], 0.0f);
 }
 
 struct TetNodeRefs {
     const uint32_t* offset;  // CSR offsets (absolute slot positions)
-    const float* slots;
+    const float4* slots;
     const uint8_t* fixed;
     const float* mass;
     const float* inv_mass;
@@ -251,12 +282,12 @@ __device__ __forceinline__ void tet_node_f32(const TetNodeRefs& d, long long n, 
     const float m = d.mass[n];
     float force[3] = {0.0f, 0.0f, -gravity * m};
     const uint32_t b = d.offset[n], e = d.offset[n + 1];
-    const float* sl = d.slots + (size_t)b * 3;
 #pragma unroll 4
-    for (uint32_t k = b; k < e; ++k, sl += 3) {
-        force[0] += ldg_coherent<CG>(sl);
-        force[1] += ldg_coherent<CG>(sl + 1);
-        force[2] += ldg_coherent<CG>(sl + 2);
+    for (uint32_t k = b; k < e; ++k) {
+        const float4 f = ldg_coherent4<CG>(d.slots + k);
+        force[0] += f.x;
+        force[1] += f.y;
+        force[2] += f.z;
     }
     float ext[3] = {0.0f, 0.0f, 0.0f};
     if (d.ext) {

@@ -10,9 +10,10 @@
 namespace fs {
 namespace {
 
+// 1024 / kBlock blocks per SM: 64 registers, 32 resident warps per SM
 template <bool KAHAN>
-__global__ void __launch_bounds__(kBlock) f32_forces(TetDevice<float> d, J2f m) {
-    __shared__ double scratch[32];
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) f32_forces(TetDevice<float> d, J2f m) {
+    __shared__ double scratch[64];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const long long s = d.counter[0];
@@ -21,15 +22,14 @@ __global__ void __launch_bounds__(kBlock) f32_forces(TetDevice<float> d, J2f m) 
     }
     double diss = 0.0, energy = 0.0;
     if (t < d.tets) {
-        const TetElementRefs r{d.index, d.slot, d.rest_inv, d.rest_vol, d.plastic, d.plastic_c, d.disp, d.slots,
-                               d.tets};
+        const TetElementRefs r{d.index,   d.slot,      d.rest_inv, d.rest_vol, d.plastic,
+                               d.plastic_c, d.disp, reinterpret_cast<float4*>(d.slots), d.tets};
         tet_element_f32<KAHAN>(r, t, m, diss, energy);
     }
-    const double bd = block_sum(diss, scratch);
-    const double be = block_sum(energy, scratch);
+    block_sum2(diss, energy, scratch);  // valid in thread 0
     if (threadIdx.x == 0) {
-        d.e_diss[blockIdx.x] += bd;
-        d.e_strain[blockIdx.x] = be;
+        d.e_diss[blockIdx.x] += diss;
+        d.e_strain[blockIdx.x] = energy;
     }
 }
 
@@ -40,7 +40,8 @@ __global__ void __launch_bounds__(kBlock) f32_nodes(TetDevice<float> d, float dt
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double work = 0.0, kin = 0.0, gwork = 0.0;
     if (n < d.nodes) {
-        const TetNodeRefs r{d.offset, d.slots, d.fixed, d.mass, d.inv_mass, d.ext, d.velocity, d.disp, d.disp_c};
+        const TetNodeRefs r{d.offset, reinterpret_cast<const float4*>(d.slots), d.fixed, d.mass, d.inv_mass, d.ext,
+                            d.velocity, d.disp, d.disp_c};
         const float lf = (float)ramp_factor(d.counter[1], ramp);
         tet_node_f32<KAHAN>(r, n, lf, dt, gravity, damping, work, kin, gwork);
     }
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(kBlock) f32_nodes(TetDevice<float> d, float dt
 void launch_f32_step(const TetDevice<float>& d, const TetParams& p, bool compensated, cudaStream_t stream,
                      int parts) {
     const int eb = blocks_for(d.tets, kBlock), nb = blocks_for(d.nodes, kBlock);
-    const J2f m{(float)p.mu, (float)p.bulk, (float)p.yield, (float)p.hardening, p.mu, p.bulk};
+    const J2f m = make_j2f(p.mu, p.bulk, p.yield, p.hardening);
     if (compensated) {
         if (parts & kElementPart) f32_forces<true><<<eb, kBlock, 0, stream>>>(d, m);
         if (parts & kNodePart)
