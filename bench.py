@@ -22,6 +22,12 @@ Workloads (synthetic and seeded; no dataset is involved):
   tet-precision   the precision-study beam, 200 x 20 x 20 cells x 6 Kuhn tets (480,000
                   tets), J2 FP32-compensated, 200 kN tip load ramped over 10,000 steps
   tet-cantilever  the 40 x 4 x 4 cantilever (3,840 tets), same element
+  tet-precision-study
+                  the precision study: the 480,000-tet beam for 20,000 steps in FP32,
+                  FP32-compensated and FP64 on the GPU; errors of displacement, von
+                  Mises stress, equivalent plastic strain and energy balance against
+                  FP64 (itself checked bit for bit against the CPU FP64 oracle over
+                  the first 100 steps)
   tet-batched     256 independent tet beams and plates, tet counts log-uniform in
                   [2e3, 2e5] (11.0 M tets), yield U[235, 355] MPa, hardening U[0.5, 2]
                   GPa, a random clamped face, a tip or pressure load of seeded size;
@@ -60,6 +66,8 @@ WORKLOADS = {
     "shell-sample": dict(kind="shell", cells=(200, 100), sample_cells=(100, 50)),
     "tet-precision": dict(kind="tet", cells=(200, 20, 20), load=200e3, ramp=10000, mode="f32k"),
     "tet-cantilever": dict(kind="tet", cells=(40, 4, 4), load=200e3, ramp=1000, mode="f32k"),
+    "tet-precision-study": dict(kind="precision", cells=(200, 20, 20), load=100e3, ramp=10000, steps=20000,
+                                oracle_steps=100),
     "tet-batched": dict(kind="pool", count=256, lo=2e3, hi=2e5),
     # the first 16 meshes of the batch (1.1 M tets): the size ncu captures are taken on
     "tet-batched-sample": dict(kind="pool", count=16, lo=2e3, hi=2e5),
@@ -309,6 +317,103 @@ def batch_specs(wl):
     return W.batch_meshes(count=wl["count"], lo=wl["lo"], hi=wl["hi"], steps=0, ramp_steps=1000)
 
 
+def tet_von_mises(position, rest, index, plastic, mu, kappa):
+    """Von Mises stress per tet in FP64 from a state (positions, plastic strain): the
+    co-rotated strain of fem.cpp's tet (four Higham iterations), sigma = 2 mu dev(e - ep)
+    + kappa tr(e - ep) I.  The same host routine for every variant, so the comparison
+    sees only the state."""
+    x = position.reshape(-1, 3)
+    X = rest.reshape(-1, 3).astype(np.float64)
+    idx = index.reshape(-1, 4).astype(np.int64)
+    dm = np.stack([X[idx[:, c]] - X[idx[:, 0]] for c in (1, 2, 3)], axis=2)
+    ds = np.stack([x[idx[:, c]] - x[idx[:, 0]] for c in (1, 2, 3)], axis=2)
+    f = ds @ np.linalg.inv(dm)
+    r = f.copy()
+    for _ in range(4):
+        r = 0.5 * (r + np.transpose(np.linalg.inv(r), (0, 2, 1)))
+    sm = np.transpose(r, (0, 2, 1)) @ f
+    e = 0.5 * (sm + np.transpose(sm, (0, 2, 1))) - np.eye(3)
+    ep = plastic
+    el = np.empty((len(idx), 6))
+    el[:, 0], el[:, 1], el[:, 2] = e[:, 0, 0] - ep[:, 0], e[:, 1, 1] - ep[:, 1], e[:, 2, 2] - ep[:, 2]
+    el[:, 3], el[:, 4], el[:, 5] = 2 * e[:, 0, 1] - ep[:, 3], 2 * e[:, 1, 2] - ep[:, 4], 2 * e[:, 2, 0] - ep[:, 5]
+    tr = el[:, 0] + el[:, 1] + el[:, 2]
+    s = 2 * mu * (el[:, :3] - tr[:, None] / 3)
+    t = mu * el[:, 3:]
+    return np.sqrt(1.5 * ((s ** 2).sum(1) + 2 * (t ** 2).sum(1)))
+
+
+def run_precision(args, wl, rank):
+    """The precision study on one GPU (rank 0 only)."""
+    import femstep as F
+    import oracle as O
+
+    if rank != 0:
+        return
+    pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
+    T = idx.size // 4
+    mu, kappa = 210e9 / 2.6, 210e9 / (3 * 0.4)
+    solvers = {m: F.TetSolver(pos, idx, mode=m, fixed=fixed, external_force=fext, density=7850.0)
+               for m in ("f64", "f32k", "f32")}
+    dt = solvers["f64"].critical_dt(210e9, 0.3, 7850.0, 0.9)
+    kw = dict(dt=dt, ramp_steps=wl["ramp"])
+    # the FP64 GPU step against the CPU FP64 oracle over a prefix, bit for bit
+    port = O.Oracle("port")
+    ref = O.TetMesh64(port, pos, idx, fixed, fext)
+    n0 = wl["oracle_steps"]
+    t0 = time.perf_counter()
+    ref.step(O.tet64_params(dt=dt, ramp_steps=wl["ramp"]), n0)
+    oracle_s = time.perf_counter() - t0
+    ms = {}
+    for m, s in solvers.items():
+        ms[m] = s.run(n0, **kw)
+    p64, _ = solvers["f64"].readback64()
+    prefix_identical = bool(np.array_equal(p64, ref.position) and
+                            np.array_equal(solvers["f64"].plastic().reshape(-1), ref.plastic))
+    with ClockSampler(0) as clocks:
+        clocks.wait_first()
+        for m, s in solvers.items():
+            ms[m] += s.run(wl["steps"] - n0, **kw)
+    rest = pos.astype(np.float64)
+    state = {}
+    for m, s in solvers.items():
+        p, _ = s.readback64()
+        pl = s.plastic()
+        e = s.energy()
+        state[m] = dict(u=p - rest, vm=tet_von_mises(p, rest, idx, pl, mu, kappa), ep=pl[:, 6], energy=e)
+    r = state["f64"]
+    yielded = float((r["ep"] > 0).mean())
+
+    def drift(e):
+        w = e[0] + e[4]  # external work incl. gravity
+        return float(abs(w - (e[1] + e[2] + e[3])) / abs(w))
+
+    out = {}
+    for m in ("f32", "f32k", "f64"):
+        v = state[m]
+        out[m] = {
+            "max_rel_displacement_error": float(np.abs(v["u"] - r["u"]).max() / np.abs(r["u"]).max()),
+            "max_rel_von_mises_error": float(np.abs(v["vm"] - r["vm"]).max() / r["vm"].max()),
+            "max_rel_plastic_strain_error": float(np.abs(v["ep"] - r["ep"]).max() / max(r["ep"].max(), 1e-300)),
+            "energy_balance_drift": drift(v["energy"]),
+            "energy_drift_vs_fp64": abs(drift(v["energy"]) - drift(r["energy"])),
+            "elem_upd_per_s": T * wl["steps"] / (ms[m] / 1e3),
+        }
+    for s in solvers.values():
+        s.close()
+    line = {"metric": METRIC, "value": out["f32k"]["elem_upd_per_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": wl["steps"], "warmup": 0, "ms_per_step": ms["f32k"] / wl["steps"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "elements": T, "nodes": pos.size // 3, "dt": dt,
+                       "tip_load_n": wl["load"], "ramp_steps": wl["ramp"], "yielded_fraction_fp64": yielded,
+                       "reference": "GPU FP64 step; bit-identical to the CPU FP64 oracle over the first %d steps: %s "
+                                    "(oracle %.1f s)" % (n0, prefix_identical, oracle_s),
+                       "errors": "max |a - a64| / max |a64| over nodes (displacement) or tets (von Mises from the "
+                                 "final state, equivalent plastic strain); energy drift |W - (U + D + K)| / W"},
+            "precision": out, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def fixed_schedule(F, pool, spec):
     """`TILE:graph|persistent` set by hand (None: let the autotuner choose)."""
     if not spec:
@@ -466,7 +571,7 @@ def run_serving(args, wl, rank, world, barrier, dist, local):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "note": "the serving loop is end to end: arrivals admitted from host arrays, results read "
                             "back; value is completed element-updates over the wall clock of the trace"},
-            "gpu_launches": None,
+            "gpu_launches": summ["launches"],
             "clocks": clocks.summary(),
         }
         if not args.no_cpu_baseline:
@@ -557,6 +662,11 @@ def main():
             torch.cuda.synchronize()
             dist.barrier()
 
+    if wl["kind"] == "precision":
+        run_precision(args, wl, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     if wl["kind"] in ("pool", "serve"):
         (run_pool if wl["kind"] == "pool" else run_serving)(args, wl, rank, world, barrier, dist, local)
         if dist is not None:
@@ -564,7 +674,9 @@ def main():
         return
     w = Solver(wl)
     s = w.s
-    s.run(args.warmup, **w.kw)
+    # W warm-up steps, at least one captured graph's worth (32 steps), so the graph the
+    # timed run replays is built before the timed region
+    s.run(max(args.warmup, 32), **w.kw)
     barrier()
     with ClockSampler(local) as clocks:
         clocks.wait_first()

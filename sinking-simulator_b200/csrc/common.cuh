@@ -10,6 +10,14 @@ constexpr int kBlock = 256;  // threads per block for the element and node kerne
 
 inline int blocks_for(long long n, int block) { return (int)((n + block - 1) / block); }
 
+// SMs of the current device.
+inline int sm_count() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+
 // Deterministic block sum in double: shuffle tree inside each warp, then warp 0 adds
 // the per-warp partials in warp order.  The association order depends only on the
 // block size, never on scheduling, so the same launch always produces the same bits.

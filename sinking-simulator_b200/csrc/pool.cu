@@ -23,8 +23,13 @@ __device__ __forceinline__ TetNodeRefs node_refs(const PoolDevice& d) {
 
 // One element tile at sub-step `sub` of the chunk (all threads of the block call it).
 // CG: data other blocks wrote earlier in the same launch is read through L2.
+// `ahead`: the tile this block prefetches into L2 (the one a wave later), or -1.
 template <bool CG>
-__device__ __forceinline__ void element_tile(const PoolDevice& d, int tile, int sub, double* scratch) {
+__device__ __forceinline__ void element_tile(const PoolDevice& d, int tile, int sub, double* scratch, int ahead) {
+    if (ahead >= 0 && ahead < d.n_etiles) {
+        const PoolTile nx = d.etiles[ahead];
+        prefetch_tet_rows(element_refs(d), nx.begin, nx.end);
+    }
     const PoolTile tl = d.etiles[tile];
     const PoolMesh& m = d.meshes[tl.mesh];
     const bool live = m.step + sub < m.target;
@@ -60,10 +65,11 @@ __device__ __forceinline__ void node_tile(const PoolDevice& d, int tile, int sub
 
 // B threads per block (the tile); 1024 / B blocks per SM bound the element pass to 64
 // registers, 32 resident warps per SM whatever the tile.
+// `wave`: the blocks resident on the whole GPU at once; block b prefetches tile b + wave.
 template <int B>
-__global__ void __launch_bounds__(B, 1024 / B) pool_elements(PoolDevice d, int sub) {
+__global__ void __launch_bounds__(B, 1024 / B) pool_elements(PoolDevice d, int sub, int wave) {
     __shared__ double scratch[64];
-    element_tile<false>(d, blockIdx.x, sub, scratch);
+    element_tile<false>(d, blockIdx.x, sub, scratch, blockIdx.x + wave);
 }
 
 template <int B>
@@ -117,7 +123,8 @@ template <int B>
 __global__ void __launch_bounds__(B, 1024 / B) pool_persistent(PoolDevice d, int steps) {
     __shared__ double scratch[64];
     for (int s = 0; s < steps; ++s) {
-        for (int tile = blockIdx.x; tile < d.n_etiles; tile += gridDim.x) element_tile<true>(d, tile, s, scratch);
+        for (int tile = blockIdx.x; tile < d.n_etiles; tile += gridDim.x)
+            element_tile<true>(d, tile, s, scratch, tile + (int)gridDim.x);
         if (!grid_sync(d.barrier, gridDim.x, d.error)) return;
         for (int tile = blockIdx.x; tile < d.n_ntiles; tile += gridDim.x) node_tile<true>(d, tile, s, scratch);
         if (!grid_sync(d.barrier, gridDim.x, d.error)) return;
@@ -135,10 +142,11 @@ __global__ void pool_set_dt(PoolMesh* meshes, int id, const double* w2, double s
 
 void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream) {
     if (!d.n_etiles) return;
+    const int wave = sm_count() * (1024 / tile);
     switch (tile) {
-        case 128: pool_elements<128><<<d.n_etiles, 128, 0, stream>>>(d, sub); break;
-        case 256: pool_elements<256><<<d.n_etiles, 256, 0, stream>>>(d, sub); break;
-        default: pool_elements<512><<<d.n_etiles, 512, 0, stream>>>(d, sub); break;
+        case 128: pool_elements<128><<<d.n_etiles, 128, 0, stream>>>(d, sub, wave); break;
+        case 256: pool_elements<256><<<d.n_etiles, 256, 0, stream>>>(d, sub, wave); break;
+        default: pool_elements<512><<<d.n_etiles, 512, 0, stream>>>(d, sub, wave); break;
     }
 }
 

@@ -102,6 +102,45 @@ __host__ __device__ inline J2f make_j2f(double mu, double kappa, double yield, d
     return J2f{(float)mu, (float)kappa, (float)yield, (float)hardening, 1.0 / (2.0 * mu), 1.0 / (3.0 * kappa)};
 }
 
+// L2 prefetch of the per-tet rows of tets [begin, end) -- one 128-byte line per thread
+// of the block: index (16 B per tet), slot map (16 B), Dm^-1 (9 rows of 4 B), volume
+// and the plastic state (7 rows).  A block issues it for the tile one wave ahead, so
+// that block's first loads, the ones whose results the gathers wait for, hit L2.  Every
+// address lies inside [begin, end) of its row.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+__device__ __forceinline__ void prefetch_tet_rows(const TetElementRefs& d, long long begin, long long end) {
+    if (end <= begin) return;
+    const int x = threadIdx.x;
+    const long long n = end - begin;
+    const int wide = (int)((n * 16 + 127) >> 7);   // lines of a 16-byte row
+    const int narrow = (int)((n * 4 + 127) >> 7);  // lines of a 4-byte row
+    int k = x;
+    if (k < wide) {
+        prefetch_l2(reinterpret_cast<const char*>(d.index + begin) + ((long long)k << 7));
+        return;
+    }
+    k -= wide;
+    if (k < wide) {
+        prefetch_l2(reinterpret_cast<const char*>(d.slot + begin) + ((long long)k << 7));
+        return;
+    }
+    k -= wide;
+    const int row = k / narrow, line = k - row * narrow;
+    const float* base;
+    if (row < 9)
+        base = d.rest_inv + (size_t)row * d.stride;
+    else if (row == 9)
+        base = d.rest_vol;
+    else if (row < 17)
+        base = d.plastic + (size_t)(row - 10) * d.stride;
+    else
+        return;
+    prefetch_l2(reinterpret_cast<const char*>(base + begin) + ((long long)line << 7));
+}
+
 // One tet: forces into the node-major slots, plastic state advanced; returns the
 // dissipation and strain energy of the element (FP64, for the energy account).
 template <bool KAHAN, bool CG = false>

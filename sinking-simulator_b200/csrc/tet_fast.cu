@@ -12,9 +12,17 @@ namespace {
 
 // 1024 / kBlock blocks per SM: 64 registers, 32 resident warps per SM
 template <bool KAHAN>
-__global__ void __launch_bounds__(kBlock, 1024 / kBlock) f32_forces(TetDevice<float> d, J2f m) {
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) f32_forces(TetDevice<float> d, J2f m, int wave) {
     __shared__ double scratch[64];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    {
+        // the rows of the block one wave later, into L2
+        const long long nb = (long long)(blockIdx.x + wave) * blockDim.x;
+        const long long ne = nb + blockDim.x < d.tets ? nb + blockDim.x : d.tets;
+        const TetElementRefs r{d.index,   d.slot,      d.rest_inv, d.rest_vol, d.plastic,
+                               d.plastic_c, d.disp, reinterpret_cast<float4*>(d.slots), d.tets};
+        prefetch_tet_rows(r, nb, ne);
+    }
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const long long s = d.counter[0];
         d.counter[1] = s;
@@ -61,12 +69,13 @@ void launch_f32_step(const TetDevice<float>& d, const TetParams& p, bool compens
                      int parts) {
     const int eb = blocks_for(d.tets, kBlock), nb = blocks_for(d.nodes, kBlock);
     const J2f m = make_j2f(p.mu, p.bulk, p.yield, p.hardening);
+    const int wave = sm_count() * (1024 / kBlock);
     if (compensated) {
-        if (parts & kElementPart) f32_forces<true><<<eb, kBlock, 0, stream>>>(d, m);
+        if (parts & kElementPart) f32_forces<true><<<eb, kBlock, 0, stream>>>(d, m, wave);
         if (parts & kNodePart)
             f32_nodes<true><<<nb, kBlock, 0, stream>>>(d, (float)p.dt, (float)p.gravity, (float)p.damping, p.ramp);
     } else {
-        if (parts & kElementPart) f32_forces<false><<<eb, kBlock, 0, stream>>>(d, m);
+        if (parts & kElementPart) f32_forces<false><<<eb, kBlock, 0, stream>>>(d, m, wave);
         if (parts & kNodePart)
             f32_nodes<false><<<nb, kBlock, 0, stream>>>(d, (float)p.dt, (float)p.gravity, (float)p.damping, p.ramp);
     }

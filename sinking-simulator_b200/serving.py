@@ -48,6 +48,7 @@ class Report:
     queue_wait_s: list = field(default_factory=list)
     max_resident: int = 0
     admit_retries: int = 0
+    launches: int = 0                                     # kernel launches of the chunks
 
     def summary(self):
         def pct(a, q):
@@ -62,7 +63,7 @@ class Report:
             "p99_step_ms": pct(self.step_latency_ms, 99), "p50_request_s": pct(self.request_latency_s, 50),
             "p99_request_s": pct(self.request_latency_s, 99), "p50_queue_s": pct(self.queue_wait_s, 50),
             "p99_queue_s": pct(self.queue_wait_s, 99), "max_resident": self.max_resident,
-            "admit_retries": self.admit_retries,
+            "admit_retries": self.admit_retries, "launches": self.launches,
         }
 
 
@@ -145,6 +146,8 @@ class Server:
             end = now()
             report.device_ms += ms
             report.chunks += 1
+            if hasattr(self.pool, "info"):
+                report.launches += self.pool.info()["launches"]
             report.max_resident = max(report.max_resident, len(live))
             for r in stepping:
                 taken = min(self.chunk, r.steps - r.done)
