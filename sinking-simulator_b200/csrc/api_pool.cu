@@ -294,8 +294,8 @@ int snapshot(femstep_pool* p, Snapshot& s, bool restore) {
             s.spans.push_back({p->d.plastic + (size_t)k * p->tet_cap, (size_t)tmax * 4});
             s.spans.push_back({p->d.plastic_c + (size_t)k * p->tet_cap, (size_t)tmax * 4});
         }
-        s.spans.push_back({p->d.disp, (size_t)nmax * 12});
-        s.spans.push_back({p->d.disp_c, (size_t)nmax * 12});
+        s.spans.push_back({p->d.disp, (size_t)nmax * 16});
+        s.spans.push_back({p->d.disp_c, (size_t)nmax * 16});
         s.spans.push_back({p->d.velocity, (size_t)nmax * 12});
         s.spans.push_back({p->d.meshes, (size_t)p->max_meshes * sizeof(PoolMesh)});
         s.spans.push_back({p->d.e_diss, (size_t)pmax * 8});
@@ -384,8 +384,8 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
     d.plastic_c = A.alloc<float>(Tc * 7);
     d.slots = A.alloc<float4>(Tc * 4 + 1);
     d.offset = A.zeros<uint32_t>(Nc);
-    d.disp = A.alloc<float>(Nc * 3);
-    d.disp_c = A.alloc<float>(Nc * 3);
+    d.disp = A.alloc<float4>(Nc);
+    d.disp_c = A.alloc<float4>(Nc);
     d.velocity = A.alloc<float>(Nc * 3);
     d.mass = A.alloc<float>(Nc);
     d.inv_mass = A.alloc<float>(Nc);
@@ -418,7 +418,7 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
 }
 
 size_t femstep_pool_bytes_per_tet(void) { return 16 + 16 + 36 + 4 + 28 + 28 + 64; }
-size_t femstep_pool_bytes_per_node(void) { return 4 + 12 + 12 + 12 + 4 + 4 + 1 + 12; }
+size_t femstep_pool_bytes_per_node(void) { return 4 + 16 + 16 + 12 + 4 + 4 + 1 + 12; }
 
 int femstep_pool_admit(femstep_pool* p, const femstep_pool_mesh* mesh, long long steps, int* id) {
     if (!p || !mesh || !id) return fail(p, FEMSTEP_EINVAL, "null argument");
@@ -531,8 +531,8 @@ int femstep_pool_admit(femstep_pool* p, const femstep_pool_mesh* mesh, long long
     send(d.inv_mass + n0, imass, (N + 1) * 4);
     send(d.fixed + n0, fixed, N + 1);
     send(d.ext + n0 * 3, ext, (N + 1) * 12);
-    cudaMemsetAsync(d.disp + n0 * 3, 0, (N + 1) * 12, st);
-    cudaMemsetAsync(d.disp_c + n0 * 3, 0, (N + 1) * 12, st);
+    cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
+    cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
     cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
     cudaMemsetAsync(d.e_diss + part0, 0, e_tiles * 8, st);
     cudaMemsetAsync(d.e_strain + part0, 0, e_tiles * 8, st);
@@ -663,16 +663,25 @@ int femstep_pool_status(femstep_pool* p, int id, long long* steps_done, long lon
 int femstep_pool_readback(femstep_pool* p, int id, double* position, double* velocity) {
     if (!valid_id(p, id)) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
     const HostMesh& h = p->meshes[id];
-    std::vector<float> u(h.N * 3), v(h.N * 3);
-    int rc = check(p, cudaMemcpyAsync(u.data(), p->d.disp + h.n0 * 3, u.size() * 4, cudaMemcpyDeviceToHost, p->stream),
+    std::vector<float4> u(h.N), c(h.N);
+    std::vector<float> v(h.N * 3);
+    int rc = check(p, cudaMemcpyAsync(u.data(), p->d.disp + h.n0, h.N * 16, cudaMemcpyDeviceToHost, p->stream),
+                   "readback");
+    if (!rc)
+        rc = check(p, cudaMemcpyAsync(c.data(), p->d.disp_c + h.n0, h.N * 16, cudaMemcpyDeviceToHost, p->stream),
                    "readback");
     if (!rc)
         rc = check(p, cudaMemcpyAsync(v.data(), p->d.velocity + h.n0 * 3, v.size() * 4, cudaMemcpyDeviceToHost,
                                       p->stream), "readback");
     if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "readback");
     if (rc) return rc;
+    // the compensated displacement u - c, in double
     if (position)
-        for (size_t i = 0; i < u.size(); ++i) position[i] = (double)h.rest[i] + (double)u[i];
+        for (long long n = 0; n < h.N; ++n) {
+            position[n * 3] = (double)h.rest[n * 3] + ((double)u[n].x - (double)c[n].x);
+            position[n * 3 + 1] = (double)h.rest[n * 3 + 1] + ((double)u[n].y - (double)c[n].y);
+            position[n * 3 + 2] = (double)h.rest[n * 3 + 2] + ((double)u[n].z - (double)c[n].z);
+        }
     if (velocity)
         for (size_t i = 0; i < v.size(); ++i) velocity[i] = v[i];
     return FEMSTEP_OK;

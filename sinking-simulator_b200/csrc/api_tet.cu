@@ -216,8 +216,8 @@ int femstep_tet_create(const femstep_tet_mesh* mesh, int mode, femstep_tet** out
         } else {
             s->rest.assign(m.position, m.position + N * 3);
             d.rest = A.upload(m.position, N * 3);
-            d.disp = A.zeros<float>(N * 3);
-            if (mode == FEMSTEP_TET_J2_F32K) d.disp_c = A.zeros<float>(N * 3);
+            d.disp = A.zeros<float>(N * 4);  // one (x, y, z, 0) float4 per node
+            if (mode == FEMSTEP_TET_J2_F32K) d.disp_c = A.zeros<float>(N * 4);
             std::vector<float> mass(N), inv_mass(N), inv(T * 9), vol(T);
             for (size_t n = 0; n < N; ++n) {
                 mass[n] = (float)mass64[n];
@@ -300,6 +300,31 @@ int femstep_tet_run(femstep_tet* s, int substeps, const femstep_tet_params* para
     return FEMSTEP_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The FP32 modes' displacement, 3N doubles: u, or the compensated u - c.
+int displacement(femstep_tet* s, std::vector<double>& out) {
+    const size_t N = s->nodes;
+    std::vector<float> u(N * 4), c;
+    int rc = check(s, cudaMemcpy(u.data(), s->d32.disp, N * 16, cudaMemcpyDeviceToHost), "readback");
+    if (!rc && s->d32.disp_c) {
+        c.resize(N * 4);
+        rc = check(s, cudaMemcpy(c.data(), s->d32.disp_c, N * 16, cudaMemcpyDeviceToHost), "readback");
+    }
+    if (rc) return rc;
+    out.resize(N * 3);
+    for (size_t n = 0; n < N; ++n)
+        for (int k = 0; k < 3; ++k)
+            out[n * 3 + k] = (double)u[n * 4 + k] - (c.empty() ? 0.0 : (double)c[n * 4 + k]);
+    return FEMSTEP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int femstep_tet_readback(femstep_tet* s, float* position, float* velocity) {
     if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
     const size_t n3 = s->nodes * 3;
@@ -319,9 +344,9 @@ int femstep_tet_readback(femstep_tet* s, float* position, float* velocity) {
         if (s->mode == FEMSTEP_TET_REF32) {
             rc = check(s, cudaMemcpy(position, s->d32.position, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
         } else {
-            std::vector<float> u(n3);
-            rc = check(s, cudaMemcpy(u.data(), s->d32.disp, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
-            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = s->rest[i] + u[i];
+            std::vector<double> u;
+            rc = displacement(s, u);
+            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = (float)((double)s->rest[i] + u[i]);
         }
         if (rc) return rc;
     }
@@ -347,8 +372,9 @@ int femstep_tet_readback_f64(femstep_tet* s, double* position, double* velocity)
             rc = check(s, cudaMemcpy(p.data(), s->d32.position, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
             for (size_t i = 0; i < n3 && !rc; ++i) position[i] = p[i];
         } else {
-            rc = check(s, cudaMemcpy(p.data(), s->d32.disp, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
-            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = (double)s->rest[i] + (double)p[i];
+            std::vector<double> u;
+            rc = displacement(s, u);
+            for (size_t i = 0; i < n3 && !rc; ++i) position[i] = (double)s->rest[i] + u[i];
         }
         if (rc) return rc;
     }

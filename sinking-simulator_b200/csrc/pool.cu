@@ -13,8 +13,8 @@ namespace fs {
 namespace {
 
 __device__ __forceinline__ TetElementRefs element_refs(const PoolDevice& d) {
-    return TetElementRefs{d.index, d.slot, d.rest_inv, d.rest_vol, d.plastic, d.plastic_c, d.disp, d.slots,
-                          d.tet_cap};
+    return TetElementRefs{d.index,     d.slot, d.rest_inv, d.rest_vol, d.plastic,
+                          d.plastic_c, d.disp, d.disp_c,   d.slots,    d.tet_cap};
 }
 
 __device__ __forceinline__ TetNodeRefs node_refs(const PoolDevice& d) {

@@ -55,8 +55,8 @@ struct PoolDevice {
     // nodes
     uint32_t* offset = nullptr;    // [node_cap]: CSR begin of each node; every mesh holds
                                    // one spare node slot after its last node for the end
-    float* disp = nullptr;
-    float* disp_c = nullptr;
+    float4* disp = nullptr;        // (ux, uy, uz, 0)
+    float4* disp_c = nullptr;
     float* velocity = nullptr;
     float* mass = nullptr;
     float* inv_mass = nullptr;

@@ -13,14 +13,15 @@
 //     plastic_c  float   [7][T]   Kahan compensation (FP32-compensated mode only)
 //   per node:
 //     position / rest   Real  [3N]   (reference AoS x,y,z)
-//     disp, disp_c      float [3N]   displacement and its compensation (FP32 modes)
+//     disp, disp_c      float [4N]   displacement and its compensation (FP32 modes),
+//                                    one (x, y, z, 0) float4 per node
 //     velocity          Real  [3N]
 //     mass, inv_mass    Real  [N]
 //     fixed             uint8 [N]
 //     offset            uint32[N+1]  CSR offsets (adjacencyOffset)
 //     ext               Real  [3N]   full-load external force (optional)
 //   per CSR entry (node-major, the reference's gather order):
-//     slots             Real  [3 * 4T]
+//     slots             Real  [3 * 4T] (REF32, FP64); float4 [4T] (FP32 J2 modes)
 //
 // The element kernel writes each corner force straight to its node-major slot, so the
 // node kernel reads its incident forces as one contiguous run and sums them in exactly

@@ -7,7 +7,12 @@
 //
 //   * nodes carry the displacement u = x - X (rest X fixed), not the position, so a
 //     step's increment v dt ~ 1e-7 m is added to a number of size |u| ~ 1e-3 m rather
-//     than |x| ~ 1 m.  The compensated variant adds it with Kahan summation;
+//     than |x| ~ 1 m.  The compensated variant adds it with Kahan summation and keeps
+//     the pair (u, c), true value u - c, as a double-float: the element forms a
+//     neighbour difference as (u_b - u_a) - (c_b - c_a), where the first difference is
+//     exact (the two are within a factor of two, Sterbenz) and the second restores the
+//     low bits u alone has lost.  A strain of 1e-4 on a displacement of 1e-2 m keeps
+//     its digits instead of losing eleven bits to the subtraction;
 //   * the element works on the displacement gradient H = Du Dm^-1 and the rotation's
 //     deviation from identity Q = R - I, never on F = I + H and R themselves, so the
 //     strain R^T F - I = H + Q^T + Q^T H is formed from small terms with no
@@ -86,7 +91,8 @@ struct TetElementRefs {
     const float* rest_vol;  // [stride]
     float* plastic;         // [7][stride]
     float* plastic_c;       // [7][stride] (compensated variant)
-    const float* disp;      // [3N]
+    const float4* disp;     // [N] (ux, uy, uz, 0)
+    const float4* disp_c;   // [N] Kahan compensation (compensated variant)
     float4* slots;          // [4 * stride]: one (fx, fy, fz, 0) per corner
     long long stride;       // SoA stride (tets, or the pool's tet capacity)
 };
@@ -148,15 +154,25 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
                                                 double& energy) {
     const uint4 idx = d.index[t];
     const unsigned nid[4] = {idx.x, idx.y, idx.z, idx.w};
-    const float* u = d.disp;
-    float u0[3];
+    float4 un[4], cn[4];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) u0[a] = ldg_coherent<CG>(u + (size_t)nid[0] * 3 + a);
+    for (int c = 0; c < 4; ++c) un[c] = ldg_coherent4<CG>(d.disp + nid[c]);
+    if (KAHAN) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cn[c] = ldg_coherent4<CG>(d.disp_c + nid[c]);
+    }
     M3<float> du, dm_inv;
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int a = 0; a < 3; ++a) du(a, c) = ldg_coherent<CG>(u + (size_t)nid[c + 1] * 3 + a) - u0[a];
+    for (int c = 0; c < 3; ++c) {
+        du(0, c) = un[c + 1].x - un[0].x;
+        du(1, c) = un[c + 1].y - un[0].y;
+        du(2, c) = un[c + 1].z - un[0].z;
+        if (KAHAN) {  // true value u - c
+            du(0, c) -= cn[c + 1].x - cn[0].x;
+            du(1, c) -= cn[c + 1].y - cn[0].y;
+            du(2, c) -= cn[c + 1].z - cn[0].z;
+        }
+    }
 #pragma unroll
     for (int k = 0; k < 9; ++k) dm_inv.m[k] = d.rest_inv[(size_t)k * d.stride + t];
     const M3<float> h = mul_fma(du, dm_inv);  // displacement gradient
@@ -302,8 +318,8 @@ struct TetNodeRefs {
     const float* inv_mass;
     const float* ext;        // may be null
     float* velocity;
-    float* disp;
-    float* disp_c;           // compensated variant
+    float4* disp;            // (ux, uy, uz, 0)
+    float4* disp_c;          // compensated variant
 };
 
 // One node: CSR gather in order, external load, symplectic Euler on the displacement.
@@ -334,25 +350,24 @@ __device__ __forceinline__ void tet_node_f32(const TetNodeRefs& d, long long n, 
         for (int k = 0; k < 3; ++k) ext[k] = lf * d.ext[(size_t)n * 3 + k];
     }
     const float im = d.inv_mass[n];
-    float* u = d.disp + (size_t)n * 3;
+    float4 u4 = d.disp[n], c4 = KAHAN ? d.disp_c[n] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float* u = &u4.x;
+    float* cu = &c4.x;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         float v = vel[k] + (force[k] + ext[k]) * im * dt;
         v *= damping;
         vel[k] = v;
         const float du = v * dt;
-        if (KAHAN) {
-            float c = d.disp_c[(size_t)n * 3 + k];
-            float s = u[k];
-            kahan_add(s, c, du);
-            u[k] = s;
-            d.disp_c[(size_t)n * 3 + k] = c;
-        } else {
+        if (KAHAN)
+            kahan_add(u[k], cu[k], du);
+        else
             u[k] += du;
-        }
         work += (double)ext[k] * (double)v * (double)dt;
         kin += 0.5 * (double)m * (double)v * (double)v;
     }
+    d.disp[n] = u4;
+    if (KAHAN) d.disp_c[n] = c4;
     gwork = -(double)gravity * (double)m * (double)vel[2] * (double)dt;
 }
 

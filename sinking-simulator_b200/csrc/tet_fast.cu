@@ -10,6 +10,20 @@
 namespace fs {
 namespace {
 
+// The FP32 modes keep disp / disp_c as float4 per node and slots as float4 per corner.
+__device__ __forceinline__ TetElementRefs refs(const TetDevice<float>& d) {
+    return TetElementRefs{d.index,
+                          d.slot,
+                          d.rest_inv,
+                          d.rest_vol,
+                          d.plastic,
+                          d.plastic_c,
+                          reinterpret_cast<const float4*>(d.disp),
+                          reinterpret_cast<const float4*>(d.disp_c),
+                          reinterpret_cast<float4*>(d.slots),
+                          d.tets};
+}
+
 // 1024 / kBlock blocks per SM: 64 registers, 32 resident warps per SM
 template <bool KAHAN>
 __global__ void __launch_bounds__(kBlock, 1024 / kBlock) f32_forces(TetDevice<float> d, J2f m, int wave) {
@@ -19,9 +33,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) f32_forces(TetDevice<fl
         // the rows of the block one wave later, into L2
         const long long nb = (long long)(blockIdx.x + wave) * blockDim.x;
         const long long ne = nb + blockDim.x < d.tets ? nb + blockDim.x : d.tets;
-        const TetElementRefs r{d.index,   d.slot,      d.rest_inv, d.rest_vol, d.plastic,
-                               d.plastic_c, d.disp, reinterpret_cast<float4*>(d.slots), d.tets};
-        prefetch_tet_rows(r, nb, ne);
+        prefetch_tet_rows(refs(d), nb, ne);
     }
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const long long s = d.counter[0];
@@ -30,9 +42,7 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) f32_forces(TetDevice<fl
     }
     double diss = 0.0, energy = 0.0;
     if (t < d.tets) {
-        const TetElementRefs r{d.index,   d.slot,      d.rest_inv, d.rest_vol, d.plastic,
-                               d.plastic_c, d.disp, reinterpret_cast<float4*>(d.slots), d.tets};
-        tet_element_f32<KAHAN>(r, t, m, diss, energy);
+        tet_element_f32<KAHAN>(refs(d), t, m, diss, energy);
     }
     block_sum2(diss, energy, scratch);  // valid in thread 0
     if (threadIdx.x == 0) {
@@ -48,8 +58,10 @@ __global__ void __launch_bounds__(kBlock) f32_nodes(TetDevice<float> d, float dt
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double work = 0.0, kin = 0.0, gwork = 0.0;
     if (n < d.nodes) {
-        const TetNodeRefs r{d.offset, reinterpret_cast<const float4*>(d.slots), d.fixed, d.mass, d.inv_mass, d.ext,
-                            d.velocity, d.disp, d.disp_c};
+        const TetNodeRefs r{d.offset,   reinterpret_cast<const float4*>(d.slots), d.fixed,
+                            d.mass,     d.inv_mass,
+                            d.ext,      d.velocity,
+                            reinterpret_cast<float4*>(d.disp), reinterpret_cast<float4*>(d.disp_c)};
         const float lf = (float)ramp_factor(d.counter[1], ramp);
         tet_node_f32<KAHAN>(r, n, lf, dt, gravity, damping, work, kin, gwork);
     }
