@@ -193,6 +193,12 @@ size_t femstep_pool_bytes_per_node(void);
    FEMSTEP_ENOMEM when it does not fit in the free space now: the caller keeps it
    queued and retries after a release. */
 int femstep_pool_admit(femstep_pool *pool, const femstep_pool_mesh *mesh, long long steps, int *id);
+/* Admit meshes[0..count) in order while they fit (a prefix is admitted; *admitted says
+   how many, their ids in ids[]).  The host work of all of them (rest state, CSR, slot
+   map) runs on all host cores at once.  FEMSTEP_ENOMEM when the rest did not fit now;
+   FEMSTEP_EINVAL, with nothing admitted, when a mesh is not valid. */
+int femstep_pool_admit_many(femstep_pool *pool, const femstep_pool_mesh *meshes, const long long *steps, int count,
+                            int *ids, int *admitted);
 /* Free a mesh's space.  Its device state is frozen behind any queued work. */
 int femstep_pool_release(femstep_pool *pool, int id);
 /* Queue one chunk: every admitted mesh that has steps left advances by up to `steps`

@@ -15,11 +15,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/femstep.h"
@@ -339,6 +341,284 @@ int refresh_mirror(femstep_pool* p) {
                                     cudaMemcpyDeviceToHost, p->stream), "mesh table");
 }
 
+// ---- admission -------------------------------------------------------------------
+
+// Where one admitted mesh goes, and where its staged arrays sit in the pinned buffer.
+struct Placement {
+    int id = -1;
+    long long T = 0, N = 0, t0 = -1, n0 = -1, part0 = -1, e_tiles = 0, n_tiles = 0;
+    size_t idx4 = 0, slot4 = 0, inv = 0, vol = 0, offs = 0, mass = 0, imass = 0, fixed = 0, ext = 0, rec = 0,
+           end = 0;
+    int status = FEMSTEP_OK;
+    std::string what;
+};
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+// Offsets of a mesh's staged arrays, from `base`.
+void stage_layout(Placement& pl, size_t base) {
+    const size_t T = pl.T, N1 = pl.N + 1;
+    size_t o = base;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o += align256(bytes);
+        return at;
+    };
+    pl.idx4 = take(T * 16);
+    pl.slot4 = take(T * 16);
+    pl.inv = take(T * 36);
+    pl.vol = take(T * 4);
+    pl.offs = take(N1 * 4);
+    pl.mass = take(N1 * 4);
+    pl.imass = take(N1 * 4);
+    pl.fixed = take(N1);
+    pl.ext = take(N1 * 12);
+    pl.rec = take(sizeof(PoolMesh));
+    pl.end = o;
+}
+
+// The host part of admitting one mesh, into its staged arrays (pinned): FP64 rest state
+// (fem.cpp:119-158), the CSR in the reference's order (fem.cpp:147-157), the slot map,
+// SoA Dm^-1, lumped masses, load; node and slot ids rebased into the pool.  Runs on
+// any host thread; touches nothing but the mesh's own staging.
+void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
+    const long long N = pl.N, T = pl.T;
+    for (long long i = 0; i < T * 4; ++i)
+        if (m.index[i] >= (uint32_t)N) {
+            pl.status = FEMSTEP_EINVAL;
+            pl.what = "tet index out of range";
+            return;
+        }
+    std::vector<double> inv64, vol64, mass64;
+    fs::tet_rest_state64((size_t)N, (size_t)T, m.position, m.index, m.density, inv64, vol64, mass64);
+    double vmax = 0.0;
+    for (double v : vol64) vmax = std::max(vmax, v);
+    if (!(vmax > 0.0)) {
+        pl.status = FEMSTEP_EINVAL;
+        pl.what = "every tet is degenerate";
+        return;
+    }
+    std::vector<uint32_t> off, entry;
+    fs::build_csr((size_t)N, (size_t)T, 4, m.index, off, entry);
+    const long long s0 = 4 * pl.t0, n0 = pl.n0;
+    uint4* idx4 = (uint4*)(stage + pl.idx4);
+    uint4* slot4 = (uint4*)(stage + pl.slot4);
+    {
+        std::vector<uint32_t> sl(T * 4);
+        for (long long n = 0; n < N; ++n)
+            for (uint32_t k = off[n]; k < off[n + 1]; ++k) sl[entry[k]] = (uint32_t)(s0 + k);
+        for (long long t = 0; t < T; ++t) {
+            idx4[t] = make_uint4((uint32_t)(n0 + m.index[t * 4]), (uint32_t)(n0 + m.index[t * 4 + 1]),
+                                 (uint32_t)(n0 + m.index[t * 4 + 2]), (uint32_t)(n0 + m.index[t * 4 + 3]));
+            slot4[t] = make_uint4(sl[t * 4], sl[t * 4 + 1], sl[t * 4 + 2], sl[t * 4 + 3]);
+        }
+    }
+    float* inv = (float*)(stage + pl.inv);
+    for (int k = 0; k < 9; ++k)
+        for (long long t = 0; t < T; ++t) inv[(size_t)k * T + t] = (float)inv64[t * 9 + k];
+    float* vol = (float*)(stage + pl.vol);
+    for (long long t = 0; t < T; ++t) vol[t] = (float)vol64[t];
+    uint32_t* offs = (uint32_t*)(stage + pl.offs);
+    for (long long n = 0; n <= N; ++n) offs[n] = (uint32_t)(s0 + off[n]);
+    float* mass = (float*)(stage + pl.mass);
+    float* imass = (float*)(stage + pl.imass);
+    uint8_t* fixed = (uint8_t*)(stage + pl.fixed);
+    float* ext = (float*)(stage + pl.ext);
+    for (long long n = 0; n < N; ++n) {
+        mass[n] = (float)mass64[n];
+        imass[n] = mass64[n] > 0.0 ? (float)(1.0 / mass64[n]) : 0.0f;
+        fixed[n] = m.fixed && m.fixed[n] ? 1 : 0;
+        for (int k = 0; k < 3; ++k) ext[n * 3 + k] = m.external_force ? (float)m.external_force[n * 3 + k] : 0.0f;
+    }
+    // the spare node slot: holds the CSR end; massless, fixed, unloaded
+    mass[N] = imass[N] = 0.0f;
+    fixed[N] = 1;
+    ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
+}
+
+// Run f(0..count-1) on the host's cores, largest work first (`weight`).
+template <class F>
+void parallel_for(int count, const std::vector<long long>& weight, F f) {
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return weight[a] > weight[b]; });
+    const int workers = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), (unsigned)count);
+    if (workers <= 1) {
+        for (int i : order) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int w = 0; w < workers; ++w)
+        pool.emplace_back([&]() {
+            for (int k; (k = next.fetch_add(1)) < count;) f(order[k]);
+        });
+    for (auto& t : pool) t.join();
+}
+
+// Admit meshes[0..count) in order while they fit; *admitted = how many did.  Returns
+// FEMSTEP_ENOMEM when some did not fit now, FEMSTEP_EINVAL (nothing admitted) when a
+// mesh is not valid.
+int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long long* steps, int count, int* ids,
+                 int* admitted) {
+    *admitted = 0;
+    if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
+    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
+    for (int i = 0; i < count; ++i) {
+        const femstep_pool_mesh& m = meshes[i];
+        if (m.nodes == 0 || m.tets == 0 || !m.position || !m.index) return fail(p, FEMSTEP_EINVAL, "empty mesh");
+        if (steps[i] < 0) return fail(p, FEMSTEP_EINVAL, "negative step count");
+        if (!(m.density > 0.0)) return fail(p, FEMSTEP_EINVAL, "density must be positive");
+        if (!(m.youngs_modulus > 0.0) || !(m.poisson_ratio > -1.0 && m.poisson_ratio < 0.5))
+            return fail(p, FEMSTEP_EINVAL, "elastic constants out of range");
+    }
+    // places, in order, while they fit
+    std::vector<Placement> pl;
+    std::vector<bool> taken_id(p->max_meshes, false);
+    int full = FEMSTEP_OK;
+    std::string full_what;
+    for (int i = 0; i < count; ++i) {
+        const femstep_pool_mesh& m = meshes[i];
+        Placement q;
+        q.T = (long long)m.tets;
+        q.N = (long long)m.nodes;
+        q.e_tiles = (q.T + kMinTile - 1) / kMinTile;
+        q.n_tiles = (q.N + kMinTile - 1) / kMinTile;
+        for (int k = 0; k < p->max_meshes; ++k)
+            if (!p->meshes[k].used && !taken_id[k]) {
+                q.id = k;
+                break;
+            }
+        if (q.id < 0) {
+            full_what = "mesh table full";
+        } else if ((q.t0 = p->tets.take(q.T)) < 0) {
+            full_what = "no room for the tets now";
+        } else if ((q.n0 = p->nodes.take(q.N + 1)) < 0) {
+            p->tets.give(q.t0, q.T);
+            full_what = "no room for the nodes now";
+        } else if ((q.part0 = p->parts.take(q.e_tiles + q.n_tiles)) < 0) {
+            p->tets.give(q.t0, q.T);
+            p->nodes.give(q.n0, q.N + 1);
+            full_what = "no room for the energy partials now";
+        } else {
+            taken_id[q.id] = true;
+            pl.push_back(q);
+            continue;
+        }
+        full = FEMSTEP_ENOMEM;
+        break;
+    }
+    auto undo = [&]() {
+        for (const Placement& q : pl) {
+            p->tets.give(q.t0, q.T);
+            p->nodes.give(q.n0, q.N + 1);
+            p->parts.give(q.part0, q.e_tiles + q.n_tiles);
+        }
+    };
+    const int n = (int)pl.size();
+    if (n == 0) return full ? fail(p, full, full_what) : FEMSTEP_OK;
+    size_t bytes = 0;
+    std::vector<long long> weight(n);
+    for (int i = 0; i < n; ++i) {
+        stage_layout(pl[i], bytes);
+        bytes = pl[i].end;
+        weight[i] = pl[i].T;
+    }
+    cudaError_t err;
+    Staging::Buf* buf = p->staging.get(bytes, err);
+    if (!buf) {
+        undo();
+        return check(p, err, "pinned staging");
+    }
+    char* stage = Staging::take(buf, bytes);
+    // the host work, on every core
+    parallel_for(n, weight, [&](int i) { prepare_mesh(meshes[i], pl[i], stage); });
+    for (int i = 0; i < n; ++i)
+        if (pl[i].status != FEMSTEP_OK) {
+            undo();
+            return fail(p, pl[i].status, pl[i].what);
+        }
+    // queue everything behind the work already on the stream
+    PoolDevice& d = p->d;
+    cudaStream_t st = p->stream;
+    auto send = [&](void* dst, size_t off, size_t n) {
+        cudaMemcpyAsync(dst, stage + off, n, cudaMemcpyHostToDevice, st);
+    };
+    for (int i = 0; i < n; ++i) {
+        const femstep_pool_mesh& m = meshes[i];
+        const Placement& q = pl[i];
+        const long long T = q.T, N = q.N, t0 = q.t0, n0 = q.n0, part0 = q.part0;
+        send(d.index + t0, q.idx4, T * sizeof(uint4));
+        send(d.slot + t0, q.slot4, T * sizeof(uint4));
+        for (int k = 0; k < 9; ++k) send(d.rest_inv + (size_t)k * p->tet_cap + t0, q.inv + (size_t)k * T * 4, T * 4);
+        send(d.rest_vol + t0, q.vol, T * 4);
+        for (int k = 0; k < 7; ++k) {
+            cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+            cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+        }
+        send(d.offset + n0, q.offs, (N + 1) * 4);
+        send(d.mass + n0, q.mass, (N + 1) * 4);
+        send(d.inv_mass + n0, q.imass, (N + 1) * 4);
+        send(d.fixed + n0, q.fixed, N + 1);
+        send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
+        cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
+        cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
+        cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
+        cudaMemsetAsync(d.e_diss + part0, 0, q.e_tiles * 8, st);
+        cudaMemsetAsync(d.e_strain + part0, 0, q.e_tiles * 8, st);
+        cudaMemsetAsync(d.n_work + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
+        cudaMemsetAsync(d.n_kin + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
+        PoolMesh* pm = (PoolMesh*)(stage + q.rec);
+        std::memset(pm, 0, sizeof(PoolMesh));
+        const double E = m.youngs_modulus, nu = m.poisson_ratio;
+        // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
+        pm->mat = fs::make_j2f(E / (2.0 * (1.0 + nu)), E / (3.0 * (1.0 - 2.0 * nu)), m.yield_strength,
+                               m.hardening_modulus);
+        pm->dt64 = m.dt > 0.0 ? m.dt : 0.0;
+        pm->dt = (float)pm->dt64;
+        pm->gravity = (float)m.gravity;
+        pm->damping = (float)(m.damping > 0.0 ? m.damping : 1.0);
+        pm->ramp = m.ramp_steps;
+        pm->step = 0;
+        pm->target = steps[i];
+        pm->e_part = part0;
+        pm->n_part = part0 + q.e_tiles;
+        pm->serial = p->next_serial + i;
+        send(d.meshes + q.id, q.rec, sizeof(PoolMesh));
+        // no step given: 0.9 x the FP64 element eigenvalue bound of the uploaded FP32
+        // Dm^-1, computed and stored on the device behind the uploads
+        if (!(m.dt > 0.0))
+            fs::launch_pool_dt(d, q.id, t0, T, E, nu, m.density, 0.9, p->d_block_max, p->d_out + 7, st);
+    }
+    Staging::submit(buf, st);
+    const int rc = check(p, cudaGetLastError(), "admit upload");
+    if (rc) {
+        undo();
+        return rc;
+    }
+    for (int i = 0; i < n; ++i) {
+        const Placement& q = pl[i];
+        HostMesh& h = p->meshes[q.id];
+        h.used = true;
+        h.t0 = q.t0;
+        h.T = q.T;
+        h.n0 = q.n0;
+        h.N = q.N;
+        h.e_part = q.part0;
+        h.n_part = q.part0 + q.e_tiles;
+        h.e_tiles = q.e_tiles;
+        h.n_tiles = q.n_tiles;
+        h.target = steps[i];
+        h.serial = p->next_serial + i;
+        h.rest.assign(meshes[i].position, meshes[i].position + q.N * 3);
+        ids[i] = q.id;
+    }
+    p->next_serial += n;
+    p->dirty = true;
+    *admitted = n;
+    return full ? fail(p, full, full_what) : FEMSTEP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -421,166 +701,16 @@ size_t femstep_pool_bytes_per_tet(void) { return 16 + 16 + 36 + 4 + 28 + 28 + 64
 size_t femstep_pool_bytes_per_node(void) { return 4 + 16 + 16 + 12 + 4 + 4 + 1 + 12; }
 
 int femstep_pool_admit(femstep_pool* p, const femstep_pool_mesh* mesh, long long steps, int* id) {
-    if (!p || !mesh || !id) return fail(p, FEMSTEP_EINVAL, "null argument");
-    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
-    const femstep_pool_mesh& m = *mesh;
-    const long long N = (long long)m.nodes, T = (long long)m.tets;
-    if (N == 0 || T == 0 || !m.position || !m.index) return fail(p, FEMSTEP_EINVAL, "empty mesh");
-    if (steps < 0) return fail(p, FEMSTEP_EINVAL, "negative step count");
-    if (!(m.density > 0.0)) return fail(p, FEMSTEP_EINVAL, "density must be positive");
-    if (!(m.youngs_modulus > 0.0) || !(m.poisson_ratio > -1.0 && m.poisson_ratio < 0.5))
-        return fail(p, FEMSTEP_EINVAL, "elastic constants out of range");
-    for (long long i = 0; i < T * 4; ++i)
-        if (m.index[i] >= (uint32_t)N) return fail(p, FEMSTEP_EINVAL, "tet index out of range");
-    int slot_id = -1;
-    for (int k = 0; k < p->max_meshes; ++k)
-        if (!p->meshes[k].used) {
-            slot_id = k;
-            break;
-        }
-    if (slot_id < 0) return fail(p, FEMSTEP_ENOMEM, "mesh table full");
-    const long long e_tiles = (T + kMinTile - 1) / kMinTile, n_tiles = (N + kMinTile - 1) / kMinTile;
-    const long long t0 = p->tets.take(T);
-    if (t0 < 0) return fail(p, FEMSTEP_ENOMEM, "no room for the tets now");
-    const long long n0 = p->nodes.take(N + 1);
-    if (n0 < 0) {
-        p->tets.give(t0, T);
-        return fail(p, FEMSTEP_ENOMEM, "no room for the nodes now");
-    }
-    const long long part0 = p->parts.take(e_tiles + n_tiles);
-    auto undo = [&]() {
-        p->tets.give(t0, T);
-        p->nodes.give(n0, N + 1);
-        if (part0 >= 0) p->parts.give(part0, e_tiles + n_tiles);
-    };
-    if (part0 < 0) {
-        undo();
-        return fail(p, FEMSTEP_ENOMEM, "no room for the energy partials now");
-    }
-    // host-side forms (while the GPU runs whatever is queued): FP64 rest state, CSR in
-    // the reference's order, slot map
-    std::vector<double> inv64, vol64, mass64;
-    fs::tet_rest_state64((size_t)N, (size_t)T, m.position, m.index, m.density, inv64, vol64, mass64);
-    double vmax = 0.0;
-    for (double v : vol64) vmax = std::max(vmax, v);
-    if (!(vmax > 0.0)) {
-        undo();
-        return fail(p, FEMSTEP_EINVAL, "every tet is degenerate");
-    }
-    std::vector<uint32_t> off, entry;
-    fs::build_csr((size_t)N, (size_t)T, 4, m.index, off, entry);
+    if (!id) return fail(p, FEMSTEP_EINVAL, "null argument");
+    int admitted = 0;
+    return admit_meshes(p, mesh, &steps, 1, id, &admitted);
+}
 
-    const size_t bytes = (size_t)T * (16 + 16 + 36 + 4) + (size_t)(N + 1) * (4 + 4 + 4 + 1 + 12) + sizeof(PoolMesh) +
-                         16 * 256;
-    cudaError_t err;
-    Staging::Buf* buf = p->staging.get(bytes, err);
-    if (!buf) {
-        undo();
-        return check(p, err, "pinned staging");
-    }
-    PoolDevice& d = p->d;
-    cudaStream_t st = p->stream;
-    auto stage = [&](size_t n) { return Staging::take(buf, n); };
-    auto send = [&](void* dst, const void* h, size_t n) { cudaMemcpyAsync(dst, h, n, cudaMemcpyHostToDevice, st); };
-
-    const long long s0 = 4 * t0;
-    uint4* idx4 = (uint4*)stage(T * sizeof(uint4));
-    uint4* slot4 = (uint4*)stage(T * sizeof(uint4));
-    {
-        std::vector<uint32_t> sl(T * 4);
-        for (long long n = 0; n < N; ++n)
-            for (uint32_t k = off[n]; k < off[n + 1]; ++k) sl[entry[k]] = (uint32_t)(s0 + k);
-        for (long long t = 0; t < T; ++t) {
-            idx4[t] = make_uint4((uint32_t)(n0 + m.index[t * 4]), (uint32_t)(n0 + m.index[t * 4 + 1]),
-                                 (uint32_t)(n0 + m.index[t * 4 + 2]), (uint32_t)(n0 + m.index[t * 4 + 3]));
-            slot4[t] = make_uint4(sl[t * 4], sl[t * 4 + 1], sl[t * 4 + 2], sl[t * 4 + 3]);
-        }
-    }
-    send(d.index + t0, idx4, T * sizeof(uint4));
-    send(d.slot + t0, slot4, T * sizeof(uint4));
-    float* inv = (float*)stage((size_t)T * 9 * 4);
-    for (int k = 0; k < 9; ++k) {
-        float* col = inv + (size_t)k * T;
-        for (long long t = 0; t < T; ++t) col[t] = (float)inv64[t * 9 + k];
-        send(d.rest_inv + (size_t)k * p->tet_cap + t0, col, T * 4);
-    }
-    float* vol = (float*)stage(T * 4);
-    for (long long t = 0; t < T; ++t) vol[t] = (float)vol64[t];
-    send(d.rest_vol + t0, vol, T * 4);
-    for (int k = 0; k < 7; ++k) {
-        cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
-        cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
-    }
-    uint32_t* offs = (uint32_t*)stage((N + 1) * 4);
-    for (long long n = 0; n <= N; ++n) offs[n] = (uint32_t)(s0 + off[n]);
-    send(d.offset + n0, offs, (N + 1) * 4);
-    float* mass = (float*)stage((N + 1) * 4);
-    float* imass = (float*)stage((N + 1) * 4);
-    uint8_t* fixed = (uint8_t*)stage(N + 1);
-    float* ext = (float*)stage((N + 1) * 12);
-    for (long long n = 0; n < N; ++n) {
-        mass[n] = (float)mass64[n];
-        imass[n] = mass64[n] > 0.0 ? (float)(1.0 / mass64[n]) : 0.0f;
-        fixed[n] = m.fixed && m.fixed[n] ? 1 : 0;
-        for (int k = 0; k < 3; ++k) ext[n * 3 + k] = m.external_force ? (float)m.external_force[n * 3 + k] : 0.0f;
-    }
-    mass[N] = imass[N] = 0.0f;
-    fixed[N] = 1;
-    ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
-    send(d.mass + n0, mass, (N + 1) * 4);
-    send(d.inv_mass + n0, imass, (N + 1) * 4);
-    send(d.fixed + n0, fixed, N + 1);
-    send(d.ext + n0 * 3, ext, (N + 1) * 12);
-    cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
-    cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
-    cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
-    cudaMemsetAsync(d.e_diss + part0, 0, e_tiles * 8, st);
-    cudaMemsetAsync(d.e_strain + part0, 0, e_tiles * 8, st);
-    cudaMemsetAsync(d.n_work + part0 + e_tiles, 0, n_tiles * 8, st);
-    cudaMemsetAsync(d.n_kin + part0 + e_tiles, 0, n_tiles * 8, st);
-    PoolMesh* pm = (PoolMesh*)stage(sizeof(PoolMesh));
-    std::memset(pm, 0, sizeof(PoolMesh));
-    const double E = m.youngs_modulus, nu = m.poisson_ratio;
-    // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
-    pm->mat = fs::make_j2f(E / (2.0 * (1.0 + nu)), E / (3.0 * (1.0 - 2.0 * nu)), m.yield_strength,
-                           m.hardening_modulus);
-    pm->dt64 = m.dt > 0.0 ? m.dt : 0.0;
-    pm->dt = (float)pm->dt64;
-    pm->gravity = (float)m.gravity;
-    pm->damping = (float)(m.damping > 0.0 ? m.damping : 1.0);
-    pm->ramp = m.ramp_steps;
-    pm->step = 0;
-    pm->target = steps;
-    pm->e_part = part0;
-    pm->n_part = part0 + e_tiles;
-    pm->serial = p->next_serial;
-    send(d.meshes + slot_id, pm, sizeof(PoolMesh));
-    // no step given: 0.9 x the FP64 element eigenvalue bound of the uploaded FP32 Dm^-1,
-    // computed and stored on the device behind the uploads
-    if (!(m.dt > 0.0))
-        fs::launch_pool_dt(d, slot_id, t0, T, E, nu, m.density, 0.9, p->d_block_max, p->d_out + 7, st);
-    Staging::submit(buf, st);
-    const int rc = check(p, cudaGetLastError(), "admit upload");
-    if (rc) {
-        undo();
-        return rc;
-    }
-    HostMesh& h = p->meshes[slot_id];
-    h.used = true;
-    h.t0 = t0;
-    h.T = T;
-    h.n0 = n0;
-    h.N = N;
-    h.e_part = part0;
-    h.n_part = part0 + e_tiles;
-    h.e_tiles = e_tiles;
-    h.n_tiles = n_tiles;
-    h.target = steps;
-    h.serial = p->next_serial++;
-    h.rest.assign(m.position, m.position + N * 3);
-    p->dirty = true;
-    *id = slot_id;
-    return FEMSTEP_OK;
+int femstep_pool_admit_many(femstep_pool* p, const femstep_pool_mesh* meshes, const long long* steps, int count,
+                            int* ids, int* admitted) {
+    if (admitted) *admitted = 0;
+    if (!admitted || (count > 0 && (!meshes || !steps || !ids))) return fail(p, FEMSTEP_EINVAL, "null argument");
+    return admit_meshes(p, meshes, steps, count, ids, admitted);
 }
 
 int femstep_pool_release(femstep_pool* p, int id) {

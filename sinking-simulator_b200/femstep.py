@@ -515,6 +515,8 @@ _pl_create = _sig("femstep_pool_create", C.c_int, [C.c_size_t, C.c_size_t, C.c_i
 _pl_bpt = _sig("femstep_pool_bytes_per_tet", C.c_size_t, [])
 _pl_bpn = _sig("femstep_pool_bytes_per_node", C.c_size_t, [])
 _pl_admit = _sig("femstep_pool_admit", C.c_int, [C.c_void_p, C.POINTER(PoolMeshC), C.c_longlong, C.POINTER(C.c_int)])
+_pl_admit_many = _sig("femstep_pool_admit_many", C.c_int, [C.c_void_p, C.POINTER(PoolMeshC), C.c_void_p, C.c_int,
+                                                           C.c_void_p, C.POINTER(C.c_int)])
 _pl_release = _sig("femstep_pool_release", C.c_int, [C.c_void_p, C.c_int])
 _pl_run_async = _sig("femstep_pool_run_async", C.c_int, [C.c_void_p, C.c_int, C.c_int])
 _pl_wait = _sig("femstep_pool_wait", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
@@ -576,20 +578,43 @@ class TetPool:
                 raise PoolFull(rc, (text or b"").decode(errors="replace"))
             _raise(rc, text)
 
-    def admit(self, position, index, steps, fixed=None, external_force=None, density=7850.0, youngs=210e9,
-              poisson=0.3, yield_strength=235e6, hardening=1e9, dt=0.0, gravity=0.0, damping=1.0,
-              ramp_steps=0) -> int:
-        """Admit a mesh for `steps` steps; raises PoolFull when it does not fit now."""
+    @staticmethod
+    def _mesh(keep, position, index, fixed=None, external_force=None, density=7850.0, youngs=210e9, poisson=0.3,
+              yield_strength=235e6, hardening=1e9, dt=0.0, gravity=0.0, damping=1.0, ramp_steps=0):
         pos = np.ascontiguousarray(position, np.float32).reshape(-1)
         idx = np.ascontiguousarray(index, np.uint32).reshape(-1)
         fx = None if fixed is None else np.ascontiguousarray(fixed, np.uint32).reshape(-1)
         fe = None if external_force is None else np.ascontiguousarray(external_force, np.float64).reshape(-1)
-        m = PoolMeshC(pos.size // 3, idx.size // 4, _p(pos), _p(idx), _p(fx), _p(fe), density, youngs, poisson,
-                      yield_strength, hardening, dt, gravity, damping, int(ramp_steps))
+        keep.extend([pos, idx, fx, fe])
+        return PoolMeshC(pos.size // 3, idx.size // 4, _p(pos), _p(idx), _p(fx), _p(fe), density, youngs, poisson,
+                         yield_strength, hardening, dt, gravity, damping, int(ramp_steps))
+
+    def admit(self, steps, **mesh) -> int:
+        """Admit a mesh for `steps` steps; raises PoolFull when it does not fit now.
+        mesh: position, index, fixed, external_force, density, youngs, poisson,
+        yield_strength, hardening, dt (0: the device bound), gravity, damping, ramp_steps."""
+        keep = []
+        m = self._mesh(keep, **mesh)
         out = C.c_int()
         self._check(_pl_admit(self._h, C.byref(m), int(steps), C.byref(out)))
-        self.sizes[out.value] = (pos.size // 3, idx.size // 4)
+        self.sizes[out.value] = (m.nodes, m.tets)
         return out.value
+
+    def admit_many(self, meshes, steps):
+        """Admit meshes (keyword dicts as for admit) in order while they fit; their host
+        work runs on all host cores.  Returns the ids of the admitted prefix."""
+        keep = []
+        arr = (PoolMeshC * max(1, len(meshes)))(*[self._mesh(keep, **m) for m in meshes])
+        st = np.ascontiguousarray(steps, np.int64)
+        ids = np.zeros(max(1, len(meshes)), np.int32)
+        n = C.c_int()
+        rc = _pl_admit_many(self._h, arr, _p(st), len(meshes), _p(ids), C.byref(n))
+        if rc and rc != ENOMEM:
+            self._check(rc)
+        out = [int(i) for i in ids[: n.value]]
+        for k, i in enumerate(out):
+            self.sizes[i] = (arr[k].nodes, arr[k].tets)
+        return out
 
     def release(self, mesh_id):
         self._check(_pl_release(self._h, int(mesh_id)))

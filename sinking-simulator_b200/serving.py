@@ -76,7 +76,7 @@ class Server:
     """
 
     def __init__(self, pool, chunk=64, clock=time.perf_counter, sleep=time.sleep, keep_results=False,
-                 full_error=Exception, max_tries=8):
+                 full_error=Exception, max_tries=8, batch=32):
         self.pool = pool
         self.chunk = int(chunk)
         self.clock = clock
@@ -84,12 +84,34 @@ class Server:
         self.keep_results = keep_results
         self.full_error = full_error
         self.max_tries = max_tries
+        self.batch = batch
 
     def _admit_queue(self, queue, live, now, report):
         """Admit queued requests in arrival order while they fit.  A request that does
         not fit stays queued; later, smaller ones may still go in (no head-of-line
-        blocking), up to `max_tries` failed admissions per chunk boundary."""
-        tries = 0
+        blocking), up to `max_tries` failed admissions per chunk boundary.  A pool with
+        admit_many takes the head of the queue in one call (its host work in parallel)."""
+        if queue and hasattr(self.pool, "admit_many"):
+            head = [queue.popleft() for _ in range(min(len(queue), self.batch))]
+            ids = self.pool.admit_many([r.build() for r in head], [r.steps for r in head])
+            t = now()
+            for r, i in zip(head, ids):
+                r.mesh_id, r.admitted = i, t
+                live[i] = r
+            rest = head[len(ids):]
+            if rest:
+                # the first of the rest did not fit: it keeps its place at the head; the
+                # others (and the rest of the queue) are tried one by one behind it
+                report.admit_retries += 1
+                others = collections.deque(rest[1:] + list(queue))
+                queue.clear()
+                self._admit_one_by_one(others, live, now, report, tries=1)
+                queue.append(rest[0])
+                queue.extend(others)
+            return
+        self._admit_one_by_one(queue, live, now, report)
+
+    def _admit_one_by_one(self, queue, live, now, report, tries=0):
         kept = collections.deque()
         while queue:
             r = queue.popleft()

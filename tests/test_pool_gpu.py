@@ -173,6 +173,33 @@ def test_admission_against_capacity(fem):
     assert e.value.code == fem.EINVAL
 
 
+def test_admit_many_is_admit_in_order(fem):
+    """admit_many (host work on all cores) gives the same pool as admitting one by one,
+    and admits the prefix that fits."""
+    meshes = [beam(fem, 12 + 2 * k, 2 + k % 2, 2, load=60e3 + 10e3 * k, clamp_end=k % 2) for k in range(6)]
+    kw = [dict(ramp_steps=100, **MATS[k % 3], **m) for k, m in enumerate(meshes)]
+    a = fem.TetPool(40000, 12000, max_meshes=8)
+    ia = [a.admit(steps=300, **k) for k in kw]
+    b = fem.TetPool(40000, 12000, max_meshes=8)
+    ib = b.admit_many(kw, [300] * len(kw))
+    assert ib == ia
+    a.run(300)
+    b.run(300)
+    for i in ia:
+        assert np.array_equal(a.readback(i)[0], b.readback(i)[0])
+        assert np.array_equal(a.energy(i), b.energy(i))
+    tets = [m["index"].size // 4 for m in meshes]
+    small = fem.TetPool(sum(tets[:3]) + 10, 12000, max_meshes=8)
+    got = small.admit_many(kw, [10] * len(kw))
+    assert got == [0, 1, 2]  # the rest did not fit now
+    bad = dict(kw[0])
+    bad["index"] = kw[0]["index"].copy()
+    bad["index"][0] = 99999
+    with pytest.raises(fem.FemStepError) as e:
+        b.admit_many([kw[1], bad], [1, 1])
+    assert e.value.code == fem.EINVAL and b.info()["meshes"] == len(ia)
+
+
 def test_device_critical_dt_matches_single_mesh_bound(fem):
     m = beam(fem, 20, 3, 3)
     pool = fem.TetPool(20000, 5000)

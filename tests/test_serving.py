@@ -62,6 +62,24 @@ class FakePool:
         return ("result", i)
 
 
+class FakeBatchPool(FakePool):
+    """The same, with the real pool's admit_many: the admitted prefix's ids."""
+
+    def admit_many(self, meshes, steps):
+        ids = []
+        for m, n in zip(meshes, steps):
+            try:
+                ids.append(self.admit(steps=n, **m))
+            except Full:
+                break
+        return ids
+
+
+@pytest.fixture(params=[FakePool, FakeBatchPool], ids=["admit", "admit_many"])
+def Pool(request):
+    return request.param
+
+
 class Clock:
     def __init__(self):
         self.t = 0.0
@@ -82,9 +100,9 @@ def events(pool, kind):
     return {e[1]: e[2] for e in pool.log if e[0] == kind}
 
 
-def test_all_requests_complete_and_work_is_accounted():
+def test_all_requests_complete_and_work_is_accounted(Pool):
     clock = Clock()
-    pool = FakePool(capacity=1000, clock=clock)
+    pool = Pool(capacity=1000, clock=clock)
     reqs = make_requests([(0.0, 300, 100), (0.01, 500, 64), (0.02, 400, 10), (0.5, 100, 1)])
     srv = S.Server(pool, chunk=16, clock=clock, sleep=clock.sleep, keep_results=True, full_error=Full)
     rep = srv.serve(reqs)
@@ -95,9 +113,9 @@ def test_all_requests_complete_and_work_is_accounted():
     assert pool.used == 0 and not pool.meshes
 
 
-def test_a_request_that_does_not_fit_waits_for_a_release():
+def test_a_request_that_does_not_fit_waits_for_a_release(Pool):
     clock = Clock()
-    pool = FakePool(capacity=1000, clock=clock)
+    pool = Pool(capacity=1000, clock=clock)
     # 600 + 500 > 1000: the second waits for the first to finish; the third (small)
     # goes in beside the first meanwhile (no head-of-line blocking)
     reqs = make_requests([(0.0, 600, 48), (0.001, 500, 16), (0.002, 300, 16)])
@@ -110,9 +128,9 @@ def test_a_request_that_does_not_fit_waits_for_a_release():
     assert admits[third.mesh_id] < releases[first.mesh_id]
 
 
-def test_arrivals_join_while_a_chunk_runs():
+def test_arrivals_join_while_a_chunk_runs(Pool):
     clock = Clock()
-    pool = FakePool(capacity=10_000, clock=clock, step_ms=1.0)
+    pool = Pool(capacity=10_000, clock=clock, step_ms=1.0)
     reqs = make_requests([(0.0, 100, 1000), (0.010, 100, 50), (0.020, 100, 50)])
     srv = S.Server(pool, chunk=32, clock=clock, sleep=clock.sleep, full_error=Full)
     rep = srv.serve(reqs)
@@ -126,9 +144,9 @@ def test_arrivals_join_while_a_chunk_runs():
     assert s["p50_step_ms"] == pytest.approx(1.0) and s["p99_step_ms"] == pytest.approx(1.0)
 
 
-def test_request_that_can_never_fit_is_reported():
+def test_request_that_can_never_fit_is_reported(Pool):
     clock = Clock()
-    pool = FakePool(capacity=100, clock=clock)
+    pool = Pool(capacity=100, clock=clock)
     srv = S.Server(pool, chunk=8, clock=clock, sleep=clock.sleep, full_error=Full)
     with pytest.raises(RuntimeError):
         srv.serve(make_requests([(0.0, 500, 10)]))
