@@ -383,12 +383,6 @@ void stage_layout(Placement& pl, size_t base) {
 // any host thread; touches nothing but the mesh's own staging.
 void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
     const long long N = pl.N, T = pl.T;
-    for (long long i = 0; i < T * 4; ++i)
-        if (m.index[i] >= (uint32_t)N) {
-            pl.status = FEMSTEP_EINVAL;
-            pl.what = "tet index out of range";
-            return;
-        }
     std::vector<double> inv64, vol64, mass64;
     fs::tet_rest_state64((size_t)N, (size_t)T, m.position, m.index, m.density, inv64, vol64, mass64);
     double vmax = 0.0;
@@ -471,6 +465,23 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
         if (!(m.density > 0.0)) return fail(p, FEMSTEP_EINVAL, "density must be positive");
         if (!(m.youngs_modulus > 0.0) || !(m.poisson_ratio > -1.0 && m.poisson_ratio < 0.5))
             return fail(p, FEMSTEP_EINVAL, "elastic constants out of range");
+    }
+    {
+        // node ids in range, before anything is placed: an invalid mesh is invalid
+        // whether or not it would fit
+        std::vector<long long> weight(count);
+        std::vector<char> bad(count, 0);
+        for (int i = 0; i < count; ++i) weight[i] = (long long)meshes[i].tets;
+        parallel_for(count, weight, [&](int i) {
+            const femstep_pool_mesh& m = meshes[i];
+            for (size_t k = 0; k < m.tets * 4; ++k)
+                if (m.index[k] >= (uint32_t)m.nodes) {
+                    bad[i] = 1;
+                    return;
+                }
+        });
+        for (int i = 0; i < count; ++i)
+            if (bad[i]) return fail(p, FEMSTEP_EINVAL, "tet index out of range");
     }
     // places, in order, while they fit
     std::vector<Placement> pl;
