@@ -494,17 +494,23 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
         t0 = time.perf_counter()
         p2 = F.TetPool(T, N + len(specs) + 1, max_meshes=len(specs) + 1)
         p2.set_schedule(tune["tile"], F.POOL_GRAPH if tune["mode"] == "graph" else F.POOL_PERSISTENT)
+        t1 = time.perf_counter()
         ids2 = p2.admit_many([b.admit_kwargs() for b in built], [args.steps] * len(built))
+        t2 = time.perf_counter()
         p2.run(args.steps)
+        t3 = time.perf_counter()
         d2h = 0
         for i in ids2:
             pp, vv = p2.readback(i)
             d2h += pp.nbytes + vv.nbytes
+        t4 = time.perf_counter()
         p2.close()
         wall = time.perf_counter() - t0
+        phases = {"create_s": t1 - t0, "admit_s": t2 - t1, "steps_s": t3 - t2, "readback_s": t4 - t3,
+                  "destroy_s": wall - (t4 - t0)}
         h2d = sum(b.position.nbytes + b.index.nbytes + b.fixed.nbytes + b.external_force.nbytes for b in built)
         e2e = {"value": T * args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-               "d2h_bytes_per_step": d2h / args.steps,
+               "d2h_bytes_per_step": d2h / args.steps, "phases": phases,
                "note": "create the pool, admit every mesh from host arrays (femstep_pool_admit_many: host rest "
                        "state on all cores + upload), K steps, read back every mesh's positions and velocities, "
                        "through the C ABI, wall clock"}

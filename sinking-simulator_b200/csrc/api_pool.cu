@@ -95,8 +95,11 @@ public:
             if (b.cap >= bytes && (!best || b.cap < best->cap)) best = &b;
         }
         if (!best) {
+            // capacities are powers of two (at least 4 MB), so buffers of one size class
+            // serve every later request of that class: a few buffers, reused
             Buf b;
-            b.cap = std::max<size_t>(bytes, size_t(4) << 20);
+            b.cap = size_t(4) << 20;
+            while (b.cap < bytes) b.cap <<= 1;
             err = cudaHostAlloc(&b.host, b.cap, cudaHostAllocDefault);
             if (err != cudaSuccess) return nullptr;
             err = cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
@@ -385,13 +388,6 @@ void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
     const long long N = pl.N, T = pl.T;
     std::vector<double> inv64, vol64, mass64;
     fs::tet_rest_state64((size_t)N, (size_t)T, m.position, m.index, m.density, inv64, vol64, mass64);
-    double vmax = 0.0;
-    for (double v : vol64) vmax = std::max(vmax, v);
-    if (!(vmax > 0.0)) {
-        pl.status = FEMSTEP_EINVAL;
-        pl.what = "every tet is degenerate";
-        return;
-    }
     std::vector<uint32_t> off, entry;
     fs::build_csr((size_t)N, (size_t)T, 4, m.index, off, entry);
     const long long s0 = 4 * pl.t0, n0 = pl.n0;
@@ -428,6 +424,23 @@ void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
     mass[N] = imass[N] = 0.0f;
     fixed[N] = 1;
     ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
+}
+
+// Whether some tet of the mesh has a non-zero volume (computeRestState's guard leaves
+// a degenerate tet without stiffness; a mesh of them only has no time step).
+bool any_volume(const femstep_pool_mesh& m) {
+    for (size_t t = 0; t < m.tets; ++t) {
+        const uint32_t* idx = &m.index[t * 4];
+        double a[3][3];
+        for (int c = 0; c < 3; ++c)
+            for (int r = 0; r < 3; ++r)
+                a[r][c] = (double)m.position[(size_t)idx[c + 1] * 3 + r] - (double)m.position[(size_t)idx[0] * 3 + r];
+        const double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+                           a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                           a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+        if (det != 0.0) return true;
+    }
+    return false;
 }
 
 // Run f(0..count-1) on the host's cores, largest work first (`weight`).
@@ -479,9 +492,12 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
                     bad[i] = 1;
                     return;
                 }
+            if (!any_volume(m)) bad[i] = 2;
         });
-        for (int i = 0; i < count; ++i)
-            if (bad[i]) return fail(p, FEMSTEP_EINVAL, "tet index out of range");
+        for (int i = 0; i < count; ++i) {
+            if (bad[i] == 1) return fail(p, FEMSTEP_EINVAL, "tet index out of range");
+            if (bad[i] == 2) return fail(p, FEMSTEP_EINVAL, "every tet is degenerate");
+        }
     }
     // places, in order, while they fit
     std::vector<Placement> pl;
@@ -528,80 +544,85 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
     };
     const int n = (int)pl.size();
     if (n == 0) return full ? fail(p, full, full_what) : FEMSTEP_OK;
-    size_t bytes = 0;
-    std::vector<long long> weight(n);
-    for (int i = 0; i < n; ++i) {
-        stage_layout(pl[i], bytes);
-        bytes = pl[i].end;
-        weight[i] = pl[i].T;
-    }
-    cudaError_t err;
-    Staging::Buf* buf = p->staging.get(bytes, err);
-    if (!buf) {
-        undo();
-        return check(p, err, "pinned staging");
-    }
-    char* stage = Staging::take(buf, bytes);
-    // the host work, on every core
-    parallel_for(n, weight, [&](int i) { prepare_mesh(meshes[i], pl[i], stage); });
-    for (int i = 0; i < n; ++i)
-        if (pl[i].status != FEMSTEP_OK) {
-            undo();
-            return fail(p, pl[i].status, pl[i].what);
-        }
-    // queue everything behind the work already on the stream
+    // Groups of at most kStageGroup staged bytes (a larger mesh is a group alone): each
+    // group is prepared on all cores into a pinned buffer and its copies queued, so a
+    // group's host work overlaps the uploads of the one before, and the pinned memory
+    // stays bounded (buffers are reused once their copies are done).
+    constexpr size_t kStageGroup = size_t(64) << 20;
     PoolDevice& d = p->d;
     cudaStream_t st = p->stream;
-    auto send = [&](void* dst, size_t off, size_t n) {
-        cudaMemcpyAsync(dst, stage + off, n, cudaMemcpyHostToDevice, st);
-    };
-    for (int i = 0; i < n; ++i) {
-        const femstep_pool_mesh& m = meshes[i];
-        const Placement& q = pl[i];
-        const long long T = q.T, N = q.N, t0 = q.t0, n0 = q.n0, part0 = q.part0;
-        send(d.index + t0, q.idx4, T * sizeof(uint4));
-        send(d.slot + t0, q.slot4, T * sizeof(uint4));
-        for (int k = 0; k < 9; ++k) send(d.rest_inv + (size_t)k * p->tet_cap + t0, q.inv + (size_t)k * T * 4, T * 4);
-        send(d.rest_vol + t0, q.vol, T * 4);
-        for (int k = 0; k < 7; ++k) {
-            cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
-            cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+    for (int g0 = 0; g0 < n;) {
+        int g1 = g0;
+        size_t bytes = 0;
+        while (g1 < n) {
+            stage_layout(pl[g1], bytes);
+            if (g1 > g0 && pl[g1].end > kStageGroup) break;
+            bytes = pl[g1].end;
+            ++g1;
         }
-        send(d.offset + n0, q.offs, (N + 1) * 4);
-        send(d.mass + n0, q.mass, (N + 1) * 4);
-        send(d.inv_mass + n0, q.imass, (N + 1) * 4);
-        send(d.fixed + n0, q.fixed, N + 1);
-        send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
-        cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
-        cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
-        cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
-        cudaMemsetAsync(d.e_diss + part0, 0, q.e_tiles * 8, st);
-        cudaMemsetAsync(d.e_strain + part0, 0, q.e_tiles * 8, st);
-        cudaMemsetAsync(d.n_work + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
-        cudaMemsetAsync(d.n_kin + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
-        PoolMesh* pm = (PoolMesh*)(stage + q.rec);
-        std::memset(pm, 0, sizeof(PoolMesh));
-        const double E = m.youngs_modulus, nu = m.poisson_ratio;
-        // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
-        pm->mat = fs::make_j2f(E / (2.0 * (1.0 + nu)), E / (3.0 * (1.0 - 2.0 * nu)), m.yield_strength,
-                               m.hardening_modulus);
-        pm->dt64 = m.dt > 0.0 ? m.dt : 0.0;
-        pm->dt = (float)pm->dt64;
-        pm->gravity = (float)m.gravity;
-        pm->damping = (float)(m.damping > 0.0 ? m.damping : 1.0);
-        pm->ramp = m.ramp_steps;
-        pm->step = 0;
-        pm->target = steps[i];
-        pm->e_part = part0;
-        pm->n_part = part0 + q.e_tiles;
-        pm->serial = p->next_serial + i;
-        send(d.meshes + q.id, q.rec, sizeof(PoolMesh));
-        // no step given: 0.9 x the FP64 element eigenvalue bound of the uploaded FP32
-        // Dm^-1, computed and stored on the device behind the uploads
-        if (!(m.dt > 0.0))
-            fs::launch_pool_dt(d, q.id, t0, T, E, nu, m.density, 0.9, p->d_block_max, p->d_out + 7, st);
+        std::vector<long long> weight(g1 - g0);
+        for (int i = g0; i < g1; ++i) weight[i - g0] = pl[i].T;
+        cudaError_t err;
+        Staging::Buf* buf = p->staging.get(bytes, err);
+        if (!buf) {
+            undo();  // earlier groups' copies went to ranges that are free again
+            return check(p, err, "pinned staging");
+        }
+        char* stage = Staging::take(buf, bytes);
+        parallel_for(g1 - g0, weight, [&](int k) { prepare_mesh(meshes[g0 + k], pl[g0 + k], stage); });
+        auto send = [&](void* dst, size_t off, size_t len) {
+            cudaMemcpyAsync(dst, stage + off, len, cudaMemcpyHostToDevice, st);
+        };
+        for (int i = g0; i < g1; ++i) {
+            const femstep_pool_mesh& m = meshes[i];
+            const Placement& q = pl[i];
+            const long long T = q.T, N = q.N, t0 = q.t0, n0 = q.n0, part0 = q.part0;
+            send(d.index + t0, q.idx4, T * sizeof(uint4));
+            send(d.slot + t0, q.slot4, T * sizeof(uint4));
+            for (int k = 0; k < 9; ++k)
+                send(d.rest_inv + (size_t)k * p->tet_cap + t0, q.inv + (size_t)k * T * 4, T * 4);
+            send(d.rest_vol + t0, q.vol, T * 4);
+            for (int k = 0; k < 7; ++k) {
+                cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+                cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
+            }
+            send(d.offset + n0, q.offs, (N + 1) * 4);
+            send(d.mass + n0, q.mass, (N + 1) * 4);
+            send(d.inv_mass + n0, q.imass, (N + 1) * 4);
+            send(d.fixed + n0, q.fixed, N + 1);
+            send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
+            cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
+            cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
+            cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
+            cudaMemsetAsync(d.e_diss + part0, 0, q.e_tiles * 8, st);
+            cudaMemsetAsync(d.e_strain + part0, 0, q.e_tiles * 8, st);
+            cudaMemsetAsync(d.n_work + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
+            cudaMemsetAsync(d.n_kin + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
+            PoolMesh* pm = (PoolMesh*)(stage + q.rec);
+            std::memset(pm, 0, sizeof(PoolMesh));
+            const double E = m.youngs_modulus, nu = m.poisson_ratio;
+            // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
+            pm->mat = fs::make_j2f(E / (2.0 * (1.0 + nu)), E / (3.0 * (1.0 - 2.0 * nu)), m.yield_strength,
+                                   m.hardening_modulus);
+            pm->dt64 = m.dt > 0.0 ? m.dt : 0.0;
+            pm->dt = (float)pm->dt64;
+            pm->gravity = (float)m.gravity;
+            pm->damping = (float)(m.damping > 0.0 ? m.damping : 1.0);
+            pm->ramp = m.ramp_steps;
+            pm->step = 0;
+            pm->target = steps[i];
+            pm->e_part = part0;
+            pm->n_part = part0 + q.e_tiles;
+            pm->serial = p->next_serial + i;
+            send(d.meshes + q.id, q.rec, sizeof(PoolMesh));
+            // no step given: 0.9 x the FP64 element eigenvalue bound of the uploaded FP32
+            // Dm^-1, computed and stored on the device behind the uploads
+            if (!(m.dt > 0.0))
+                fs::launch_pool_dt(d, q.id, t0, T, E, nu, m.density, 0.9, p->d_block_max, p->d_out + 7, st);
+        }
+        Staging::submit(buf, st);
+        g0 = g1;
     }
-    Staging::submit(buf, st);
     const int rc = check(p, cudaGetLastError(), "admit upload");
     if (rc) {
         undo();

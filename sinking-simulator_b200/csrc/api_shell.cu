@@ -333,9 +333,14 @@ int femstep_shell_readback(femstep_shell* s, double* position, double* velocity)
     std::vector<float> buf(n3);
     int rc = FEMSTEP_OK;
     if (position) {
+        // the compensated displacement u - c (c stays 0 without compensation)
+        std::vector<float> comp(n3);
         rc = check(s, cudaMemcpy(buf.data(), s->d.disp, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+        if (!rc)
+            rc = check(s, cudaMemcpy(comp.data(), s->d.disp_c, n3 * sizeof(float), cudaMemcpyDeviceToHost),
+                       "readback");
         if (rc) return rc;
-        for (size_t i = 0; i < n3; ++i) position[i] = s->rest[i] + (double)buf[i];
+        for (size_t i = 0; i < n3; ++i) position[i] = s->rest[i] + ((double)buf[i] - (double)comp[i]);
     }
     if (velocity) {
         rc = check(s, cudaMemcpy(buf.data(), s->d.velocity, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");

@@ -177,6 +177,20 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             dd[a][1] = d.disp[o + 1] - v0;
             dd[a][2] = d.disp[o + 2] - w0;
         }
+        if (KAHAN) {
+            // the compensated displacement u - c as a double-float: the differences above
+            // are exact (neighbouring values within a factor of two), and the difference
+            // of the compensations restores the low bits u alone has lost
+            const float c0 = d.disp_c[(size_t)nid[0] * 3], c1 = d.disp_c[(size_t)nid[0] * 3 + 1],
+                        c2 = d.disp_c[(size_t)nid[0] * 3 + 2];
+#pragma unroll
+            for (int a = 1; a < 8; ++a) {
+                const size_t o = (size_t)nid[a] * 3;
+                dd[a][0] -= d.disp_c[o] - c0;
+                dd[a][1] -= d.disp_c[o + 1] - c1;
+                dd[a][2] -= d.disp_c[o + 2] - c2;
+            }
+        }
     }
     // ---- rotation: H = (sum_a dN_a(0) (x) dd_a) J0^-1, R = I + Q ----
     float q[9];
