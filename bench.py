@@ -102,8 +102,12 @@ def shell_panel(nx, ny):
 # algorithmic bytes (each array counted once per launch; 4-byte ints)
 
 def tet_bytes(T, N, mode):
+    """Element pass: index 16, slot map 16, Dm^-1 36, volume 4, plastic state R/W 2 x 28
+    (and its compensation), four corner forces 4 x 12; per node the displacement (and
+    its compensation) read once.  Node pass: offsets 4, displacement (+ compensation)
+    R/W, velocity R/W 24, mass 4, 1/mass 4, flag 1, load 12; the corner forces read."""
     comp = 2 if mode == "f32k" else 1
-    elem = T * (16 + 16 + 36 + 4 + comp * 2 * 28 + 4 * 12) + N * 12
+    elem = T * (16 + 16 + 36 + 4 + comp * 2 * 28 + 4 * 12) + N * 12 * comp
     node = N * (4 + comp * 2 * 12 + 2 * 12 + 4 + 4 + 1 + 12) + T * 4 * 12
     return elem, node
 
@@ -176,6 +180,25 @@ class ClockSampler:
         reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
+
+
+def max_over_ranks(value, dist):
+    """The largest `value` over all ranks: a multi-GPU step takes as long as its slowest
+    rank.  The collective runs on the process group's own device (CUDA under NCCL, the
+    host under gloo)."""
+    if dist is None:
+        return value
+    import torch
+
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, steps, world, ms):
+    """Whole-job element-updates/s: every rank steps its own replica (weak scaling)."""
+    return units_per_rank * steps * world / (ms / 1e3)
 
 
 def measured_peak():
@@ -464,13 +487,8 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
         launches = pool.info()["launches"]
         barrier()
         time.sleep(0.25)
-    if dist is not None:
-        import torch
-
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = T * args.steps * world / (ms / 1e3)
+    ms = max_over_ranks(ms, dist)
+    value = job_rate(T, args.steps, world, ms)
     elem_ms, node_ms = pool.profile(5)
     eb = sum(tet_bytes(sp.tets, sp.nodes, "f32k")[0] for sp in specs)
     nb = sum(tet_bytes(sp.tets, sp.nodes, "f32k")[1] for sp in specs)
@@ -692,13 +710,8 @@ def main():
         launches = s.launches
         barrier()
         time.sleep(0.25)
-    if dist is not None:
-        import torch
-
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = w.units * args.steps * world / (ms / 1e3)
+    ms = max_over_ranks(ms, dist)
+    value = job_rate(w.units, args.steps, world, ms)
 
     # per-kernel device time for the roofline (outside the timed region)
     elem_ms, node_ms = s.profile(5, **w.kw)

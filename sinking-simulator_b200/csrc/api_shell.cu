@@ -58,10 +58,12 @@ int check(femstep_shell* s, cudaError_t e, const char* what) {
 ShellParams make_params(const femstep_shell_params& p) {
     ShellParams q{};
     const double E = p.youngs_modulus, nu = p.poisson_ratio;
-    q.dmu = E / (2.0 * (1.0 + nu));
-    q.dkappa = E / (3.0 * (1.0 - 2.0 * nu));
-    q.mu = (float)q.dmu;
-    q.kappa = (float)q.dkappa;
+    // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
+    const double mu = E / (2.0 * (1.0 + nu)), kappa = E / (3.0 * (1.0 - 2.0 * nu));
+    q.inv_2mu = 1.0 / (2.0 * mu);
+    q.inv_3kappa = 1.0 / (3.0 * kappa);
+    q.mu = (float)mu;
+    q.kappa = (float)kappa;
     q.yield = (float)p.yield_strength;
     q.hardening = (float)p.hardening_modulus;
     q.dt = (float)p.dt;

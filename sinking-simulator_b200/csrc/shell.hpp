@@ -66,7 +66,7 @@ struct ShellDevice {
 
 struct ShellParams {
     float mu, kappa, yield, hardening;   // J2 point law, linear isotropic hardening
-    double dmu, dkappa;                   // the same in double, for the energy account
+    double inv_2mu, inv_3kappa;           // 1 / (2 mu), 1 / (3 kappa) in double (energy account)
     float dt, damping;
     double dt64, rise_time;               // load factor min((step+1) dt / rise, 1)
     int max_iterations;                   // EAS Newton cap

@@ -134,10 +134,11 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
     for (int i = 3; i < 6; ++i) out[i] = 0.5f * a * g[i] - b * o.n[i];
 }
 
-// Blocks per SM the register budget is sized for: 3 (168 registers, 12 warps per SM)
-// measured 1.32x faster than 2 (177 registers, 8 warps) on the 2 M-element panel.
+// Blocks per SM the register budget is sized for.  On the 2 M-element panel: 2 (177
+// registers, 8 warps per SM) 6.0 ms; 3 (168, 12 warps, no spill) 4.61 ms; 4 (128, 16
+// warps, ~140 bytes of spill to L1) 4.43 ms; 5 (102, 20 warps, ~400 bytes) 4.60 ms.
 #ifndef FEMSTEP_SHELL_MINB
-#define FEMSTEP_SHELL_MINB 3
+#define FEMSTEP_SHELL_MINB 4
 #endif
 
 template <bool KAHAN>
@@ -219,8 +220,8 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
 #pragma unroll
             for (int j = 0; j < 3; ++j) q[i * 3 + j] = jd[i * 3] * j0[j] + jd[i * 3 + 1] * j0[3 + j] + jd[i * 3 + 2] * j0[6 + j];
         // Higham iteration to convergence in FP32 (the CPU runs it to 1e-16 in double,
-        // solid_shell.cpp:473-487): stop once a step moves Q by less than FP32 can see
-        // against |Q|, at most six iterations.
+        // solid_shell.cpp:473-487): stop once a step moves Q by no more than a few FP32
+        // ulps of |Q| (2^-21), at most six iterations.
 #pragma unroll 1
         for (int it = 0; it < 6; ++it) {
             float ipq[9], m[9];
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
                 size = fmaxf(size, fabsf(ipq[k]));
                 q[k] = ipq[k];
             }
-            if (step <= 1e-7f * size) break;
+            if (step <= 4.8e-7f * size) break;  // within ~4 ulps: only rounding left to move
         }
     }
     // ---- co-rotated relative displacement u'_a = Q^T dX_a + dd_a + Q^T dd_a ----
@@ -385,11 +386,11 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
                     float s = kaa[t];
 #pragma unroll
                     for (int k = 0; k < j; ++k) s -= l[i * (i + 1) / 2 + k] * l[j * (j + 1) / 2 + k];
-                    if (i == j) {
+                    if (i == j) {  // the diagonal is kept as its reciprocal
                         spd = spd && (s > 0.0f);
-                        l[t] = sqrtf(fmaxf(s, 1e-30f));
+                        l[t] = 1.0f / sqrtf(fmaxf(s, 1e-30f));
                     } else {
-                        l[t] = s / l[j * (j + 1) / 2 + j];
+                        l[t] = s * l[j * (j + 1) / 2 + j];
                     }
                     ++t;
                 }
@@ -408,20 +409,21 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             }
             spd = true;
         }
+        // L L^T delta = -r; the factor's diagonal holds 1 / l_ii
         float delta[7];
 #pragma unroll
         for (int i = 0; i < 7; ++i) {
             float s = -r[i];
 #pragma unroll
             for (int k = 0; k < i; ++k) s -= l[i * (i + 1) / 2 + k] * delta[k];
-            delta[i] = s / l[i * (i + 1) / 2 + i];
+            delta[i] = s * l[i * (i + 1) / 2 + i];
         }
 #pragma unroll
         for (int i = 6; i >= 0; --i) {
             float s = delta[i];
 #pragma unroll
             for (int k = i + 1; k < 7; ++k) s -= l[k * (k + 1) / 2 + i] * delta[k];
-            delta[i] = s / l[i * (i + 1) / 2 + i];
+            delta[i] = s * l[i * (i + 1) / 2 + i];
         }
         float work = 0.0f;
 #pragma unroll
@@ -464,12 +466,13 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         if (gp < 7) d.alpha[e * 8 + gp] = alpha[gp];
         const double s0 = o.sigma[0], s1 = o.sigma[1], s2 = o.sigma[2], s3 = o.sigma[3], s4 = o.sigma[4],
                      s5 = o.sigma[5];
-        const double pr = (s0 + s1 + s2) / 3.0;
-        double density = 0.5 * s0 * ((s0 - pr) / (2.0 * p.dmu) + pr / (3.0 * p.dkappa)) +
-                         0.5 * s1 * ((s1 - pr) / (2.0 * p.dmu) + pr / (3.0 * p.dkappa)) +
-                         0.5 * s2 * ((s2 - pr) / (2.0 * p.dmu) + pr / (3.0 * p.dkappa));
-        density += 0.5 * (s3 * s3 + s4 * s4 + s5 * s5) / p.dmu;
-        energy = (double)w * density;
+        // 1/2 sigma : C^-1 : sigma = 1/2 [s_dev : s_dev / (2 mu) + p tr(sigma) / (3 kappa)],
+        // p = tr(sigma) / 3, the engineering shears counted twice
+        const double tr = s0 + s1 + s2;
+        const double pr = tr * (1.0 / 3.0);
+        const double d0 = s0 - pr, d1 = s1 - pr, d2 = s2 - pr;
+        const double dev = d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (s3 * s3 + s4 * s4 + s5 * s5);
+        energy = (double)w * 0.5 * (dev * p.inv_2mu + pr * tr * p.inv_3kappa);
     }
 
     // ---- f = -R sum_g w_g B_g^T sigma_g, reduce-scattered so lane a holds node a ----
@@ -590,8 +593,9 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
 
 // The elastic K_aa = sum_g w_g G_g^T C G_g of every element, from the FP32 forms the
 // step uses, accumulated in double, and its Cholesky factor (packed lower triangle,
-// 28 of 32 floats per element).  A zero first entry marks an element whose elastic
-// K_aa is not positive definite; the step then forms K_aa itself.
+// 28 of 32 floats per element, each diagonal entry stored as its reciprocal, as the
+// step's own factorisation keeps it).  A zero first entry marks an element whose
+// elastic K_aa is not positive definite; the step then forms K_aa itself.
 __global__ void shell_elastic_factor(ShellDevice d, double lambda, double mu, float* out) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= d.elements) return;
@@ -639,6 +643,7 @@ __global__ void shell_elastic_factor(ShellDevice d, double lambda, double mu, fl
             ++t;
         }
     for (int k = 0; k < 28; ++k) l[k] = (float)ld[k];
+    for (int i = 0; i < 7; ++i) l[i * (i + 1) / 2 + i] = (float)(1.0 / ld[i * (i + 1) / 2 + i]);  // as the step keeps it
     l[28] = l[29] = l[30] = l[31] = 0.0f;
     if (!spd) l[0] = 0.0f;
     float4* o = reinterpret_cast<float4*>(out + e * 32);
