@@ -134,9 +134,10 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
     for (int i = 3; i < 6; ++i) out[i] = 0.5f * a * g[i] - b * o.n[i];
 }
 
-// Blocks per SM the register budget is sized for.  On the 2 M-element panel: 2 (177
-// registers, 8 warps per SM) 6.0 ms; 3 (168, 12 warps, no spill) 4.61 ms; 4 (128, 16
-// warps, ~140 bytes of spill to L1) 4.43 ms; 5 (102, 20 warps, ~400 bytes) 4.60 ms.
+// Blocks per SM the register budget is sized for.  On the 2 M-element panel: 3 (168
+// registers, 12 warps per SM, no spill) 4.61 ms per step and 1.32x faster than 2 (177
+// registers, 8 warps); 4 (128, 16 warps, ~140 bytes of spill to L1) 4.43 ms; 5 (102,
+// 20 warps, ~400 bytes of spill) 4.60 ms.
 #ifndef FEMSTEP_SHELL_MINB
 #define FEMSTEP_SHELL_MINB 4
 #endif
