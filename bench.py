@@ -443,7 +443,8 @@ def fixed_schedule(F, pool, spec):
     if not spec:
         return None
     tile, mode = spec.split(":")
-    pool.set_schedule(int(tile), F.POOL_GRAPH if mode == "graph" else F.POOL_PERSISTENT)
+    code = {v: k for k, v in F.POOL_MODE_NAMES.items()}[mode]
+    pool.set_schedule(int(tile), code)
     return {"tile": int(tile), "mode": mode, "ms_per_step": None, "set_by": "--schedule"}
 
 
@@ -511,7 +512,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
     if not args.no_e2e:
         t0 = time.perf_counter()
         p2 = F.TetPool(T, N + len(specs) + 1, max_meshes=len(specs) + 1)
-        p2.set_schedule(tune["tile"], F.POOL_GRAPH if tune["mode"] == "graph" else F.POOL_PERSISTENT)
+        p2.set_schedule(tune["tile"], {v: k for k, v in F.POOL_MODE_NAMES.items()}[tune["mode"]])
         t1 = time.perf_counter()
         ids2 = p2.admit_many([b.admit_kwargs() for b in built], [args.steps] * len(built))
         t2 = time.perf_counter()
@@ -656,7 +657,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="tet-batched: skip the one-mesh-at-a-time comparison")
     ap.add_argument("--schedule", default=None,
-                    help="pool workloads: TILE:graph|persistent instead of the autotuner (for profiling)")
+                    help="pool workloads: TILE:graph|persistent|graph-staged instead of the autotuner")
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--serve-chunk", type=int, default=64)
     args = ap.parse_args()

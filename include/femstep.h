@@ -180,6 +180,8 @@ typedef struct femstep_pool femstep_pool;
 #define FEMSTEP_POOL_AUTO 0        /* the pool's schedule (set by autotune or set_schedule) */
 #define FEMSTEP_POOL_GRAPH 1       /* two launches per step, replayed from a CUDA graph */
 #define FEMSTEP_POOL_PERSISTENT 2  /* one cooperative launch per chunk, grid barriers */
+#define FEMSTEP_POOL_GRAPH_STAGED 3 /* GRAPH, each tile's per-tet rows staged in shared memory by
+                                       bulk async copies (tiles of 128 and 256) */
 
 /* A pool holding up to `tet_capacity` tets and `node_capacity` nodes (each mesh also
    takes one spare node slot) of at most `max_meshes` meshes; tile = threads per block
@@ -222,11 +224,11 @@ int femstep_pool_plastic(femstep_pool *pool, int id, double *plastic);
 int femstep_pool_energy(femstep_pool *pool, int id, double out[4]);
 /* The time step a mesh runs with (its own, or the bound computed at admission). */
 int femstep_pool_dt(femstep_pool *pool, int id, double *dt);
-/* The autotuner: times every tile size in {128, 256, 512} with both schedules for
+/* The autotuner: times every tile size in {128, 256, 512} with every schedule for
    `steps` steps on the pool as it is, restores the pool's state after each trial (so
    tuning does not change any result), keeps the fastest, and reports it. */
 int femstep_pool_autotune(femstep_pool *pool, int steps, int *tile, int *mode, double *ms_per_step);
-/* Set the schedule by hand (tile 128 / 256 / 512; GRAPH or PERSISTENT). */
+/* Set the schedule by hand (tile 128 / 256 / 512; GRAPH, PERSISTENT or GRAPH_STAGED). */
 int femstep_pool_set_schedule(femstep_pool *pool, int tile, int mode);
 /* Mean device milliseconds per launch of [0] the element pass and [1] the node pass,
    over `steps` steps taken one launch at a time (the steps count as taken). */

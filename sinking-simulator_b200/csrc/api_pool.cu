@@ -168,6 +168,7 @@ struct femstep_pool {
     int* d_active = nullptr;
     double* d_block_max = nullptr;  // critical-dt scratch
     cudaGraphExec_t graph = nullptr;
+    bool graph_staged = false;  // which element pass the graph was captured with
     long long launches = 0;
     bool in_flight = false;
     bool broken = false;
@@ -244,6 +245,8 @@ int rebuild(femstep_pool* p) {
 
 int launch_chunk(femstep_pool* p, int steps, int mode) {
     if (steps <= 0 || p->d.n_etiles == 0) return FEMSTEP_OK;
+    const bool staged = mode == FEMSTEP_POOL_GRAPH_STAGED;
+    if (p->graph && p->graph_staged != staged) drop_graph(p);
     if (mode == FEMSTEP_POOL_PERSISTENT) {
         const int blocks = std::min(fs::pool_persistent_max_blocks(p->tile), p->d.n_etiles);
         if (blocks <= 0) return fail(p, FEMSTEP_ECUDA, "no co-resident blocks for the persistent launch");
@@ -258,12 +261,13 @@ int launch_chunk(femstep_pool* p, int steps, int mode) {
             cudaGraph_t g = nullptr;
             int rc = check(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "capture");
             if (rc) return rc;
-            fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream);
+            fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream, staged);
             rc = check(p, cudaStreamEndCapture(p->stream, &g), "capture end");
             if (rc) return rc;
             rc = check(p, cudaGraphInstantiate(&p->graph, g, 0), "graph instantiate");
             cudaGraphDestroy(g);
             if (rc) return rc;
+            p->graph_staged = staged;
         }
         for (; left >= kGraphSteps; left -= kGraphSteps) {
             const int rc = check(p, cudaGraphLaunch(p->graph, p->stream), "graph launch");
@@ -272,7 +276,7 @@ int launch_chunk(femstep_pool* p, int steps, int mode) {
         }
     }
     if (left > 0) {
-        fs::launch_pool_steps(p->d, p->tile, left, p->stream);
+        fs::launch_pool_steps(p->d, p->tile, left, p->stream, staged);
         p->launches += 2 * left + 1;
     }
     return check(p, cudaGetLastError(), "kernel launch");
@@ -666,6 +670,8 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
     const int dev = fs::device_status();
     if (dev != FEMSTEP_OK) return dev;
     femstep_pool* p = new femstep_pool();
+    // rows of 4-byte per-tet data start on 16-byte boundaries (bulk copies need them)
+    tet_capacity = (tet_capacity + 3) & ~size_t(3);
     p->tet_cap = (long long)tet_capacity;
     p->node_cap = (long long)node_capacity;
     p->max_meshes = max_meshes;
@@ -764,7 +770,8 @@ int femstep_pool_run_async(femstep_pool* p, int steps, int mode) {
     if (steps < 0) return fail(p, FEMSTEP_EINVAL, "negative step count");
     if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is already running: wait for it first");
     if (mode == FEMSTEP_POOL_AUTO) mode = p->mode;
-    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT) return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT && mode != FEMSTEP_POOL_GRAPH_STAGED)
+        return fail(p, FEMSTEP_EINVAL, "bad mode");
     int rc = rebuild(p);
     if (rc) return rc;
     p->launches = 0;
@@ -900,12 +907,13 @@ int femstep_pool_autotune(femstep_pool* p, int steps, int* tile_out, int* mode_o
     int rc = snapshot(p, snap, false);
     if (rc) return rc;
     const int tiles[3] = {128, 256, 512};
-    const int modes[2] = {FEMSTEP_POOL_GRAPH, FEMSTEP_POOL_PERSISTENT};
+    const int modes[3] = {FEMSTEP_POOL_GRAPH, FEMSTEP_POOL_PERSISTENT, FEMSTEP_POOL_GRAPH_STAGED};
     const int tile0 = p->tile, mode0 = p->mode;
     double best = INFINITY;
     int best_tile = tile0, best_mode = mode0;
     for (int ti = 0; ti < 3 && !rc; ++ti)
-        for (int mi = 0; mi < 2 && !rc; ++mi) {
+        for (int mi = 0; mi < 3 && !rc; ++mi) {
+            if (modes[mi] == FEMSTEP_POOL_GRAPH_STAGED && tiles[ti] == 512) continue;  // staged: 128, 256
             p->tile = tiles[ti];
             p->dirty = true;
             double ms = 0.0;
@@ -940,7 +948,10 @@ int femstep_pool_set_schedule(femstep_pool* p, int tile, int mode) {
     if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
     if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
     if (tile != 128 && tile != 256 && tile != 512) return fail(p, FEMSTEP_EINVAL, "tile must be 128, 256 or 512");
-    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT) return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT && mode != FEMSTEP_POOL_GRAPH_STAGED)
+        return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (mode == FEMSTEP_POOL_GRAPH_STAGED && tile == 512)
+        return fail(p, FEMSTEP_EINVAL, "the staged element pass runs tiles of 128 or 256");
     if (tile != p->tile) {
         // the instantaneous partials of the old tiling are stale
         cudaMemsetAsync(p->d.e_strain, 0, (size_t)p->part_cap * 8, p->stream);
@@ -963,7 +974,7 @@ int femstep_pool_profile(femstep_pool* p, int steps, double out[2]) {
     double te = 0.0, tn = 0.0;
     for (int s = 0; s < steps && !rc; ++s) {
         cudaEventRecord(ev[0], p->stream);
-        fs::launch_pool_element_pass(p->d, p->tile, s, p->stream);
+        fs::launch_pool_element_pass(p->d, p->tile, s, p->stream, p->mode == FEMSTEP_POOL_GRAPH_STAGED);
         cudaEventRecord(ev[1], p->stream);
         fs::launch_pool_node_pass(p->d, p->tile, s, p->stream);
         cudaEventRecord(ev[2], p->stream);

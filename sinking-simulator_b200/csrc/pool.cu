@@ -5,6 +5,7 @@
 // (its tiles do nothing) until the host retires it.  The energy partial of a tile goes
 // to the slot its mesh was given at admission, so nothing in a mesh's result depends
 // on what else is in the pool.
+#include "bulk.cuh"
 #include "common.cuh"
 #include "pool.hpp"
 #include "tet.hpp"
@@ -70,6 +71,70 @@ template <int B>
 __global__ void __launch_bounds__(B, 1024 / B) pool_elements(PoolDevice d, int sub, int wave) {
     __shared__ double scratch[64];
     element_tile<false>(d, blockIdx.x, sub, scratch, blockIdx.x + wave);
+}
+
+// The element pass with each tile's own rows staged in shared memory: one thread arms
+// an mbarrier and issues 19 bulk copies (node ids, slot map, 9 rows of Dm^-1, volume,
+// 7 rows of plastic state); the block then reads them from shared memory.  The 4-byte
+// rows are copied from the tile's first tet rounded down to a multiple of 4 (the pool's
+// row stride is a multiple of 4, so every copy starts on a 16-byte boundary) to its last
+// rounded up; the extra tets are never used.  The wait is bounded: a tile whose copies
+// do not land in time sets the pool's error flag, waits (bounded) for its copies to
+// finish, and is skipped.  B is 128 or 256 (static shared memory).
+constexpr uint32_t kStageWaitPolls = 1u << 22;
+
+template <int B>
+__global__ void __launch_bounds__(B, 1024 / B) pool_elements_staged(PoolDevice d, int sub, int wave) {
+    constexpr int kPitch = B + 4;
+    __shared__ double scratch[64];
+    __shared__ __align__(16) uint4 s_idx[B];
+    __shared__ __align__(16) uint4 s_slot[B];
+    __shared__ __align__(16) float s_rows[17 * kPitch];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_ok;
+    {
+        const int ahead = blockIdx.x + wave;
+        if (ahead < d.n_etiles) {
+            const PoolTile nx = d.etiles[ahead];
+            prefetch_tet_rows(element_refs(d), nx.begin, nx.end);
+        }
+    }
+    const PoolTile tl = d.etiles[blockIdx.x];
+    const PoolMesh& m = d.meshes[tl.mesh];
+    const bool live = m.step + sub < m.target;  // the same in every thread of the block
+    double diss = 0.0, energy = 0.0;
+    const long long first = tl.begin, n = tl.end - tl.begin;
+    const long long base = first & ~3LL, last4 = (tl.end + 3) & ~3LL;
+    if (live) {
+        if (threadIdx.x == 0) {
+            const uint32_t row_bytes = (uint32_t)((last4 - base) * 4);
+            mbar_init(&bar, 1);
+            mbar_arrive_expect_tx(&bar, 2u * (uint32_t)n * 16u + 17u * row_bytes);
+            bulk_copy_g2s(s_idx, d.index + first, (uint32_t)n * 16u, &bar);
+            bulk_copy_g2s(s_slot, d.slot + first, (uint32_t)n * 16u, &bar);
+            for (int k = 0; k < 9; ++k)
+                bulk_copy_g2s(s_rows + k * kPitch, d.rest_inv + (size_t)k * d.tet_cap + base, row_bytes, &bar);
+            bulk_copy_g2s(s_rows + 9 * kPitch, d.rest_vol + base, row_bytes, &bar);
+            for (int i = 0; i < 7; ++i)
+                bulk_copy_g2s(s_rows + (10 + i) * kPitch, d.plastic + (size_t)i * d.tet_cap + base, row_bytes, &bar);
+            bool ok = mbar_wait_bounded(&bar, 0, kStageWaitPolls);
+            if (!ok) {
+                atomicExch(d.error, 1);
+                mbar_wait_bounded(&bar, 0, kStageWaitPolls);  // let the copies in flight finish
+            }
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        const long long t = first + threadIdx.x;
+        if (s_ok && t < tl.end)
+            tet_element_f32<true, false, SharedRows>(element_refs(d), SharedRows{s_idx, s_slot, s_rows, kPitch, first, base},
+                                                     t, m.mat, diss, energy);
+    }
+    block_sum2(diss, energy, scratch);  // valid in thread 0
+    if (live && threadIdx.x == 0 && s_ok) {
+        d.e_diss[tl.part] += diss;
+        d.e_strain[tl.part] = energy;
+    }
 }
 
 template <int B>
@@ -140,9 +205,17 @@ __global__ void pool_set_dt(PoolMesh* meshes, int id, const double* w2, double s
 
 }  // namespace
 
-void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream) {
+void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream, bool staged) {
     if (!d.n_etiles) return;
     const int wave = sm_count() * (1024 / tile);
+    if (staged && tile == 128) {
+        pool_elements_staged<128><<<d.n_etiles, 128, 0, stream>>>(d, sub, wave);
+        return;
+    }
+    if (staged && tile == 256) {
+        pool_elements_staged<256><<<d.n_etiles, 256, 0, stream>>>(d, sub, wave);
+        return;
+    }
     switch (tile) {
         case 128: pool_elements<128><<<d.n_etiles, 128, 0, stream>>>(d, sub, wave); break;
         case 256: pool_elements<256><<<d.n_etiles, 256, 0, stream>>>(d, sub, wave); break;
@@ -159,10 +232,10 @@ void launch_pool_node_pass(const PoolDevice& d, int tile, int sub, cudaStream_t 
     }
 }
 
-void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream) {
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream, bool staged) {
     if (d.n_etiles == 0 || steps <= 0) return;
     for (int s = 0; s < steps; ++s) {
-        launch_pool_element_pass(d, tile, s, stream);
+        launch_pool_element_pass(d, tile, s, stream, staged);
         launch_pool_node_pass(d, tile, s, stream);
     }
     pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);

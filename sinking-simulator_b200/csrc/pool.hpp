@@ -80,10 +80,12 @@ struct PoolDevice {
 };
 
 // Two launches per step (element, node), `steps` times, then the advance, on `stream`.
-void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream);
+// staged: the element pass stages each tile's rows in shared memory by bulk async
+// copies (tiles of 128 and 256; a 512 tile runs the direct pass).
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream, bool staged);
 // The passes one at a time (per-kernel timing): element or node pass of sub-step
 // `sub`, and the advance by `steps`.
-void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream);
+void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream, bool staged);
 void launch_pool_node_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream);
 void launch_pool_advance(const PoolDevice& d, int steps, cudaStream_t stream);
 // One persistent cooperative launch for `steps` steps on `blocks` co-resident blocks,

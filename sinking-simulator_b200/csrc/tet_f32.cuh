@@ -147,12 +147,42 @@ __device__ __forceinline__ void prefetch_tet_rows(const TetElementRefs& d, long 
     prefetch_l2(reinterpret_cast<const char*>(base + begin) + ((long long)line << 7));
 }
 
+// Where a tet's own rows (node ids, slot map, Dm^-1, volume, plastic state) are read:
+// straight from global memory, or from a block's copy of its tile in shared memory.
+struct GlobalRows {
+    const TetElementRefs& d;
+    __device__ __forceinline__ uint4 index(long long t) const { return d.index[t]; }
+    __device__ __forceinline__ uint4 slot(long long t) const { return d.slot[t]; }
+    __device__ __forceinline__ float inv(int k, long long t) const { return d.rest_inv[(size_t)k * d.stride + t]; }
+    __device__ __forceinline__ float vol(long long t) const { return d.rest_vol[t]; }
+    __device__ __forceinline__ float plastic(int i, long long t) const { return d.plastic[(size_t)i * d.stride + t]; }
+};
+
+// A tile's rows in shared memory: index and slot map per tet from `first`, and 17
+// float rows (Dm^-1 0..8, volume 9, plastic state 10..16) of `pitch` floats each from
+// `base` (`first` rounded down to a multiple of 4, the 16-byte boundary of a row).
+struct SharedRows {
+    const uint4* idx;
+    const uint4* slt;
+    const float* rows;
+    int pitch;
+    long long first, base;
+    __device__ __forceinline__ uint4 index(long long t) const { return idx[t - first]; }
+    __device__ __forceinline__ uint4 slot(long long t) const { return slt[t - first]; }
+    __device__ __forceinline__ float inv(int k, long long t) const { return rows[k * pitch + (int)(t - base)]; }
+    __device__ __forceinline__ float vol(long long t) const { return rows[9 * pitch + (int)(t - base)]; }
+    __device__ __forceinline__ float plastic(int i, long long t) const {
+        return rows[(10 + i) * pitch + (int)(t - base)];
+    }
+};
+
 // One tet: forces into the node-major slots, plastic state advanced; returns the
-// dissipation and strain energy of the element (FP64, for the energy account).
-template <bool KAHAN, bool CG = false>
-__device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long long t, const J2f& m, double& diss,
-                                                double& energy) {
-    const uint4 idx = d.index[t];
+// dissipation and strain energy of the element (FP64, for the energy account).  The
+// arithmetic is the same whichever `Rows` supplies the tet's own rows.
+template <bool KAHAN, bool CG = false, class Rows = GlobalRows>
+__device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const Rows& rows, long long t, const J2f& m,
+                                                double& diss, double& energy) {
+    const uint4 idx = rows.index(t);
     const unsigned nid[4] = {idx.x, idx.y, idx.z, idx.w};
     float4 un[4], cn[4];
 #pragma unroll
@@ -174,7 +204,7 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
         }
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) dm_inv.m[k] = d.rest_inv[(size_t)k * d.stride + t];
+    for (int k = 0; k < 9; ++k) dm_inv.m[k] = rows.inv(k, t);
     const M3<float> h = mul_fma(du, dm_inv);  // displacement gradient
     // rotation deviation Q = R - I by the Higham iteration on F = I + H
     M3<float> q = h;
@@ -206,7 +236,7 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
     // form below, which the CPU's Newton reaches in one step.
     float ps[7], pc[7];
 #pragma unroll
-    for (int i = 0; i < 7; ++i) ps[i] = d.plastic[(size_t)i * d.stride + t];
+    for (int i = 0; i < 7; ++i) ps[i] = rows.plastic(i, t);
     if (KAHAN) {
 #pragma unroll
         for (int i = 0; i < 7; ++i) pc[i] = d.plastic_c[(size_t)i * d.stride + t];
@@ -269,7 +299,7 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
             sv[3 + i] = trial[3 + i];
         }
     }
-    const double vol = (double)d.rest_vol[t];
+    const double vol = (double)rows.vol(t);
     diss *= vol;
     {
         const double s0 = sv[0], s1 = sv[1], s2 = sv[2], s3 = sv[3], s4 = sv[4], s5 = sv[5];
@@ -293,8 +323,8 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
 #pragma unroll
     for (int k = 0; k < 9; ++k) sig.m[k] += qs.m[k];
     const M3<float> hf = mul_fma(sig, transpose(dm_inv));
-    const float scale = -d.rest_vol[t];
-    const uint4 sl = d.slot[t];
+    const float scale = -rows.vol(t);
+    const uint4 sl = rows.slot(t);
     const unsigned sid[4] = {sl.x, sl.y, sl.z, sl.w};
     float f0[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -308,6 +338,12 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long lo
         d.slots[sid[c + 1]] = make_float4(v[0], v[1], v[2], 0.0f);  // one 16-byte store
     }
     d.slots[sid[0]] = make_float4(f0[0], f0[1], f0[2], 0.0f);
+}
+
+template <bool KAHAN, bool CG = false>
+__device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, long long t, const J2f& m, double& diss,
+                                                double& energy) {
+    tet_element_f32<KAHAN, CG, GlobalRows>(d, GlobalRows{d}, t, m, diss, energy);
 }
 
 struct TetNodeRefs {

@@ -500,7 +500,8 @@ def stiffened_panel(nx=2000, ny=1000, lx=20.0, ly=10.0, thickness=0.012, stiffen
 # Pool of many tet meshes: the batched and the served step (no reference counterpart:
 # the reference steps one mesh at a time, fem.cpp:187).
 
-POOL_AUTO, POOL_GRAPH, POOL_PERSISTENT = 0, 1, 2
+POOL_AUTO, POOL_GRAPH, POOL_PERSISTENT, POOL_GRAPH_STAGED = 0, 1, 2, 3
+POOL_MODE_NAMES = {POOL_GRAPH: "graph", POOL_PERSISTENT: "persistent", POOL_GRAPH_STAGED: "graph-staged"}
 
 
 class PoolMeshC(C.Structure):
@@ -671,8 +672,7 @@ class TetPool:
     def autotune(self, steps=32):
         tile, mode, ms = C.c_int(), C.c_int(), C.c_double()
         self._check(_pl_autotune(self._h, int(steps), C.byref(tile), C.byref(mode), C.byref(ms)))
-        return {"tile": tile.value, "mode": "graph" if mode.value == POOL_GRAPH else "persistent",
-                "ms_per_step": ms.value}
+        return {"tile": tile.value, "mode": POOL_MODE_NAMES[mode.value], "ms_per_step": ms.value}
 
     def set_schedule(self, tile, mode):
         self._check(_pl_schedule(self._h, int(tile), int(mode)))

@@ -54,7 +54,7 @@ def test_pool_mesh_bit_identical_to_single_mesh_step(fem):
               beam(fem, 40, 4, 4, load=250e3)]
     dts = [crit(fem, m) for m in meshes]
     steps = [1200, 937, 1201]
-    for mode in (fem.POOL_GRAPH, fem.POOL_PERSISTENT):
+    for mode in (fem.POOL_GRAPH, fem.POOL_PERSISTENT, fem.POOL_GRAPH_STAGED):
         pool = fem.TetPool(200000, 50000, max_meshes=8)
         ids = [pool.admit(steps=steps[k], dt=dts[k], ramp_steps=400, **MATS[k], **meshes[k]) for k in range(3)]
         # uneven chunks, more steps than some meshes want
@@ -91,8 +91,8 @@ def test_result_is_the_same_alone_and_in_the_mix(fem):
     mix.run(50, fem.POOL_PERSISTENT)
     ib = mix.admit(steps=1500, ramp_steps=500, **MATS[0], **a)  # mid-run
     assert mix.dt(ib) == alone.dt(ia)
-    for chunk in (3, 64, 200, 133, 1100):
-        mix.run(chunk, fem.POOL_GRAPH if chunk % 2 else fem.POOL_PERSISTENT)
+    for k, chunk in enumerate((3, 64, 200, 133, 1100)):
+        mix.run(chunk, (fem.POOL_GRAPH, fem.POOL_PERSISTENT, fem.POOL_GRAPH_STAGED)[k % 3])
     assert mix.status(ib)[0] == 1500
     pb, vb = mix.readback(ib)
     assert np.array_equal(pa, pb) and np.array_equal(va, vb)
@@ -128,10 +128,11 @@ def test_async_admission_behind_a_running_chunk(fem):
 def test_tile_sizes_and_autotune_leave_results_unchanged(fem):
     m = beam(fem, 36, 3, 3, load=170e3)
     base = None
-    for tile in (128, 256, 512):
+    for tile, mode in ((128, fem.POOL_GRAPH), (256, fem.POOL_GRAPH), (512, fem.POOL_GRAPH),
+                       (128, fem.POOL_GRAPH_STAGED), (256, fem.POOL_GRAPH_STAGED), (512, fem.POOL_PERSISTENT)):
         pool = fem.TetPool(50000, 15000, max_meshes=2, tile=tile)
         i = pool.admit(steps=300, ramp_steps=150, **MATS[0], **m)
-        pool.run(300)
+        pool.run(300, mode)
         p, v = pool.readback(i)
         e = pool.energy(i)
         if base is None:
@@ -139,6 +140,8 @@ def test_tile_sizes_and_autotune_leave_results_unchanged(fem):
         else:
             assert np.array_equal(p, base[0]) and np.array_equal(v, base[1])
             assert np.allclose(e, base[2], rtol=1e-12, atol=0.0)
+            if tile == 128:
+                assert np.array_equal(e, base[2])  # the same tiles: the same energy bits
         pool.close()
     pool = fem.TetPool(50000, 15000, max_meshes=2)
     i = pool.admit(steps=300, ramp_steps=150, **MATS[0], **m)
