@@ -267,6 +267,20 @@ typedef struct {
     double density;                 /* kg/m^3, for the lumped mass when mass is NULL */
 } femstep_shell_mesh;
 
+/* The general point law (plasticity::update, engine/sim/plasticity.cpp:319-505): the
+   flow curve (plasticity.hpp:112-128), kinematic hardening and the ductile damage law
+   (plasticity.hpp:193-199).  Each element's failure strain comes from the state handed
+   to femstep_shell_create (ElementPlasticState::failureStrain; +inf without one). */
+#define FEMSTEP_SHELL_LINEAR 0
+#define FEMSTEP_SHELL_SWIFT 1
+typedef struct {
+    int hardening;                 /* FEMSTEP_SHELL_LINEAR (yield_strength, hardening_modulus of
+                                      femstep_shell_params) or FEMSTEP_SHELL_SWIFT: K (eps0 + p)^n */
+    double strength_coefficient, reference_strain, hardening_exponent;  /* Swift K, eps0, n */
+    double kinematic_modulus;      /* back-stress modulus, Pa */
+    double triaxiality_sensitivity, reference_triaxiality, cutoff_triaxiality;  /* Failure */
+} femstep_shell_material;
+
 typedef struct {
     double youngs_modulus, poisson_ratio;      /* plasticity::Material (plasticity.hpp:220-228) */
     double yield_strength, hardening_modulus;  /* linear curve (plasticity.hpp:115-118) */
@@ -275,6 +289,10 @@ typedef struct {
     int max_iterations;                        /* EAS Newton cap (CPU: 40) */
     double tol_residual, tol_work;             /* Newton stops on ||r|| or |delta.r| below tol * sigma_y V */
     int compensated;                           /* 1: Kahan-compensated displacement and plastic strain */
+    const femstep_shell_material *material;    /* NULL: the linear law, no back stress, no damage;
+                                                  else the general law and the element failure rules
+                                                  (no enhanced modes after a point fails, one retry
+                                                  without them, torn when all eight points have) */
 } femstep_shell_params;
 
 typedef struct femstep_shell femstep_shell;
@@ -293,6 +311,17 @@ int femstep_shell_state(femstep_shell *solver, double *state);
 /* [0] external work [1] plastic dissipation [2] strain energy [3] kinetic, FP64 reduced
    on the device in fixed order (zone::Solver::accumulateEnergy, zone.cpp:1014-1044). */
 int femstep_shell_energy(femstep_shell *solver, double out[4]);
+/* The punch of zone::Solver::step (engine/sim/zone.cpp:1150-1198) as the reference's GPU
+   zone step drives it (engine/gpu/shaders/solidshell_integrate.comp, zone_gpu.cpp:889-919):
+   every step each node in `driven` has its velocity along `axis` set to -speed, after the
+   force update and the damping; the speed rises linearly over ramp_time seconds from the
+   time the punch is set.  The impulse it takes is the punch's work, summed in FP64 in a
+   fixed order (the shader used a fixed-point atomic).  count 0 removes the punch. */
+int femstep_shell_set_punch(femstep_shell *solver, const uint32_t *driven, size_t count, const double axis[3],
+                            double speed, double ramp_time);
+/* [0] punch work (J) [1] penetration (m) [2] time (s) [3] steps since the punch was set:
+   ZoneGpuState::work / penetration / time / steps (zone_gpu.hpp:116-126). */
+int femstep_shell_punch_state(femstep_shell *solver, double out[4]);
 /* [0] element-steps whose EAS Newton hit its cap, [1] yielded Gauss points last step. */
 int femstep_shell_stats(femstep_shell *solver, long long out[2]);
 /* Smallest element critical step, FP64 power iteration per element on the device

@@ -1509,6 +1509,25 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
                 work += ext * m->velocity[d] * p->dt;
             }
         }
+        /* the prescribed punch, after the damping and before the positions (zone.cpp:1150-1198):
+         * each gripped node moves at -speed along the axis; the impulse that takes is the
+         * resisting force, its work -impulse * speed.  The speed ramps from the time at the
+         * start of the step. */
+        if (m->driven) {
+            const double t0 = (double)m->step * p->dt;
+            double speed = p->punch_speed;
+            if (p->punch_ramp > 0 && t0 < p->punch_ramp) speed = p->punch_speed * (t0 / p->punch_ramp);
+            double impulse = 0.0;
+            for (size_t node = 0; node < m->nodes; ++node) {
+                if (!m->driven[node]) continue;
+                double *v = &m->velocity[node * 3];
+                const double along = v[0] * m->axis[0] + v[1] * m->axis[1] + v[2] * m->axis[2];
+                const double change = -speed - along;
+                for (int k = 0; k < 3; ++k) v[k] += change * m->axis[k];
+                impulse += m->mass[node] * change;
+            }
+            m->energy[4] += -impulse * speed;
+        }
         for (size_t d = 0; d < m->nodes * 3; ++d) m->position[d] += m->velocity[d] * p->dt;
         m->energy[0] += work;
         m->energy[1] += dissipation;

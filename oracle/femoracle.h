@@ -175,13 +175,17 @@ typedef struct {
     uint32_t *adj_offset;     /* N+1 */
     uint32_t *adj_entry;      /* 8E  */
     double *fext;             /* 3N load at full amplitude, or NULL */
-    double energy[5];         /* work, dissipation, strain, kinetic, unused */
+    double energy[5];         /* work, dissipation, strain, kinetic, punch work */
     long step;
+    uint8_t *driven;          /* N: 1 for a node the punch grips, or NULL (no punch) */
+    double axis[3];           /* the punch travels along -axis */
 } or_shell;
 
 typedef struct {
     double dt, damping;
     double rise_time;         /* load factor min(t / rise_time, 1), t = (step+1) dt */
+    double punch_speed;       /* the prescribed punch (zone.cpp:1150-1198) */
+    double punch_ramp;        /* s over which its speed rises linearly from rest */
 } or_shell_params;
 
 void or_shell_setup(or_shell *m, const double *mat, double density);

@@ -74,11 +74,13 @@ class Shell(C.Structure):
                 ("element_force", C.POINTER(C.c_double)), ("stress", C.POINTER(C.c_double)),
                 ("gauss_volume", C.POINTER(C.c_double)), ("adj_offset", C.POINTER(C.c_uint32)),
                 ("adj_entry", C.POINTER(C.c_uint32)), ("fext", C.POINTER(C.c_double)),
-                ("energy", C.c_double * 5), ("step", C.c_long)]
+                ("energy", C.c_double * 5), ("step", C.c_long), ("driven", C.POINTER(C.c_uint8)),
+                ("axis", C.c_double * 3)]
 
 
 class ShellParams(C.Structure):
-    _fields_ = [("dt", C.c_double), ("damping", C.c_double), ("rise_time", C.c_double)]
+    _fields_ = [("dt", C.c_double), ("damping", C.c_double), ("rise_time", C.c_double),
+                ("punch_speed", C.c_double), ("punch_ramp", C.c_double)]
 
 
 def build_port() -> str:
@@ -321,8 +323,20 @@ class ShellModel:
     def steps(self):
         return self._s.step
 
-    def step(self, dt, steps, damping=1.0, rise_time=0.0):
-        p = ShellParams(dt, damping, rise_time)
+    def set_punch(self, driven_nodes, axis):
+        """The prescribed punch (zone.cpp:1150-1198) grips these nodes and travels along -axis."""
+        self.driven = np.zeros(self.nodes, np.uint8)
+        self.driven[np.asarray(driven_nodes, np.int64)] = 1
+        self._s.driven = _ptr(self.driven, C.c_uint8)
+        for k in range(3):
+            self._s.axis[k] = float(axis[k])
+
+    @property
+    def punch_work(self):
+        return self._s.energy[4]
+
+    def step(self, dt, steps, damping=1.0, rise_time=0.0, punch_speed=0.0, punch_ramp=0.0):
+        p = ShellParams(dt, damping, rise_time, punch_speed, punch_ramp)
         self.o.shell_step(C.byref(self._s), self.mat, C.byref(p), steps)
 
     def compute_energy(self):
@@ -330,5 +344,5 @@ class ShellModel:
         return self.energy
 
     def time_parallel(self, dt, steps, workers=0, rise_time=0.0):
-        p = ShellParams(dt, 1.0, rise_time)
+        p = ShellParams(dt, 1.0, rise_time, 0.0, 0.0)
         return self.o.shell_time_parallel(C.byref(self._s), self.mat, C.byref(p), steps, workers)

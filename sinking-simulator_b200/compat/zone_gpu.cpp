@@ -1,0 +1,214 @@
+// compat/zone_gpu.cpp -- gpu::ZoneGpuSolver over libfemstep.so (see engine/gpu/zone_gpu.hpp
+// in this directory).
+#include "engine/gpu/zone_gpu.hpp"
+
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "femstep.h"
+
+namespace gpu {
+
+namespace {
+
+// ElementPlasticState <-> the 129 doubles of femstep_shell_state (zone_gpu.cpp:36-40).
+void pack(const sim::solidshell::ElementPlasticState& s, double* x) {
+    for (int gp = 0; gp < sim::solidshell::kGauss; ++gp) {
+        const sim::plasticity::State& p = s.point[gp];
+        double* y = x + gp * 15;
+        for (int i = 0; i < 6; ++i) {
+            y[i] = p.plasticStrain[i];
+            y[6 + i] = p.backStress[i];
+        }
+        y[12] = p.equivalentPlasticStrain;
+        y[13] = p.damage;
+        y[14] = p.failed ? 1.0 : 0.0;
+    }
+    for (int k = 0; k < sim::solidshell::kEas; ++k) x[120 + k] = s.enhanced[k];
+    x[127] = s.failureStrain;
+    x[128] = s.torn ? 1.0 : 0.0;
+}
+
+void unpack(const double* x, sim::solidshell::ElementPlasticState& s) {
+    for (int gp = 0; gp < sim::solidshell::kGauss; ++gp) {
+        sim::plasticity::State& p = s.point[gp];
+        const double* y = x + gp * 15;
+        for (int i = 0; i < 6; ++i) {
+            p.plasticStrain[i] = y[i];
+            p.backStress[i] = y[6 + i];
+        }
+        p.equivalentPlasticStrain = y[12];
+        p.damage = y[13];
+        p.failed = y[14] != 0.0;
+    }
+    for (int k = 0; k < sim::solidshell::kEas; ++k) s.enhanced[k] = x[120 + k];
+    s.failureStrain = x[127];
+    s.torn = x[128] != 0.0;
+}
+
+}  // namespace
+
+struct ZoneGpuSolver::Impl {
+    femstep_shell* handle = nullptr;
+    femstep_shell_params params{};
+    femstep_shell_material material{};
+    std::size_t nodes = 0, elements = 0;
+};
+
+std::string describeElementPipelines(const std::string& /*shaderDirectory*/) {
+    return "libfemstep.so shell_forces: one element per 8 lanes of a warp (lane = Gauss point), FP32 with "
+           "Kahan-compensated displacement and plastic strain, FP64 energy partials; the same kernel for both "
+           "mappings (ptxas reports its registers and spills at build time)\n";
+}
+
+ZoneGpuSolver::~ZoneGpuSolver() {
+    if (impl_) femstep_shell_destroy(impl_->handle);
+    delete impl_;
+}
+
+bool ZoneGpuSolver::initialise(const sim::zone::Patch& patch, const sim::zone::Solver& cpu,
+                               const sim::plasticity::Material& material, const sim::zone::SolveParams& params,
+                               const std::string& /*shaderDirectory*/, std::string& error, Mapping mapping,
+                               EasPrecision eas) {
+    // the reference's own refusals (zone_gpu.cpp:500-517)
+    if (cpu.restForms().size() != patch.elementCount()) {
+        error = "the CPU solver was built without SolveParams::cacheRestForms, so there is nothing to upload";
+        return false;
+    }
+    if (!params.plastic) {
+        error = "the GPU path implements the elastoplastic element only";
+        return false;
+    }
+    if (eas != EasPrecision::Float && mapping != Mapping::Workgroup) {
+        error = "the fp64 enhanced-strain variants are compiled for the workgroup mapping only; the one-invocation "
+                "kernel is float throughout";
+        return false;
+    }
+    if (eas != EasPrecision::Float && eas != EasPrecision::FloatTight) {
+        error = "the fp64 enhanced-strain variants are not built: the element runs in FP32 with Kahan-compensated "
+                "state";
+        return false;
+    }
+    if (impl_) femstep_shell_destroy(impl_->handle);
+    delete impl_;
+    impl_ = new Impl();
+    device_ = nullptr;
+    Impl& d = *impl_;
+    const std::size_t N = patch.nodeCount(), E = patch.elementCount();
+    d.nodes = N;
+    d.elements = E;
+
+    // rest forms in zone_gpu.cpp's order: B [8][6][24], G [8][6][7], w [8], J0^-1 [9]
+    std::vector<double> forms(E * 1505);
+    for (std::size_t e = 0; e < E; ++e) {
+        const sim::solidshell::RestForms& f = cpu.restForms()[e];
+        double* x = forms.data() + e * 1505;
+        for (int gp = 0; gp < 8; ++gp)
+            for (int i = 0; i < 6; ++i) {
+                for (int c = 0; c < 24; ++c) x[(gp * 6 + i) * 24 + c] = f.b[gp][i][c];
+                for (int k = 0; k < 7; ++k) x[1152 + (gp * 6 + i) * 7 + k] = f.g[gp][i][k];
+            }
+        for (int gp = 0; gp < 8; ++gp) x[1488 + gp] = f.weight[gp];
+        for (int k = 0; k < 9; ++k) x[1496 + k] = f.restJacobianInverse[k];
+    }
+    std::vector<double> state(E * 129);
+    for (std::size_t e = 0; e < E; ++e) pack(cpu.elementState()[e], state.data() + e * 129);
+    const std::vector<uint32_t> index(patch.mesh.index.begin(), patch.mesh.index.end());
+
+    femstep_shell_mesh m{};
+    m.nodes = N;
+    m.elements = E;
+    m.rest = cpu.rest().data();
+    m.position = cpu.position().data();
+    m.velocity = cpu.velocity().data();
+    m.index = index.data();
+    m.pinned = cpu.pinnedDof().data();
+    m.load = nullptr;
+    m.forms = forms.data();
+    m.mass = cpu.nodalMass().data();
+    m.state = state.data();
+    m.adjacency_offset = cpu.adjacencyOffset().data();
+    m.adjacency_entry = cpu.adjacencyEntry().data();
+    m.density = 0.0;
+    if (femstep_shell_create(&m, &d.handle) != FEMSTEP_OK) {
+        error = femstep_last_error();
+        d.handle = nullptr;
+        return false;
+    }
+
+    // the point law
+    const sim::plasticity::FlowCurve& flow = material.flow;
+    d.material.hardening = flow.kind == sim::plasticity::Hardening::Swift ? FEMSTEP_SHELL_SWIFT : FEMSTEP_SHELL_LINEAR;
+    d.material.strength_coefficient = flow.strengthCoefficient;
+    d.material.reference_strain = flow.referenceStrain;
+    d.material.hardening_exponent = flow.hardeningExponent;
+    d.material.kinematic_modulus = flow.kinematicModulus;
+    d.material.triaxiality_sensitivity = material.failure.triaxialitySensitivity;
+    d.material.reference_triaxiality = material.failure.referenceTriaxiality;
+    d.material.cutoff_triaxiality = material.failure.cutoffTriaxiality;
+    femstep_shell_params& p = d.params;
+    p.youngs_modulus = material.youngsModulus;
+    p.poisson_ratio = material.poissonRatio;
+    p.yield_strength = flow.yieldStrength;
+    p.hardening_modulus = flow.hardeningModulus;
+    // SolveParams::timestep, or the patch's critical step at timestepSafety (zone_gpu.cpp:526-527)
+    p.dt = params.timestep > 0 ? params.timestep : patch.criticalTimestep * (params.timestepSafety / 0.9);
+    p.damping = params.damping;
+    p.rise_time = 0.0;
+    p.max_iterations = eas == EasPrecision::FloatTight ? 40 : 12;
+    p.tol_residual = eas == EasPrecision::FloatTight ? 1e-6 : 5e-5;
+    p.tol_work = eas == EasPrecision::FloatTight ? 1e-16 : 1e-13;
+    p.compensated = 1;
+    p.material = &d.material;
+
+    // the punch: the CPU solver's driven nodes, along -axis
+    const std::vector<uint32_t> driven(cpu.drivenNodes().begin(), cpu.drivenNodes().end());
+    const double axis[3] = {patch.axis.x, patch.axis.y, patch.axis.z};
+    if (femstep_shell_set_punch(d.handle, driven.data(), driven.size(), axis, params.indenter.speed,
+                                params.indenter.rampTime) != FEMSTEP_OK) {
+        error = femstep_shell_error(d.handle);
+        return false;
+    }
+    char name[256] = {0};
+    if (femstep_device_name(name, sizeof(name)) == FEMSTEP_OK) deviceName_ = name;
+    elementShader_ = "shell_forces (libfemstep.so, 8 lanes per element, FP32 compensated)";
+    device_ = d.handle;
+    steps_ = 0;
+    return true;
+}
+
+double ZoneGpuSolver::run(int substeps) {
+    if (!impl_ || !impl_->handle) return -1.0;
+    double ms = 0.0;
+    if (femstep_shell_run(impl_->handle, substeps, &impl_->params, &ms) != FEMSTEP_OK) return -1.0;
+    steps_ += substeps;
+    return ms;
+}
+
+ZoneGpuState ZoneGpuSolver::readback() const {
+    ZoneGpuState out;
+    if (!impl_ || !impl_->handle) return out;
+    const Impl& d = *impl_;
+    out.position.resize(d.nodes * 3);
+    out.velocity.resize(d.nodes * 3);
+    femstep_shell_readback(d.handle, out.position.data(), out.velocity.data());
+    std::vector<double> state(d.elements * 129);
+    femstep_shell_state(d.handle, state.data());
+    out.plastic.resize(d.elements);
+    for (std::size_t e = 0; e < d.elements; ++e) {
+        unpack(state.data() + e * 129, out.plastic[e]);
+        if (out.plastic[e].torn) ++out.tornElements;
+    }
+    double energy[4] = {0, 0, 0, 0}, punch[4] = {0, 0, 0, 0};
+    femstep_shell_energy(d.handle, energy);
+    femstep_shell_punch_state(d.handle, punch);
+    out.dissipation = energy[1];
+    out.work = punch[0];
+    out.penetration = punch[1];
+    out.time = punch[2];
+    out.steps = static_cast<int>(punch[3]);
+    return out;
+}
+
+}  // namespace gpu

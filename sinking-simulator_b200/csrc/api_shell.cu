@@ -36,7 +36,15 @@ struct femstep_shell {
     cudaGraphExec_t graph = nullptr;
     ShellParams graph_params{};
     long long launches = 0;
-    double failure_strain = INFINITY;
+    float* fail_strain = nullptr;  // [E] per-element failure strain (+inf: never fails)
+    // the punch (femstep_shell_set_punch) and its host-side account, as the reference's
+    // GPU zone step keeps it (zone_gpu.cpp:889-919)
+    uint8_t* driven = nullptr;     // [N]
+    double* n_punch = nullptr;     // [nblocks]
+    bool punch = false;
+    double punch_speed = 0.0, punch_ramp = 0.0, axis[3] = {0.0, 0.0, 0.0};
+    double punch_time = 0.0, punch_penetration = 0.0;
+    long long punch_steps = 0;
     std::vector<double> rest;  // host copy for readback
     std::string error;
 };
@@ -74,6 +82,19 @@ ShellParams make_params(const femstep_shell_params& p) {
     q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 5e-5);
     q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-13);
     q.compensated = p.compensated;
+    if (p.material) {
+        const femstep_shell_material& m = *p.material;
+        q.general = 1;
+        q.swift = m.hardening == FEMSTEP_SHELL_SWIFT ? 1 : 0;
+        if (q.swift) q.yield = (float)(m.strength_coefficient * std::pow(m.reference_strain, m.hardening_exponent));
+        q.swift_k = (float)m.strength_coefficient;
+        q.swift_eps0 = (float)m.reference_strain;
+        q.swift_n = (float)m.hardening_exponent;
+        q.kinematic = (float)m.kinematic_modulus;
+        q.tri_sens = (float)m.triaxiality_sensitivity;
+        q.tri_ref = (float)m.reference_triaxiality;
+        q.tri_cut = (float)m.cutoff_triaxiality;
+    }
     return q;
 }
 
@@ -163,6 +184,12 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.j0inv = j0;
     d.state = A.zeros<float>((size_t)s->groups * fs::kShellStateQ * 32);
     d.alpha = A.zeros<float>(Epad * 8);
+    d.state2 = A.zeros<float>((size_t)s->groups * fs::kShellState2Q * 32);
+    {
+        const std::vector<float> never(E, INFINITY);
+        s->fail_strain = A.upload(never.data(), E);
+        d.fail_strain = s->fail_strain;
+    }
     d.slots = A.zeros<float>(E * 8 * 3 + 4);
     d.counter = A.zeros<long long>(2);
     d.e_diss = A.zeros<double>(s->ewarps);
@@ -253,19 +280,30 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
         cudaMemcpy(inv_mass, im.data(), N * sizeof(float), cudaMemcpyHostToDevice);
     }
     if (A.ok() && m.state) {
-        std::vector<float> st((size_t)s->groups * fs::kShellStateQ * 32, 0.0f), al(Epad * 8, 0.0f);
+        // ElementPlasticState (zone_gpu.cpp:36-40): per point plastic strain 0-5, back
+        // stress 6-11, eq. plastic strain 12, damage 13, failed 14; enhanced 120-126;
+        // failure strain 127; torn 128
+        std::vector<float> st((size_t)s->groups * fs::kShellStateQ * 32, 0.0f), al(Epad * 8, 0.0f),
+            st2((size_t)s->groups * fs::kShellState2Q * 32, 0.0f), fs_(E);
         for (size_t e = 0; e < E; ++e) {
             const double* x = m.state + e * 129;
             for (int gp = 0; gp < 8; ++gp) {
                 const size_t base = (e / 4) * fs::kShellStateQ * 32 + (e % 4) * 8 + gp;
                 for (int k = 0; k < 6; ++k) st[base + (size_t)k * 32] = (float)x[gp * 15 + k];
                 st[base + (size_t)6 * 32] = (float)x[gp * 15 + 12];
+                const size_t b2 = (e / 4) * fs::kShellState2Q * 32 + (e % 4) * 8 + gp;
+                for (int k = 0; k < 6; ++k) st2[b2 + (size_t)k * 32] = (float)x[gp * 15 + 6 + k];
+                st2[b2 + (size_t)6 * 32] = (float)x[gp * 15 + 13];
+                st2[b2 + (size_t)7 * 32] = x[gp * 15 + 14] != 0.0 ? 1.0f : 0.0f;
             }
             for (int k = 0; k < 7; ++k) al[e * 8 + k] = (float)x[120 + k];
+            al[e * 8 + 7] = x[128] != 0.0 ? 1.0f : 0.0f;
+            fs_[e] = (float)x[127];
         }
-        s->failure_strain = m.state[127];
         cudaMemcpy(d.state, st.data(), st.size() * sizeof(float), cudaMemcpyHostToDevice);
         cudaMemcpy(d.alpha, al.data(), al.size() * sizeof(float), cudaMemcpyHostToDevice);
+        cudaMemcpy(d.state2, st2.data(), st2.size() * sizeof(float), cudaMemcpyHostToDevice);
+        cudaMemcpy(s->fail_strain, fs_.data(), E * sizeof(float), cudaMemcpyHostToDevice);
     }
     if (!A.ok()) {
         const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;
@@ -286,7 +324,24 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
     if (!s || !params) return fail(s, FEMSTEP_EINVAL, "null solver or params");
     if (substeps < 0) return fail(s, FEMSTEP_EINVAL, "negative step count");
     if (!(params->dt > 0.0) || !std::isfinite(params->dt)) return fail(s, FEMSTEP_EINVAL, "dt must be positive");
-    const ShellParams q = make_params(*params);
+    ShellParams q = make_params(*params);
+    if (s->punch) {
+        q.punch_speed = (float)s->punch_speed;
+        q.punch_ramp = s->punch_ramp;
+        q.axis_x = (float)s->axis[0];
+        q.axis_y = (float)s->axis[1];
+        q.axis_z = (float)s->axis[2];
+        // penetration and time accumulate on the host, step by step, as the reference's
+        // GPU zone step does (zone_gpu.cpp:889-919): the speed from the time at the step's start
+        for (int k = 0; k < substeps; ++k) {
+            const double speed = s->punch_ramp > 0.0 && s->punch_time < s->punch_ramp
+                                     ? s->punch_speed * (s->punch_time / s->punch_ramp)
+                                     : s->punch_speed;
+            s->punch_penetration += speed * params->dt;
+            s->punch_time += params->dt;
+            ++s->punch_steps;
+        }
+    }
     s->launches = 0;
     int rc = ensure_factor(s, *params);
     if (rc) return rc;
@@ -352,12 +407,66 @@ int femstep_shell_readback(femstep_shell* s, double* position, double* velocity)
     return FEMSTEP_OK;
 }
 
+int femstep_shell_set_punch(femstep_shell* s, const uint32_t* driven, size_t count, const double axis[3],
+                            double speed, double ramp_time) {
+    if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
+    if (count > 0 && (!driven || !axis)) return fail(s, FEMSTEP_EINVAL, "null argument");
+    for (size_t i = 0; i < count; ++i)
+        if (driven[i] >= s->nodes) return fail(s, FEMSTEP_EINVAL, "driven node out of range");
+    if (count > 0 && !(std::isfinite(speed) && ramp_time >= 0.0)) return fail(s, FEMSTEP_EINVAL, "bad punch speed");
+    if (!s->driven) {
+        s->driven = s->arena.zeros<uint8_t>(s->nodes);
+        s->n_punch = s->arena.zeros<double>(s->nblocks);
+        if (!s->arena.ok()) return check(s, s->arena.status(), "punch allocation");
+    }
+    std::vector<uint8_t> flag(s->nodes, 0);
+    for (size_t i = 0; i < count; ++i) flag[driven[i]] = 1;
+    int rc = check(s, cudaMemcpy(s->driven, flag.data(), s->nodes, cudaMemcpyHostToDevice), "punch upload");
+    if (!rc) rc = check(s, cudaMemset(s->n_punch, 0, s->nblocks * sizeof(double)), "punch upload");
+    if (rc) return rc;
+    s->punch = count > 0;
+    s->d.driven = s->punch ? s->driven : nullptr;
+    s->d.n_punch = s->n_punch;
+    s->punch_speed = speed;
+    s->punch_ramp = ramp_time;
+    for (int k = 0; k < 3; ++k) s->axis[k] = count > 0 ? axis[k] : 0.0;
+    s->punch_time = s->punch_penetration = 0.0;
+    s->punch_steps = 0;
+    if (s->graph) {  // the graph baked the device layout in
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_punch_state(femstep_shell* s, double out[4]) {
+    if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    out[0] = 0.0;
+    if (s->punch) {
+        fs::launch_reduce_sum(s->n_punch, s->nblocks, s->d_out + 4, s->stream);
+        int rc = check(s, cudaGetLastError(), "reduce");
+        if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out + 4, sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+                            "readback");
+        if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "reduce");
+        if (rc) return rc;
+    }
+    out[1] = s->punch_penetration;
+    out[2] = s->punch_time;
+    out[3] = (double)s->punch_steps;
+    return FEMSTEP_OK;
+}
+
 int femstep_shell_state(femstep_shell* s, double* state) {
     if (!s || !state) return fail(s, FEMSTEP_EINVAL, "null argument");
     const size_t E = s->elements;
-    std::vector<float> st((size_t)s->groups * fs::kShellStateQ * 32), al((size_t)s->groups * 4 * 8);
+    std::vector<float> st((size_t)s->groups * fs::kShellStateQ * 32), al((size_t)s->groups * 4 * 8),
+        st2((size_t)s->groups * fs::kShellState2Q * 32), fs_(E);
     int rc = check(s, cudaMemcpy(st.data(), s->d.state, st.size() * sizeof(float), cudaMemcpyDeviceToHost), "readback");
     if (!rc) rc = check(s, cudaMemcpy(al.data(), s->d.alpha, al.size() * sizeof(float), cudaMemcpyDeviceToHost), "readback");
+    if (!rc)
+        rc = check(s, cudaMemcpy(st2.data(), s->d.state2, st2.size() * sizeof(float), cudaMemcpyDeviceToHost),
+                   "readback");
+    if (!rc) rc = check(s, cudaMemcpy(fs_.data(), s->fail_strain, E * sizeof(float), cudaMemcpyDeviceToHost), "readback");
     if (rc) return rc;
     for (size_t e = 0; e < E; ++e) {
         double* x = state + e * 129;
@@ -366,9 +475,14 @@ int femstep_shell_state(femstep_shell* s, double* state) {
             const size_t base = (e / 4) * fs::kShellStateQ * 32 + (e % 4) * 8 + gp;
             for (int k = 0; k < 6; ++k) x[gp * 15 + k] = st[base + (size_t)k * 32];
             x[gp * 15 + 12] = st[base + (size_t)6 * 32];
+            const size_t b2 = (e / 4) * fs::kShellState2Q * 32 + (e % 4) * 8 + gp;
+            for (int k = 0; k < 6; ++k) x[gp * 15 + 6 + k] = st2[b2 + (size_t)k * 32];
+            x[gp * 15 + 13] = st2[b2 + (size_t)6 * 32];
+            x[gp * 15 + 14] = st2[b2 + (size_t)7 * 32];
         }
         for (int k = 0; k < 7; ++k) x[120 + k] = al[e * 8 + k];
-        x[127] = s->failure_strain;
+        x[127] = fs_[e];
+        x[128] = al[e * 8 + 7];
     }
     return FEMSTEP_OK;
 }

@@ -32,6 +32,7 @@ namespace fs {
 constexpr int kShellRec = 188;       // floats per lane record
 constexpr int kShellRec4 = kShellRec / 4;
 constexpr int kShellStateQ = 14;     // floats of state per lane
+constexpr int kShellState2Q = 8;     // back stress (6), damage, failed: the general point law
 constexpr int kShellLanesPerElement = 8;
 constexpr int kShellElementsPerWarp = 4;
 
@@ -54,6 +55,13 @@ struct ShellDevice {
     const uint32_t* offset = nullptr;
     float* slots = nullptr;
     const float* kaa_factor = nullptr; // [E][32]: Cholesky factor of the elastic K_aa (may be null)
+    // the general point law (ShellParams::general): per lane back stress (6), damage,
+    // failed flag, in the state's lane-interleaved layout; per element failure strain
+    float* state2 = nullptr;          // [groups][kShellState2Q][32]
+    // the punch (zone.cpp:1150-1198): 1 for a node the indenter grips; null without one
+    const uint8_t* driven = nullptr;
+    double* n_punch = nullptr;        // FP64 punch work per node block (+=)
+    const float* fail_strain = nullptr;  // [E]; +inf never fails
     long long* counter = nullptr;     // [0] steps taken, [1] step of the current node pass
     // FP64 partials with a fixed mapping: one entry per warp of the element kernel
     // (a warp = a group of 4 elements), one per block of the node kernel
@@ -66,6 +74,22 @@ struct ShellDevice {
 
 struct ShellParams {
     float mu, kappa, yield, hardening;   // J2 point law, linear isotropic hardening
+    // The general point law of plasticity::update (plasticity.cpp:319-505): a Swift
+    // curve K (eps0 + p)^n instead of the linear one, linear kinematic hardening (back
+    // stress), ductile damage D += d(eps_p) / (eps_f f(eta)) with eps_f the element's
+    // failure strain and f(eta) = exp(-c (eta - eta_ref)) above the cutoff, a point
+    // failing at D = 1; and the element rules that go with it (solid_shell.cpp:870-1000):
+    // no enhanced modes once a point has failed, one retry without them in the step a
+    // point fails, torn when all eight have.
+    int general;
+    int swift;                            // 1: Swift curve; 0: linear
+    float swift_k, swift_eps0, swift_n;
+    float kinematic;
+    float tri_sens, tri_ref, tri_cut;
+    // the punch: speed along -axis, ramped linearly over punch_ramp seconds from rest
+    float punch_speed;
+    double punch_ramp;
+    float axis_x, axis_y, axis_z;
     double inv_2mu, inv_3kappa;           // 1 / (2 mu), 1 / (3 kappa) in double (energy account)
     float dt, damping;
     double dt64, rise_time;               // load factor min((step+1) dt / rise, 1)

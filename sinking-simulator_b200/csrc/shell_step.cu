@@ -66,6 +66,11 @@ struct PointOut {
     float dp[6];       // plastic strain increment (engineering shears)
     float deq;
     bool yielded;
+    // the general point law's trial state
+    float back[6];     // back stress after the increment
+    float damage;
+    bool failed;       // failed (stress and tangent zero)
+    float diss;        // dissipation density (sigma - back) : d(eps_p)
 };
 
 // Radial return, linear isotropic hardening, no back stress, failure off
@@ -87,8 +92,10 @@ __device__ __forceinline__ void point_law(const float eps[6], const float ps[7],
     const float root23 = 0.81649658092772603f;
     const float radius = root23 * (p.yield + p.hardening * fmaxf(ps[6], 0.0f));
     const float excess = norm - radius;
+    o.failed = false;  // the linear law has no damage
     if (!(excess > 0.0f)) {
         o.yielded = false;
+        o.diss = 0.0f;
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             o.sigma[i] = pressure + trial[i];
@@ -120,11 +127,145 @@ __device__ __forceinline__ void point_law(const float eps[6], const float ps[7],
     o.deq = root23 * gamma;
     o.theta = 1.0f - k * inv_norm;
     o.theta_bar = 1.0f / (1.0f + p.hardening / (3.0f * p.mu)) - (1.0f - o.theta);
+    float diss = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) diss += o.sigma[i] * o.dp[i];
+    o.diss = diss;
+}
+
+// Flow stress and its slope (plasticity.cpp:116-133): linear or Swift.
+__device__ __forceinline__ float flow_stress(const ShellParams& p, float eq) {
+    const float q = fmaxf(eq, 0.0f);
+    return p.swift ? p.swift_k * powf(p.swift_eps0 + q, p.swift_n) : p.yield + p.hardening * q;
+}
+
+__device__ __forceinline__ float flow_slope(const ShellParams& p, float eq) {
+    const float q = fmaxf(eq, 0.0f);
+    return p.swift ? p.swift_k * p.swift_n * powf(p.swift_eps0 + q, p.swift_n - 1.0f) : p.hardening;
+}
+
+// The general point law (plasticity.cpp:319-505) from the point's start state: radial
+// return against the back stress with the bracketed Newton on the consistency
+// condition (FP32 tolerances: a few ulps of the yield radius and of the multiplier),
+// back stress, damage with the triaxiality factor (plasticity.cpp:171-174), failure.
+__device__ __forceinline__ void point_law_general(const float eps[6], const float ps[7], const float back0[6],
+                                                  float damage0, bool failed0, float fstrain, const ShellParams& p,
+                                                  PointOut& o) {
+    o.yielded = false;
+    o.failed = failed0;
+    o.damage = damage0;
+    o.deq = 0.0f;
+    o.diss = 0.0f;
+    o.theta = 1.0f;
+    o.theta_bar = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        o.back[i] = back0[i];
+        o.n[i] = 0.0f;
+        o.dp[i] = 0.0f;
+    }
+    if (failed0) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) o.sigma[i] = 0.0f;
+        o.theta = 0.0f;
+        return;
+    }
+    float el[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) el[i] = eps[i] - ps[i];
+    const float vol = el[0] + el[1] + el[2];
+    const float pressure = p.kappa * vol;
+    float trial[6], rel[6];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        trial[i] = 2.0f * p.mu * (el[i] - vol * (1.0f / 3.0f));
+        trial[3 + i] = p.mu * el[3 + i];
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) rel[i] = trial[i] - back0[i];
+    const float rnorm = sqrtf(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2] +
+                              2.0f * (rel[3] * rel[3] + rel[4] * rel[4] + rel[5] * rel[5]));
+    const float root23 = 0.81649658092772603f;
+    const float radius = root23 * flow_stress(p, ps[6]);
+    const float excess = rnorm - radius;
+    if (!(excess > 0.0f)) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            o.sigma[i] = pressure + trial[i];
+            o.sigma[3 + i] = trial[3 + i];
+        }
+        return;
+    }
+    const float linear_part = 2.0f * p.mu + (2.0f / 3.0f) * p.kinematic;
+    float lo = 0.0f, hi = excess / linear_part, gamma = hi;
+#pragma unroll 1
+    for (int it = 0; it < 50; ++it) {
+        const float acc = ps[6] + root23 * gamma;
+        const float res = rnorm - linear_part * gamma - root23 * flow_stress(p, acc);
+        if (res > 0.0f)
+            lo = gamma;
+        else
+            hi = gamma;
+        if (fabsf(res) <= 5e-7f * radius) break;
+        const float slope = -linear_part - (2.0f / 3.0f) * flow_slope(p, acc);
+        float next = gamma - res / slope;
+        if (!(next > lo && next < hi)) next = 0.5f * (lo + hi);
+        if (fabsf(next - gamma) <= 1e-7f * gamma) {
+            gamma = next;
+            break;
+        }
+        gamma = next;
+    }
+    o.yielded = true;
+    const float inv_norm = 1.0f / rnorm;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) o.n[i] = rel[i] * inv_norm;
+    const float k = 2.0f * p.mu * gamma;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        o.dp[i] = gamma * o.n[i];
+        o.dp[3 + i] = 2.0f * gamma * o.n[3 + i];
+        o.sigma[i] = pressure + trial[i] - k * o.n[i];
+        o.sigma[3 + i] = trial[3 + i] - k * o.n[3 + i];
+    }
+    float diss = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        o.back[i] = back0[i] + (2.0f / 3.0f) * p.kinematic * gamma * o.n[i];
+        diss += (o.sigma[i] - o.back[i]) * o.dp[i];
+    }
+    o.diss = diss;
+    o.deq = root23 * gamma;
+    // damage: Rice-Tracey factor on the triaxiality sigma_m / sigma_vm
+    const float mean = (o.sigma[0] + o.sigma[1] + o.sigma[2]) * (1.0f / 3.0f);
+    const float d0 = o.sigma[0] - mean, d1 = o.sigma[1] - mean, d2 = o.sigma[2] - mean;
+    const float vm = sqrtf(1.5f * (d0 * d0 + d1 * d1 + d2 * d2 +
+                                   2.0f * (o.sigma[3] * o.sigma[3] + o.sigma[4] * o.sigma[4] + o.sigma[5] * o.sigma[5])));
+    const float eta = vm > 0.0f ? mean / vm : 0.0f;
+    const float critical = eta <= p.tri_cut ? INFINITY : fstrain * expf(-p.tri_sens * (eta - p.tri_ref));
+    if (critical > 0.0f && isfinite(critical)) o.damage += o.deq / critical;
+    if (o.damage >= 1.0f) {
+        o.damage = 1.0f;
+        o.failed = true;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) o.sigma[i] = 0.0f;
+        o.theta = 0.0f;
+        o.theta_bar = 0.0f;
+        return;
+    }
+    o.theta = 1.0f - k * inv_norm;
+    const float pm = flow_slope(p, ps[6] + o.deq) + p.kinematic;
+    o.theta_bar = 1.0f / (1.0f + pm / (3.0f * p.mu)) - (1.0f - o.theta);
 }
 
 // C g for the algorithmic tangent C = kappa 1(x)1 + 2 mu theta I_dev - 2 mu thetaBar n(x)n
 // in the reference's Voigt convention (engineering strain in, tensor stress out).
 __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellParams& p, const float g[6], float out[6]) {
+    if (o.failed) {  // a failed point carries nothing
+#pragma unroll
+        for (int i = 0; i < 6; ++i) out[i] = 0.0f;
+        return;
+    }
     const float tr = g[0] + g[1] + g[2];
     const float ng = o.n[0] * g[0] + o.n[1] * g[1] + o.n[2] * g[2] + o.n[3] * g[3] + o.n[4] * g[4] + o.n[5] * g[5];
     const float a = 2.0f * p.mu * o.theta, b = 2.0f * p.mu * o.theta_bar * ng;
@@ -142,7 +283,9 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
 #define FEMSTEP_SHELL_MINB 4
 #endif
 
-template <bool KAHAN>
+// GENERAL: the general point law and the element failure rules (ShellParams::general);
+// otherwise the linear law, whose state is only the plastic strain.
+template <bool KAHAN, bool GENERAL>
 __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(ShellDevice d, ShellParams p) {
     const int lane = threadIdx.x & 31;
     const int gp = lane & 7;
@@ -303,9 +446,22 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
 #pragma unroll
         for (int k = 0; k < 7; ++k) pc[k] = d.state[sbase + (size_t)(7 + k) * 32];
     }
+    float back0[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, damage0 = 0.0f, fstrain = INFINITY;
+    bool failed0 = false;
+    const size_t sbase2 = (size_t)group * kShellState2Q * 32 + lane;
+    if (GENERAL) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) back0[k] = d.state2[sbase2 + (size_t)k * 32];
+        damage0 = d.state2[sbase2 + (size_t)6 * 32];
+        failed0 = d.state2[sbase2 + (size_t)7 * 32] != 0.0f;
+        fstrain = d.fail_strain[e];
+    }
+    // An element with a failed point runs without enhanced modes (solid_shell.cpp:871-874).
+    bool eas_on = true;
+    if (GENERAL) eas_on = ((__ballot_sync(0xffffffffu, failed0) >> (lane & 24)) & 0xffu) == 0u;
     float alpha[7];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) alpha[k] = d.alpha[e * 8 + k];
+    for (int k = 0; k < 7; ++k) alpha[k] = eas_on ? d.alpha[e * 8 + k] : 0.0f;
     // the elastic K_aa factor of this element is usable (formed, and positive definite)
     const bool have_factor = d.kaa_factor != nullptr && __ldg(d.kaa_factor + e * 32) > 0.0f;
 
@@ -325,7 +481,10 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             for (int k = 0; k < 7; ++k) s += G[i * 7 + k] * alpha[k];
             eps[i] = s;
         }
-        point_law(eps, ps, p, o);
+        if (GENERAL)
+            point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
+        else
+            point_law(eps, ps, p, o);
         float r[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
@@ -333,6 +492,10 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
 #pragma unroll
             for (int i = 0; i < 6; ++i) s += G[i * 7 + k] * o.sigma[i];
             r[k] = sum8(w * s);
+        }
+        if (!done && !eas_on) {  // no enhanced modes: one evaluation is the update
+            converged = true;
+            done = true;
         }
         if (!done) {
             float rn = 0.0f;
@@ -442,14 +605,41 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         }
     }
 
+    // A point that failed in this step's Newton sends its element round once more
+    // without enhanced modes, from the step's start state (solid_shell.cpp:990-996).  The
+    // other elements of the warp re-evaluate at their final alpha, which reproduces
+    // their points exactly.
+    if (GENERAL) {
+        // every lane takes part in the ballot (a short-circuit would leave lanes out of it)
+        const unsigned failed_mask = __ballot_sync(0xffffffffu, o.failed);
+        const bool died = eas_on && ((failed_mask >> (lane & 24)) & 0xffu) != 0u;
+        if (__any_sync(0xffffffffu, died)) {
+            if (died) {
+                eas_on = false;
+                converged = true;
+#pragma unroll
+                for (int k = 0; k < 7; ++k) alpha[k] = 0.0f;
+            }
+            float eps[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                float s = eps_u[i];
+#pragma unroll
+                for (int k = 0; k < 7; ++k) s += G[i * 7 + k] * alpha[k];
+                eps[i] = s;
+            }
+            point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
+        }
+    }
+
     // ---- commit ----
     double diss = 0.0, energy = 0.0;
+    bool torn = false;
+    if (GENERAL) torn = ((__ballot_sync(0xffffffffu, o.failed) >> (lane & 24)) & 0xffu) == 0xffu;
+    if (GENERAL && valid && gp == 7) d.alpha[e * 8 + 7] = torn ? 1.0f : 0.0f;  // all eight points failed
     if (valid) {
         if (o.yielded) {
-            float dsum = 0.0f;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) dsum += o.sigma[i] * o.dp[i];
-            diss = (double)w * (double)dsum;
+            diss = (double)w * (double)o.diss;
             if (KAHAN) {
 #pragma unroll
                 for (int i = 0; i < 6; ++i) kahan_add(ps[i], pc[i], o.dp[i]);
@@ -463,6 +653,12 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             }
 #pragma unroll
             for (int k = 0; k < 7; ++k) d.state[sbase + (size_t)k * 32] = ps[k];
+            if (GENERAL) {
+#pragma unroll
+                for (int k = 0; k < 6; ++k) d.state2[sbase2 + (size_t)k * 32] = o.back[k];
+                d.state2[sbase2 + (size_t)6 * 32] = o.damage;
+                d.state2[sbase2 + (size_t)7 * 32] = o.failed ? 1.0f : 0.0f;
+            }
         }
         if (gp < 7) d.alpha[e * 8 + gp] = alpha[gp];
         const double s0 = o.sigma[0], s1 = o.sigma[1], s2 = o.sigma[2], s3 = o.sigma[3], s4 = o.sigma[4],
@@ -542,7 +738,7 @@ template <bool KAHAN>
 __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, ShellParams p) {
     __shared__ double scratch[32];
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double work = 0.0, kin = 0.0;
+    double work = 0.0, kin = 0.0, pwork = 0.0;
     if (n < d.nodes) {
         const double t = (double)(d.counter[1] + 1) * p.dt64;
         const float lf = p.rise_time > 0.0 ? (float)(t / p.rise_time < 1.0 ? t / p.rise_time : 1.0) : 1.0f;
@@ -570,6 +766,25 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
             }
             v *= p.damping;
             vel[k] = v;
+            work += (double)ext * (double)v * (double)p.dt;
+        }
+        // The punch holds the nodes it grips at -speed along its axis; the impulse that
+        // takes is its work (zone.cpp:1190-1198; solidshell_integrate.comp).  After the
+        // force update and the damping, before the position update.
+        if (d.driven && d.driven[n]) {
+            const double t0 = (double)d.counter[1] * p.dt64;  // time at the start of the step
+            const float speed = p.punch_ramp > 0.0 && t0 < p.punch_ramp ? (float)(p.punch_speed * (t0 / p.punch_ramp))
+                                                                         : p.punch_speed;
+            const float along = vel[0] * p.axis_x + vel[1] * p.axis_y + vel[2] * p.axis_z;
+            const float change = -speed - along;
+            vel[0] += change * p.axis_x;
+            vel[1] += change * p.axis_y;
+            vel[2] += change * p.axis_z;
+            pwork = -((double)m * (double)change) * (double)speed;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float v = vel[k];
             const float du = v * p.dt;
             if (KAHAN) {
                 float c = d.disp_c[(size_t)n * 3 + k];
@@ -580,15 +795,16 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
             } else {
                 u[k] += du;
             }
-            work += (double)ext * (double)v * (double)p.dt;
             kin += 0.5 * (double)m * (double)v * (double)v;
         }
     }
     const double bw = block_sum(work, scratch);
     const double bk = block_sum(kin, scratch);
+    const double bp = d.driven ? block_sum(pwork, scratch) : 0.0;
     if (threadIdx.x == 0) {
         d.n_work[blockIdx.x] += bw;
         d.n_kin[blockIdx.x] = bk;
+        if (d.driven) d.n_punch[blockIdx.x] += bp;
     }
 }
 
@@ -664,10 +880,20 @@ void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t 
     const int eb = blocks_for(d.groups * 32, kShellBlock);
     const int nb = blocks_for(d.nodes, kShellNodeBlock);
     if (p.compensated) {
-        if (parts & 1) shell_forces<true><<<eb, kShellBlock, 0, stream>>>(d, p);
+        if (parts & 1) {
+            if (p.general)
+                shell_forces<true, true><<<eb, kShellBlock, 0, stream>>>(d, p);
+            else
+                shell_forces<true, false><<<eb, kShellBlock, 0, stream>>>(d, p);
+        }
         if (parts & 2) shell_nodes<true><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
     } else {
-        if (parts & 1) shell_forces<false><<<eb, kShellBlock, 0, stream>>>(d, p);
+        if (parts & 1) {
+            if (p.general)
+                shell_forces<false, true><<<eb, kShellBlock, 0, stream>>>(d, p);
+            else
+                shell_forces<false, false><<<eb, kShellBlock, 0, stream>>>(d, p);
+        }
         if (parts & 2) shell_nodes<false><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
     }
 }

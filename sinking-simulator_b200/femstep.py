@@ -276,11 +276,23 @@ class ShellMeshC(C.Structure):
                 ("adjacency_offset", C.c_void_p), ("adjacency_entry", C.c_void_p), ("density", C.c_double)]
 
 
+class ShellMaterialC(C.Structure):
+    """femstep_shell_material: the general point law (Swift or linear flow, kinematic
+    hardening, ductile damage)."""
+    _fields_ = [("hardening", C.c_int), ("strength_coefficient", C.c_double), ("reference_strain", C.c_double),
+                ("hardening_exponent", C.c_double), ("kinematic_modulus", C.c_double),
+                ("triaxiality_sensitivity", C.c_double), ("reference_triaxiality", C.c_double),
+                ("cutoff_triaxiality", C.c_double)]
+
+
+SHELL_LINEAR, SHELL_SWIFT = 0, 1
+
+
 class ShellParamsC(C.Structure):
     _fields_ = [("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double), ("yield_strength", C.c_double),
                 ("hardening_modulus", C.c_double), ("dt", C.c_double), ("damping", C.c_double),
                 ("rise_time", C.c_double), ("max_iterations", C.c_int), ("tol_residual", C.c_double),
-                ("tol_work", C.c_double), ("compensated", C.c_int)]
+                ("tol_work", C.c_double), ("compensated", C.c_int), ("material", C.c_void_p)]
 
 
 _sh_create = _sig("femstep_shell_create", C.c_int, [C.POINTER(ShellMeshC), C.POINTER(C.c_void_p)])
@@ -296,6 +308,9 @@ _sh_launches = _sig("femstep_shell_launches", C.c_longlong, [C.c_void_p])
 _sh_bytes = _sig("femstep_shell_device_bytes", C.c_size_t, [C.c_void_p])
 _sh_error = _sig("femstep_shell_error", C.c_char_p, [C.c_void_p])
 _sh_destroy = _sig("femstep_shell_destroy", None, [C.c_void_p])
+_sh_set_punch = _sig("femstep_shell_set_punch", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                                           C.c_double, C.c_double])
+_sh_punch_state = _sig("femstep_shell_punch_state", C.c_int, [C.c_void_p, C.c_void_p])
 _sh_forms = _sig("femstep_shell_forms", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_double, C.c_double,
                                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p])
 
@@ -347,11 +362,22 @@ class ShellSolver:
         if rc:
             _raise(rc, _sh_error(self._h))
 
-    @staticmethod
-    def params(youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9, dt=1e-7, damping=1.0,
-               rise_time=0.0, max_iterations=12, tol_residual=5e-5, tol_work=1e-13, compensated=True):
-        return ShellParamsC(youngs, poisson, yield_strength, hardening, dt, damping, rise_time, int(max_iterations),
-                            tol_residual, tol_work, int(bool(compensated)))
+    def params(self, youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9, dt=1e-7, damping=1.0,
+               rise_time=0.0, max_iterations=12, tol_residual=5e-5, tol_work=1e-13, compensated=True, material=None):
+        """material: None (the linear law) or a dict of femstep_shell_material fields
+        (hardening=SHELL_SWIFT|SHELL_LINEAR, strength_coefficient, reference_strain,
+        hardening_exponent, kinematic_modulus, triaxiality_sensitivity,
+        reference_triaxiality, cutoff_triaxiality)."""
+        p = ShellParamsC(youngs, poisson, yield_strength, hardening, dt, damping, rise_time, int(max_iterations),
+                         tol_residual, tol_work, int(bool(compensated)), None)
+        if material is not None:
+            m = dict(hardening=SHELL_LINEAR, strength_coefficient=0.0, reference_strain=0.0, hardening_exponent=1.0,
+                     kinematic_modulus=0.0, triaxiality_sensitivity=1.5, reference_triaxiality=1.0 / 3.0,
+                     cutoff_triaxiality=-1.0 / 3.0)
+            m.update(material)
+            self._material = ShellMaterialC(**m)  # kept alive while the handle may read it
+            p.material = C.addressof(self._material)
+        return p
 
     def run(self, substeps, **kw) -> float:
         p = self.params(**kw)
@@ -375,6 +401,19 @@ class ShellSolver:
         out = np.zeros(4)
         self._check(_sh_energy(self._h, _p(out)))
         return out
+
+    def set_punch(self, driven_nodes, axis, speed, ramp_time=0.0):
+        """The prescribed punch (zone.cpp:1150-1198): each step the driven nodes move at
+        -speed along `axis` (speed ramped over ramp_time seconds)."""
+        dn = np.ascontiguousarray(driven_nodes, np.uint32)
+        ax = np.ascontiguousarray(axis, np.float64)
+        self._check(_sh_set_punch(self._h, _p(dn), dn.size, _p(ax), float(speed), float(ramp_time)))
+
+    def punch_state(self):
+        """{work, penetration, time, steps} of the punch (ZoneGpuState)."""
+        out = np.zeros(4)
+        self._check(_sh_punch_state(self._h, _p(out)))
+        return {"work": out[0], "penetration": out[1], "time": out[2], "steps": int(out[3])}
 
     def stats(self):
         out = np.zeros(2, np.int64)

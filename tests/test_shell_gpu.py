@@ -99,3 +99,103 @@ def test_rest_stays_at_rest(fem):
     s.run(64, dt=s.critical_dt())
     p, v = s.readback()
     assert np.abs(p - rest).max() == 0.0 and np.abs(v).max() == 0.0
+
+
+# The general point law: BASELINE's configs use the linear curve with failure off, but
+# the reference's zone step (and its GPU shader) carries Swift hardening, kinematic
+# hardening, ductile damage and the element failure rules.
+SWIFT = (600e6, 0.02, 0.18)   # K, eps0, n: sigma_y(0) = 600e6 * 0.02^0.18 ~ 296 MPa
+
+
+def general(kinematic, failure):
+    mat = O.material(E=206e9, nu=0.3, yield_=SWIFT[0] * SWIFT[1] ** SWIFT[2], hardening=0.0, kinematic=kinematic,
+                     swift=SWIFT, failure=failure)
+    dev = dict(hardening=1, strength_coefficient=SWIFT[0], reference_strain=SWIFT[1], hardening_exponent=SWIFT[2],
+               kinematic_modulus=kinematic, triaxiality_sensitivity=1.5, reference_triaxiality=1.0 / 3.0,
+               cutoff_triaxiality=-1.0 / 3.0)
+    return mat, dev
+
+
+def run_general(fem, port, mat, dev, steps, peak):
+    rest, index, pinned, load = small_plate(fem, peak=peak)
+    ref = O.ShellModel(port, rest, index, pinned, mat, fext=load)
+    state0 = ref.state.copy()  # the oracle's initial state: per-element failure strains
+    s = fem.ShellSolver(rest, index, pinned=pinned, load=load, density=7850.0, state=state0.reshape(-1, 129))
+    dt = s.critical_dt(206e9, 0.3, 7850.0, 0.9)
+    rise = 200 * dt
+    ref.step(dt, steps, rise_time=rise)
+    s.run(steps, dt=dt, rise_time=rise, compensated=True, max_iterations=40, material=dev)
+    p, _ = s.readback()
+    u, ur = p - rest, ref.position - rest
+    return np.abs(u - ur).max() / np.abs(ur).max(), s.state(), ref.state.reshape(-1, 129)
+
+
+def test_swift_and_kinematic_hardening_against_fp64_oracle(fem, port):
+    mat, dev = general(kinematic=2e9, failure=None)
+    err, st, sr = run_general(fem, port, mat, dev, 400, 6e7)
+    ep, epr = st[:, 12:120:15], sr[:, 12:120:15]
+    assert epr.max() > 1e-3, "the case must yield"
+    assert err < 5e-5, err
+    assert np.abs(ep - epr).max() <= 2e-3 * epr.max()
+    back, backr = st[:, [g * 15 + 6 + k for g in range(8) for k in range(6)]], sr[:, [g * 15 + 6 + k for g in range(8)
+                                                                                      for k in range(6)]]
+    assert np.abs(backr).max() > 0 and np.abs(back - backr).max() <= 5e-3 * np.abs(backr).max()
+
+
+def test_damage_failure_and_degraded_elements_against_fp64_oracle(fem, port):
+    """A short failure strain: points fail, their elements lose the enhanced modes and
+    retry, some tear.  Failure is a threshold, so the comparison is on the failed set
+    and the damage field rather than bit for bit."""
+    mat, dev = general(kinematic=0.0, failure=(0.004, 0.008))
+    err, st, sr = run_general(fem, port, mat, dev, 400, 6e7)
+    failed = st[:, 14:120:15] != 0
+    failed_r = sr[:, 14:120:15] != 0
+    assert failed_r.sum() > 8, "the case must fail points"
+    # the same points fail, up to the few at the threshold
+    assert (failed != failed_r).sum() <= max(2, 0.05 * failed_r.sum()), ((failed != failed_r).sum(), failed_r.sum())
+    dmg, dmg_r = st[:, 13:120:15], sr[:, 13:120:15]
+    assert np.abs(dmg - dmg_r)[~(failed | failed_r)].max() <= 2e-2
+    # an element with a failed point carries no enhanced modes
+    assert np.all(st[failed.any(axis=1)][:, 120:127] == 0.0)
+    assert (st[:, 128] != 0).sum() == (sr[:, 128] != 0).sum()
+    assert err < 5e-3, err
+
+
+@pytest.mark.parametrize("law", ["linear", "swift"])
+def test_punch_against_fp64_oracle(fem, port, law):
+    """The prescribed punch of zone::Solver::step (zone.cpp:1150-1198): the nodes under a
+    small footprint in the middle of the plate's top face are driven down at a ramped
+    speed; positions and the punch's work against the FP64 oracle."""
+    rest, index, pinned, load = small_plate(fem, peak=0.0)
+    p = rest.reshape(-1, 3)
+    top = p[:, 2] > 0.0
+    centre = (np.abs(p[:, 0] - 0.06) < 0.011) & (np.abs(p[:, 1] - 0.04) < 0.011)
+    pinned3 = pinned.reshape(-1, 3).any(axis=1)
+    driven = np.nonzero(top & centre & ~pinned3)[0]
+    assert driven.size >= 4
+    if law == "linear":
+        mat, dev = O.material(E=206e9, nu=0.3, yield_=355e6, hardening=1e9), None
+    else:
+        mat, dev = general(kinematic=0.0, failure=None)
+    ref = O.ShellModel(port, rest, index, pinned, mat)
+    ref.set_punch(driven, (0.0, 0.0, 1.0))
+    s = fem.ShellSolver(rest, index, pinned=pinned, density=7850.0, state=ref.state.copy().reshape(-1, 129))
+    dt = s.critical_dt(206e9, 0.3, 7850.0, 0.9)
+    s.set_punch(driven, (0.0, 0.0, 1.0), speed=4.0, ramp_time=100 * dt)
+    steps = 400
+    ref.step(dt, steps, punch_speed=4.0, punch_ramp=100 * dt)
+    kw = dict(dt=dt, compensated=True, max_iterations=40, yield_strength=355e6, hardening=1e9)
+    if dev is not None:
+        kw["material"] = dev
+    s.run(steps, **kw)
+    pos, _ = s.readback()
+    u, ur = pos - rest, ref.position - rest
+    err = np.abs(u - ur).max() / np.abs(ur).max()
+    st = s.punch_state()
+    assert st["steps"] == steps
+    assert st["penetration"] == pytest.approx(sum(4.0 * min(k * dt / (100 * dt), 1.0) * dt for k in range(steps)),
+                                              rel=1e-12)
+    assert ref.punch_work > 0 and abs(st["work"] - ref.punch_work) <= 2e-3 * ref.punch_work
+    assert err < 1e-4, err
+    # the driven nodes went down with the punch
+    assert np.all(u.reshape(-1, 3)[driven, 2] < 0)
