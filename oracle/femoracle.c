@@ -1463,7 +1463,9 @@ void or_shell_setup(or_shell *m, const double *mat, double density) {
 /* Solver::step for a patch with no punch and no driven edge, with an external
  * nodal load: zone.cpp:928-989, 1094-1121, 1200-1202. */
 void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int steps) {
-    for (int s = 0; s < steps; ++s) {
+    /* the velocity each driven-edge DOF would have taken had nothing held it */
+    double *edge_free = m->prescribed ? (double *)calloc(m->nodes * 3, sizeof(double)) : NULL;
+    for (int s = 0; s < steps && !m->arrested; ++s) {
         const double time = (double)(m->step + 1) * p->dt;
         const double lf = p->rise_time > 0 ? dmin(time / p->rise_time, 1.0) : 1.0;
         double dissipation = 0.0;
@@ -1486,7 +1488,9 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
             or_shell_plastic_update(m->forms + e * OR_FORMS_LEN, rest, current, mat, st, out, stress, info);
             dissipation += info[4];
         }
-        double work = 0.0;
+        /* force -> velocity (zone.cpp:1094-1111); the kinetic energy before the damping
+           and the damping's loss (zone.cpp:1113-1121) */
+        double work = 0.0, before = 0.0;
         for (size_t node = 0; node < m->nodes; ++node) {
             double sum[3] = {0, 0, 0};
             for (uint32_t k = m->adj_offset[node]; k < m->adj_offset[node + 1]; ++k) {
@@ -1496,27 +1500,72 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
                 sum[1] += f[1];
                 sum[2] += f[2];
             }
+            double ext[3];
             for (int k = 0; k < 3; ++k) {
                 const size_t d = node * 3 + (size_t)k;
-                const double ext = m->fext ? lf * m->fext[d] : 0.0;
-                const double force = sum[k] + ext;
+                ext[k] = m->fext ? lf * m->fext[d] : 0.0;
+                const double force = sum[k] + ext[k];
                 if (m->pinned[d]) {
+                    if (edge_free && m->prescribed[d] != 0.0) {
+                        double free_velocity = m->velocity[d];
+                        if (m->mass[node] > 0) free_velocity += force / m->mass[node] * p->dt;
+                        edge_free[d] = free_velocity;
+                    }
                     m->velocity[d] = 0.0;
                     continue;
                 }
                 if (m->mass[node] > 0) m->velocity[d] += force / m->mass[node] * p->dt;
+            }
+            const double *v = &m->velocity[node * 3];
+            before += 0.5 * m->mass[node] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            for (int k = 0; k < 3; ++k) {
+                const size_t d = node * 3 + (size_t)k;
+                if (m->pinned[d]) continue;
                 m->velocity[d] *= p->damping;
-                work += ext * m->velocity[d] * p->dt;
+                work += ext[k] * m->velocity[d] * p->dt;
             }
         }
-        /* the prescribed punch, after the damping and before the positions (zone.cpp:1150-1198):
-         * each gripped node moves at -speed along the axis; the impulse that takes is the
-         * resisting force, its work -impulse * speed.  The speed ramps from the time at the
-         * start of the step. */
+        if (p->damping != 1.0) m->account[0] += before * (1.0 - p->damping * p->damping);
+        /* the driven edge, after the damping and before the punch (zone.cpp:1123-1145):
+           the velocity that lands the DOF on its drive this step; the boundary's work is
+           what that velocity costs over the free one */
+        if (edge_free) {
+            double fraction = 1.0;
+            if (m->edge_ramp > 0) {
+                /* the time at the step's end, as the running sum the solver keeps */
+                const double r = dmin(1.0, dmax(0.0, (m->account[3] + p->dt) / m->edge_ramp));
+                fraction = r * r * (3.0 - 2.0 * r);
+            }
+            for (size_t d = 0; d < m->nodes * 3; ++d) {
+                if (!m->pinned[d] || m->prescribed[d] == 0.0) continue;
+                const size_t node = d / 3;
+                const double base = m->meshed ? m->meshed[d] : m->rest[d];
+                const double target = (base + m->prescribed[d] * fraction - m->position[d]) / p->dt;
+                m->account[1] += m->mass[node] * (target - edge_free[d]) * target;
+                m->velocity[d] = target;
+            }
+        }
+        /* the punch, after the edge and before the positions (zone.cpp:1147-1198): each
+           gripped node moves at -speed along the axis; the impulse that takes is the
+           resisting force.  Prescribed: the speed ramps from the time at the start of the
+           step.  Inertial: the grip is a perfectly inelastic collision of the striking
+           body with the gripped nodes, momentum along the axis conserved. */
+        double speed = 0.0;
         if (m->driven) {
-            const double t0 = (double)m->step * p->dt;
-            double speed = p->punch_speed;
+            const double t0 = m->account[3];  /* the time at the step's start (a running sum) */
+            speed = p->punch_speed;
             if (p->punch_ramp > 0 && t0 < p->punch_ramp) speed = p->punch_speed * (t0 / p->punch_ramp);
+            if (m->punch_mass > 0) {
+                double node_momentum = 0.0, driven_mass = 0.0;
+                for (size_t node = 0; node < m->nodes; ++node) {
+                    if (!m->driven[node]) continue;
+                    const double *v = &m->velocity[node * 3];
+                    node_momentum -= m->mass[node] * (v[0] * m->axis[0] + v[1] * m->axis[1] + v[2] * m->axis[2]);
+                    driven_mass += m->mass[node];
+                }
+                m->punch_velocity = (m->punch_mass * m->punch_velocity + node_momentum) / (m->punch_mass + driven_mass);
+                speed = m->punch_velocity;
+            }
             double impulse = 0.0;
             for (size_t node = 0; node < m->nodes; ++node) {
                 if (!m->driven[node]) continue;
@@ -1526,13 +1575,19 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
                 for (int k = 0; k < 3; ++k) v[k] += change * m->axis[k];
                 impulse += m->mass[node] * change;
             }
-            m->energy[4] += -impulse * speed;
+            const double force = -impulse / p->dt;
+            m->energy[4] += force * speed * p->dt;
         }
         for (size_t d = 0; d < m->nodes * 3; ++d) m->position[d] += m->velocity[d] * p->dt;
+        m->account[2] += speed * p->dt;
+        m->account[3] += p->dt;
         m->energy[0] += work;
         m->energy[1] += dissipation;
         ++m->step;
+        /* the striking body has spent what it arrived with (zone.cpp:1225-1230) */
+        if (m->driven && m->punch_mass > 0 && !(m->punch_velocity > 0)) m->arrested = 1;
     }
+    free(edge_free);
 }
 
 /* accumulateEnergy, zone.cpp:1014-1044 */

@@ -179,6 +179,18 @@ typedef struct {
     long step;
     uint8_t *driven;          /* N: 1 for a node the punch grips, or NULL (no punch) */
     double axis[3];           /* the punch travels along -axis */
+    /* The driven edge (zone.cpp:833-842, 1123-1145): a pinned DOF whose prescribed value
+       is non-zero follows meshed + prescribed * smoothstep(t / edge_ramp), t the time at
+       the step's end; NULL = every pinned DOF is a clamp. */
+    double *prescribed;       /* 3N or NULL */
+    double *meshed;           /* 3N: the position the drive is measured from; NULL = rest */
+    double edge_ramp;         /* s; 0 = the whole drive at once */
+    /* The inertial punch (zone.cpp:1154-1185): mass > 0 makes the grip a perfectly
+       inelastic collision with a striking body of that mass; 0 = the prescribed punch. */
+    double punch_mass;
+    double punch_velocity;    /* m/s along -axis (state of the striking body) */
+    int arrested;             /* the striking body has stopped: no further steps run */
+    double account[4];        /* damping loss, boundary work, penetration, time */
 } or_shell;
 
 typedef struct {
@@ -187,6 +199,37 @@ typedef struct {
     double punch_speed;       /* the prescribed punch (zone.cpp:1150-1198) */
     double punch_ramp;        /* s over which its speed rises linearly from rest */
 } or_shell_params;
+
+/* A flat plate stepped by the reference's zone::Solver itself (ref_shim.cpp only; the
+   port has no twin: tests run or_shell_step on the arrays it returns and compare).  The
+   plate is built as the reference's own zone tests build theirs: makePlateMesh, the
+   perimeter pinned, the punch footprint round the centre of the outer face. */
+typedef struct {
+    double lx, ly, thickness;
+    int nx, ny, nz;
+    double half_length, half_width;   /* the punch footprint; 0 = no punch */
+    double speed, ramp_time;          /* prescribed punch; the arrival speed if mass > 0 */
+    double mass;                      /* > 0: the inertial punch (Drive::Inertial) */
+    double damping, edge_ramp;
+    double edge_drive[3];             /* a perimeter DOF's prescribed value: edge_drive * x / lx */
+    int steps;
+} or_zone_case;
+typedef struct {
+    double *rest;                     /* 3N meshed position (= rest) */
+    uint32_t *index;                  /* 8E */
+    uint8_t *pinned;                  /* 3N */
+    double *prescribed;               /* 3N */
+    uint8_t *driven;                  /* N: the solver's driven nodes */
+    double *mass;                     /* N lumped */
+    double *state0;                   /* OR_SHELL_STATE_LEN * E, at construction */
+    double *position, *velocity;      /* 3N after the steps */
+    double *state;                    /* OR_SHELL_STATE_LEN * E after the steps */
+    double mat[OR_MAT_LEN];           /* plasticity::shipSteel() */
+    double density, dt;
+    double account[10];               /* work, dissipation, penetration, time, damping loss,
+                                         boundary work, indenter speed, steps, arrested,
+                                         driven edge DOFs */
+} or_zone_out;
 
 void or_shell_setup(or_shell *m, const double *mat, double density);
 void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int steps);

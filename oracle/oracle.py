@@ -75,12 +75,35 @@ class Shell(C.Structure):
                 ("gauss_volume", C.POINTER(C.c_double)), ("adj_offset", C.POINTER(C.c_uint32)),
                 ("adj_entry", C.POINTER(C.c_uint32)), ("fext", C.POINTER(C.c_double)),
                 ("energy", C.c_double * 5), ("step", C.c_long), ("driven", C.POINTER(C.c_uint8)),
-                ("axis", C.c_double * 3)]
+                ("axis", C.c_double * 3), ("prescribed", C.POINTER(C.c_double)),
+                ("meshed", C.POINTER(C.c_double)), ("edge_ramp", C.c_double), ("punch_mass", C.c_double),
+                ("punch_velocity", C.c_double), ("arrested", C.c_int), ("account", C.c_double * 4)]
 
 
 class ShellParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("damping", C.c_double), ("rise_time", C.c_double),
                 ("punch_speed", C.c_double), ("punch_ramp", C.c_double)]
+
+
+class ZoneCase(C.Structure):
+    _fields_ = [("lx", C.c_double), ("ly", C.c_double), ("thickness", C.c_double), ("nx", C.c_int),
+                ("ny", C.c_int), ("nz", C.c_int), ("half_length", C.c_double), ("half_width", C.c_double),
+                ("speed", C.c_double), ("ramp_time", C.c_double), ("mass", C.c_double), ("damping", C.c_double),
+                ("edge_ramp", C.c_double), ("edge_drive", C.c_double * 3), ("steps", C.c_int)]
+
+
+class ZoneOut(C.Structure):
+    _fields_ = [("rest", C.POINTER(C.c_double)), ("index", C.POINTER(C.c_uint32)),
+                ("pinned", C.POINTER(C.c_uint8)), ("prescribed", C.POINTER(C.c_double)),
+                ("driven", C.POINTER(C.c_uint8)), ("mass", C.POINTER(C.c_double)),
+                ("state0", C.POINTER(C.c_double)), ("position", C.POINTER(C.c_double)),
+                ("velocity", C.POINTER(C.c_double)), ("state", C.POINTER(C.c_double)),
+                ("mat", C.c_double * MAT_LEN), ("density", C.c_double), ("dt", C.c_double),
+                ("account", C.c_double * 10)]
+
+
+ZONE_ACCOUNT = ("work", "dissipation", "penetration", "time", "damping_loss", "boundary_work", "punch_speed",
+                "steps", "arrested", "edge_dof")
 
 
 def build_port() -> str:
@@ -144,6 +167,34 @@ class Oracle:
             g("default_workers", C.c_uint, [])
             g("tet64_time_parallel", C.c_double, [C.POINTER(Tet64), C.POINTER(Tet64Params), C.c_int, C.c_int])
             g("tet32_time", C.c_double, [C.POINTER(Tet32), C.c_float, C.c_float, C.c_float, C.c_float, C.c_int])
+            g("zone_sizes", C.c_int, [C.POINTER(ZoneCase), C.POINTER(C.c_size_t)])
+            g("zone_run", C.c_int, [C.POINTER(ZoneCase), C.POINTER(ZoneOut)])
+
+    def zone_plate(self, lx=0.4, ly=0.2, thickness=0.01, nx=8, ny=4, nz=1, half_length=0.05, half_width=0.05,
+                   speed=20.0, ramp_time=1e-4, mass=0.0, damping=1.0, edge_ramp=0.0, edge_drive=(0.0, 0.0, 0.0),
+                   steps=100) -> dict:
+        """The reference's zone::Solver stepped `steps` times on a flat plate (ref only):
+        the arrays it was built from, where it ended and its account."""
+        c = ZoneCase(lx, ly, thickness, nx, ny, nz, half_length, half_width, speed, ramp_time, mass, damping,
+                     edge_ramp, (C.c_double * 3)(*edge_drive), steps)
+        sizes = (C.c_size_t * 2)()
+        self.zone_sizes(C.byref(c), sizes)
+        n, e = sizes[0], sizes[1]
+        r = dict(rest=np.zeros(3 * n), index=np.zeros(8 * e, np.uint32), pinned=np.zeros(3 * n, np.uint8),
+                 prescribed=np.zeros(3 * n), driven=np.zeros(n, np.uint8), mass=np.zeros(n),
+                 state0=np.zeros(SHELL_STATE_LEN * e), position=np.zeros(3 * n), velocity=np.zeros(3 * n),
+                 state=np.zeros(SHELL_STATE_LEN * e))
+        o = ZoneOut()
+        for name, ct in (("rest", C.c_double), ("index", C.c_uint32), ("pinned", C.c_uint8),
+                         ("prescribed", C.c_double), ("driven", C.c_uint8), ("mass", C.c_double),
+                         ("state0", C.c_double), ("position", C.c_double), ("velocity", C.c_double),
+                         ("state", C.c_double)):
+            setattr(o, name, _ptr(r[name], ct))
+        r["problems"] = self.zone_run(C.byref(c), C.byref(o))
+        r["mat"] = np.array(list(o.mat))
+        r["density"], r["dt"] = o.density, o.dt
+        r["account"] = dict(zip(ZONE_ACCOUNT, list(o.account)))
+        return r
 
     def _fn(self, name, res, args):
         f = getattr(self.lib, self.p + name)
@@ -323,13 +374,34 @@ class ShellModel:
     def steps(self):
         return self._s.step
 
-    def set_punch(self, driven_nodes, axis):
-        """The prescribed punch (zone.cpp:1150-1198) grips these nodes and travels along -axis."""
+    def set_punch(self, driven_nodes, axis, mass=0.0, speed=0.0):
+        """The punch (zone.cpp:1147-1198) grips these nodes and travels along -axis.  With
+        mass > 0 it is a striking body of that mass arriving at `speed` (the inertial
+        punch); otherwise the speed is prescribed per step (ShellModel.step)."""
         self.driven = np.zeros(self.nodes, np.uint8)
         self.driven[np.asarray(driven_nodes, np.int64)] = 1
         self._s.driven = _ptr(self.driven, C.c_uint8)
         for k in range(3):
             self._s.axis[k] = float(axis[k])
+        self._s.punch_mass = float(mass)
+        self._s.punch_velocity = float(speed) if mass > 0 else 0.0
+
+    def set_edge(self, prescribed, meshed=None, ramp=0.0):
+        """The driven edge (zone.cpp:833-842, 1123-1145): each pinned DOF with a non-zero
+        prescribed value follows meshed + prescribed * smoothstep(t / ramp)."""
+        self.prescribed = np.ascontiguousarray(prescribed, np.float64).reshape(-1).copy()
+        self._s.prescribed = _ptr(self.prescribed, C.c_double)
+        if meshed is not None:
+            self.meshed = np.ascontiguousarray(meshed, np.float64).reshape(-1).copy()
+            self._s.meshed = _ptr(self.meshed, C.c_double)
+        self._s.edge_ramp = float(ramp)
+
+    @property
+    def account(self):
+        """dict: damping loss, boundary work, penetration, time, punch speed, arrested."""
+        a = self._s.account
+        return dict(damping_loss=a[0], boundary_work=a[1], penetration=a[2], time=a[3],
+                    punch_speed=self._s.punch_velocity, arrested=bool(self._s.arrested))
 
     @property
     def punch_work(self):

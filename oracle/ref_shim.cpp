@@ -14,6 +14,7 @@
 #include "engine/core/jobs.hpp"
 #include "engine/sim/fem.hpp"
 #include "engine/sim/plasticity.hpp"
+#include "engine/sim/scantlings.hpp"
 #include "engine/sim/solid_shell.hpp"
 #include "engine/sim/zone.hpp"
 
@@ -687,6 +688,115 @@ void ref_shell_step(or_shell* m, const double* mat, const or_shell_params* p, in
         m->energy[1] += dissipation;
         ++m->step;
     }
+}
+
+// --- zone::Solver itself --------------------------------------------------------
+
+namespace {
+
+void materialOut(const pl::Material& m, double* out) {
+    out[0] = m.youngsModulus;
+    out[1] = m.poissonRatio;
+    out[2] = m.flow.yieldStrength;
+    out[3] = m.flow.hardeningModulus;
+    out[4] = m.flow.kinematicModulus;
+    out[5] = m.flow.kind == pl::Hardening::Swift ? 1.0 : 0.0;
+    out[6] = m.flow.strengthCoefficient;
+    out[7] = m.flow.referenceStrain;
+    out[8] = m.flow.hardeningExponent;
+    out[9] = m.failure.uniformStrain;
+    out[10] = m.failure.fractureStrain;
+    out[11] = m.failure.triaxialitySensitivity;
+    out[12] = m.failure.referenceTriaxiality;
+    out[13] = m.failure.cutoffTriaxiality;
+}
+
+// The plate patch of the reference's zone GPU tests (tests/test_zone_gpu.cpp:163-197),
+// with a driven perimeter when edge_drive is non-zero.
+sim::zone::Patch platePatch(const or_zone_case* c) {
+    ss::HexMesh flat = ss::makePlateMesh(c->lx, c->ly, c->thickness, c->nx, c->ny, c->nz);
+    flat.prescribed.assign(flat.nodeCount() * 3, 0.0);
+    for (std::size_t n = 0; n < flat.nodeCount(); ++n) {
+        const double x = flat.position[n * 3], y = flat.position[n * 3 + 1];
+        if (x <= 1e-9 || x >= c->lx - 1e-9 || y <= 1e-9 || y >= c->ly - 1e-9)
+            for (int k = 0; k < 3; ++k) flat.pin(n, k, c->edge_drive[k] * (x / c->lx));
+    }
+    sim::zone::Patch patch;
+    patch.mesh = flat;
+    patch.axis = sim::Vec3{0, 0, 1};
+    patch.right = sim::Vec3{1, 0, 0};
+    patch.up = sim::Vec3{0, 1, 0};
+    patch.centre = sim::Vec3{0.5 * c->lx, 0.5 * c->ly, 0.0};
+    patch.outerFace.assign(flat.nodeCount(), 0u);
+    for (std::size_t n = 0; n < flat.nodeCount(); ++n)
+        patch.outerFace[n] = flat.position[n * 3 + 2] > 0.0 ? 1u : 0u;
+    patch.elementArea.assign(flat.elementCount(), c->lx * c->ly / (double)(c->nx * c->ny));
+    patch.panelOf.assign(flat.elementCount(), 0);
+    patch.panels.push_back(0);
+    patch.panelArea.push_back(c->lx * c->ly);
+    patch.material = sim::ah36Steel();
+    patch.thickness = c->thickness;
+    patch.criticalTimestep =
+        ss::criticalTimestep(flat, patch.material, ss::Formulation::SolidShell);
+    return patch;
+}
+
+sim::zone::SolveParams plateParams(const or_zone_case* c) {
+    sim::zone::SolveParams params;
+    params.indenter.halfLength = c->half_length;
+    params.indenter.halfWidth = c->half_width;
+    params.indenter.speed = c->speed;
+    params.indenter.rampTime = c->mass > 0 ? 0.0 : c->ramp_time;
+    params.indenter.stopAt = 1.0;
+    if (c->mass > 0) {
+        params.indenter.drive = sim::zone::Drive::Inertial;
+        params.indenter.mass = c->mass;
+    }
+    params.damping = c->damping;
+    params.edgeRamp = c->edge_ramp;
+    return params;
+}
+
+}  // namespace
+
+extern "C" int ref_zone_sizes(const or_zone_case* c, size_t out[2]) {
+    const ss::HexMesh flat = ss::makePlateMesh(c->lx, c->ly, c->thickness, c->nx, c->ny, c->nz);
+    out[0] = flat.nodeCount();
+    out[1] = flat.elementCount();
+    return 0;
+}
+
+// Build the plate, construct zone::Solver on it and call step() `steps` times; return
+// the arrays the solver was built from and where it ended.  Returns the number of
+// problems the solver reported.
+extern "C" int ref_zone_run(const or_zone_case* c, or_zone_out* o) {
+    const sim::zone::Patch patch = platePatch(c);
+    const sim::zone::SolveParams params = plateParams(c);
+    const pl::Material material = pl::shipSteel();
+    sim::zone::Solver solver(patch, material, params);
+    const std::size_t N = patch.nodeCount(), E = patch.elementCount();
+    std::copy(patch.mesh.position.begin(), patch.mesh.position.end(), o->rest);
+    std::copy(patch.mesh.index.begin(), patch.mesh.index.end(), o->index);
+    std::copy(solver.pinnedDof().begin(), solver.pinnedDof().end(), o->pinned);
+    std::copy(patch.mesh.prescribed.begin(), patch.mesh.prescribed.end(), o->prescribed);
+    std::fill(o->driven, o->driven + N, uint8_t{0});
+    for (uint32_t n : solver.drivenNodes()) o->driven[n] = 1;
+    std::copy(solver.nodalMass().begin(), solver.nodalMass().end(), o->mass);
+    for (std::size_t e = 0; e < E; ++e) shellStateOut(solver.elementState()[e], o->state0 + e * OR_SHELL_STATE_LEN);
+    materialOut(material, o->mat);
+    o->density = patch.material.density;
+    for (int s = 0; s < c->steps; ++s)
+        if (!solver.step()) break;
+    const sim::zone::SolveResult& r = solver.result();
+    o->dt = r.timestep;
+    std::copy(solver.position().begin(), solver.position().end(), o->position);
+    std::copy(solver.velocity().begin(), solver.velocity().end(), o->velocity);
+    for (std::size_t e = 0; e < E; ++e) shellStateOut(solver.elementState()[e], o->state + e * OR_SHELL_STATE_LEN);
+    const double account[10] = {r.work, r.dissipation, r.penetration, r.time, r.dampingLoss, r.boundaryWork,
+                                r.indenterSpeed, (double)r.steps, r.indenterArrested ? 1.0 : 0.0,
+                                (double)r.drivenEdgeDof};
+    std::copy(account, account + 10, o->account);
+    return (int)r.problems.size();
 }
 
 // zone.cpp:1014-1044 (kinetic and the plastic strain energy).
