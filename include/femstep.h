@@ -203,6 +203,17 @@ int femstep_pool_admit_many(femstep_pool *pool, const femstep_pool_mesh *meshes,
                             int *ids, int *admitted);
 /* Free a mesh's space.  Its device state is frozen behind any queued work. */
 int femstep_pool_release(femstep_pool *pool, int id);
+/* Eviction.  checkpoint copies one mesh's whole mutable state (displacement and
+   velocity, plastic strain, both with their compensation, its energy partials and step
+   counter) into a host buffer of femstep_pool_checkpoint_size bytes; release it, and
+   admit_resume the same mesh later -- anywhere in this or another pool -- with that
+   buffer and a target >= the steps already taken.  It then steps on bit-identically
+   to a mesh that never left (and its energy sums are bit-identical too when the pool's
+   tile is the same).  Not while a chunk is in flight. */
+int femstep_pool_checkpoint_size(femstep_pool *pool, int id, size_t *bytes);
+int femstep_pool_checkpoint(femstep_pool *pool, int id, void *buffer, size_t bytes);
+int femstep_pool_admit_resume(femstep_pool *pool, const femstep_pool_mesh *mesh, long long steps,
+                              const void *checkpoint, size_t bytes, int *id);
 /* Queue one chunk: every admitted mesh that has steps left advances by up to `steps`
    steps (meshes that reach their count stop there).  Returns without waiting. */
 int femstep_pool_run_async(femstep_pool *pool, int steps, int mode);
@@ -311,17 +322,37 @@ int femstep_shell_state(femstep_shell *solver, double *state);
 /* [0] external work [1] plastic dissipation [2] strain energy [3] kinetic, FP64 reduced
    on the device in fixed order (zone::Solver::accumulateEnergy, zone.cpp:1014-1044). */
 int femstep_shell_energy(femstep_shell *solver, double out[4]);
-/* The punch of zone::Solver::step (engine/sim/zone.cpp:1150-1198) as the reference's GPU
-   zone step drives it (engine/gpu/shaders/solidshell_integrate.comp, zone_gpu.cpp:889-919):
-   every step each node in `driven` has its velocity along `axis` set to -speed, after the
-   force update and the damping; the speed rises linearly over ramp_time seconds from the
-   time the punch is set.  The impulse it takes is the punch's work, summed in FP64 in a
-   fixed order (the shader used a fixed-point atomic).  count 0 removes the punch. */
+/* The punch of zone::Solver::step (engine/sim/zone.cpp:1147-1198).
+   mass == 0: the prescribed punch, as the reference's GPU zone step drives it
+   (engine/gpu/shaders/solidshell_integrate.comp, zone_gpu.cpp:889-919): every step each
+   node in `driven` has its velocity along `axis` set to -speed, after the force update,
+   the damping and the driven edge; the speed rises linearly over ramp_time seconds from
+   the time the punch is set.
+   mass > 0: the inertial punch (Drive::Inertial, zone.cpp:1154-1185), which the
+   reference runs on the CPU only: a striking body of that mass arrives at `speed` and
+   the grip is a perfectly inelastic collision with the gripped nodes; ramp_time is
+   ignored, as the reference ignores it.  Once the body has stopped, every later step is
+   skipped on the device (the run has ended, zone.cpp:1225-1230).  speed must be > 0.
+   Either way the impulse it takes is the punch's work, summed in FP64 in a fixed order
+   (the shader used a fixed-point atomic).  count 0 removes the punch. */
 int femstep_shell_set_punch(femstep_shell *solver, const uint32_t *driven, size_t count, const double axis[3],
-                            double speed, double ramp_time);
+                            double speed, double ramp_time, double mass);
 /* [0] punch work (J) [1] penetration (m) [2] time (s) [3] steps since the punch was set:
    ZoneGpuState::work / penetration / time / steps (zone_gpu.hpp:116-126). */
 int femstep_shell_punch_state(femstep_shell *solver, double out[4]);
+/* The driven edge (zone.cpp:833-842, 1123-1145): each pinned DOF d with prescribed[d]
+   != 0 follows meshed[d] + prescribed[d] * smoothstep(t / edge_ramp) (t at the step's
+   end; edge_ramp 0: the whole drive at once) instead of staying clamped; the others stay
+   clamps.  meshed (3N) is the position the drive is measured from; NULL takes the rest
+   position.  The boundary's work is kept in FP64 (femstep_shell_account).  prescribed
+   NULL, or all zero, removes the drive. */
+int femstep_shell_set_edge(femstep_shell *solver, const double *prescribed, const double *meshed,
+                           double edge_ramp);
+/* The rest of zone::Solver's account (SolveResult, zone.hpp:750-815): [0] damping loss
+   (J) [1] boundary work of the driven edge (J) [2] the punch's speed now (m/s) [3] the
+   striking body's kinetic energy (J; 0 for a prescribed punch) [4] 1 once an inertial
+   punch has stopped [5] driven edge DOFs. */
+int femstep_shell_account(femstep_shell *solver, double out[6]);
 /* [0] element-steps whose EAS Newton hit its cap, [1] yielded Gauss points last step. */
 int femstep_shell_stats(femstep_shell *solver, long long out[2]);
 /* Smallest element critical step, FP64 power iteration per element on the device
@@ -333,6 +364,17 @@ int femstep_shell_profile(femstep_shell *solver, int steps, const femstep_shell_
 long long femstep_shell_launches(const femstep_shell *solver);
 /* Bytes of device memory the solver holds. */
 size_t femstep_shell_device_bytes(const femstep_shell *solver);
+/* Checkpoint and resume (ZoneGpuState's role in zone_gpu.hpp:116-126, kept whole):
+   the solver's entire mutable device state -- displacement with its compensation,
+   velocity, element state with its compensation, enhanced parameters, step counter,
+   the FP64 energy and punch partials -- and the punch clock, as one host buffer of
+   femstep_shell_checkpoint_size bytes.  Restore into a solver created from the same
+   mesh with the same punch and driven edge set; running on from it is bit-identical to
+   never having stopped (also across destroy / create, e.g. to evict a zone from the
+   GPU and bring it back later). */
+int femstep_shell_checkpoint_size(femstep_shell *solver, size_t *bytes);
+int femstep_shell_checkpoint(femstep_shell *solver, void *buffer, size_t bytes);
+int femstep_shell_restore(femstep_shell *solver, const void *buffer, size_t bytes);
 const char *femstep_shell_error(const femstep_shell *solver);
 void femstep_shell_destroy(femstep_shell *solver);
 

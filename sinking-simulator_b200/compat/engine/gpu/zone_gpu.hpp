@@ -15,7 +15,9 @@
 //     forms, on an elastic-only solve, and on a combination it does not build;
 //   - the step is the element update (the general point law: linear or Swift flow,
 //     kinematic hardening, ductile damage, the degraded-EAS retry, tearing), the CSR
-//     gather, the node update and the prescribed punch, all on the device;
+//     gather, the node update with its damping, the driven edge and the punch, all on
+//     the device.  Beyond the reference's GPU path, which drives a prescribed punch
+//     only: the inertial punch (Drive::Inertial) and the driven edge run here too;
 //   - run executes `substeps` steps with the host out of the loop and returns the
 //     device-measured milliseconds; readback returns the ZoneGpuState that
 //     zone::Solver::adopt takes.

@@ -162,11 +162,22 @@ bool ZoneGpuSolver::initialise(const sim::zone::Patch& patch, const sim::zone::S
     p.compensated = 1;
     p.material = &d.material;
 
-    // the punch: the CPU solver's driven nodes, along -axis
+    // the punch: the CPU solver's driven nodes, along -axis; prescribed, or the striking
+    // body of Drive::Inertial (zone.cpp:1154-1185)
     const std::vector<uint32_t> driven(cpu.drivenNodes().begin(), cpu.drivenNodes().end());
     const double axis[3] = {patch.axis.x, patch.axis.y, patch.axis.z};
+    const double striker =
+        params.indenter.drive == sim::zone::Drive::Inertial ? params.indenter.mass : 0.0;
     if (femstep_shell_set_punch(d.handle, driven.data(), driven.size(), axis, params.indenter.speed,
-                                params.indenter.rampTime) != FEMSTEP_OK) {
+                                params.indenter.rampTime, striker) != FEMSTEP_OK) {
+        error = femstep_shell_error(d.handle);
+        return false;
+    }
+    // the driven edge: pinned DOFs with a prescribed value, measured from the meshed
+    // position (zone.cpp:833-842, 1123-1145)
+    if (patch.mesh.prescribed.size() == N * 3 &&
+        femstep_shell_set_edge(d.handle, patch.mesh.prescribed.data(), patch.mesh.position.data(),
+                               params.edgeRamp) != FEMSTEP_OK) {
         error = femstep_shell_error(d.handle);
         return false;
     }

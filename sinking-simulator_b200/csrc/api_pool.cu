@@ -764,6 +764,125 @@ int femstep_pool_release(femstep_pool* p, int id) {
     return check(p, cudaGetLastError(), "release");
 }
 
+// ---- eviction: checkpoint one mesh, bring it back later ----
+//
+// A mesh's mutable state in the pool -- displacement and its compensation, velocity,
+// plastic strain and its compensation, its energy partial slots and its record (step
+// counter, step size) -- as one host buffer.  admit_resume admits the same mesh again
+// (anywhere in the pool) and puts the state back; it then steps on exactly as if it
+// had never left, since no per-tet or per-node arithmetic depends on where a mesh
+// sits or who its neighbours are.
+
+namespace {
+
+constexpr uint64_t kPoolCheckpointMagic = 0x3150484c4f4f5046ull;  // "FPOOLHP1"
+
+struct PoolCheckpointHeader {
+    uint64_t magic;
+    int64_t T, N, e_tiles, n_tiles, tile;
+    PoolMesh rec;
+};
+
+struct PoolSegment {
+    void* dev;      // device address
+    size_t bytes;
+};
+
+std::vector<PoolSegment> pool_segments(femstep_pool* p, const HostMesh& h) {
+    PoolDevice& d = p->d;
+    std::vector<PoolSegment> v = {
+        {d.disp + h.n0, (size_t)(h.N + 1) * sizeof(float4)},
+        {d.disp_c + h.n0, (size_t)(h.N + 1) * sizeof(float4)},
+        {d.velocity + h.n0 * 3, (size_t)(h.N + 1) * 3 * sizeof(float)},
+    };
+    for (int k = 0; k < 7; ++k) v.push_back({d.plastic + (size_t)k * p->tet_cap + h.t0, (size_t)h.T * sizeof(float)});
+    for (int k = 0; k < 7; ++k) v.push_back({d.plastic_c + (size_t)k * p->tet_cap + h.t0, (size_t)h.T * sizeof(float)});
+    v.push_back({d.e_diss + h.e_part, (size_t)h.e_tiles * sizeof(double)});
+    v.push_back({d.e_strain + h.e_part, (size_t)h.e_tiles * sizeof(double)});
+    v.push_back({d.n_work + h.n_part, (size_t)h.n_tiles * sizeof(double)});
+    v.push_back({d.n_kin + h.n_part, (size_t)h.n_tiles * sizeof(double)});
+    return v;
+}
+
+size_t pool_checkpoint_bytes(femstep_pool* p, const HostMesh& h) {
+    size_t total = sizeof(PoolCheckpointHeader);
+    for (const PoolSegment& g : pool_segments(p, h)) total += g.bytes;
+    return total;
+}
+
+}  // namespace
+
+int femstep_pool_checkpoint_size(femstep_pool* p, int id, size_t* bytes) {
+    if (!valid_id(p, id) || !bytes) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    *bytes = pool_checkpoint_bytes(p, p->meshes[id]);
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_checkpoint(femstep_pool* p, int id, void* buffer, size_t bytes) {
+    if (!valid_id(p, id) || !buffer) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
+    const HostMesh& h = p->meshes[id];
+    if (bytes < pool_checkpoint_bytes(p, h)) return fail(p, FEMSTEP_EINVAL, "checkpoint buffer too small");
+    PoolCheckpointHeader hd{};
+    hd.magic = kPoolCheckpointMagic;
+    hd.T = h.T;
+    hd.N = h.N;
+    hd.e_tiles = h.e_tiles;
+    hd.n_tiles = h.n_tiles;
+    hd.tile = p->tile;
+    int rc = check(p, cudaMemcpyAsync(&hd.rec, p->d.meshes + id, sizeof(PoolMesh), cudaMemcpyDeviceToHost, p->stream),
+                   "checkpoint");
+    char* out = static_cast<char*>(buffer) + sizeof(hd);
+    for (const PoolSegment& g : pool_segments(p, h)) {
+        if (!rc) rc = check(p, cudaMemcpyAsync(out, g.dev, g.bytes, cudaMemcpyDeviceToHost, p->stream), "checkpoint");
+        out += g.bytes;
+    }
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "checkpoint");
+    if (rc) return rc;
+    std::memcpy(buffer, &hd, sizeof(hd));
+    return FEMSTEP_OK;
+}
+
+int femstep_pool_admit_resume(femstep_pool* p, const femstep_pool_mesh* mesh, long long steps, const void* buffer,
+                              size_t bytes, int* id) {
+    if (!p || !mesh || !buffer || !id) return fail(p, FEMSTEP_EINVAL, "null argument");
+    PoolCheckpointHeader hd;
+    if (bytes < sizeof(hd)) return fail(p, FEMSTEP_EINVAL, "not a pool checkpoint");
+    std::memcpy(&hd, buffer, sizeof(hd));
+    if (hd.magic != kPoolCheckpointMagic) return fail(p, FEMSTEP_EINVAL, "not a pool checkpoint");
+    if (hd.T != (int64_t)mesh->tets || hd.N != (int64_t)mesh->nodes)
+        return fail(p, FEMSTEP_EINVAL, "checkpoint of a different mesh");
+    if (steps < hd.rec.step) return fail(p, FEMSTEP_EINVAL, "target below the steps already taken");
+    int admitted = 0;
+    int rc = admit_meshes(p, mesh, &steps, 1, id, &admitted);
+    if (rc || admitted != 1) return rc ? rc : fail(p, FEMSTEP_ENOMEM, "no room now");
+    HostMesh& h = p->meshes[*id];
+    if (bytes < pool_checkpoint_bytes(p, h) || hd.e_tiles != h.e_tiles || hd.n_tiles != h.n_tiles) {
+        femstep_pool_release(p, *id);
+        return fail(p, FEMSTEP_EINVAL, "checkpoint size does not match this mesh");
+    }
+    // behind the admission's own uploads on the stream: the state, then the record with
+    // this placement's partial slots, serial and target
+    const char* in = static_cast<const char*>(buffer) + sizeof(hd);
+    for (const PoolSegment& g : pool_segments(p, h)) {
+        if (!rc) rc = check(p, cudaMemcpyAsync(g.dev, in, g.bytes, cudaMemcpyHostToDevice, p->stream), "resume");
+        in += g.bytes;
+    }
+    PoolMesh rec = hd.rec;
+    rec.e_part = h.e_part;
+    rec.n_part = h.n_part;
+    rec.serial = h.serial;
+    rec.target = steps;
+    if (!rc) rc = check(p, cudaMemcpyAsync(p->d.meshes + *id, &rec, sizeof(rec), cudaMemcpyHostToDevice, p->stream),
+                        "resume");
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "resume");
+    if (rc) {
+        femstep_pool_release(p, *id);
+        return rc;
+    }
+    return FEMSTEP_OK;
+}
+
 int femstep_pool_run_async(femstep_pool* p, int steps, int mode) {
     if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
     if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");

@@ -45,6 +45,19 @@ struct femstep_shell {
     double punch_speed = 0.0, punch_ramp = 0.0, axis[3] = {0.0, 0.0, 0.0};
     double punch_time = 0.0, punch_penetration = 0.0;
     long long punch_steps = 0;
+    // the inertial punch (mass > 0): its state lives on the device
+    double punch_mass = 0.0;
+    uint32_t* driven_list = nullptr;
+    size_t driven_capacity = 0;
+    double* punch_state = nullptr;    // [8]
+    int* halt = nullptr;
+    // the driven edge (femstep_shell_set_edge)
+    int* edge_map = nullptr;
+    double* edge_rows = nullptr;      // [2][rows][3]: meshed - rest, prescribed
+    size_t edge_capacity = 0, edge_dof = 0;
+    double edge_ramp = 0.0;
+    double* n_edge = nullptr;         // [nblocks]
+    std::vector<uint8_t> pin;         // host copy of the pinned bits (0-2)
     std::vector<double> rest;  // host copy for readback
     std::string error;
 };
@@ -77,6 +90,7 @@ ShellParams make_params(const femstep_shell_params& p) {
     q.dt = (float)p.dt;
     q.dt64 = p.dt;
     q.damping = (float)p.damping;
+    q.damping64 = p.damping;
     q.rise_time = p.rise_time;
     q.max_iterations = p.max_iterations > 0 ? p.max_iterations : 12;
     q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 5e-5);
@@ -197,19 +211,29 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.e_stats = A.zeros<int>((size_t)s->ewarps * 2);
     s->kaa_factor = A.zeros<float>(E * 32);
     d.n_work = A.zeros<double>(s->nblocks);
-    d.n_kin = A.zeros<double>(s->nblocks);
+    d.n_kin = A.zeros<double>(s->nblocks + 1);  // + the gripped nodes of an inertial punch
+    d.punch_kin = d.n_kin + s->nblocks;
+    d.n_damp = A.zeros<double>(s->nblocks);
     s->d_out = A.zeros<double>(8);
 
-    // nodes
-    std::vector<float> disp(N * 3, 0.0f), vel(N * 3, 0.0f);
+    // nodes.  The displacement is held as a float u and its Kahan compensation c with
+    // position = rest + (u - c): u = fl(x) for the caller's x = position - rest, and c =
+    // fl(u - x) carries the part of x that u cannot, so a position read back from this
+    // solver (rest + u - c, in double) and handed to a new one continues bit for bit.
+    std::vector<float> disp(N * 3, 0.0f), comp(N * 3, 0.0f), vel(N * 3, 0.0f);
     if (m.position)
-        for (size_t i = 0; i < N * 3; ++i) disp[i] = (float)(m.position[i] - m.rest[i]);
+        for (size_t i = 0; i < N * 3; ++i) {
+            const double x = m.position[i] - m.rest[i];
+            disp[i] = (float)x;
+            comp[i] = (float)((double)disp[i] - x);
+        }
     if (m.velocity)
         for (size_t i = 0; i < N * 3; ++i) vel[i] = (float)m.velocity[i];
     d.disp = A.upload(disp.data(), N * 3);
-    d.disp_c = A.zeros<float>(N * 3);
+    d.disp_c = A.upload(comp.data(), N * 3);
     d.velocity = A.upload(vel.data(), N * 3);
-    std::vector<uint8_t> pin(N, 0);
+    std::vector<uint8_t>& pin = s->pin;
+    pin.assign(N, 0);
     if (m.pinned)
         for (size_t n = 0; n < N; ++n)
             pin[n] = (uint8_t)((m.pinned[n * 3] ? 1 : 0) | (m.pinned[n * 3 + 1] ? 2 : 0) | (m.pinned[n * 3 + 2] ? 4 : 0));
@@ -289,8 +313,14 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
             const double* x = m.state + e * 129;
             for (int gp = 0; gp < 8; ++gp) {
                 const size_t base = (e / 4) * fs::kShellStateQ * 32 + (e % 4) * 8 + gp;
-                for (int k = 0; k < 6; ++k) st[base + (size_t)k * 32] = (float)x[gp * 15 + k];
-                st[base + (size_t)6 * 32] = (float)x[gp * 15 + 12];
+                // plastic strain and eq. plastic strain as a value and its compensation
+                // (value - compensation = the caller's double, as for the displacement)
+                for (int k = 0; k < 7; ++k) {
+                    const double v = x[gp * 15 + (k < 6 ? k : 12)];
+                    const float f = (float)v;
+                    st[base + (size_t)k * 32] = f;
+                    st[base + (size_t)(7 + k) * 32] = (float)((double)f - v);
+                }
                 const size_t b2 = (e / 4) * fs::kShellState2Q * 32 + (e % 4) * 8 + gp;
                 for (int k = 0; k < 6; ++k) st2[b2 + (size_t)k * 32] = (float)x[gp * 15 + 6 + k];
                 st2[b2 + (size_t)6 * 32] = (float)x[gp * 15 + 13];
@@ -325,12 +355,17 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
     if (substeps < 0) return fail(s, FEMSTEP_EINVAL, "negative step count");
     if (!(params->dt > 0.0) || !std::isfinite(params->dt)) return fail(s, FEMSTEP_EINVAL, "dt must be positive");
     ShellParams q = make_params(*params);
+    q.edge_ramp = s->edge_ramp;
     if (s->punch) {
         q.punch_speed = (float)s->punch_speed;
         q.punch_ramp = s->punch_ramp;
         q.axis_x = (float)s->axis[0];
         q.axis_y = (float)s->axis[1];
         q.axis_z = (float)s->axis[2];
+        q.inertial = s->punch_mass > 0.0 ? 1 : 0;
+        q.punch_mass = s->punch_mass;
+    }
+    if (s->punch && !q.inertial) {
         // penetration and time accumulate on the host, step by step, as the reference's
         // GPU zone step does (zone_gpu.cpp:889-919): the speed from the time at the step's start
         for (int k = 0; k < substeps; ++k) {
@@ -343,6 +378,7 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
         }
     }
     s->launches = 0;
+    const int per_step = q.inertial ? 3 : 2;
     int rc = ensure_factor(s, *params);
     if (rc) return rc;
     rc = check(s, cudaEventRecord(s->ev0, s->stream), "event record");
@@ -367,12 +403,12 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
             rc = check(s, cudaGraphLaunch(s->graph, s->stream), "graph launch");
             if (rc) return rc;
             left -= kGraphSteps;
-            s->launches += 2 * kGraphSteps;
+            s->launches += per_step * kGraphSteps;
         }
     }
     for (; left > 0; --left) {
         fs::launch_shell_step(s->d, q, s->stream, 3);
-        s->launches += 2;
+        s->launches += per_step;
     }
     rc = check(s, cudaGetLastError(), "kernel launch");
     if (!rc) rc = check(s, cudaEventRecord(s->ev1, s->stream), "event record");
@@ -408,25 +444,53 @@ int femstep_shell_readback(femstep_shell* s, double* position, double* velocity)
 }
 
 int femstep_shell_set_punch(femstep_shell* s, const uint32_t* driven, size_t count, const double axis[3],
-                            double speed, double ramp_time) {
+                            double speed, double ramp_time, double mass) {
     if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
     if (count > 0 && (!driven || !axis)) return fail(s, FEMSTEP_EINVAL, "null argument");
     for (size_t i = 0; i < count; ++i)
         if (driven[i] >= s->nodes) return fail(s, FEMSTEP_EINVAL, "driven node out of range");
     if (count > 0 && !(std::isfinite(speed) && ramp_time >= 0.0)) return fail(s, FEMSTEP_EINVAL, "bad punch speed");
+    if (!(mass >= 0.0) || !std::isfinite(mass)) return fail(s, FEMSTEP_EINVAL, "bad punch mass");
+    // zone.cpp:779-801: a striking body with no approach speed carries no energy
+    if (count > 0 && mass > 0.0 && !(speed > 0.0))
+        return fail(s, FEMSTEP_EINVAL, "an inertial punch needs a positive striking mass and approach speed");
     if (!s->driven) {
         s->driven = s->arena.zeros<uint8_t>(s->nodes);
         s->n_punch = s->arena.zeros<double>(s->nblocks);
+        s->punch_state = s->arena.zeros<double>(8);
+        s->halt = s->arena.zeros<int>(1);
         if (!s->arena.ok()) return check(s, s->arena.status(), "punch allocation");
     }
     std::vector<uint8_t> flag(s->nodes, 0);
     for (size_t i = 0; i < count; ++i) flag[driven[i]] = 1;
+    // the list in node order, each node once (the reference's drivenNodes() order)
+    std::vector<uint32_t> list;
+    for (size_t n = 0; n < s->nodes; ++n)
+        if (flag[n]) list.push_back((uint32_t)n);
+    if (mass > 0.0 && list.size() > s->driven_capacity) {
+        s->driven_list = s->arena.alloc<uint32_t>(list.size());
+        if (!s->arena.ok()) return check(s, s->arena.status(), "punch allocation");
+        s->driven_capacity = list.size();
+    }
     int rc = check(s, cudaMemcpy(s->driven, flag.data(), s->nodes, cudaMemcpyHostToDevice), "punch upload");
     if (!rc) rc = check(s, cudaMemset(s->n_punch, 0, s->nblocks * sizeof(double)), "punch upload");
+    const double state0[8] = {mass > 0.0 ? speed : 0.0, 0, 0, 0, 0, 0, 0, 0};
+    if (!rc) rc = check(s, cudaMemcpy(s->punch_state, state0, sizeof(state0), cudaMemcpyHostToDevice), "punch upload");
+    if (!rc) rc = check(s, cudaMemset(s->halt, 0, sizeof(int)), "punch upload");
+    if (!rc) rc = check(s, cudaMemset(s->d.punch_kin, 0, sizeof(double)), "punch upload");
+    if (!rc && mass > 0.0 && !list.empty())
+        rc = check(s, cudaMemcpy(s->driven_list, list.data(), list.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
+                   "punch upload");
     if (rc) return rc;
     s->punch = count > 0;
+    s->punch_mass = s->punch ? mass : 0.0;
     s->d.driven = s->punch ? s->driven : nullptr;
     s->d.n_punch = s->n_punch;
+    const bool inertial = s->punch && mass > 0.0;
+    s->d.driven_list = inertial ? s->driven_list : nullptr;
+    s->d.n_driven = inertial ? (int)list.size() : 0;
+    s->d.punch_state = s->punch_state;
+    s->d.halt = inertial ? s->halt : nullptr;
     s->punch_speed = speed;
     s->punch_ramp = ramp_time;
     for (int k = 0; k < 3; ++k) s->axis[k] = count > 0 ? axis[k] : 0.0;
@@ -441,18 +505,119 @@ int femstep_shell_set_punch(femstep_shell* s, const uint32_t* driven, size_t cou
 
 int femstep_shell_punch_state(femstep_shell* s, double out[4]) {
     if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
-    out[0] = 0.0;
-    if (s->punch) {
-        fs::launch_reduce_sum(s->n_punch, s->nblocks, s->d_out + 4, s->stream);
-        int rc = check(s, cudaGetLastError(), "reduce");
-        if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out + 4, sizeof(double), cudaMemcpyDeviceToHost, s->stream),
-                            "readback");
-        if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "reduce");
+    out[0] = out[1] = out[2] = out[3] = 0.0;
+    if (!s->punch) return FEMSTEP_OK;
+    if (s->punch_mass > 0.0) {  // the inertial punch keeps its account on the device
+        double st[8];
+        const int rc = check(s, cudaMemcpy(st, s->punch_state, sizeof(st), cudaMemcpyDeviceToHost), "readback");
         if (rc) return rc;
+        out[0] = st[1];
+        out[1] = st[2];
+        out[2] = st[3];
+        out[3] = st[4];
+        return FEMSTEP_OK;
     }
+    fs::launch_reduce_sum(s->n_punch, s->nblocks, s->d_out + 4, s->stream);
+    int rc = check(s, cudaGetLastError(), "reduce");
+    if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out + 4, sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+                        "readback");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "reduce");
+    if (rc) return rc;
     out[1] = s->punch_penetration;
     out[2] = s->punch_time;
     out[3] = (double)s->punch_steps;
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_set_edge(femstep_shell* s, const double* prescribed, const double* meshed, double edge_ramp) {
+    if (!s) return fail(s, FEMSTEP_EINVAL, "null solver");
+    if (!(edge_ramp >= 0.0) || !std::isfinite(edge_ramp)) return fail(s, FEMSTEP_EINVAL, "bad edge ramp");
+    const size_t N = s->nodes;
+    // zone.cpp:838-840: a pinned DOF with a non-zero prescribed value is driven
+    std::vector<uint8_t> pin = s->pin;
+    std::vector<int> map(N, -1);
+    std::vector<double> base, drive;
+    size_t dof = 0;
+    for (size_t n = 0; prescribed && n < N; ++n) {
+        uint8_t marks = 0;
+        for (int k = 0; k < 3; ++k)
+            if ((pin[n] & (1u << k)) && prescribed[n * 3 + k] != 0.0) {
+                if (!std::isfinite(prescribed[n * 3 + k])) return fail(s, FEMSTEP_EINVAL, "prescribed value not finite");
+                marks |= (uint8_t)(8u << k);
+            }
+        if (!marks) continue;
+        map[n] = (int)(base.size() / 3);
+        for (int k = 0; k < 3; ++k) {
+            const bool on = marks & (8u << k);
+            base.push_back(on && meshed ? meshed[n * 3 + k] - s->rest[n * 3 + k] : 0.0);
+            drive.push_back(on ? prescribed[n * 3 + k] : 0.0);
+            dof += on ? 1 : 0;
+        }
+        pin[n] |= marks;
+    }
+    const size_t rows = base.size() / 3;
+    fs::DeviceArena& A = s->arena;
+    if (rows > 0 && !s->edge_map) {
+        s->edge_map = A.alloc<int>(N);
+        s->n_edge = A.zeros<double>(s->nblocks);
+    }
+    if (rows > s->edge_capacity) {
+        s->edge_rows = A.alloc<double>(rows * 6);
+        s->edge_capacity = rows;
+    }
+    if (!A.ok()) return check(s, A.status(), "edge allocation");
+    int rc = check(s, cudaMemcpy((void*)s->d.pinned, pin.data(), N, cudaMemcpyHostToDevice), "edge upload");
+    if (!rc && rows > 0) {
+        rc = check(s, cudaMemcpy(s->edge_map, map.data(), N * sizeof(int), cudaMemcpyHostToDevice), "edge upload");
+        if (!rc) rc = check(s, cudaMemcpy(s->edge_rows, base.data(), rows * 3 * sizeof(double), cudaMemcpyHostToDevice),
+                            "edge upload");
+        if (!rc)
+            rc = check(s, cudaMemcpy(s->edge_rows + rows * 3, drive.data(), rows * 3 * sizeof(double),
+                                     cudaMemcpyHostToDevice),
+                       "edge upload");
+        if (!rc) rc = check(s, cudaMemset(s->n_edge, 0, s->nblocks * sizeof(double)), "edge upload");
+    }
+    if (rc) return rc;
+    s->d.edge_map = rows > 0 ? s->edge_map : nullptr;
+    s->d.edge_base = rows > 0 ? s->edge_rows : nullptr;
+    s->d.edge_drive = rows > 0 ? s->edge_rows + rows * 3 : nullptr;
+    s->d.n_edge = s->n_edge;
+    s->edge_dof = dof;
+    s->edge_ramp = edge_ramp;
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_account(femstep_shell* s, double out[6]) {
+    if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    for (int i = 0; i < 6; ++i) out[i] = 0.0;
+    fs::launch_reduce_sum(s->d.n_damp, s->nblocks, s->d_out + 5, s->stream);
+    if (s->n_edge) fs::launch_reduce_sum(s->n_edge, s->nblocks, s->d_out + 6, s->stream);
+    double r[2] = {0.0, 0.0};
+    int rc = check(s, cudaGetLastError(), "reduce");
+    if (!rc) rc = check(s, cudaMemcpyAsync(r, s->d_out + 5, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+                        "readback");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "reduce");
+    if (rc) return rc;
+    out[0] = r[0];
+    out[1] = s->n_edge ? r[1] : 0.0;
+    if (s->punch && s->punch_mass > 0.0) {
+        double st[8];
+        int halted = 0;
+        rc = check(s, cudaMemcpy(st, s->punch_state, sizeof(st), cudaMemcpyDeviceToHost), "readback");
+        if (!rc) rc = check(s, cudaMemcpy(&halted, s->halt, sizeof(int), cudaMemcpyDeviceToHost), "readback");
+        if (rc) return rc;
+        out[2] = st[0];
+        out[3] = 0.5 * s->punch_mass * st[0] * st[0];
+        out[4] = halted ? 1.0 : 0.0;
+    } else if (s->punch) {
+        out[2] = s->punch_ramp > 0.0 && s->punch_time < s->punch_ramp ? s->punch_speed * (s->punch_time / s->punch_ramp)
+                                                                      : s->punch_speed;
+    }
+    out[5] = (double)s->edge_dof;
     return FEMSTEP_OK;
 }
 
@@ -473,8 +638,10 @@ int femstep_shell_state(femstep_shell* s, double* state) {
         std::fill(x, x + 129, 0.0);
         for (int gp = 0; gp < 8; ++gp) {
             const size_t base = (e / 4) * fs::kShellStateQ * 32 + (e % 4) * 8 + gp;
-            for (int k = 0; k < 6; ++k) x[gp * 15 + k] = st[base + (size_t)k * 32];
-            x[gp * 15 + 12] = st[base + (size_t)6 * 32];
+            // the compensated value (value - compensation; the compensation is 0 when the
+            // step ran uncompensated from a state with no compensation)
+            for (int k = 0; k < 7; ++k)
+                x[gp * 15 + (k < 6 ? k : 12)] = (double)st[base + (size_t)k * 32] - (double)st[base + (size_t)(7 + k) * 32];
             const size_t b2 = (e / 4) * fs::kShellState2Q * 32 + (e % 4) * 8 + gp;
             for (int k = 0; k < 6; ++k) x[gp * 15 + 6 + k] = st2[b2 + (size_t)k * 32];
             x[gp * 15 + 13] = st2[b2 + (size_t)6 * 32];
@@ -490,7 +657,7 @@ int femstep_shell_state(femstep_shell* s, double* state) {
 int femstep_shell_energy(femstep_shell* s, double out[4]) {
     if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
     const double* arrays[4] = {s->d.n_work, s->d.e_diss, s->d.e_strain, s->d.n_kin};
-    const long long counts[4] = {s->nblocks, s->ewarps, s->ewarps, s->nblocks};
+    const long long counts[4] = {s->nblocks, s->ewarps, s->ewarps, s->nblocks + 1};
     for (int i = 0; i < 4; ++i) fs::launch_reduce_sum(arrays[i], counts[i], s->d_out + i, s->stream);
     int rc = check(s, cudaGetLastError(), "reduce");
     if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
@@ -577,6 +744,132 @@ int femstep_shell_profile(femstep_shell* s, int steps, const femstep_shell_param
 long long femstep_shell_launches(const femstep_shell* s) { return s ? s->launches : 0; }
 size_t femstep_shell_device_bytes(const femstep_shell* s) { return s ? s->arena.bytes() : 0; }
 const char* femstep_shell_error(const femstep_shell* s) { return s ? s->error.c_str() : fs::last_error(); }
+
+// ---- checkpoint / restore ----
+//
+// The solver's whole mutable state, in a fixed order of device segments after a small
+// header: displacement and its compensation, velocity, the element state (plastic
+// strain with its compensation, back stress, damage, failed flags, enhanced
+// parameters, torn flags), the step counter, every FP64 partial of the energy account
+// and the punch, and the host-side punch clock.  What is configuration (mesh, forms,
+// mass, the punch's nodes, the driven edge) is not in it: restore into a solver made
+// from the same mesh, with the same punch and edge set.  Restoring and running on is
+// bit-identical to never having stopped.
+
+namespace {
+
+constexpr uint64_t kShellCheckpointMagic = 0x315048434c485346ull;  // "FSHLCHP1"
+
+struct Segment {
+    void* ptr;
+    size_t bytes;
+};
+
+std::vector<Segment> shell_segments(femstep_shell* s) {
+    const size_t N = s->nodes, E = s->elements, Epad = (size_t)s->groups * 4;
+    const ShellDevice& d = s->d;
+    std::vector<Segment> v = {
+        {d.disp, N * 3 * sizeof(float)},
+        {d.disp_c, N * 3 * sizeof(float)},
+        {d.velocity, N * 3 * sizeof(float)},
+        {d.state, (size_t)s->groups * fs::kShellStateQ * 32 * sizeof(float)},
+        {d.state2, (size_t)s->groups * fs::kShellState2Q * 32 * sizeof(float)},
+        {d.alpha, Epad * 8 * sizeof(float)},
+        {d.counter, 2 * sizeof(long long)},
+        {d.e_diss, (size_t)s->ewarps * sizeof(double)},
+        {d.e_strain, (size_t)s->ewarps * sizeof(double)},
+        {d.e_stats, (size_t)s->ewarps * 2 * sizeof(int)},
+        {d.n_work, (size_t)s->nblocks * sizeof(double)},
+        {d.n_kin, (size_t)(s->nblocks + 1) * sizeof(double)},
+        {d.n_damp, (size_t)s->nblocks * sizeof(double)},
+    };
+    (void)E;
+    if (s->driven) {
+        v.push_back({s->n_punch, (size_t)s->nblocks * sizeof(double)});
+        v.push_back({s->punch_state, 8 * sizeof(double)});
+        v.push_back({s->halt, sizeof(int)});
+    }
+    if (s->n_edge) v.push_back({s->n_edge, (size_t)s->nblocks * sizeof(double)});
+    return v;
+}
+
+struct CheckpointHeader {
+    uint64_t magic;
+    uint64_t nodes, elements, segments, payload;
+    uint64_t flags;  // 1: punch arrays, 2: edge arrays
+    double punch_time, punch_penetration;
+    int64_t punch_steps;
+};
+
+size_t shell_checkpoint_bytes(femstep_shell* s) {
+    size_t total = sizeof(CheckpointHeader);
+    for (const Segment& g : shell_segments(s)) total += g.bytes;
+    return total;
+}
+
+}  // namespace
+
+int femstep_shell_checkpoint_size(femstep_shell* s, size_t* bytes) {
+    if (!s || !bytes) return fail(s, FEMSTEP_EINVAL, "null argument");
+    *bytes = shell_checkpoint_bytes(s);
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_checkpoint(femstep_shell* s, void* buffer, size_t bytes) {
+    if (!s || !buffer) return fail(s, FEMSTEP_EINVAL, "null argument");
+    if (bytes < shell_checkpoint_bytes(s)) return fail(s, FEMSTEP_EINVAL, "checkpoint buffer too small");
+    const std::vector<Segment> segs = shell_segments(s);
+    CheckpointHeader h{};
+    h.magic = kShellCheckpointMagic;
+    h.nodes = s->nodes;
+    h.elements = s->elements;
+    h.segments = segs.size();
+    h.payload = shell_checkpoint_bytes(s) - sizeof(h);
+    h.flags = (s->driven ? 1u : 0u) | (s->n_edge ? 2u : 0u);
+    h.punch_time = s->punch_time;
+    h.punch_penetration = s->punch_penetration;
+    h.punch_steps = s->punch_steps;
+    int rc = check(s, cudaStreamSynchronize(s->stream), "checkpoint");
+    if (rc) return rc;
+    char* out = static_cast<char*>(buffer);
+    std::memcpy(out, &h, sizeof(h));
+    out += sizeof(h);
+    for (const Segment& g : segs) {
+        rc = check(s, cudaMemcpy(out, g.ptr, g.bytes, cudaMemcpyDeviceToHost), "checkpoint");
+        if (rc) return rc;
+        out += g.bytes;
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_restore(femstep_shell* s, const void* buffer, size_t bytes) {
+    if (!s || !buffer) return fail(s, FEMSTEP_EINVAL, "null argument");
+    if (bytes < sizeof(CheckpointHeader)) return fail(s, FEMSTEP_EINVAL, "not a shell checkpoint");
+    CheckpointHeader h;
+    std::memcpy(&h, buffer, sizeof(h));
+    if (h.magic != kShellCheckpointMagic) return fail(s, FEMSTEP_EINVAL, "not a shell checkpoint");
+    if (h.nodes != s->nodes || h.elements != s->elements)
+        return fail(s, FEMSTEP_EINVAL, "checkpoint of a different mesh");
+    const uint64_t flags = (s->driven ? 1u : 0u) | (s->n_edge ? 2u : 0u);
+    if (h.flags != flags)
+        return fail(s, FEMSTEP_EINVAL, "set the punch and the driven edge as at the checkpoint before restoring");
+    const std::vector<Segment> segs = shell_segments(s);
+    if (h.segments != segs.size() || h.payload + sizeof(h) != shell_checkpoint_bytes(s) ||
+        bytes < shell_checkpoint_bytes(s))
+        return fail(s, FEMSTEP_EINVAL, "checkpoint size does not match this solver");
+    int rc = check(s, cudaStreamSynchronize(s->stream), "restore");
+    if (rc) return rc;
+    const char* in = static_cast<const char*>(buffer) + sizeof(h);
+    for (const Segment& g : segs) {
+        rc = check(s, cudaMemcpy(g.ptr, in, g.bytes, cudaMemcpyHostToDevice), "restore");
+        if (rc) return rc;
+        in += g.bytes;
+    }
+    s->punch_time = h.punch_time;
+    s->punch_penetration = h.punch_penetration;
+    s->punch_steps = h.punch_steps;
+    return FEMSTEP_OK;
+}
 
 void femstep_shell_destroy(femstep_shell* s) {
     if (!s) return;

@@ -19,7 +19,8 @@
 //
 //   nodes:  rest double[3N] (rest positions), disp/disp_c float[3N] (displacement and
 //           its compensation), velocity float[3N], mass/inv_mass float[N],
-//           pinned uint8[N] (bit k pins DOF k), load float[3N] (full-amplitude load),
+//           pinned uint8[N] (bit k pins DOF k; bit 3+k: DOF k is a driven edge DOF),
+//           load float[3N] (full-amplitude load),
 //           offset uint32[N+1] (CSR)
 //   slots:  float[3 * 8E] in CSR order
 #pragma once
@@ -61,6 +62,21 @@ struct ShellDevice {
     // the punch (zone.cpp:1150-1198): 1 for a node the indenter grips; null without one
     const uint8_t* driven = nullptr;
     double* n_punch = nullptr;        // FP64 punch work per node block (+=)
+    // The inertial punch (zone.cpp:1154-1185, ShellParams::inertial): the gripped nodes
+    // as a list for the one-block punch kernel, the striking body's account, and a halt
+    // flag that every kernel of the step reads first (set once the body has stopped).
+    const uint32_t* driven_list = nullptr;
+    int n_driven = 0;
+    double* punch_state = nullptr;    // [0] speed, [1] work, [2] penetration, [3] time, [4] steps
+    double* punch_kin = nullptr;      // kinetic energy of the gripped nodes (= per step)
+    int* halt = nullptr;
+    // The driven edge (zone.cpp:833-842, 1123-1145): pinned bit 3+k marks DOF k as
+    // driven rather than clamped.  Rows of the edge arrays are read only for marked nodes.
+    const int* edge_map = nullptr;    // [N]: the node's row
+    const double* edge_base = nullptr;   // [rows][3]: meshed - rest
+    const double* edge_drive = nullptr;  // [rows][3]: the prescribed value
+    double* n_edge = nullptr;         // FP64 boundary work per node block (+=)
+    double* n_damp = nullptr;         // FP64 damping loss per node block (+=)
     const float* fail_strain = nullptr;  // [E]; +inf never fails
     long long* counter = nullptr;     // [0] steps taken, [1] step of the current node pass
     // FP64 partials with a fixed mapping: one entry per warp of the element kernel
@@ -86,12 +102,17 @@ struct ShellParams {
     float swift_k, swift_eps0, swift_n;
     float kinematic;
     float tri_sens, tri_ref, tri_cut;
-    // the punch: speed along -axis, ramped linearly over punch_ramp seconds from rest
+    // the punch: speed along -axis, ramped linearly over punch_ramp seconds from rest;
+    // or, with inertial set, a striking body of punch_mass whose speed the grip sets
     float punch_speed;
     double punch_ramp;
+    int inertial;
+    double punch_mass;
+    double edge_ramp;                     // smoothstep ramp of the driven edge, s (0: at once)
     float axis_x, axis_y, axis_z;
     double inv_2mu, inv_3kappa;           // 1 / (2 mu), 1 / (3 kappa) in double (energy account)
     float dt, damping;
+    double damping64;                     // the damping as given: velocities are scaled in double
     double dt64, rise_time;               // load factor min((step+1) dt / rise, 1)
     int max_iterations;                   // EAS Newton cap
     float tol_residual, tol_work;         // relative to sigma_y V
@@ -100,6 +121,7 @@ struct ShellParams {
 
 constexpr int kShellBlock = 128;          // 16 elements per block
 constexpr int kShellNodeBlock = 256;
+constexpr int kShellPunchBlock = 256;   // the inertial punch: one block
 
 void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts);
 // Factor of the elastic K_aa per element for this material (into `out`, [E][32]).

@@ -287,6 +287,8 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
 // otherwise the linear law, whose state is only the plastic strain.
 template <bool KAHAN, bool GENERAL>
 __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(ShellDevice d, ShellParams p) {
+    // an inertial punch has stopped: the run is over (every thread reads the same flag)
+    if (d.halt && *d.halt) return;
     const int lane = threadIdx.x & 31;
     const int gp = lane & 7;
     const long long group_raw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -735,12 +737,27 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
 }
 
 template <bool KAHAN>
+__device__ __forceinline__ void shell_move(float* u, float* uc, float v, float dt) {
+    const float du = v * dt;
+    if (KAHAN) {
+        float c = *uc;
+        float s = *u;
+        kahan_add(s, c, du);
+        *u = s;
+        *uc = c;
+    } else {
+        *u += du;
+    }
+}
+
+template <bool KAHAN>
 __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, ShellParams p) {
     __shared__ double scratch[32];
+    if (d.halt && *d.halt) return;  // an inertial punch has stopped: the run is over
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double work = 0.0, kin = 0.0, pwork = 0.0;
+    double work = 0.0, kin = 0.0, pwork = 0.0, damp = 0.0, bwork = 0.0;
     if (n < d.nodes) {
-        const double t = (double)(d.counter[1] + 1) * p.dt64;
+        const double t = (double)(d.counter[1] + 1) * p.dt64;  // the time at the step's end
         const float lf = p.rise_time > 0.0 ? (float)(t / p.rise_time < 1.0 ? t / p.rise_time : 1.0) : 1.0f;
         float force[3] = {0.0f, 0.0f, 0.0f};
         const uint32_t b = d.offset[n], e = d.offset[n + 1];
@@ -755,23 +772,60 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
         const float im = d.inv_mass[n], m = d.mass[n];
         float* vel = d.velocity + (size_t)n * 3;
         float* u = d.disp + (size_t)n * 3;
+        float* uc = d.disp_c + (size_t)n * 3;
+        // force -> velocity; a driven edge DOF keeps the velocity it would have taken,
+        // for its work (zone.cpp:1094-1111)
+        float v3[3], ext[3], free_v[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float ext = d.load ? lf * d.load[(size_t)n * 3 + k] : 0.0f;
+            ext[k] = d.load ? lf * d.load[(size_t)n * 3 + k] : 0.0f;
             float v = vel[k];
             if (pin & (1u << k)) {
+                if (pin & (8u << k)) free_v[k] = m > 0.0f ? v + (force[k] + ext[k]) * im * p.dt : v;
                 v = 0.0f;
             } else if (m > 0.0f) {
-                v += (force[k] + ext) * im * p.dt;
+                v += (force[k] + ext[k]) * im * p.dt;
             }
-            v *= p.damping;
-            vel[k] = v;
-            work += (double)ext * (double)v * (double)p.dt;
+            v3[k] = v;
         }
-        // The punch holds the nodes it grips at -speed along its axis; the impulse that
-        // takes is its work (zone.cpp:1190-1198; solidshell_integrate.comp).  After the
-        // force update and the damping, before the position update.
-        if (d.driven && d.driven[n]) {
+        // the damping and the kinetic energy it removes (zone.cpp:1113-1121); the factor
+        // is applied in double, as given (its float would be off by ~1e-8, which is 1e-5
+        // of the loss 1 - d^2 at d = 0.999)
+        if (p.damping64 != 1.0)
+            damp = 0.5 * (double)m * ((double)v3[0] * v3[0] + (double)v3[1] * v3[1] + (double)v3[2] * v3[2]) *
+                   (1.0 - p.damping64 * p.damping64);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float v = (float)((double)v3[k] * p.damping64);
+            vel[k] = v;
+            work += (double)ext[k] * (double)v * (double)p.dt;
+        }
+        // The driven edge, after the damping and before the punch (zone.cpp:1123-1145):
+        // the velocity that lands the DOF on meshed + prescribed * smoothstep(t / ramp)
+        // this step; the boundary's work is what that costs over the free velocity.
+        if (pin & 0x38u) {
+            const int row = d.edge_map[n];
+            double fraction = 1.0;
+            if (p.edge_ramp > 0.0) {
+                const double r = fmin(1.0, fmax(0.0, t / p.edge_ramp));
+                fraction = r * r * (3.0 - 2.0 * r);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (!(pin & (8u << k))) continue;
+                const double now = KAHAN ? (double)u[k] - (double)uc[k] : (double)u[k];
+                const double target =
+                    (d.edge_base[(size_t)row * 3 + k] + d.edge_drive[(size_t)row * 3 + k] * fraction - now) / p.dt64;
+                bwork += (double)m * (target - (double)free_v[k]) * target;
+                vel[k] = (float)target;
+            }
+        }
+        // The prescribed punch holds the nodes it grips at -speed along its axis; the
+        // impulse that takes is its work (zone.cpp:1190-1198; solidshell_integrate.comp).
+        // After the edge, before the position update.  The inertial punch is the
+        // one-block shell_punch kernel that follows: it moves the gripped nodes itself.
+        bool gripped = d.driven && d.driven[n];
+        if (gripped && !p.inertial) {
             const double t0 = (double)d.counter[1] * p.dt64;  // time at the start of the step
             const float speed = p.punch_ramp > 0.0 && t0 < p.punch_ramp ? (float)(p.punch_speed * (t0 / p.punch_ramp))
                                                                          : p.punch_speed;
@@ -781,30 +835,93 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
             vel[1] += change * p.axis_y;
             vel[2] += change * p.axis_z;
             pwork = -((double)m * (double)change) * (double)speed;
+            gripped = false;
         }
+        if (!gripped) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float v = vel[k];
-            const float du = v * p.dt;
-            if (KAHAN) {
-                float c = d.disp_c[(size_t)n * 3 + k];
-                float s = u[k];
-                kahan_add(s, c, du);
-                u[k] = s;
-                d.disp_c[(size_t)n * 3 + k] = c;
-            } else {
-                u[k] += du;
+            for (int k = 0; k < 3; ++k) {
+                const float v = vel[k];
+                shell_move<KAHAN>(u + k, uc + k, v, p.dt);
+                kin += 0.5 * (double)m * (double)v * (double)v;
             }
-            kin += 0.5 * (double)m * (double)v * (double)v;
         }
     }
     const double bw = block_sum(work, scratch);
     const double bk = block_sum(kin, scratch);
-    const double bp = d.driven ? block_sum(pwork, scratch) : 0.0;
+    const double bp = d.driven && !p.inertial ? block_sum(pwork, scratch) : 0.0;
+    const double bd = p.damping64 != 1.0 ? block_sum(damp, scratch) : 0.0;
+    const double be = d.edge_map ? block_sum(bwork, scratch) : 0.0;
     if (threadIdx.x == 0) {
         d.n_work[blockIdx.x] += bw;
         d.n_kin[blockIdx.x] = bk;
-        if (d.driven) d.n_punch[blockIdx.x] += bp;
+        if (d.driven && !p.inertial) d.n_punch[blockIdx.x] += bp;
+        if (p.damping64 != 1.0) d.n_damp[blockIdx.x] += bd;
+        if (d.edge_map) d.n_edge[blockIdx.x] += be;
+    }
+}
+
+// The inertial punch (zone.cpp:1154-1198), one block after the node pass.  The grip is
+// a perfectly inelastic collision of the striking body with the gripped nodes:
+// momentum along the axis is conserved, V' = (M V + sum_i m_i u_i) / (M + sum_i m_i)
+// with u_i each node's speed along -axis; then every gripped node moves at V' along
+// -axis, the impulse that takes is the resisting force, and its work is the punch's.
+// The sums run in a fixed order (strided per thread, then block_sum), so the run is
+// deterministic.  A body that has stopped (V' <= 0) sets the halt flag, and every
+// kernel of the following steps returns at once, as zone::Solver ends the run
+// (zone.cpp:1225-1230).
+template <bool KAHAN>
+__global__ void __launch_bounds__(kShellPunchBlock) shell_punch(ShellDevice d, ShellParams p) {
+    __shared__ double scratch[32];
+    __shared__ double speed_s;
+    if (*d.halt) return;
+    double momentum = 0.0, gripped_mass = 0.0;
+    for (int i = threadIdx.x; i < d.n_driven; i += blockDim.x) {
+        const uint32_t n = d.driven_list[i];
+        const float* v = d.velocity + (size_t)n * 3;
+        const float along = v[0] * p.axis_x + v[1] * p.axis_y + v[2] * p.axis_z;
+        const double m = d.mass[n];
+        momentum -= m * (double)along;
+        gripped_mass += m;
+    }
+    momentum = block_sum(momentum, scratch);
+    gripped_mass = block_sum(gripped_mass, scratch);
+    if (threadIdx.x == 0) {
+        const double V = (p.punch_mass * d.punch_state[0] + momentum) / (p.punch_mass + gripped_mass);
+        d.punch_state[0] = V;
+        speed_s = V;
+    }
+    __syncthreads();
+    const double V = speed_s;
+    const float speed = (float)V;
+    double impulse = 0.0, kin = 0.0;
+    for (int i = threadIdx.x; i < d.n_driven; i += blockDim.x) {
+        const uint32_t n = d.driven_list[i];
+        float* v = d.velocity + (size_t)n * 3;
+        const float m = d.mass[n];
+        const float along = v[0] * p.axis_x + v[1] * p.axis_y + v[2] * p.axis_z;
+        const float change = -speed - along;
+        v[0] += change * p.axis_x;
+        v[1] += change * p.axis_y;
+        v[2] += change * p.axis_z;
+        impulse += (double)m * (double)change;
+        float* u = d.disp + (size_t)n * 3;
+        float* uc = d.disp_c + (size_t)n * 3;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            shell_move<KAHAN>(u + k, uc + k, v[k], p.dt);
+            kin += 0.5 * (double)m * (double)v[k] * (double)v[k];
+        }
+    }
+    impulse = block_sum(impulse, scratch);
+    kin = block_sum(kin, scratch);
+    if (threadIdx.x == 0) {
+        const double force = -impulse / p.dt64;
+        d.punch_state[1] += force * V * p.dt64;
+        d.punch_state[2] += V * p.dt64;
+        d.punch_state[3] += p.dt64;
+        d.punch_state[4] += 1.0;
+        *d.punch_kin = kin;
+        if (!(V > 0.0)) *d.halt = 1;
     }
 }
 
@@ -887,6 +1004,7 @@ void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t 
                 shell_forces<true, false><<<eb, kShellBlock, 0, stream>>>(d, p);
         }
         if (parts & 2) shell_nodes<true><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
+        if ((parts & 2) && p.inertial) shell_punch<true><<<1, kShellPunchBlock, 0, stream>>>(d, p);
     } else {
         if (parts & 1) {
             if (p.general)
@@ -895,6 +1013,7 @@ void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t 
                 shell_forces<false, false><<<eb, kShellBlock, 0, stream>>>(d, p);
         }
         if (parts & 2) shell_nodes<false><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
+        if ((parts & 2) && p.inertial) shell_punch<false><<<1, kShellPunchBlock, 0, stream>>>(d, p);
     }
 }
 

@@ -309,8 +309,13 @@ _sh_bytes = _sig("femstep_shell_device_bytes", C.c_size_t, [C.c_void_p])
 _sh_error = _sig("femstep_shell_error", C.c_char_p, [C.c_void_p])
 _sh_destroy = _sig("femstep_shell_destroy", None, [C.c_void_p])
 _sh_set_punch = _sig("femstep_shell_set_punch", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
-                                                           C.c_double, C.c_double])
+                                                           C.c_double, C.c_double, C.c_double])
 _sh_punch_state = _sig("femstep_shell_punch_state", C.c_int, [C.c_void_p, C.c_void_p])
+_sh_set_edge = _sig("femstep_shell_set_edge", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double])
+_sh_account = _sig("femstep_shell_account", C.c_int, [C.c_void_p, C.c_void_p])
+_sh_ck_size = _sig("femstep_shell_checkpoint_size", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)])
+_sh_ck = _sig("femstep_shell_checkpoint", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t])
+_sh_restore = _sig("femstep_shell_restore", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t])
 _sh_forms = _sig("femstep_shell_forms", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_double, C.c_double,
                                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p])
 
@@ -402,18 +407,48 @@ class ShellSolver:
         self._check(_sh_energy(self._h, _p(out)))
         return out
 
-    def set_punch(self, driven_nodes, axis, speed, ramp_time=0.0):
-        """The prescribed punch (zone.cpp:1150-1198): each step the driven nodes move at
-        -speed along `axis` (speed ramped over ramp_time seconds)."""
+    def set_punch(self, driven_nodes, axis, speed, ramp_time=0.0, mass=0.0):
+        """The punch (zone.cpp:1147-1198).  mass 0: prescribed, each step the driven nodes
+        move at -speed along `axis` (speed ramped over ramp_time seconds).  mass > 0: a
+        striking body of that mass arriving at `speed`, which the plating decelerates."""
         dn = np.ascontiguousarray(driven_nodes, np.uint32)
         ax = np.ascontiguousarray(axis, np.float64)
-        self._check(_sh_set_punch(self._h, _p(dn), dn.size, _p(ax), float(speed), float(ramp_time)))
+        self._check(_sh_set_punch(self._h, _p(dn), dn.size, _p(ax), float(speed), float(ramp_time), float(mass)))
 
     def punch_state(self):
         """{work, penetration, time, steps} of the punch (ZoneGpuState)."""
         out = np.zeros(4)
         self._check(_sh_punch_state(self._h, _p(out)))
         return {"work": out[0], "penetration": out[1], "time": out[2], "steps": int(out[3])}
+
+    def set_edge(self, prescribed, meshed=None, ramp=0.0):
+        """The driven edge (zone.cpp:833-842, 1123-1145): every pinned DOF with a non-zero
+        prescribed value follows meshed + prescribed * smoothstep(t / ramp)."""
+        pr = np.ascontiguousarray(prescribed, np.float64).reshape(-1)
+        me = None if meshed is None else np.ascontiguousarray(meshed, np.float64).reshape(-1)
+        if pr.size != 3 * self.nodes or (me is not None and me.size != 3 * self.nodes):
+            raise ValueError("prescribed and meshed are 3 values per node")
+        self._check(_sh_set_edge(self._h, _p(pr), None if me is None else _p(me), float(ramp)))
+
+    def checkpoint(self) -> np.ndarray:
+        """The whole mutable state as a host byte array (femstep_shell_checkpoint)."""
+        n = C.c_size_t()
+        self._check(_sh_ck_size(self._h, C.byref(n)))
+        buf = np.zeros(n.value, np.uint8)
+        self._check(_sh_ck(self._h, _p(buf), buf.size))
+        return buf
+
+    def restore(self, buf):
+        """Continue from a checkpoint of a solver of the same mesh, punch and edge."""
+        b = np.ascontiguousarray(buf, np.uint8)
+        self._check(_sh_restore(self._h, _p(b), b.size))
+
+    def account(self):
+        """{damping_loss, boundary_work, punch_speed, striker_kinetic, arrested, edge_dof}."""
+        out = np.zeros(6)
+        self._check(_sh_account(self._h, _p(out)))
+        return {"damping_loss": out[0], "boundary_work": out[1], "punch_speed": out[2], "striker_kinetic": out[3],
+                "arrested": bool(out[4]), "edge_dof": int(out[5])}
 
     def stats(self):
         out = np.zeros(2, np.int64)
@@ -558,6 +593,10 @@ _pl_admit = _sig("femstep_pool_admit", C.c_int, [C.c_void_p, C.POINTER(PoolMeshC
 _pl_admit_many = _sig("femstep_pool_admit_many", C.c_int, [C.c_void_p, C.POINTER(PoolMeshC), C.c_void_p, C.c_int,
                                                            C.c_void_p, C.POINTER(C.c_int)])
 _pl_release = _sig("femstep_pool_release", C.c_int, [C.c_void_p, C.c_int])
+_pl_ck_size = _sig("femstep_pool_checkpoint_size", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)])
+_pl_ck = _sig("femstep_pool_checkpoint", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t])
+_pl_resume = _sig("femstep_pool_admit_resume", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p,
+                                                          C.c_size_t, C.POINTER(C.c_int)])
 _pl_run_async = _sig("femstep_pool_run_async", C.c_int, [C.c_void_p, C.c_int, C.c_int])
 _pl_wait = _sig("femstep_pool_wait", C.c_int, [C.c_void_p, C.POINTER(C.c_double)])
 _pl_run = _sig("femstep_pool_run", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)])
@@ -659,6 +698,25 @@ class TetPool:
     def release(self, mesh_id):
         self._check(_pl_release(self._h, int(mesh_id)))
         self.sizes.pop(mesh_id, None)
+
+    def checkpoint(self, mesh_id) -> np.ndarray:
+        """One mesh's whole mutable state as a host byte array (for eviction)."""
+        n = C.c_size_t()
+        self._check(_pl_ck_size(self._h, int(mesh_id), C.byref(n)))
+        buf = np.zeros(n.value, np.uint8)
+        self._check(_pl_ck(self._h, int(mesh_id), _p(buf), buf.size))
+        return buf
+
+    def admit_resume(self, checkpoint, steps, **mesh) -> int:
+        """Admit the mesh of `checkpoint` again and continue from it, up to `steps` in
+        total; raises PoolFull when it does not fit now."""
+        keep = []
+        m = self._mesh(keep, **mesh)
+        b = np.ascontiguousarray(checkpoint, np.uint8)
+        out = C.c_int()
+        self._check(_pl_resume(self._h, C.byref(m), int(steps), _p(b), b.size, C.byref(out)))
+        self.sizes[out.value] = (m.nodes, m.tets)
+        return out.value
 
     def run(self, steps, mode=POOL_AUTO) -> float:
         ms = C.c_double()

@@ -139,6 +139,35 @@ def shell_plate(ref):
                         state=m.state, energy=energy, mass=m.mass)
 
 
+ZONE_CASES = {
+    # name: (zone_plate keyword arguments); the plate of the reference's zone GPU tests
+    "prescribed": dict(steps=300),
+    "inertial_damped_edge": dict(steps=300, mass=40.0, speed=20.0, damping=0.999, edge_drive=(2e-3, 1e-3, 3e-3),
+                                 edge_ramp=2e-4),
+    "arrest": dict(steps=3000, mass=0.6, speed=6.0),
+    "tearing": dict(steps=3000, edge_drive=(1e-3, 0.0, 2e-3), edge_ramp=1e-3),
+}
+
+
+def zone_plate(ref):
+    # zone::Solver itself (engine/sim/zone.cpp) on the flat plate of the reference's zone
+    # GPU tests: the arrays it was built from and, per case, where it ended.
+    out = {}
+    for name, case in ZONE_CASES.items():
+        r = ref.zone_plate(**case)
+        assert r["problems"] == 0, name
+        if not out:
+            out.update(rest=r["rest"], index=r["index"], pinned=r["pinned"], driven=r["driven"], mass=r["mass"],
+                       state0=r["state0"], material=r["mat"], density=r["density"], dt=r["dt"])
+        assert np.array_equal(out["state0"], r["state0"]) and out["dt"] == r["dt"]
+        out[f"{name}_prescribed"] = r["prescribed"]
+        out[f"{name}_position"] = r["position"]
+        out[f"{name}_velocity"] = r["velocity"]
+        out[f"{name}_state"] = r["state"]
+        out[f"{name}_account"] = np.array([r["account"][k] for k in O.ZONE_ACCOUNT])
+    np.savez_compressed(os.path.join(HERE, "zone_plate.npz"), **out)
+
+
 if __name__ == "__main__":
     ref = O.Oracle("ref")
     port = O.Oracle("port")
@@ -147,5 +176,6 @@ if __name__ == "__main__":
     tet64(ref, port)
     shell(ref)
     shell_plate(ref)
+    zone_plate(ref)
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

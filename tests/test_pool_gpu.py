@@ -236,3 +236,42 @@ def test_pool_meshes_against_fp64_oracle(fem, port, k):
     assert abs(e[0] - er[0]) / er[0] < 5e-3
     for j in (1, 2, 3):
         assert abs(e[j] - er[j]) <= 5e-3 * er[0]
+
+
+def test_evict_and_resume_is_bit_identical(fem):
+    """A mesh checkpointed mid-run, released, and admitted again later (elsewhere in the
+    pool, next to other meshes, after the others moved on) ends with the same bits --
+    state and FP64 energy account -- as when it never left."""
+    a = beam(fem, 30, 3, 3, load=400e3)
+    others = [beam(fem, 16, 2, 2, load=80e3), beam(fem, 50, 4, 4, length=2.0, load=120e3)]
+    alone = fem.TetPool(100000, 30000, max_meshes=4)
+    ia = alone.admit(steps=1500, ramp_steps=500, **MATS[0], **a)
+    alone.run(1500)
+    pa, va = alone.readback(ia)
+    ea, pla = alone.energy(ia), alone.plastic(ia)
+    assert (pla[:, 6] > 0).mean() > 0.05, "the case must exercise plasticity"
+
+    pool = fem.TetPool(300000, 90000, max_meshes=8)
+    j0 = pool.admit(steps=4000, ramp_steps=300, **MATS[1], **others[0])
+    ib = pool.admit(steps=1500, ramp_steps=500, **MATS[0], **a)
+    pool.run(333)
+    ck = pool.checkpoint(ib)
+    pool.release(ib)
+    # someone else takes the space, the pool moves on without the mesh
+    j1 = pool.admit(steps=4000, ramp_steps=300, **MATS[2], **others[1])
+    pool.run(71, fem.POOL_PERSISTENT)
+    with pytest.raises(fem.FemStepError):
+        pool.admit_resume(ck, 100, ramp_steps=500, **MATS[0], **a)  # below the steps taken
+    ic = pool.admit_resume(ck, 1500, ramp_steps=500, **MATS[0], **a)
+    assert pool.status(ic) == (333, 1500)
+    for k, chunk in enumerate((5, 400, 29, 900)):
+        pool.run(chunk, (fem.POOL_GRAPH, fem.POOL_GRAPH_STAGED, fem.POOL_PERSISTENT, fem.POOL_GRAPH)[k])
+    assert pool.status(ic)[0] == 1500
+    pc, vc = pool.readback(ic)
+    assert np.array_equal(pa, pc) and np.array_equal(va, vc)
+    assert np.array_equal(pla, pool.plastic(ic))
+    assert np.array_equal(ea, pool.energy(ic))
+    assert pool.status(j0)[0] == 333 + 71 + 1334 and pool.status(j1)[0] == 71 + 1334
+    # a checkpoint of another mesh is refused
+    with pytest.raises(fem.FemStepError):
+        pool.admit_resume(ck, 1500, **MATS[0], **others[0])

@@ -70,3 +70,35 @@ def test_oracle_zone_step_is_the_reference_solver(ref, port, name):
         assert ra["arrested"] and ra["steps"] < case["steps"]
     if name in ("tearing", "everything"):
         assert (st[:, 128] != 0).sum() > 0 and (st[:, 14:120:15] != 0).sum() > 0
+
+
+def golden_zone():
+    """The zone fixture and the cases it was made with (tests/golden/make_golden.py)."""
+    import importlib.util
+    import os
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(here, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.ZONE_CASES, np.load(os.path.join(here, "zone_plate.npz"))
+
+
+@pytest.mark.parametrize("name", ["prescribed", "inertial_damped_edge", "arrest", "tearing"])
+def test_oracle_zone_step_golden(port, name):
+    """The same pin without the compiled reference: the restatement reproduces the
+    fixture zone::Solver wrote, bit for bit."""
+    cases, g = golden_zone()
+    case = cases[name]
+    r = dict(rest=g["rest"], index=g["index"], pinned=g["pinned"], mat=g["material"], density=float(g["density"]),
+             driven=g["driven"], prescribed=g[f"{name}_prescribed"], dt=float(g["dt"]))
+    m = port_zone(port, r, case)
+    assert np.array_equal(m.mass, g["mass"])
+    assert np.array_equal(m.position, g[f"{name}_position"])
+    assert np.array_equal(m.velocity, g[f"{name}_velocity"])
+    assert np.array_equal(m.state, g[f"{name}_state"])
+    acc = dict(zip(O.ZONE_ACCOUNT, g[f"{name}_account"]))
+    a = m.account
+    assert (m.punch_work, a["penetration"], a["damping_loss"], a["boundary_work"]) == (
+        acc["work"], acc["penetration"], acc["damping_loss"], acc["boundary_work"])
+    assert m.steps == acc["steps"] and a["arrested"] == bool(acc["arrested"])
