@@ -1462,9 +1462,91 @@ void or_shell_setup(or_shell *m, const double *mat, double density) {
 
 /* Solver::step for a patch with no punch and no driven edge, with an external
  * nodal load: zone.cpp:928-989, 1094-1121, 1200-1202. */
+/* The uniaxial return of a fibre (constraint.cpp:39-95): backward Euler on the flow
+   rule, isotropic hardening only, a Newton solve of the consistency condition (32
+   iterations, 1e-13 relative), then the damage increment with the bar's closed-form
+   triaxiality +-1/3 (constraint.cpp:102-109).  st: plastic strain, eq. plastic
+   strain, damage, failed. */
+static double fiber_return(const double *mat, double failure_strain, double strain, double *st,
+                           double *dissipation_per_volume) {
+    *dissipation_per_volume = 0.0;
+    if (st[3] != 0.0) return 0.0;
+    const double youngs = mat[0];
+    const double trial = youngs * (strain - st[0]);
+    const double yield = flow_stress(mat, st[1]);
+    if (fabs(trial) <= yield) return trial;
+    const double slope0 = flow_slope(mat, st[1]);
+    double increment = (fabs(trial) - yield) / (youngs + slope0);
+    for (int it = 0; it < 32; ++it) {
+        const double residual = fabs(trial) - youngs * increment - flow_stress(mat, st[1] + increment);
+        if (fabs(residual) <= 1e-13 * (yield + fabs(trial))) break;
+        const double slope = youngs + flow_slope(mat, st[1] + increment);
+        if (!(slope > 0)) break;
+        increment += residual / slope;
+        if (increment < 0) increment = 0;
+    }
+    const double direction = trial >= 0 ? 1.0 : -1.0;
+    const double stress = trial - direction * youngs * increment;
+    st[0] += direction * increment;
+    st[1] += increment;
+    *dissipation_per_volume = fabs(stress) * increment;
+    const double eta = stress == 0.0 ? 0.0 : (stress > 0.0 ? 1.0 : -1.0) / 3.0;
+    const double critical = failure_strain * triax_factor(mat, eta);
+    if (critical > 0.0 && isfinite(critical)) st[2] += increment / critical;
+    if (st[2] >= 1.0) {
+        st[2] = 1.0;
+        st[3] = 1.0;
+        return 0.0;
+    }
+    return stress;
+}
+
+/* fiberForces (constraint.cpp:198-258): every fibre's co-rotational axial force, added
+   into `force` through its ties in fibre order.  Returns the plastic dissipation of
+   the increment; the recoverable strain energy goes to m->fiber_energy. */
+static double fiber_forces(or_shell *m, const double *mat, double *force) {
+    double dissipation = 0.0, energy = 0.0;
+    const double youngs = mat[0];
+    for (size_t i = 0; i < m->fibers; ++i) {
+        const double rest_length = m->fiber_length[i], area = m->fiber_area[i];
+        if (!(rest_length > 0) || !(area > 0)) continue;
+        const uint32_t *tie = m->fiber_tie + i * 4;
+        const double *w = m->fiber_weight + i * 2;
+        double end[2][3];
+        for (int e = 0; e < 2; ++e)
+            for (int k = 0; k < 3; ++k)
+                end[e][k] = m->position[(size_t)tie[2 * e] * 3 + k] * (1.0 - w[e]) +
+                            m->position[(size_t)tie[2 * e + 1] * 3 + k] * w[e];
+        double span[3];
+        for (int k = 0; k < 3; ++k) span[k] = end[1][k] - end[0][k];
+        const double l = sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
+        if (!(l > 0)) continue;
+        double axis[3];
+        for (int k = 0; k < 3; ++k) axis[k] = span[k] / l;
+        const double strain = (l - rest_length) / rest_length;
+        double dpv = 0.0;
+        const double stress = fiber_return(mat, m->fiber_fail[i], strain, m->fiber_state + i * 4, &dpv);
+        dissipation += dpv * area * rest_length;
+        const double axial = stress * area;
+        for (int e = 0; e < 2; ++e) {
+            const double sign_axial = e == 0 ? axial : -axial;
+            const size_t bottom = (size_t)tie[2 * e] * 3, top = (size_t)tie[2 * e + 1] * 3;
+            for (int k = 0; k < 3; ++k) {
+                const double f = axis[k] * sign_axial;
+                force[bottom + k] += (1.0 - w[e]) * f;
+                force[top + k] += w[e] * f;
+            }
+        }
+        energy += 0.5 * stress * stress / youngs * area * rest_length;
+    }
+    m->fiber_energy = energy;
+    return dissipation;
+}
+
 void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int steps) {
     /* the velocity each driven-edge DOF would have taken had nothing held it */
     double *edge_free = m->prescribed ? (double *)calloc(m->nodes * 3, sizeof(double)) : NULL;
+    double *gathered = (double *)malloc(m->nodes * 3 * sizeof(double));
     for (int s = 0; s < steps && !m->arrested; ++s) {
         const double time = (double)(m->step + 1) * p->dt;
         const double lf = p->rise_time > 0 ? dmin(time / p->rise_time, 1.0) : 1.0;
@@ -1488,9 +1570,8 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
             or_shell_plastic_update(m->forms + e * OR_FORMS_LEN, rest, current, mat, st, out, stress, info);
             dissipation += info[4];
         }
-        /* force -> velocity (zone.cpp:1094-1111); the kinetic energy before the damping
-           and the damping's loss (zone.cpp:1113-1121) */
-        double work = 0.0, before = 0.0;
+        /* the gather (zone.cpp:976-989), then the stiffeners' forces through their ties,
+           in fibre order (zone.cpp:990-1002) */
         for (size_t node = 0; node < m->nodes; ++node) {
             double sum[3] = {0, 0, 0};
             for (uint32_t k = m->adj_offset[node]; k < m->adj_offset[node + 1]; ++k) {
@@ -1500,11 +1581,18 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
                 sum[1] += f[1];
                 sum[2] += f[2];
             }
+            for (int k = 0; k < 3; ++k) gathered[node * 3 + (size_t)k] = sum[k];
+        }
+        if (m->fibers) dissipation += fiber_forces(m, mat, gathered);
+        /* force -> velocity (zone.cpp:1094-1111); the kinetic energy before the damping
+           and the damping's loss (zone.cpp:1113-1121) */
+        double work = 0.0, before = 0.0;
+        for (size_t node = 0; node < m->nodes; ++node) {
             double ext[3];
             for (int k = 0; k < 3; ++k) {
                 const size_t d = node * 3 + (size_t)k;
                 ext[k] = m->fext ? lf * m->fext[d] : 0.0;
-                const double force = sum[k] + ext[k];
+                const double force = gathered[d] + ext[k];
                 if (m->pinned[d]) {
                     if (edge_free && m->prescribed[d] != 0.0) {
                         double free_velocity = m->velocity[d];
@@ -1588,6 +1676,7 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
         if (m->driven && m->punch_mass > 0 && !(m->punch_velocity > 0)) m->arrested = 1;
     }
     free(edge_free);
+    free(gathered);
 }
 
 /* accumulateEnergy, zone.cpp:1014-1044 */

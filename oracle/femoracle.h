@@ -191,6 +191,18 @@ typedef struct {
     double punch_velocity;    /* m/s along -axis (state of the striking body) */
     int arrested;             /* the striking body has stopped: no further steps run */
     double account[4];        /* damping loss, boundary work, penetration, time */
+    /* Constraint fibres (engine/sim/constraint.hpp, zone.cpp:990-1002): the axial bars of
+       eccentric stiffeners, each end tied to a through-thickness node pair as
+       (1 - w) x[bottom] + w x[top].  Their forces are added after the plating's gather,
+       in fibre order. */
+    size_t fibers;
+    uint32_t *fiber_tie;      /* 4 per fibre: end 0 bottom, top; end 1 bottom, top */
+    double *fiber_weight;     /* 2 per fibre: the ties' weights */
+    double *fiber_area;       /* m^2 */
+    double *fiber_length;     /* rest length, m (restFibers) */
+    double *fiber_fail;       /* failure strain (fiberFailureStrain); inf never fails */
+    double *fiber_state;      /* 4 per fibre: plastic strain, eq. plastic strain, damage, failed */
+    double fiber_energy;      /* the fibres' recoverable strain energy after the last step */
 } or_shell;
 
 typedef struct {
@@ -213,6 +225,10 @@ typedef struct {
     double damping, edge_ramp;
     double edge_drive[3];             /* a perimeter DOF's prescribed value: edge_drive * x / lx */
     int steps;
+    /* flat-bar stiffeners along x, as constraint fibres (constraint::addStiffener) */
+    int stiffeners;                   /* lines at y = ly (s + 1) / (stiffeners + 1), on grid lines */
+    double web_height, web_thickness;
+    int fiber_failure;                /* SolveParams::fiberFailure */
 } or_zone_case;
 typedef struct {
     double *rest;                     /* 3N meshed position (= rest) */
@@ -229,6 +245,11 @@ typedef struct {
     double account[10];               /* work, dissipation, penetration, time, damping loss,
                                          boundary work, indenter speed, steps, arrested,
                                          driven edge DOFs */
+    /* the fibres as or_shell takes them, and their state after the steps */
+    uint32_t *fiber_tie;              /* 4F */
+    double *fiber_weight;             /* 2F */
+    double *fiber_area, *fiber_length, *fiber_fail;  /* F */
+    double *fiber_state;              /* 4F */
 } or_zone_out;
 
 void or_shell_setup(or_shell *m, const double *mat, double density);

@@ -77,7 +77,11 @@ class Shell(C.Structure):
                 ("energy", C.c_double * 5), ("step", C.c_long), ("driven", C.POINTER(C.c_uint8)),
                 ("axis", C.c_double * 3), ("prescribed", C.POINTER(C.c_double)),
                 ("meshed", C.POINTER(C.c_double)), ("edge_ramp", C.c_double), ("punch_mass", C.c_double),
-                ("punch_velocity", C.c_double), ("arrested", C.c_int), ("account", C.c_double * 4)]
+                ("punch_velocity", C.c_double), ("arrested", C.c_int), ("account", C.c_double * 4),
+                ("fibers", C.c_size_t), ("fiber_tie", C.POINTER(C.c_uint32)), ("fiber_weight", C.POINTER(C.c_double)),
+                ("fiber_area", C.POINTER(C.c_double)), ("fiber_length", C.POINTER(C.c_double)),
+                ("fiber_fail", C.POINTER(C.c_double)), ("fiber_state", C.POINTER(C.c_double)),
+                ("fiber_energy", C.c_double)]
 
 
 class ShellParams(C.Structure):
@@ -89,7 +93,9 @@ class ZoneCase(C.Structure):
     _fields_ = [("lx", C.c_double), ("ly", C.c_double), ("thickness", C.c_double), ("nx", C.c_int),
                 ("ny", C.c_int), ("nz", C.c_int), ("half_length", C.c_double), ("half_width", C.c_double),
                 ("speed", C.c_double), ("ramp_time", C.c_double), ("mass", C.c_double), ("damping", C.c_double),
-                ("edge_ramp", C.c_double), ("edge_drive", C.c_double * 3), ("steps", C.c_int)]
+                ("edge_ramp", C.c_double), ("edge_drive", C.c_double * 3), ("steps", C.c_int),
+                ("stiffeners", C.c_int), ("web_height", C.c_double), ("web_thickness", C.c_double),
+                ("fiber_failure", C.c_int)]
 
 
 class ZoneOut(C.Structure):
@@ -99,7 +105,10 @@ class ZoneOut(C.Structure):
                 ("state0", C.POINTER(C.c_double)), ("position", C.POINTER(C.c_double)),
                 ("velocity", C.POINTER(C.c_double)), ("state", C.POINTER(C.c_double)),
                 ("mat", C.c_double * MAT_LEN), ("density", C.c_double), ("dt", C.c_double),
-                ("account", C.c_double * 10)]
+                ("account", C.c_double * 10), ("fiber_tie", C.POINTER(C.c_uint32)),
+                ("fiber_weight", C.POINTER(C.c_double)), ("fiber_area", C.POINTER(C.c_double)),
+                ("fiber_length", C.POINTER(C.c_double)), ("fiber_fail", C.POINTER(C.c_double)),
+                ("fiber_state", C.POINTER(C.c_double))]
 
 
 ZONE_ACCOUNT = ("work", "dissipation", "penetration", "time", "damping_loss", "boundary_work", "punch_speed",
@@ -172,23 +181,28 @@ class Oracle:
 
     def zone_plate(self, lx=0.4, ly=0.2, thickness=0.01, nx=8, ny=4, nz=1, half_length=0.05, half_width=0.05,
                    speed=20.0, ramp_time=1e-4, mass=0.0, damping=1.0, edge_ramp=0.0, edge_drive=(0.0, 0.0, 0.0),
-                   steps=100) -> dict:
+                   steps=100, stiffeners=0, web_height=0.05, web_thickness=0.008, fiber_failure=True) -> dict:
         """The reference's zone::Solver stepped `steps` times on a flat plate (ref only):
         the arrays it was built from, where it ended and its account."""
         c = ZoneCase(lx, ly, thickness, nx, ny, nz, half_length, half_width, speed, ramp_time, mass, damping,
-                     edge_ramp, (C.c_double * 3)(*edge_drive), steps)
-        sizes = (C.c_size_t * 2)()
+                     edge_ramp, (C.c_double * 3)(*edge_drive), steps, stiffeners, web_height, web_thickness,
+                     int(bool(fiber_failure)))
+        sizes = (C.c_size_t * 3)()
         self.zone_sizes(C.byref(c), sizes)
-        n, e = sizes[0], sizes[1]
+        n, e, f = sizes[0], sizes[1], sizes[2]
         r = dict(rest=np.zeros(3 * n), index=np.zeros(8 * e, np.uint32), pinned=np.zeros(3 * n, np.uint8),
                  prescribed=np.zeros(3 * n), driven=np.zeros(n, np.uint8), mass=np.zeros(n),
                  state0=np.zeros(SHELL_STATE_LEN * e), position=np.zeros(3 * n), velocity=np.zeros(3 * n),
-                 state=np.zeros(SHELL_STATE_LEN * e))
+                 state=np.zeros(SHELL_STATE_LEN * e), fiber_tie=np.zeros(4 * f, np.uint32),
+                 fiber_weight=np.zeros(2 * f), fiber_area=np.zeros(f), fiber_length=np.zeros(f),
+                 fiber_fail=np.zeros(f), fiber_state=np.zeros(4 * f))
         o = ZoneOut()
         for name, ct in (("rest", C.c_double), ("index", C.c_uint32), ("pinned", C.c_uint8),
                          ("prescribed", C.c_double), ("driven", C.c_uint8), ("mass", C.c_double),
                          ("state0", C.c_double), ("position", C.c_double), ("velocity", C.c_double),
-                         ("state", C.c_double)):
+                         ("state", C.c_double), ("fiber_tie", C.c_uint32), ("fiber_weight", C.c_double),
+                         ("fiber_area", C.c_double), ("fiber_length", C.c_double), ("fiber_fail", C.c_double),
+                         ("fiber_state", C.c_double)):
             setattr(o, name, _ptr(r[name], ct))
         r["problems"] = self.zone_run(C.byref(c), C.byref(o))
         r["mat"] = np.array(list(o.mat))
@@ -395,6 +409,32 @@ class ShellModel:
             self.meshed = np.ascontiguousarray(meshed, np.float64).reshape(-1).copy()
             self._s.meshed = _ptr(self.meshed, C.c_double)
         self._s.edge_ramp = float(ramp)
+
+    def set_fibers(self, tie, weight, area, length, fail, density=None):
+        """Constraint fibres (constraint.hpp): tie [F][4] node ids (end 0 bottom, top; end 1
+        bottom, top), weight [F][2], area, rest length and failure strain [F].  With a
+        density, each fibre's mass is lumped a quarter to each of its four nodes, in fibre
+        order (lumpFiberMass, constraint.cpp:260-276)."""
+        f = int(np.asarray(area).size)
+        if density is not None:
+            t = np.asarray(tie, np.int64).reshape(-1, 4)
+            for i in range(f):
+                if not (length[i] > 0 and area[i] > 0):
+                    continue
+                quarter = 0.25 * density * float(area[i]) * float(length[i])
+                for k in range(4):
+                    self.mass[t[i, k]] += quarter
+        self.fiber_tie = np.ascontiguousarray(tie, np.uint32).reshape(-1).copy()
+        self.fiber_weight = np.ascontiguousarray(weight, np.float64).reshape(-1).copy()
+        self.fiber_area = np.ascontiguousarray(area, np.float64).reshape(-1).copy()
+        self.fiber_length = np.ascontiguousarray(length, np.float64).reshape(-1).copy()
+        self.fiber_fail = np.ascontiguousarray(fail, np.float64).reshape(-1).copy()
+        self.fiber_state = np.zeros(4 * f)
+        s = self._s
+        s.fibers = f
+        for name, ct in (("fiber_tie", C.c_uint32), ("fiber_weight", C.c_double), ("fiber_area", C.c_double),
+                         ("fiber_length", C.c_double), ("fiber_fail", C.c_double), ("fiber_state", C.c_double)):
+            setattr(s, name, _ptr(getattr(self, name), ct))
 
     @property
     def account(self):

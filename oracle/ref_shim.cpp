@@ -12,6 +12,7 @@
 // (the J2 tet, the pressure-loaded shell step), the composition is written here on
 // top of the reference's functions, and says which ones.
 #include "engine/core/jobs.hpp"
+#include "engine/sim/constraint.hpp"
 #include "engine/sim/fem.hpp"
 #include "engine/sim/plasticity.hpp"
 #include "engine/sim/scantlings.hpp"
@@ -738,6 +739,23 @@ sim::zone::Patch platePatch(const or_zone_case* c) {
     patch.thickness = c->thickness;
     patch.criticalTimestep =
         ss::criticalTimestep(flat, patch.material, ss::Formulation::SolidShell);
+    // flat-bar stiffeners along x on grid lines, the web on the -z side
+    if (c->stiffeners > 0) {
+        patch.stiffening.material = sim::ah36Steel();
+        const int nzp = c->nz + 1;
+        for (int s = 0; s < c->stiffeners; ++s) {
+            const int j = (int)std::lround((double)c->ny * (s + 1) / (c->stiffeners + 1));
+            sim::constraint::SeamRun run;
+            run.sign = -1.0;
+            for (int i = 0; i <= c->nx; ++i) {
+                const uint32_t base = (uint32_t)((i * (c->ny + 1) + j) * nzp);
+                run.bottom.push_back(base);
+                run.top.push_back(base + (uint32_t)c->nz);
+            }
+            sim::constraint::addStiffener(run, sim::flatBar(c->web_height, c->web_thickness), c->thickness,
+                                          patch.mesh.position, patch.stiffening);
+        }
+    }
     return patch;
 }
 
@@ -754,15 +772,17 @@ sim::zone::SolveParams plateParams(const or_zone_case* c) {
     }
     params.damping = c->damping;
     params.edgeRamp = c->edge_ramp;
+    params.fiberFailure = c->fiber_failure != 0;
     return params;
 }
 
 }  // namespace
 
-extern "C" int ref_zone_sizes(const or_zone_case* c, size_t out[2]) {
-    const ss::HexMesh flat = ss::makePlateMesh(c->lx, c->ly, c->thickness, c->nx, c->ny, c->nz);
-    out[0] = flat.nodeCount();
-    out[1] = flat.elementCount();
+extern "C" int ref_zone_sizes(const or_zone_case* c, size_t out[3]) {
+    const sim::zone::Patch patch = platePatch(c);
+    out[0] = patch.nodeCount();
+    out[1] = patch.elementCount();
+    out[2] = patch.stiffening.fiberCount();
     return 0;
 }
 
@@ -796,6 +816,30 @@ extern "C" int ref_zone_run(const or_zone_case* c, or_zone_out* o) {
                                 r.indenterSpeed, (double)r.steps, r.indenterArrested ? 1.0 : 0.0,
                                 (double)r.drivenEdgeDof};
     std::copy(account, account + 10, o->account);
+    // the fibres as the solver holds them (zone.cpp:724-733): rest lengths from rest_,
+    // each fibre's own failure strain, and their state after the steps
+    const sim::constraint::Stiffening& st = patch.stiffening;
+    const sim::constraint::RestFibers forms = sim::constraint::restFibers(st, solver.rest());
+    for (std::size_t i = 0; i < st.fiberCount(); ++i) {
+        const sim::constraint::Fiber& f = st.fiber[i];
+        o->fiber_tie[i * 4] = f.end[0].bottom;
+        o->fiber_tie[i * 4 + 1] = f.end[0].top;
+        o->fiber_tie[i * 4 + 2] = f.end[1].bottom;
+        o->fiber_tie[i * 4 + 3] = f.end[1].top;
+        o->fiber_weight[i * 2] = f.end[0].weight;
+        o->fiber_weight[i * 2 + 1] = f.end[1].weight;
+        o->fiber_area[i] = f.area;
+        o->fiber_length[i] = forms.length[i];
+        o->fiber_fail[i] = params.fiberFailure
+                               ? sim::constraint::fiberFailureStrain(material.failure, forms.length[i], f.neckWidth)
+                               : pl::kNeverFails;
+        const sim::constraint::FiberState zero{};
+        const sim::constraint::FiberState& fs = i < solver.fiberState().size() ? solver.fiberState()[i] : zero;
+        o->fiber_state[i * 4] = fs.plasticStrain;
+        o->fiber_state[i * 4 + 1] = fs.equivalentPlasticStrain;
+        o->fiber_state[i * 4 + 2] = fs.damage;
+        o->fiber_state[i * 4 + 3] = fs.failed ? 1.0 : 0.0;
+    }
     return (int)r.problems.size();
 }
 

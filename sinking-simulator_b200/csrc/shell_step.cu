@@ -441,13 +441,9 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
 
     // ---- start-of-step state ----
     const size_t sbase = (size_t)group * kShellStateQ * 32 + lane;
-    float ps[7], pc[7];
+    float ps[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) ps[k] = d.state[sbase + (size_t)k * 32];
-    if (KAHAN) {
-#pragma unroll
-        for (int k = 0; k < 7; ++k) pc[k] = d.state[sbase + (size_t)(7 + k) * 32];
-    }
     float back0[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, damage0 = 0.0f, fstrain = INFINITY;
     bool failed0 = false;
     const size_t sbase2 = (size_t)group * kShellState2Q * 32 + lane;
@@ -520,27 +516,22 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         float l[28];
         bool spd = true;
         if (__any_sync(0xffffffffu, !elastic_element)) {
-        // K_aa = sum_g w_g G^T C G, lower triangle
+        // K_aa = sum_g w_g G^T C G, lower triangle, one column of C G at a time (six
+        // live values rather than 42: the same products in the same order)
         float kaa[28];
-        {
-            float cg[7][6];
 #pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                float g[6];
+        for (int b = 0; b < 7; ++b) {
+            float g[6], cgb[6];
 #pragma unroll
-                for (int i = 0; i < 6; ++i) g[i] = G[i * 7 + k];
-                tangent_apply(o, p, g, cg[k]);
+            for (int i = 0; i < 6; ++i) g[i] = G[i * 7 + b];
+            tangent_apply(o, p, g, cgb);
+#pragma unroll
+            for (int a = b; a < 7; ++a) {
+                float s = 0.0f;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) s += G[i * 7 + a] * cgb[i];
+                kaa[a * (a + 1) / 2 + b] = sum8(w * s);
             }
-            int t = 0;
-#pragma unroll
-            for (int a = 0; a < 7; ++a)
-#pragma unroll
-                for (int b = 0; b <= a; ++b) {
-                    float s = 0.0f;
-#pragma unroll
-                    for (int i = 0; i < 6; ++i) s += G[i * 7 + a] * cg[b][i];
-                    kaa[t++] = sum8(w * s);
-                }
         }
         // Cholesky (solid_shell.cpp:432-457), identical in every lane
         {
@@ -643,6 +634,10 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         if (o.yielded) {
             diss = (double)w * (double)o.diss;
             if (KAHAN) {
+                // the compensations are read only here, where a yielded point needs them
+                float pc[7];
+#pragma unroll
+                for (int k = 0; k < 7; ++k) pc[k] = d.state[sbase + (size_t)(7 + k) * 32];
 #pragma unroll
                 for (int i = 0; i < 6; ++i) kahan_add(ps[i], pc[i], o.dp[i]);
                 kahan_add(ps[6], pc[6], o.deq);

@@ -146,6 +146,9 @@ ZONE_CASES = {
                                  edge_ramp=2e-4),
     "arrest": dict(steps=3000, mass=0.6, speed=6.0),
     "tearing": dict(steps=3000, edge_drive=(1e-3, 0.0, 2e-3), edge_ramp=1e-3),
+    # flat-bar stiffeners as constraint fibres (constraint::addStiffener), yielding and tearing
+    "stiffened": dict(steps=300, stiffeners=1),
+    "stiffened_tearing": dict(steps=3000, stiffeners=2, web_height=0.03, web_thickness=0.006),
 }
 
 
@@ -161,6 +164,9 @@ def zone_plate(ref):
                        state0=r["state0"], material=r["mat"], density=r["density"], dt=r["dt"])
         assert np.array_equal(out["state0"], r["state0"]) and out["dt"] == r["dt"]
         out[f"{name}_prescribed"] = r["prescribed"]
+        out[f"{name}_mass"] = r["mass"]  # with the fibres' lumped mass when there are stiffeners
+        for k in ("fiber_tie", "fiber_weight", "fiber_area", "fiber_length", "fiber_fail", "fiber_state"):
+            out[f"{name}_{k}"] = r[k]
         out[f"{name}_position"] = r["position"]
         out[f"{name}_velocity"] = r["velocity"]
         out[f"{name}_state"] = r["state"]

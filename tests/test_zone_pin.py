@@ -24,6 +24,9 @@ CASES = {
     "tearing": dict(steps=3000),
     "everything": dict(steps=3000, mass=400.0, speed=20.0, damping=0.9995, edge_drive=(1e-3, 0.0, 2e-3),
                        edge_ramp=1e-3),
+    "stiffened": dict(steps=300, stiffeners=1),
+    "stiffened-tearing": dict(steps=3000, stiffeners=2, web_height=0.03, web_thickness=0.006),
+    "stiffened-no-fibre-failure": dict(steps=3000, stiffeners=1, fiber_failure=False),
 }
 
 
@@ -33,6 +36,9 @@ def port_zone(port, r, case):
                 speed=case.get("speed", 20.0))
     if any(case.get("edge_drive", (0.0, 0.0, 0.0))):
         m.set_edge(r["prescribed"], ramp=case.get("edge_ramp", 0.0))
+    if case.get("stiffeners", 0):
+        m.set_fibers(r["fiber_tie"], r["fiber_weight"], r["fiber_area"], r["fiber_length"], r["fiber_fail"],
+                     density=r["density"])
     m.step(r["dt"], case["steps"], damping=case.get("damping", 1.0), punch_speed=case.get("speed", 20.0),
            punch_ramp=1e-4)
     return m
@@ -70,6 +76,15 @@ def test_oracle_zone_step_is_the_reference_solver(ref, port, name):
         assert ra["arrested"] and ra["steps"] < case["steps"]
     if name in ("tearing", "everything"):
         assert (st[:, 128] != 0).sum() > 0 and (st[:, 14:120:15] != 0).sum() > 0
+    if case.get("stiffeners", 0):
+        # the stiffeners: lumped mass (checked above), and the fibres' own state
+        fs = r["fiber_state"].reshape(-1, 4)
+        assert np.array_equal(m.fiber_state, r["fiber_state"])
+        assert fs.shape[0] > 0 and (fs[:, 1] > 0).any(), "the fibres must yield"
+        if name == "stiffened-tearing":
+            assert (fs[:, 3] != 0).any(), "and some must tear"
+        if not case.get("fiber_failure", True):
+            assert not (fs[:, 3] != 0).any()
 
 
 def golden_zone():
@@ -84,7 +99,8 @@ def golden_zone():
     return mod.ZONE_CASES, np.load(os.path.join(here, "zone_plate.npz"))
 
 
-@pytest.mark.parametrize("name", ["prescribed", "inertial_damped_edge", "arrest", "tearing"])
+@pytest.mark.parametrize("name", ["prescribed", "inertial_damped_edge", "arrest", "tearing", "stiffened",
+                                  "stiffened_tearing"])
 def test_oracle_zone_step_golden(port, name):
     """The same pin without the compiled reference: the restatement reproduces the
     fixture zone::Solver wrote, bit for bit."""
@@ -92,8 +108,12 @@ def test_oracle_zone_step_golden(port, name):
     case = cases[name]
     r = dict(rest=g["rest"], index=g["index"], pinned=g["pinned"], mat=g["material"], density=float(g["density"]),
              driven=g["driven"], prescribed=g[f"{name}_prescribed"], dt=float(g["dt"]))
+    for k in ("fiber_tie", "fiber_weight", "fiber_area", "fiber_length", "fiber_fail"):
+        r[k] = g[f"{name}_{k}"]
     m = port_zone(port, r, case)
-    assert np.array_equal(m.mass, g["mass"])
+    assert np.array_equal(m.mass, g[f"{name}_mass"])
+    if case.get("stiffeners", 0):
+        assert np.array_equal(m.fiber_state, g[f"{name}_fiber_state"])
     assert np.array_equal(m.position, g[f"{name}_position"])
     assert np.array_equal(m.velocity, g[f"{name}_velocity"])
     assert np.array_equal(m.state, g[f"{name}_state"])
