@@ -348,6 +348,27 @@ int femstep_shell_punch_state(femstep_shell *solver, double out[4]);
    NULL, or all zero, removes the drive. */
 int femstep_shell_set_edge(femstep_shell *solver, const double *prescribed, const double *meshed,
                            double edge_ramp);
+/* Constraint fibres (engine/sim/constraint.hpp; zone.cpp:990-1002): the axial bars an
+   eccentric stiffener is made of, each end tied to a through-thickness node pair as
+   (1 - w) x[bottom] + w x[top].  Every step each fibre's co-rotational strain
+   (l - L) / L goes through the uniaxial return (isotropic hardening on the solver's
+   flow curve, damage with the bar's triaxiality +-1/3, tearing at the fibre's failure
+   strain), in FP64, and N = sigma A is added to the four tie nodes after the plating's
+   gather, in fibre order.  Their dissipation and strain energy join
+   femstep_shell_energy's.  count 0 removes them. */
+typedef struct {
+    size_t count;
+    const uint32_t *tie;           /* 4 per fibre: end 0 bottom, top; end 1 bottom, top */
+    const double *weight;          /* 2 per fibre: the ties' weights (constraint::tieWeight) */
+    const double *area;            /* m^2 per fibre */
+    const double *rest_length;     /* m per fibre; NULL: from the rest positions (restFibers) */
+    const double *failure_strain;  /* per fibre (constraint::fiberFailureStrain); NULL: never fails */
+    double density;                /* > 0: add the fibres' lumped mass (lumpFiberMass); 0: the
+                                      solver's mass already holds it, as zone::Solver's does */
+} femstep_shell_fibers;
+int femstep_shell_set_fibers(femstep_shell *solver, const femstep_shell_fibers *fibers);
+/* 4 doubles per fibre: plastic strain, eq. plastic strain, damage, failed (FiberState). */
+int femstep_shell_fiber_state(femstep_shell *solver, double *out);
 /* The rest of zone::Solver's account (SolveResult, zone.hpp:750-815): [0] damping loss
    (J) [1] boundary work of the driven edge (J) [2] the punch's speed now (m/s) [3] the
    striking body's kinetic energy (J; 0 for a prescribed punch) [4] 1 once an inertial

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "engine/sim/constraint.hpp"
 #include "femstep.h"
 
 namespace gpu {
@@ -180,6 +181,34 @@ bool ZoneGpuSolver::initialise(const sim::zone::Patch& patch, const sim::zone::S
                                params.edgeRamp) != FEMSTEP_OK) {
         error = femstep_shell_error(d.handle);
         return false;
+    }
+    // the stiffeners as constraint fibres (zone.cpp:724-733, 990-1002): the rest
+    // lengths from the CPU solver's rest array and each fibre's own failure strain; the
+    // CPU solver's lumped mass already holds their mass
+    const sim::constraint::Stiffening& st = patch.stiffening;
+    if (!st.empty()) {
+        const sim::constraint::RestFibers rest = sim::constraint::restFibers(st, cpu.rest());
+        const std::size_t F = st.fiberCount();
+        std::vector<uint32_t> tie(F * 4);
+        std::vector<double> weight(F * 2), area(F), fail(F);
+        for (std::size_t i = 0; i < F; ++i) {
+            const sim::constraint::Fiber& f = st.fiber[i];
+            tie[i * 4] = f.end[0].bottom;
+            tie[i * 4 + 1] = f.end[0].top;
+            tie[i * 4 + 2] = f.end[1].bottom;
+            tie[i * 4 + 3] = f.end[1].top;
+            weight[i * 2] = f.end[0].weight;
+            weight[i * 2 + 1] = f.end[1].weight;
+            area[i] = f.area;
+            fail[i] = params.fiberFailure
+                          ? sim::constraint::fiberFailureStrain(material.failure, rest.length[i], f.neckWidth)
+                          : sim::plasticity::kNeverFails;
+        }
+        femstep_shell_fibers fibers{F, tie.data(), weight.data(), area.data(), rest.length.data(), fail.data(), 0.0};
+        if (femstep_shell_set_fibers(d.handle, &fibers) != FEMSTEP_OK) {
+            error = femstep_shell_error(d.handle);
+            return false;
+        }
     }
     char name[256] = {0};
     if (femstep_device_name(name, sizeof(name)) == FEMSTEP_OK) deviceName_ = name;

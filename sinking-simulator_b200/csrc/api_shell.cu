@@ -57,6 +57,9 @@ struct femstep_shell {
     size_t edge_capacity = 0, edge_dof = 0;
     double edge_ramp = 0.0;
     double* n_edge = nullptr;         // [nblocks]
+    // constraint fibres (femstep_shell_set_fibers)
+    size_t fiber_capacity = 0;
+    int fblocks = 0;
     std::vector<uint8_t> pin;         // host copy of the pinned bits (0-2)
     std::vector<double> rest;  // host copy for readback
     std::string error;
@@ -96,6 +99,24 @@ ShellParams make_params(const femstep_shell_params& p) {
     q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 5e-5);
     q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-13);
     q.compensated = p.compensated;
+    // the fibres' law in double: the same material, linear unless the curve is Swift
+    q.fiber.youngs = E;
+    q.fiber.yield = p.yield_strength;
+    q.fiber.hardening = p.hardening_modulus;
+    q.fiber.swift = 0;
+    q.fiber.tri_sens = 1.5;
+    q.fiber.tri_ref = 1.0 / 3.0;
+    q.fiber.tri_cut = -1.0 / 3.0;
+    if (p.material) {
+        const femstep_shell_material& m = *p.material;
+        q.fiber.swift = m.hardening == FEMSTEP_SHELL_SWIFT ? 1 : 0;
+        q.fiber.swift_k = m.strength_coefficient;
+        q.fiber.swift_eps0 = m.reference_strain;
+        q.fiber.swift_n = m.hardening_exponent;
+        q.fiber.tri_sens = m.triaxiality_sensitivity;
+        q.fiber.tri_ref = m.reference_triaxiality;
+        q.fiber.tri_cut = m.cutoff_triaxiality;
+    }
     if (p.material) {
         const femstep_shell_material& m = *p.material;
         q.general = 1;
@@ -214,7 +235,7 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.n_kin = A.zeros<double>(s->nblocks + 1);  // + the gripped nodes of an inertial punch
     d.punch_kin = d.n_kin + s->nblocks;
     d.n_damp = A.zeros<double>(s->nblocks);
-    s->d_out = A.zeros<double>(8);
+    s->d_out = A.zeros<double>(16);
 
     // nodes.  The displacement is held as a float u and its Kahan compensation c with
     // position = rest + (u - c): u = fl(x) for the caller's x = position - rest, and c =
@@ -378,7 +399,7 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
         }
     }
     s->launches = 0;
-    const int per_step = q.inertial ? 3 : 2;
+    const int per_step = 2 + (q.inertial ? 1 : 0) + (s->d.fibers ? 1 : 0);
     int rc = ensure_factor(s, *params);
     if (rc) return rc;
     rc = check(s, cudaEventRecord(s->ev0, s->stream), "event record");
@@ -591,6 +612,115 @@ int femstep_shell_set_edge(femstep_shell* s, const double* prescribed, const dou
     return FEMSTEP_OK;
 }
 
+int femstep_shell_set_fibers(femstep_shell* s, const femstep_shell_fibers* f) {
+    if (!s || !f) return fail(s, FEMSTEP_EINVAL, "null argument");
+    const size_t F = f->count, N = s->nodes;
+    if (F > 0 && (!f->tie || !f->weight || !f->area)) return fail(s, FEMSTEP_EINVAL, "fibre arrays missing");
+    if (F >= 0x3fffffffu) return fail(s, FEMSTEP_EINVAL, "too many fibres");
+    if (!(f->density >= 0.0)) return fail(s, FEMSTEP_EINVAL, "bad fibre density");
+    for (size_t i = 0; i < F * 4; ++i)
+        if (f->tie[i] >= N) return fail(s, FEMSTEP_EINVAL, "fibre tie node out of range");
+    // rest lengths: the caller's, or from the rest positions as restFibers does
+    // (constraint.cpp:185-196)
+    std::vector<double> length(F);
+    for (size_t i = 0; i < F; ++i) {
+        if (f->rest_length) {
+            length[i] = f->rest_length[i];
+            continue;
+        }
+        double span[3];
+        for (int k = 0; k < 3; ++k) {
+            const double* r = s->rest.data();
+            const double w0 = f->weight[i * 2], w1 = f->weight[i * 2 + 1];
+            const double a = r[(size_t)f->tie[i * 4] * 3 + k] * (1.0 - w0) + r[(size_t)f->tie[i * 4 + 1] * 3 + k] * w0;
+            const double b =
+                r[(size_t)f->tie[i * 4 + 2] * 3 + k] * (1.0 - w1) + r[(size_t)f->tie[i * 4 + 3] * 3 + k] * w1;
+            span[k] = b - a;
+        }
+        length[i] = std::sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
+    }
+    std::vector<double> never(F, INFINITY);
+    // node -> fibre slot CSR, ascending fibre order per node
+    std::vector<uint32_t> offset(N + 1, 0u), entry(F * 4);
+    for (size_t i = 0; i < F * 4; ++i) ++offset[f->tie[i] + 1];
+    for (size_t n = 0; n < N; ++n) offset[n + 1] += offset[n];
+    {
+        std::vector<uint32_t> cursor(offset.begin(), offset.end() - 1);
+        for (size_t i = 0; i < F * 4; ++i) entry[cursor[f->tie[i]]++] = (uint32_t)i;
+    }
+    fs::DeviceArena& A = s->arena;
+    ShellDevice& d = s->d;
+    const int fblocks = F ? fs::blocks_for((long long)F, fs::kShellFiberBlock) : 0;
+    if (F > s->fiber_capacity) {
+        d.fiber_tie = A.alloc<uint4>(F);
+        d.fiber_weight = A.alloc<double2>(F);
+        d.fiber_area = A.alloc<double>(F);
+        d.fiber_length = A.alloc<double>(F);
+        d.fiber_fail = A.alloc<double>(F);
+        d.fiber_state = A.alloc<double>(F * 4);
+        d.fiber_slots = A.alloc<float>(F * 12);
+        d.fiber_entry = A.alloc<uint32_t>(F * 4);
+        d.f_diss = A.alloc<double>(fblocks);
+        d.f_energy = A.alloc<double>(fblocks);
+        s->fiber_capacity = F;
+    }
+    if (F > 0 && !d.fiber_offset) d.fiber_offset = A.alloc<uint32_t>(N + 1);
+    if (!A.ok()) return check(s, A.status(), "fibre allocation");
+    int rc = FEMSTEP_OK;
+    auto put = [&](const void* dst, const void* src, size_t bytes) {
+        if (!rc && bytes) rc = check(s, cudaMemcpy((void*)dst, src, bytes, cudaMemcpyHostToDevice), "fibre upload");
+    };
+    if (F > 0) {
+        put(d.fiber_tie, f->tie, F * sizeof(uint4));
+        put(d.fiber_weight, f->weight, F * sizeof(double2));
+        put(d.fiber_area, f->area, F * sizeof(double));
+        put(d.fiber_length, length.data(), F * sizeof(double));
+        put(d.fiber_fail, f->failure_strain ? f->failure_strain : never.data(), F * sizeof(double));
+        put(d.fiber_offset, offset.data(), (N + 1) * sizeof(uint32_t));
+        put(d.fiber_entry, entry.data(), F * 4 * sizeof(uint32_t));
+        if (!rc) rc = check(s, cudaMemset(d.fiber_state, 0, F * 4 * sizeof(double)), "fibre upload");
+        if (!rc) rc = check(s, cudaMemset(d.fiber_slots, 0, F * 12 * sizeof(float)), "fibre upload");
+        if (!rc) rc = check(s, cudaMemset(d.f_diss, 0, fblocks * sizeof(double)), "fibre upload");
+        if (!rc) rc = check(s, cudaMemset(d.f_energy, 0, fblocks * sizeof(double)), "fibre upload");
+    }
+    // the fibres' mass, a quarter to each tie node in fibre order (lumpFiberMass,
+    // constraint.cpp:260-276), when the solver's mass does not hold it yet
+    if (!rc && F > 0 && f->density > 0.0) {
+        std::vector<float> mf(N);
+        rc = check(s, cudaMemcpy(mf.data(), d.mass, N * sizeof(float), cudaMemcpyDeviceToHost), "fibre mass");
+        if (!rc) {
+            std::vector<double> m(mf.begin(), mf.end());
+            for (size_t i = 0; i < F; ++i) {
+                if (!(length[i] > 0.0) || !(f->area[i] > 0.0)) continue;
+                const double quarter = 0.25 * f->density * f->area[i] * length[i];
+                for (int k = 0; k < 4; ++k) m[f->tie[i * 4 + k]] += quarter;
+            }
+            std::vector<float> im(N);
+            for (size_t n = 0; n < N; ++n) {
+                mf[n] = (float)m[n];
+                im[n] = m[n] > 0.0 ? (float)(1.0 / m[n]) : 0.0f;
+            }
+            put(d.mass, mf.data(), N * sizeof(float));
+            put(d.inv_mass, im.data(), N * sizeof(float));
+        }
+    }
+    if (rc) return rc;
+    d.fibers = (long long)F;
+    s->fblocks = fblocks;
+    if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return FEMSTEP_OK;
+}
+
+int femstep_shell_fiber_state(femstep_shell* s, double* out) {
+    if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
+    if (!s->d.fibers) return FEMSTEP_OK;
+    return check(s, cudaMemcpy(out, s->d.fiber_state, (size_t)s->d.fibers * 4 * sizeof(double), cudaMemcpyDeviceToHost),
+                 "readback");
+}
+
 int femstep_shell_account(femstep_shell* s, double out[6]) {
     if (!s || !out) return fail(s, FEMSTEP_EINVAL, "null argument");
     for (int i = 0; i < 6; ++i) out[i] = 0.0;
@@ -659,10 +789,20 @@ int femstep_shell_energy(femstep_shell* s, double out[4]) {
     const double* arrays[4] = {s->d.n_work, s->d.e_diss, s->d.e_strain, s->d.n_kin};
     const long long counts[4] = {s->nblocks, s->ewarps, s->ewarps, s->nblocks + 1};
     for (int i = 0; i < 4; ++i) fs::launch_reduce_sum(arrays[i], counts[i], s->d_out + i, s->stream);
+    if (s->d.fibers) {  // the stiffeners' dissipation and strain energy (zone.cpp:1000-1001, 1069)
+        fs::launch_reduce_sum(s->d.f_diss, s->fblocks, s->d_out + 8, s->stream);
+        fs::launch_reduce_sum(s->d.f_energy, s->fblocks, s->d_out + 9, s->stream);
+    }
+    double r[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     int rc = check(s, cudaGetLastError(), "reduce");
-    if (!rc) rc = check(s, cudaMemcpyAsync(out, s->d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
+    if (!rc) rc = check(s, cudaMemcpyAsync(r, s->d_out, sizeof(r), cudaMemcpyDeviceToHost, s->stream), "readback");
     if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "reduce");
-    return rc;
+    if (rc) return rc;
+    out[0] = r[0];
+    out[1] = s->d.fibers ? r[1] + r[8] : r[1];
+    out[2] = s->d.fibers ? r[2] + r[9] : r[2];
+    out[3] = r[3];
+    return FEMSTEP_OK;
 }
 
 int femstep_shell_stats(femstep_shell* s, long long out[2]) {
@@ -790,6 +930,11 @@ std::vector<Segment> shell_segments(femstep_shell* s) {
         v.push_back({s->halt, sizeof(int)});
     }
     if (s->n_edge) v.push_back({s->n_edge, (size_t)s->nblocks * sizeof(double)});
+    if (d.fibers) {
+        v.push_back({d.fiber_state, (size_t)d.fibers * 4 * sizeof(double)});
+        v.push_back({d.f_diss, (size_t)s->fblocks * sizeof(double)});
+        v.push_back({d.f_energy, (size_t)s->fblocks * sizeof(double)});
+    }
     return v;
 }
 
@@ -825,7 +970,7 @@ int femstep_shell_checkpoint(femstep_shell* s, void* buffer, size_t bytes) {
     h.elements = s->elements;
     h.segments = segs.size();
     h.payload = shell_checkpoint_bytes(s) - sizeof(h);
-    h.flags = (s->driven ? 1u : 0u) | (s->n_edge ? 2u : 0u);
+    h.flags = (s->driven ? 1u : 0u) | (s->n_edge ? 2u : 0u) | (s->d.fibers ? 4u : 0u);
     h.punch_time = s->punch_time;
     h.punch_penetration = s->punch_penetration;
     h.punch_steps = s->punch_steps;
@@ -850,9 +995,10 @@ int femstep_shell_restore(femstep_shell* s, const void* buffer, size_t bytes) {
     if (h.magic != kShellCheckpointMagic) return fail(s, FEMSTEP_EINVAL, "not a shell checkpoint");
     if (h.nodes != s->nodes || h.elements != s->elements)
         return fail(s, FEMSTEP_EINVAL, "checkpoint of a different mesh");
-    const uint64_t flags = (s->driven ? 1u : 0u) | (s->n_edge ? 2u : 0u);
+    const uint64_t flags = (s->driven ? 1u : 0u) | (s->n_edge ? 2u : 0u) | (s->d.fibers ? 4u : 0u);
     if (h.flags != flags)
-        return fail(s, FEMSTEP_EINVAL, "set the punch and the driven edge as at the checkpoint before restoring");
+        return fail(s, FEMSTEP_EINVAL,
+                    "set the punch, the driven edge and the fibres as at the checkpoint before restoring");
     const std::vector<Segment> segs = shell_segments(s);
     if (h.segments != segs.size() || h.payload + sizeof(h) != shell_checkpoint_bytes(s) ||
         bytes < shell_checkpoint_bytes(s))

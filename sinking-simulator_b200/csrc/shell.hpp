@@ -77,6 +77,22 @@ struct ShellDevice {
     const double* edge_drive = nullptr;  // [rows][3]: the prescribed value
     double* n_edge = nullptr;         // FP64 boundary work per node block (+=)
     double* n_damp = nullptr;         // FP64 damping loss per node block (+=)
+    // Constraint fibres (constraint.hpp; zone.cpp:990-1002): axial bars of eccentric
+    // stiffeners, each end tied to a through-thickness node pair.  One FP64 thread per
+    // fibre writes the force on its four tie nodes into fiber_slots; the node pass adds
+    // them after the element gather through a second CSR, in fibre order.
+    long long fibers = 0;
+    const uint4* fiber_tie = nullptr;       // [F]: end 0 bottom, top; end 1 bottom, top
+    const double2* fiber_weight = nullptr;  // [F]: the two ties' weights
+    const double* fiber_area = nullptr;     // [F]
+    const double* fiber_length = nullptr;   // [F] rest length
+    const double* fiber_fail = nullptr;     // [F] failure strain (inf: never)
+    double* fiber_state = nullptr;          // [F][4]: plastic strain, eq. plastic strain, damage, failed
+    float* fiber_slots = nullptr;           // [F][4][3]
+    const uint32_t* fiber_offset = nullptr; // [N+1]
+    const uint32_t* fiber_entry = nullptr;  // [4F]: fibre * 4 + tie node (0..3), ascending per node
+    double* f_diss = nullptr;               // FP64 fibre dissipation per fibre block (+=)
+    double* f_energy = nullptr;             // FP64 fibre strain energy per fibre block (=)
     const float* fail_strain = nullptr;  // [E]; +inf never fails
     long long* counter = nullptr;     // [0] steps taken, [1] step of the current node pass
     // FP64 partials with a fixed mapping: one entry per warp of the element kernel
@@ -111,6 +127,12 @@ struct ShellParams {
     double edge_ramp;                     // smoothstep ramp of the driven edge, s (0: at once)
     float axis_x, axis_y, axis_z;
     double inv_2mu, inv_3kappa;           // 1 / (2 mu), 1 / (3 kappa) in double (energy account)
+    // the fibres' uniaxial law, in double (constraint.cpp:39-95): E, the flow curve,
+    // and the Rice-Tracey factor's constants
+    struct FiberLaw {
+        double youngs, yield, hardening, swift_k, swift_eps0, swift_n, tri_sens, tri_ref, tri_cut;
+        int swift;
+    } fiber;
     float dt, damping;
     double damping64;                     // the damping as given: velocities are scaled in double
     double dt64, rise_time;               // load factor min((step+1) dt / rise, 1)
@@ -122,6 +144,7 @@ struct ShellParams {
 constexpr int kShellBlock = 128;          // 16 elements per block
 constexpr int kShellNodeBlock = 256;
 constexpr int kShellPunchBlock = 256;   // the inertial punch: one block
+constexpr int kShellFiberBlock = 128;
 
 void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts);
 // Factor of the elastic K_aa per element for this material (into `out`, [E][32]).

@@ -763,6 +763,15 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
             force[1] += sl[1];
             force[2] += sl[2];
         }
+        // the stiffeners' forces through their ties, after the plating, in fibre order
+        if (d.fibers) {
+            for (uint32_t k = d.fiber_offset[n]; k < d.fiber_offset[n + 1]; ++k) {
+                const float* fs = d.fiber_slots + (size_t)d.fiber_entry[k] * 3;
+                force[0] += fs[0];
+                force[1] += fs[1];
+                force[2] += fs[2];
+            }
+        }
         const uint8_t pin = d.pinned[n];
         const float im = d.inv_mass[n], m = d.mass[n];
         float* vel = d.velocity + (size_t)n * 3;
@@ -852,6 +861,126 @@ __global__ void __launch_bounds__(kShellNodeBlock) shell_nodes(ShellDevice d, Sh
         if (d.driven && !p.inertial) d.n_punch[blockIdx.x] += bp;
         if (p.damping64 != 1.0) d.n_damp[blockIdx.x] += bd;
         if (d.edge_map) d.n_edge[blockIdx.x] += be;
+    }
+}
+
+// flowStress / flowSlope of the fibres' curve (plasticity.cpp:124-142), in double
+__device__ __forceinline__ double fiber_flow_stress(const ShellParams::FiberLaw& m, double eq) {
+    const double q = fmax(0.0, eq);
+    return m.swift ? m.swift_k * pow(m.swift_eps0 + q, m.swift_n) : m.yield + m.hardening * q;
+}
+__device__ __forceinline__ double fiber_flow_slope(const ShellParams::FiberLaw& m, double eq) {
+    const double q = fmax(0.0, eq);
+    return m.swift ? m.swift_k * m.swift_n * pow(m.swift_eps0 + q, m.swift_n - 1.0) : m.hardening;
+}
+
+// The fibre's uniaxial return (constraint.cpp:39-95): backward Euler on the flow rule
+// with isotropic hardening, the consistency condition solved by Newton (at most 32
+// iterations, 1e-13 relative), then the damage increment with the bar's closed-form
+// triaxiality +-1/3 (constraint.cpp:102-109).  st: plastic strain, eq. plastic strain,
+// damage, failed.
+__device__ __forceinline__ double fiber_return(const ShellParams::FiberLaw& m, double failure_strain, double strain,
+                                               double st[4], double& dissipation_per_volume) {
+    dissipation_per_volume = 0.0;
+    if (st[3] != 0.0) return 0.0;
+    const double trial = m.youngs * (strain - st[0]);
+    const double yield = fiber_flow_stress(m, st[1]);
+    if (fabs(trial) <= yield) return trial;
+    double increment = (fabs(trial) - yield) / (m.youngs + fiber_flow_slope(m, st[1]));
+    for (int it = 0; it < 32; ++it) {
+        const double residual = fabs(trial) - m.youngs * increment - fiber_flow_stress(m, st[1] + increment);
+        if (fabs(residual) <= 1e-13 * (yield + fabs(trial))) break;
+        const double slope = m.youngs + fiber_flow_slope(m, st[1] + increment);
+        if (!(slope > 0.0)) break;
+        increment += residual / slope;
+        if (increment < 0.0) increment = 0.0;
+    }
+    const double direction = trial >= 0.0 ? 1.0 : -1.0;
+    const double stress = trial - direction * m.youngs * increment;
+    st[0] += direction * increment;
+    st[1] += increment;
+    dissipation_per_volume = fabs(stress) * increment;
+    const double eta = stress == 0.0 ? 0.0 : (stress > 0.0 ? 1.0 : -1.0) / 3.0;
+    const double factor = eta <= m.tri_cut ? INFINITY : exp(-m.tri_sens * (eta - m.tri_ref));
+    const double critical = failure_strain * factor;
+    if (critical > 0.0 && isfinite(critical)) st[2] += increment / critical;
+    if (st[2] >= 1.0) {
+        st[2] = 1.0;
+        st[3] = 1.0;
+        return 0.0;
+    }
+    return stress;
+}
+
+// Constraint fibres (constraint.cpp:198-258), one thread per fibre in FP64: the tied
+// end points from the positions at the start of the step (rest + u - c), the
+// co-rotational axial strain (l - L) / L, the uniaxial return, and N = sigma A along
+// the current axis, split over each end's node pair by the tie weights.  Written to
+// the fibre's four force slots; the node pass gathers them.
+template <bool KAHAN>
+__global__ void __launch_bounds__(kShellFiberBlock) shell_fibers(ShellDevice d, ShellParams p) {
+    __shared__ double scratch[64];
+    if (d.halt && *d.halt) return;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double diss = 0.0, energy = 0.0;
+    if (i < d.fibers) {
+        float out[4][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+        const double rest_length = d.fiber_length[i], area = d.fiber_area[i];
+        if (rest_length > 0.0 && area > 0.0) {
+            const uint4 t = d.fiber_tie[i];
+            const double2 w = d.fiber_weight[i];
+            const uint32_t node[4] = {t.x, t.y, t.z, t.w};
+            const double weight[2] = {w.x, w.y};
+            double pos[4][3];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const size_t o = (size_t)node[j] * 3 + k;
+                    const double u = KAHAN ? (double)d.disp[o] - (double)d.disp_c[o] : (double)d.disp[o];
+                    pos[j][k] = d.rest[o] + u;
+                }
+            double span[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double a = pos[0][k] * (1.0 - weight[0]) + pos[1][k] * weight[0];
+                const double b = pos[2][k] * (1.0 - weight[1]) + pos[3][k] * weight[1];
+                span[k] = b - a;
+            }
+            const double l = sqrt(span[0] * span[0] + span[1] * span[1] + span[2] * span[2]);
+            if (l > 0.0) {
+                double st[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) st[k] = d.fiber_state[i * 4 + k];
+                double dpv = 0.0;
+                const double stress = fiber_return(p.fiber, d.fiber_fail[i], (l - rest_length) / rest_length, st, dpv);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) d.fiber_state[i * 4 + k] = st[k];
+                diss = dpv * area * rest_length;
+                const double axial = stress * area;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const double sa = e == 0 ? axial : -axial;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const double f = span[k] / l * sa;
+                        out[2 * e][k] = (float)((1.0 - weight[e]) * f);
+                        out[2 * e + 1][k] = (float)(weight[e] * f);
+                    }
+                }
+                energy = 0.5 * stress * stress / p.fiber.youngs * area * rest_length;
+            }
+        }
+        float* slot = d.fiber_slots + (size_t)i * 12;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) slot[j * 3 + k] = out[j][k];
+    }
+    block_sum2(diss, energy, scratch);
+    if (threadIdx.x == 0) {
+        d.f_diss[blockIdx.x] += diss;
+        d.f_energy[blockIdx.x] = energy;
     }
 }
 
@@ -991,6 +1120,13 @@ void launch_shell_elastic_factor(const ShellDevice& d, double youngs, double poi
 void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts) {
     const int eb = blocks_for(d.groups * 32, kShellBlock);
     const int nb = blocks_for(d.nodes, kShellNodeBlock);
+    const int fb = blocks_for(d.fibers, kShellFiberBlock);
+    if ((parts & 1) && d.fibers) {
+        if (p.compensated)
+            shell_fibers<true><<<fb, kShellFiberBlock, 0, stream>>>(d, p);
+        else
+            shell_fibers<false><<<fb, kShellFiberBlock, 0, stream>>>(d, p);
+    }
     if (p.compensated) {
         if (parts & 1) {
             if (p.general)

@@ -313,6 +313,13 @@ _sh_set_punch = _sig("femstep_shell_set_punch", C.c_int, [C.c_void_p, C.c_void_p
 _sh_punch_state = _sig("femstep_shell_punch_state", C.c_int, [C.c_void_p, C.c_void_p])
 _sh_set_edge = _sig("femstep_shell_set_edge", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double])
 _sh_account = _sig("femstep_shell_account", C.c_int, [C.c_void_p, C.c_void_p])
+class ShellFibersC(C.Structure):
+    _fields_ = [("count", C.c_size_t), ("tie", C.c_void_p), ("weight", C.c_void_p), ("area", C.c_void_p),
+                ("rest_length", C.c_void_p), ("failure_strain", C.c_void_p), ("density", C.c_double)]
+
+
+_sh_set_fibers = _sig("femstep_shell_set_fibers", C.c_int, [C.c_void_p, C.POINTER(ShellFibersC)])
+_sh_fiber_state = _sig("femstep_shell_fiber_state", C.c_int, [C.c_void_p, C.c_void_p])
 _sh_ck_size = _sig("femstep_shell_checkpoint_size", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)])
 _sh_ck = _sig("femstep_shell_checkpoint", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t])
 _sh_restore = _sig("femstep_shell_restore", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t])
@@ -429,6 +436,30 @@ class ShellSolver:
         if pr.size != 3 * self.nodes or (me is not None and me.size != 3 * self.nodes):
             raise ValueError("prescribed and meshed are 3 values per node")
         self._check(_sh_set_edge(self._h, _p(pr), None if me is None else _p(me), float(ramp)))
+
+    def set_fibers(self, tie, weight, area, rest_length=None, failure_strain=None, density=0.0):
+        """Constraint fibres (constraint.hpp): tie [F][4] (end 0 bottom, top; end 1 bottom,
+        top), weight [F][2], area [F]; rest length (None: from the rest positions) and
+        failure strain (None: never) per fibre; density > 0 adds their lumped mass."""
+        t = np.ascontiguousarray(tie, np.uint32).reshape(-1)
+        w = np.ascontiguousarray(weight, np.float64).reshape(-1)
+        a = np.ascontiguousarray(area, np.float64).reshape(-1)
+        n = a.size
+        if t.size != 4 * n or w.size != 2 * n:
+            raise ValueError("tie is 4 and weight 2 values per fibre")
+        ln = None if rest_length is None else np.ascontiguousarray(rest_length, np.float64).reshape(-1)
+        fs = None if failure_strain is None else np.ascontiguousarray(failure_strain, np.float64).reshape(-1)
+        self._fibers = (t, w, a, ln, fs)  # kept alive for the call
+        f = ShellFibersC(n, _p(t), _p(w), _p(a), _p(ln), _p(fs), float(density))
+        self._check(_sh_set_fibers(self._h, C.byref(f)))
+        self.fibers = n
+
+    def fiber_state(self) -> np.ndarray:
+        """[F][4]: plastic strain, eq. plastic strain, damage, failed."""
+        out = np.zeros(4 * getattr(self, "fibers", 0))
+        if out.size:
+            self._check(_sh_fiber_state(self._h, _p(out)))
+        return out.reshape(-1, 4)
 
     def checkpoint(self) -> np.ndarray:
         """The whole mutable state as a host byte array (femstep_shell_checkpoint)."""

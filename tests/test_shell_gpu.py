@@ -224,10 +224,12 @@ def device_material(mat):
 # 2.6e-6; damping loss and boundary work within 1.7e-7.  A point failing a step apart
 # from the reference would move its neighbours, so the tearing case keeps more margin.
 ZONE_TOL = {"prescribed": (2e-5, 1e-5, 1e-5), "inertial_damped_edge": (2e-5, 1e-5, 1e-5),
-            "arrest": (2e-5, 1e-4, 1e-5), "tearing": (1e-4, 1e-4, 1e-4)}
+            "arrest": (2e-5, 1e-4, 1e-5), "tearing": (1e-4, 1e-4, 1e-4), "stiffened": (2e-5, 1e-5, 1e-5),
+            "stiffened_tearing": (1e-3, 1e-3, 1e-3)}
 
 
-@pytest.mark.parametrize("name", ["prescribed", "inertial_damped_edge", "arrest", "tearing"])
+@pytest.mark.parametrize("name", ["prescribed", "inertial_damped_edge", "arrest", "tearing", "stiffened",
+                                  "stiffened_tearing"])
 def test_zone_step_against_reference_solver(fem, name):
     """The full zone step (zone.cpp:1088-1230) on the device -- the general point law with
     failure and tearing, damping and its loss, the driven edge and its work, the punch
@@ -236,15 +238,9 @@ def test_zone_step_against_reference_solver(fem, name):
     cases, g = zone_fixture()
     case = cases[name]
     rest = g["rest"]
-    s = fem.ShellSolver(rest, g["index"], pinned=g["pinned"], mass=g["mass"], state=g["state0"].reshape(-1, 129))
     mass = case.get("mass", 0.0)
-    s.set_punch(np.nonzero(g["driven"])[0], (0.0, 0.0, 1.0), speed=case.get("speed", 20.0),
-                ramp_time=0.0 if mass > 0 else 1e-4, mass=mass)
-    if any(case.get("edge_drive", (0.0, 0.0, 0.0))):
-        s.set_edge(g[f"{name}_prescribed"], ramp=case.get("edge_ramp", 0.0))
-    mat = g["material"]
-    s.run(case["steps"], dt=float(g["dt"]), damping=case.get("damping", 1.0), youngs=mat[0], poisson=mat[1],
-          compensated=True, max_iterations=40, tol_residual=1e-6, tol_work=1e-16, material=device_material(mat))
+    s = zone_solver(fem, g, name, case)
+    zone_run(s, g, case, case["steps"])
     acc = dict(zip(O.ZONE_ACCOUNT, g[f"{name}_account"]))
     pos, _ = s.readback()
     ref_pos = g[f"{name}_position"]
@@ -270,15 +266,26 @@ def test_zone_step_against_reference_solver(fem, name):
         assert a["edge_dof"] == acc["edge_dof"]
         assert abs(a["boundary_work"] - acc["boundary_work"]) <= tol_acc * abs(acc["boundary_work"])
     st, sr = s.state(), g[f"{name}_state"].reshape(-1, 129)
-    if name == "tearing":
+    if name in ("tearing", "stiffened_tearing"):
         torn, torn_r = (st[:, 128] != 0).sum(), (sr[:, 128] != 0).sum()
         assert torn_r > 0 and abs(int(torn) - int(torn_r)) <= max(1, torn_r // 10), (torn, torn_r)
+    if case.get("stiffeners", 0):
+        fs, fr = s.fiber_state(), g[f"{name}_fiber_state"].reshape(-1, 4)
+        print(name, "fibres: eps_p", np.abs(fs[:, 1] - fr[:, 1]).max(), "of", fr[:, 1].max(), "failed",
+              int((fs[:, 3] != 0).sum()), int((fr[:, 3] != 0).sum()))
+        assert (fr[:, 1] > 0).any()
+        assert np.abs(fs[:, 1] - fr[:, 1]).max() <= tol_pos * 10 * fr[:, 1].max()
+        assert np.array_equal(fs[:, 3] != 0, fr[:, 3] != 0)
 
 
 def zone_solver(fem, g, name, case, **extra):
-    s = fem.ShellSolver(g["rest"], g["index"], pinned=g["pinned"], mass=g["mass"],
+    # the solver's lumped mass, which holds the fibres' when the case has stiffeners
+    s = fem.ShellSolver(g["rest"], g["index"], pinned=g["pinned"], mass=g[f"{name}_mass"],
                         state=extra.get("state", g["state0"].reshape(-1, 129)), position=extra.get("position"),
                         velocity=extra.get("velocity"))
+    if case.get("stiffeners", 0):
+        s.set_fibers(g[f"{name}_fiber_tie"], g[f"{name}_fiber_weight"], g[f"{name}_fiber_area"],
+                     rest_length=g[f"{name}_fiber_length"], failure_strain=g[f"{name}_fiber_fail"])
     mass = case.get("mass", 0.0)
     s.set_punch(np.nonzero(g["driven"])[0], (0.0, 0.0, 1.0), speed=case.get("speed", 20.0),
                 ramp_time=0.0 if mass > 0 else 1e-4, mass=mass)
@@ -296,7 +303,7 @@ def zone_run(s, g, case, steps):
 def everything(s):
     p, v = s.readback()
     return dict(position=p, velocity=v, state=s.state(), energy=s.energy(), account=s.account(),
-                punch=s.punch_state())
+                punch=s.punch_state(), fibers=s.fiber_state())
 
 
 def same(a, b):
@@ -307,13 +314,13 @@ def same(a, b):
             assert np.array_equal(a[k], b[k]), k
 
 
-@pytest.mark.parametrize("name", ["inertial_damped_edge", "tearing"])
+@pytest.mark.parametrize("name", ["inertial_damped_edge", "tearing", "stiffened_tearing"])
 def test_checkpoint_resume_is_bit_identical(fem, name):
     """Checkpoint, then run on: the same bits as restoring the checkpoint into the same
     solver, or into a fresh one built from the same mesh (evict and bring back)."""
     cases, g = zone_fixture()
     case = cases[name]
-    first, rest_steps = (120, 180) if name != "tearing" else (1500, 1500)
+    first, rest_steps = (120, 180) if "tearing" not in name else (1500, 1500)
     s = zone_solver(fem, g, name, case)
     zone_run(s, g, case, first)
     ck = s.checkpoint()
