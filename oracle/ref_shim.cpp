@@ -8,7 +8,7 @@
 // tests check the pair against each other.
 //
 // Where the reference has the function, the shim only marshals arrays and calls it.
-// Where the north star composes something the reference does not have in one piece
+// Where a workload composes something the reference does not have in one piece
 // (the J2 tet, the pressure-loaded shell step), the composition is written here on
 // top of the reference's functions, and says which ones.
 #include "engine/core/jobs.hpp"

@@ -14,7 +14,7 @@
 //          linear isotropic hardening, failure off, and the fem.cpp node update with a
 //          ramped external load.  This is the plain FP64 single-mesh step.
 //
-// Memory-bound kernels (SURVEY 8d roofline: ~240 B per update for REF32, ~435 B for
+// Memory-bound kernels (algorithmic bytes: ~240 B per update for REF32, ~435 B for
 // F64): one thread per tet / per node, SoA element arrays so each warp load is one
 // contiguous 128 B line, node-major force slots so each node's gather is contiguous.
 #include "common.cuh"

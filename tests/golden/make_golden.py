@@ -67,7 +67,7 @@ def tet32(ref):
 
 
 def tet64(ref, port):
-    # BASELINE config 0 mesh: 40x4x4 cells, 3840 tets; clamped at x = 0, a 20 kN tip
+    # The CPU-runnable cantilever: 40x4x4 cells, 3840 tets; clamped at x = 0, a 20 kN tip
     # load spread over the x = 1 face, ramped over 2000 steps.  The FP64 J2 tet is a
     # composition (fem.cpp kinematics + plasticity::update), run here with the
     # reference's compiled point law.

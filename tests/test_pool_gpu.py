@@ -5,7 +5,7 @@ state must be bit-identical to a single-mesh FEMSTEP_TET_J2_F32K handle given th
 time step, whatever else is in the pool, whichever schedule (graph or persistent) and
 tile size runs it, and whenever it was admitted.  Against the FP64 oracle (the
 reference's tet kinematics with plasticity::update, in double) each mesh keeps the
-1e-5 relative displacement and energy within 0.5 %.
+target tolerance: 1e-5 relative displacement and energy within 0.5 %.
 """
 import ctypes as C
 

@@ -93,6 +93,35 @@ def test_rigid_translation_carries_no_force(fem):
     assert np.abs((p - rest) - v0 * 100 * dt).max() < 1e-9
 
 
+def test_frame_indifference(fem):
+    """tests/test_solid_shell.cpp:1493: the co-rotational element is objective.  The
+    same plate, clamped round its edge and set moving in a bending bump, run once as
+    meshed and once rigidly rotated by 40 degrees about an oblique axis (positions and
+    velocities rotated alike): the rotated run ends at the rotated positions."""
+    rest, index = fem.plate_mesh(0.06, 0.04, 0.012, 6, 4, 1)
+    p0 = rest.reshape(-1, 3)
+    edge = (p0[:, 0] < 1e-9) | (p0[:, 0] > 0.06 - 1e-9) | (p0[:, 1] < 1e-9) | (p0[:, 1] > 0.04 - 1e-9)
+    pinned = np.repeat(edge, 3).astype(np.uint8)
+    bump = np.sin(np.pi * p0[:, 0] / 0.06) * np.sin(np.pi * p0[:, 1] / 0.04)
+    v0 = np.zeros_like(p0)
+    v0[:, 2] = 3.0 * bump * ~edge
+    axis = np.array([1.0, 2.0, 2.0]) / 3.0
+    a = np.deg2rad(40.0)
+    k = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    R = np.eye(3) + np.sin(a) * k + (1 - np.cos(a)) * k @ k
+    runs, dt = [], None
+    for rot in (np.eye(3), R):
+        r = (p0 @ rot.T).reshape(-1)
+        s = fem.ShellSolver(r, index, pinned=pinned, velocity=(v0 @ rot.T).reshape(-1), density=7850.0)
+        dt = dt or s.critical_dt()  # one step size for both runs
+        s.run(300, dt=dt, yield_strength=355e6, hardening=1e9, compensated=True)
+        runs.append(s.readback()[0].reshape(-1, 3))
+    u = runs[0] - p0
+    assert np.abs(u).max() > 1e-5, "the plate must move"
+    err = np.abs(runs[1] - runs[0] @ R.T).max() / np.abs(u).max()
+    assert err < 1e-4, err
+
+
 def test_rest_stays_at_rest(fem):
     rest, index, pinned, _ = small_plate(fem, nx=6, ny=4)
     s = fem.ShellSolver(rest, index, pinned=pinned, density=7850.0)
@@ -101,7 +130,7 @@ def test_rest_stays_at_rest(fem):
     assert np.abs(p - rest).max() == 0.0 and np.abs(v).max() == 0.0
 
 
-# The general point law: BASELINE's configs use the linear curve with failure off, but
+# The general point law: the benchmark workloads use the linear curve with failure off, but
 # the reference's zone step (and its GPU shader) carries Swift hardening, kinematic
 # hardening, ductile damage and the element failure rules.
 SWIFT = (600e6, 0.02, 0.18)   # K, eps0, n: sigma_y(0) = 600e6 * 0.02^0.18 ~ 296 MPa

@@ -1,7 +1,7 @@
 """Tet step on the GPU, through the C ABI, against the oracle.
 
 REF32 and J2_F64 must be bit-identical to their CPU counterparts; the FP32 modes are
-held to the north-star tolerance against the FP64 oracle (1e-5 relative displacement,
+held to the target tolerance against the FP64 oracle (1e-5 relative displacement,
 0.5 % energy-balance drift).
 """
 import ctypes as C
@@ -17,7 +17,7 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def cantilever(fem, nx=40, ny=4, nz=4, load=20e3):
-    """1.0 x 0.1 x 0.1 m, 6 Kuhn tets per cell, clamped at x = 0,
+    """The CPU-runnable cantilever: 1.0 x 0.1 x 0.1 m, 6 Kuhn tets per cell, clamped at x = 0,
     tip load spread equally over the x = 1 face nodes in -z."""
     pos, idx = fem.box_tet_mesh(1.0, 0.1, 0.1, nx, ny, nz)
     fixed = (pos[0::3] < 1e-6).astype(np.uint32)
