@@ -122,6 +122,24 @@ def shell_bytes(E, N):
     return elem, node
 
 
+# FP32 operations per solid-shell element update, counted by ncu on the shell-sample
+# workload (SASS thread instructions: 2 x FFMA + FADD + FMUL, 13,263 per element; the
+# 449 FP64 operations of the energy account are left out).  The second roofline of the
+# shell element, against the FP32 SIMT peak: SMs x 128 lanes x 2 x the SM clock.
+SHELL_FP32_FLOP_PER_ELEMENT = 13263
+
+
+def simt_roofline(flop_per_unit, units, kernel_ms, max_mhz):
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    peak = sms * 128 * 2 * max_mhz * 1e6 / 1e12
+    achieved = flop_per_unit * units / (kernel_ms / 1e3) / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "flop_per_unit": flop_per_unit,
+            "peak_source": f"nominal: {sms} SMs x 128 FP32 lanes x 2 x {max_mhz:.0f} MHz (max SM clock)"}
+
+
 # ---------------------------------------------------------------------------------
 # clocks during the timed region
 
@@ -752,6 +770,9 @@ def main():
                          "frac": achieved / peak, "traffic": ncu_traffic(args.workload), "kernel": w.kernel,
                          "peak_source": peak_kind},
         }
+        if wl["kind"] == "shell":
+            out["roofline_simt"] = simt_roofline(SHELL_FP32_FLOP_PER_ELEMENT, w.units, elem_ms,
+                                                 out["clocks"].get("sm_max_mhz") or 1965.0)
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(wl)
         print(json.dumps(out), flush=True)
