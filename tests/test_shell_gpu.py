@@ -385,3 +385,34 @@ def test_readback_round_trip_is_exact(fem):
     p2, v2 = t.readback()
     assert np.array_equal(p2, p) and np.array_equal(v2, v)
     assert np.array_equal(t.state(), st)
+
+
+def test_zone_inputs_are_checked(fem):
+    """Bad zone inputs are refused with a reason, before any device work, and leave the
+    solver usable."""
+    cases, g = zone_fixture()
+    s = fem.ShellSolver(g["rest"], g["index"], pinned=g["pinned"], mass=g["prescribed_mass"])
+    n = s.nodes
+    driven = np.nonzero(g["driven"])[0]
+    with pytest.raises(fem.FemStepError, match="out of range"):
+        s.set_punch(np.array([n]), (0.0, 0.0, 1.0), speed=1.0)
+    with pytest.raises(fem.FemStepError, match="approach speed"):
+        s.set_punch(driven, (0.0, 0.0, 1.0), speed=0.0, mass=10.0)  # zone.cpp:779-801
+    with pytest.raises(fem.FemStepError, match="mass"):
+        s.set_punch(driven, (0.0, 0.0, 1.0), speed=1.0, mass=-1.0)
+    bad = np.zeros(3 * n)
+    bad[np.nonzero(g["pinned"])[0][0]] = np.nan
+    with pytest.raises(fem.FemStepError, match="not finite"):
+        s.set_edge(bad)
+    with pytest.raises(fem.FemStepError, match="ramp"):
+        s.set_edge(np.zeros(3 * n), ramp=-1.0)
+    with pytest.raises(fem.FemStepError, match="out of range"):
+        s.set_fibers(np.array([[0, 1, 2, n]]), np.array([[0.5, 0.5]]), np.array([1e-4]))
+    with pytest.raises(fem.FemStepError, match="not a shell checkpoint"):
+        s.restore(np.zeros(64, np.uint8))
+    with pytest.raises(fem.FemStepError, match="dt"):
+        s.run(1, dt=0.0)
+    # still usable: a clean run from rest stays at rest
+    s.run(16, dt=float(g["dt"]))
+    p, v = s.readback()
+    assert np.array_equal(p, g["rest"]) and not np.abs(v).any()
