@@ -1,0 +1,93 @@
+"""The reference's own drivers and GPU test suite, compiled unchanged against the
+drop-in classes of sinking-simulator_b200/compat (oracle/Makefile targets spike, probe
+and zone_gpu_tests; `__graft_entry__.build()` builds them where the reference
+checkout is present):
+
+  fem_spike          tools/fem_spike/main.cpp over gpu::FemGpuSolver
+  zone_gpu_probe     tools/zone_gpu_probe/main.cpp over gpu::ZoneGpuSolver
+  zone_gpu_tests     tests/test_zone_gpu.cpp (with its harness) over gpu::ZoneGpuSolver
+
+Without a device they must skip, as the reference's do; on a B200 they must pass, except
+for the zone suite's three checks that look for the Vulkan back-end's own artefacts
+(its two GLSL files, and a different shader per mapping: both mappings run one CUDA
+kernel here).  The binaries are test infrastructure built from the reference's
+sources; they are skipped where they were not built.
+"""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref")
+PKG = os.path.join(ROOT, "sinking-simulator_b200")
+# the zone suite's checks that ask for the Vulkan back-end's artefacts
+VULKAN_ONLY = {"solidshell_forces.comp is readable", "solidshell_forces_wg.comp is readable",
+               "the two mappings really did load different element shaders"}
+
+
+def run(name, *args, timeout=900):
+    path = os.path.join(REF, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} is not built (make -C oracle spike probe zone_gpu_tests)")
+    env = dict(os.environ, LD_LIBRARY_PATH=PKG + os.pathsep + os.environ.get("LD_LIBRARY_PATH", ""))
+    p = subprocess.run([path, *args], capture_output=True, text=True, timeout=timeout, env=env)
+    return p.returncode, p.stdout + p.stderr
+
+
+def failures(out):
+    return {line.strip()[len("FAIL "):].strip() for line in out.splitlines() if line.strip().startswith("FAIL ")}
+
+
+def have_device():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+no_device = pytest.mark.skipif(have_device(), reason="checks the no-device path")
+
+
+@no_device
+def test_fem_spike_skips_without_a_device():
+    rc, out = run("fem_spike")
+    assert rc == 0, out[-2000:]
+    assert "GPU section(s) were skipped" in out
+
+
+@no_device
+def test_zone_gpu_probe_skips_without_a_device():
+    rc, out = run("zone_gpu_probe", "--steps=10")
+    assert rc == 0, out[-2000:]
+    assert "skipped:" in out
+
+
+@no_device
+def test_zone_gpu_suite_without_a_device():
+    rc, out = run("zone_gpu_tests")
+    # the refusals are checked before any device is touched; the device tests skip
+    assert "skipped:" in out
+    assert failures(out) == VULKAN_ONLY - {"the two mappings really did load different element shaders"}, out
+
+
+@pytest.mark.gpu
+def test_fem_spike_on_the_device():
+    rc, out = run("fem_spike")
+    assert rc == 0 and "all checks passed" in out and "skipped" not in out.split("all checks passed")[-1], out[-3000:]
+
+
+@pytest.mark.gpu
+def test_zone_gpu_probe_on_the_device():
+    rc, out = run("zone_gpu_probe", "--steps=1000")
+    assert rc == 0, out[-3000:]
+    assert out.rstrip().endswith("ok"), out[-3000:]
+
+
+@pytest.mark.gpu
+def test_zone_gpu_suite_on_the_device():
+    rc, out = run("zone_gpu_tests")
+    assert "checks," in out, out[-3000:]
+    assert failures(out) == VULKAN_ONLY, out[-4000:]
