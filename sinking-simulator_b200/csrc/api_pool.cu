@@ -354,8 +354,7 @@ int refresh_mirror(femstep_pool* p) {
 struct Placement {
     int id = -1;
     long long T = 0, N = 0, t0 = -1, n0 = -1, part0 = -1, e_tiles = 0, n_tiles = 0;
-    size_t idx4 = 0, slot4 = 0, inv = 0, vol = 0, offs = 0, mass = 0, imass = 0, fixed = 0, ext = 0, rec = 0,
-           end = 0;
+    size_t idx4 = 0, slot4 = 0, offs = 0, pos = 0, fixed = 0, ext = 0, rec = 0, end = 0;
     int status = FEMSTEP_OK;
     std::string what;
 };
@@ -373,25 +372,22 @@ void stage_layout(Placement& pl, size_t base) {
     };
     pl.idx4 = take(T * 16);
     pl.slot4 = take(T * 16);
-    pl.inv = take(T * 36);
-    pl.vol = take(T * 4);
     pl.offs = take(N1 * 4);
-    pl.mass = take(N1 * 4);
-    pl.imass = take(N1 * 4);
+    pl.pos = take(N1 * 12);
     pl.fixed = take(N1);
     pl.ext = take(N1 * 12);
     pl.rec = take(sizeof(PoolMesh));
     pl.end = o;
 }
 
-// The host part of admitting one mesh, into its staged arrays (pinned): FP64 rest state
-// (fem.cpp:119-158), the CSR in the reference's order (fem.cpp:147-157), the slot map,
-// SoA Dm^-1, lumped masses, load; node and slot ids rebased into the pool.  Runs on
-// any host thread; touches nothing but the mesh's own staging.
+// The host part of admitting one mesh, into its staged arrays (pinned): the CSR in the
+// reference's order (fem.cpp:147-157), the slot map, the rest positions, pins and load;
+// node and slot ids rebased into the pool.  The FP64 rest state (Dm^-1, volumes, lumped
+// masses; fem.cpp:119-158) is computed on the device from the staged positions
+// (launch_pool_rest_state).  Runs on any host thread; touches nothing but the mesh's
+// own staging.
 void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
     const long long N = pl.N, T = pl.T;
-    std::vector<double> inv64, vol64, mass64;
-    fs::tet_rest_state64((size_t)N, (size_t)T, m.position, m.index, m.density, inv64, vol64, mass64);
     std::vector<uint32_t> off, entry;
     fs::build_csr((size_t)N, (size_t)T, 4, m.index, off, entry);
     const long long s0 = 4 * pl.t0, n0 = pl.n0;
@@ -407,25 +403,18 @@ void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
             slot4[t] = make_uint4(sl[t * 4], sl[t * 4 + 1], sl[t * 4 + 2], sl[t * 4 + 3]);
         }
     }
-    float* inv = (float*)(stage + pl.inv);
-    for (int k = 0; k < 9; ++k)
-        for (long long t = 0; t < T; ++t) inv[(size_t)k * T + t] = (float)inv64[t * 9 + k];
-    float* vol = (float*)(stage + pl.vol);
-    for (long long t = 0; t < T; ++t) vol[t] = (float)vol64[t];
     uint32_t* offs = (uint32_t*)(stage + pl.offs);
     for (long long n = 0; n <= N; ++n) offs[n] = (uint32_t)(s0 + off[n]);
-    float* mass = (float*)(stage + pl.mass);
-    float* imass = (float*)(stage + pl.imass);
+    float* pos = (float*)(stage + pl.pos);
+    std::memcpy(pos, m.position, (size_t)N * 12);
     uint8_t* fixed = (uint8_t*)(stage + pl.fixed);
     float* ext = (float*)(stage + pl.ext);
     for (long long n = 0; n < N; ++n) {
-        mass[n] = (float)mass64[n];
-        imass[n] = mass64[n] > 0.0 ? (float)(1.0 / mass64[n]) : 0.0f;
         fixed[n] = m.fixed && m.fixed[n] ? 1 : 0;
         for (int k = 0; k < 3; ++k) ext[n * 3 + k] = m.external_force ? (float)m.external_force[n * 3 + k] : 0.0f;
     }
-    // the spare node slot: holds the CSR end; massless, fixed, unloaded
-    mass[N] = imass[N] = 0.0f;
+    // the spare node slot: holds the CSR end; massless (set on the device), fixed, unloaded
+    pos[N * 3] = pos[N * 3 + 1] = pos[N * 3 + 2] = 0.0f;
     fixed[N] = 1;
     ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
 }
@@ -583,20 +572,19 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
             const long long T = q.T, N = q.N, t0 = q.t0, n0 = q.n0, part0 = q.part0;
             send(d.index + t0, q.idx4, T * sizeof(uint4));
             send(d.slot + t0, q.slot4, T * sizeof(uint4));
-            for (int k = 0; k < 9; ++k)
-                send(d.rest_inv + (size_t)k * p->tet_cap + t0, q.inv + (size_t)k * T * 4, T * 4);
-            send(d.rest_vol + t0, q.vol, T * 4);
             for (int k = 0; k < 7; ++k) {
                 cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
                 cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
             }
             send(d.offset + n0, q.offs, (N + 1) * 4);
-            send(d.mass + n0, q.mass, (N + 1) * 4);
-            send(d.inv_mass + n0, q.imass, (N + 1) * 4);
             send(d.fixed + n0, q.fixed, N + 1);
             send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
             cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
             cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
+            // the rest state from the rest positions, staged in the mesh's velocity rows,
+            // which then start at rest
+            send(d.velocity + n0 * 3, q.pos, (N + 1) * 12);
+            fs::launch_pool_rest_state(d, t0, T, n0, N, m.density, st);
             cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
             cudaMemsetAsync(d.e_diss + part0, 0, q.e_tiles * 8, st);
             cudaMemsetAsync(d.e_strain + part0, 0, q.e_tiles * 8, st);

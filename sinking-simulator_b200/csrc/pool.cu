@@ -279,6 +279,75 @@ cudaError_t launch_pool_persistent(const PoolDevice& d, int tile, int steps, int
     return cudaGetLastError();
 }
 
+namespace {
+
+// The rest state of an admitted mesh on the device, in FP64 as the single-mesh handle
+// computes it on the host (fem.cpp:119-158): per tet Dm^-1 and the volume, stored as
+// float rows, and the tet's quarter of its lumped mass parked in the first 8 bytes of
+// each corner's force slot (the element pass writes every slot before anything reads
+// it).  The mesh's rest positions are staged in its own velocity rows (indexed by
+// pool node id), which the admission zeroes afterwards.
+__global__ void pool_rest_tets(PoolDevice d, long long t0, long long T, double density) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const float* pos = d.velocity;
+    const uint4 id4 = d.index[t0 + t];
+    const uint32_t id[4] = {id4.x, id4.y, id4.z, id4.w};
+    double a[9];  // column-major, as the host
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r)
+            a[c * 3 + r] = (double)pos[(size_t)id[c + 1] * 3 + r] - (double)pos[(size_t)id[0] * 3 + r];
+#define A(r, c) a[(c) * 3 + (r)]
+    const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
+                       A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                       A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+    const double volume = fabs(det / 6.0);
+    const double inv_det = fabs(det) > 1e-300 ? 1.0 / det : 0.0;
+    double r[9];
+#define R(rr, cc) r[(cc) * 3 + (rr)]
+    R(0, 0) = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) * inv_det;
+    R(0, 1) = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * inv_det;
+    R(0, 2) = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * inv_det;
+    R(1, 0) = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) * inv_det;
+    R(1, 1) = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * inv_det;
+    R(1, 2) = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * inv_det;
+    R(2, 0) = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) * inv_det;
+    R(2, 1) = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * inv_det;
+    R(2, 2) = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * inv_det;
+#undef R
+#undef A
+    for (int k = 0; k < 9; ++k) d.rest_inv[(size_t)k * d.tet_cap + t0 + t] = (float)r[k];
+    d.rest_vol[t0 + t] = (float)volume;
+    const double quarter = density * volume * 0.25;
+    const uint4 sl = d.slot[t0 + t];
+    const uint32_t slot[4] = {sl.x, sl.y, sl.z, sl.w};
+    for (int c = 0; c < 4; ++c) *reinterpret_cast<double*>(d.slots + slot[c]) = quarter;
+}
+
+// Lumped node masses: the tets' quarters over the node's CSR run, which lists its tets
+// in ascending order -- the order the host loop adds them in.  Then the spare node.
+__global__ void pool_rest_nodes(PoolDevice d, long long n0, long long N) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n > N) return;
+    if (n == N) {  // the spare node slot holds the CSR end and has no mass
+        d.mass[n0 + N] = 0.0f;
+        d.inv_mass[n0 + N] = 0.0f;
+        return;
+    }
+    double m = 0.0;
+    for (uint32_t k = d.offset[n0 + n]; k < d.offset[n0 + n + 1]; ++k) m += *reinterpret_cast<const double*>(d.slots + k);
+    d.mass[n0 + n] = (float)m;
+    d.inv_mass[n0 + n] = m > 0.0 ? (float)(1.0 / m) : 0.0f;
+}
+
+}  // namespace
+
+void launch_pool_rest_state(const PoolDevice& d, long long t0, long long T, long long n0, long long N, double density,
+                            cudaStream_t stream) {
+    pool_rest_tets<<<blocks_for(T, kBlock), kBlock, 0, stream>>>(d, t0, T, density);
+    pool_rest_nodes<<<blocks_for(N + 1, kBlock), kBlock, 0, stream>>>(d, n0, N);
+}
+
 void launch_pool_dt(const PoolDevice& d, int id, long long t0, long long T, double E, double nu, double rho,
                     double safety, double* block_max, double* w2, cudaStream_t stream) {
     const int blocks = blocks_for(T, kBlock);

@@ -95,6 +95,11 @@ int pool_persistent_max_blocks(int tile);
 // meshes[id].dt = safety * 2 / sqrt(max omega^2) of the mesh's tets [t0, t0 + T),
 // from the pool's FP32 Dm^-1; 0 when the bound is not positive.  `block_max` holds
 // ceil(T / 256) doubles and `w2` one double of scratch.
+// An admitted mesh's rest state on the device (fem.cpp:119-158 in FP64): Dm^-1 and
+// volume rows, lumped masses.  Needs the mesh's index, slot map and CSR offsets in
+// place, and its rest positions (float, by pool node id) staged in d.velocity.
+void launch_pool_rest_state(const PoolDevice& d, long long t0, long long T, long long n0, long long N, double density,
+                            cudaStream_t stream);
 void launch_pool_dt(const PoolDevice& d, int id, long long t0, long long T, double E, double nu, double rho,
                     double safety, double* block_max, double* w2, cudaStream_t stream);
 
