@@ -537,8 +537,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
         p2.run(args.steps)
         t3 = time.perf_counter()
         d2h = 0
-        for i in ids2:
-            pp, vv = p2.readback(i)
+        for pp, vv in p2.readback_many(ids2):
             d2h += pp.nbytes + vv.nbytes
         t4 = time.perf_counter()
         p2.close()

@@ -228,6 +228,12 @@ int femstep_pool_finished(femstep_pool *pool, int *ids, int capacity, int *count
 int femstep_pool_status(femstep_pool *pool, int id, long long *steps_done, long long *steps_target);
 /* Positions (rest + displacement) and velocities of one mesh, 3N doubles each. */
 int femstep_pool_readback(femstep_pool *pool, int id, double *position, double *velocity);
+/* The same for ids[0..count): positions[k] / velocities[k] receive mesh ids[k]'s (3N
+   doubles each; velocities may be NULL).  The copies of all meshes are queued at once
+   through pinned buffers and converted on all host cores as they land: for reading a
+   whole batch back, one call instead of one per mesh. */
+int femstep_pool_readback_many(femstep_pool *pool, int count, const int *ids, double *const *positions,
+                               double *const *velocities);
 /* Plastic strain of one mesh, 7 per tet (6 engineering components, equivalent). */
 int femstep_pool_plastic(femstep_pool *pool, int id, double *plastic);
 /* [0] external work (load and gravity) [1] dissipation [2] strain energy [3] kinetic

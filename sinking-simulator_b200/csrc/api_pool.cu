@@ -963,6 +963,77 @@ int femstep_pool_readback(femstep_pool* p, int id, double* position, double* vel
     return FEMSTEP_OK;
 }
 
+int femstep_pool_readback_many(femstep_pool* p, int count, const int* ids, double* const* positions,
+                               double* const* velocities) {
+    if (!p || count < 0 || (count > 0 && (!ids || !positions))) return fail(p, FEMSTEP_EINVAL, "null argument");
+    for (int i = 0; i < count; ++i)
+        if (!valid_id(p, ids[i])) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
+    // Groups of at most 64 MB: each group's node rows go device -> pinned staging in three
+    // copies per mesh, all groups queued at once; then each group is converted on all host
+    // cores as soon as its copies have landed, while the later groups are still copying.
+    constexpr size_t kGroup = size_t(64) << 20;
+    struct Group {
+        int first = 0, last = 0;
+        Staging::Buf* buf = nullptr;
+        std::vector<size_t> at;  // per mesh: offset of its rows in the buffer
+    };
+    std::vector<Group> groups;
+    for (int i = 0; i < count;) {
+        Group g;
+        g.first = i;
+        size_t bytes = 0;
+        while (i < count) {
+            const size_t b = (size_t)p->meshes[ids[i]].N * 44 + 3 * 256;
+            if (i > g.first && bytes + b > kGroup) break;
+            bytes += b;
+            ++i;
+        }
+        g.last = i;
+        cudaError_t err;
+        g.buf = p->staging.get(bytes, err);
+        if (!g.buf) return check(p, err, "pinned staging");
+        for (int k = g.first; k < g.last; ++k) {
+            const HostMesh& h = p->meshes[ids[k]];
+            char* u = Staging::take(g.buf, (size_t)h.N * 16);
+            char* c = Staging::take(g.buf, (size_t)h.N * 16);
+            char* v = Staging::take(g.buf, (size_t)h.N * 12);
+            g.at.push_back((size_t)(u - g.buf->host));
+            cudaMemcpyAsync(u, p->d.disp + h.n0, h.N * 16, cudaMemcpyDeviceToHost, p->stream);
+            cudaMemcpyAsync(c, p->d.disp_c + h.n0, h.N * 16, cudaMemcpyDeviceToHost, p->stream);
+            cudaMemcpyAsync(v, p->d.velocity + h.n0 * 3, h.N * 12, cudaMemcpyDeviceToHost, p->stream);
+        }
+        Staging::submit(g.buf, p->stream);
+        groups.push_back(std::move(g));
+    }
+    int rc = check(p, cudaGetLastError(), "readback");
+    if (rc) return rc;
+    for (Group& g : groups) {
+        rc = check(p, cudaEventSynchronize(g.buf->done), "readback");
+        if (rc) return rc;
+        const int n = g.last - g.first;
+        std::vector<long long> weight(n);
+        for (int k = 0; k < n; ++k) weight[k] = p->meshes[ids[g.first + k]].N;
+        parallel_for(n, weight, [&](int k) {
+            const HostMesh& h = p->meshes[ids[g.first + k]];
+            const char* base = g.buf->host + g.at[k];
+            const float4* u = reinterpret_cast<const float4*>(base);
+            const float4* c = reinterpret_cast<const float4*>(base + ((h.N * 16 + 255) & ~255LL));
+            const float* v = reinterpret_cast<const float*>(base + 2 * ((h.N * 16 + 255) & ~255LL));
+            double* pos = positions[g.first + k];
+            double* vel = velocities ? velocities[g.first + k] : nullptr;
+            for (long long i = 0; i < h.N; ++i) {
+                // the compensated displacement u - c, in double
+                pos[i * 3] = (double)h.rest[i * 3] + ((double)u[i].x - (double)c[i].x);
+                pos[i * 3 + 1] = (double)h.rest[i * 3 + 1] + ((double)u[i].y - (double)c[i].y);
+                pos[i * 3 + 2] = (double)h.rest[i * 3 + 2] + ((double)u[i].z - (double)c[i].z);
+            }
+            if (vel)
+                for (long long i = 0; i < h.N * 3; ++i) vel[i] = v[i];
+        });
+    }
+    return FEMSTEP_OK;
+}
+
 int femstep_pool_plastic(femstep_pool* p, int id, double* plastic) {
     if (!valid_id(p, id) || !plastic) return fail(p, FEMSTEP_EINVAL, "unknown mesh");
     const HostMesh& h = p->meshes[id];

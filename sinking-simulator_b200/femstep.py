@@ -636,6 +636,8 @@ _pl_status = _sig("femstep_pool_status", C.c_int, [C.c_void_p, C.c_int, C.POINTE
                                                      C.POINTER(C.c_longlong)])
 _pl_readback = _sig("femstep_pool_readback", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p])
 _pl_plastic = _sig("femstep_pool_plastic", C.c_int, [C.c_void_p, C.c_int, C.c_void_p])
+_pl_readback_many = _sig("femstep_pool_readback_many", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                                                  C.c_void_p])
 _pl_energy = _sig("femstep_pool_energy", C.c_int, [C.c_void_p, C.c_int, C.c_void_p])
 _pl_dt = _sig("femstep_pool_dt", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)])
 _pl_autotune = _sig("femstep_pool_autotune", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -779,6 +781,15 @@ class TetPool:
         v = np.zeros(3 * n)
         self._check(_pl_readback(self._h, int(mesh_id), _p(p), _p(v)))
         return p, v
+
+    def readback_many(self, mesh_ids):
+        """[(positions, velocities)] of several meshes in one call (3N doubles each)."""
+        ids = np.ascontiguousarray(mesh_ids, np.int32)
+        outs = [(np.zeros(3 * self.sizes[int(i)][0]), np.zeros(3 * self.sizes[int(i)][0])) for i in ids]
+        pp = (C.c_void_p * max(len(outs), 1))(*[o[0].ctypes.data for o in outs])
+        vp = (C.c_void_p * max(len(outs), 1))(*[o[1].ctypes.data for o in outs])
+        self._check(_pl_readback_many(self._h, ids.size, _p(ids), C.cast(pp, C.c_void_p), C.cast(vp, C.c_void_p)))
+        return outs
 
     def plastic(self, mesh_id):
         t = self.sizes[mesh_id][1]

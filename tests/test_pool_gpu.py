@@ -275,3 +275,17 @@ def test_evict_and_resume_is_bit_identical(fem):
     # a checkpoint of another mesh is refused
     with pytest.raises(fem.FemStepError):
         pool.admit_resume(ck, 1500, **MATS[0], **others[0])
+
+
+def test_readback_many_is_readback(fem):
+    """The batch readback gives each mesh exactly what the per-mesh readback gives."""
+    meshes = [beam(fem, 12, 2, 2, load=80e3), beam(fem, 30, 3, 3, load=300e3), beam(fem, 7, 2, 2, length=0.4)]
+    pool = fem.TetPool(100000, 30000, max_meshes=8)
+    ids = [pool.admit(steps=300, ramp_steps=100, **MATS[k], **meshes[k]) for k in range(3)]
+    pool.run(300)
+    many = pool.readback_many(ids[::-1])
+    for i, (p, v) in zip(ids[::-1], many):
+        pe, ve = pool.readback(i)
+        assert np.array_equal(p, pe) and np.array_equal(v, ve)
+    assert np.abs(many[1][0] - meshes[1]["position"]).max() > 0
+    pool.close()
