@@ -21,6 +21,7 @@
 #include <deque>
 #include <map>
 #include <string>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -73,6 +74,48 @@ private:
     std::map<long long, long long> free_;  // start -> length
 };
 
+// Pinned host memory outlives the pools that staged through it: pinning is the slow
+// part of getting it (tens of milliseconds per 64 MB), so a destroyed pool hands its
+// buffers to this process-wide cache, up to kHostCacheBytes, and the next pool takes
+// them from here before it pins anything new.  Buffers are portable (usable from any
+// device of the process); the memory returns to the system when the process exits.
+class HostCache {
+public:
+    static HostCache& get() {
+        static HostCache* cache = new HostCache();  // never destroyed: no CUDA calls at exit
+        return *cache;
+    }
+    // The smallest cached buffer of at least `bytes`, or null.
+    char* take(size_t bytes, size_t& cap) {
+        std::lock_guard<std::mutex> lock(mu_);
+        auto it = free_.lower_bound(bytes);
+        if (it == free_.end()) return nullptr;
+        cap = it->first;
+        char* p = it->second;
+        total_ -= cap;
+        free_.erase(it);
+        return p;
+    }
+    // Keep `p` for a later pool, or free it when the cache is full.
+    void give(char* p, size_t cap) {
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            if (total_ + cap <= kHostCacheBytes) {
+                free_.emplace(cap, p);
+                total_ += cap;
+                return;
+            }
+        }
+        cudaFreeHost(p);
+    }
+
+private:
+    static constexpr size_t kHostCacheBytes = size_t(512) << 20;
+    std::mutex mu_;
+    std::multimap<size_t, char*> free_;
+    size_t total_ = 0;
+};
+
 // Pinned host buffers for uploads queued behind device work.  A buffer is reused once
 // the event recorded after its copies has completed.
 class Staging {
@@ -96,15 +139,22 @@ public:
         }
         if (!best) {
             // capacities are powers of two (at least 4 MB), so buffers of one size class
-            // serve every later request of that class: a few buffers, reused
+            // serve every later request of that class: a few buffers, reused -- and kept
+            // across pools by the host cache
             Buf b;
             b.cap = size_t(4) << 20;
             while (b.cap < bytes) b.cap <<= 1;
-            err = cudaHostAlloc(&b.host, b.cap, cudaHostAllocDefault);
-            if (err != cudaSuccess) return nullptr;
+            size_t cached = 0;
+            b.host = HostCache::get().take(b.cap, cached);
+            if (b.host) {
+                b.cap = cached;
+            } else {
+                err = cudaHostAlloc(&b.host, b.cap, cudaHostAllocPortable);
+                if (err != cudaSuccess) return nullptr;
+            }
             err = cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
             if (err != cudaSuccess) {
-                cudaFreeHost(b.host);
+                HostCache::get().give(b.host, b.cap);
                 return nullptr;
             }
             bufs_.push_back(b);
@@ -123,10 +173,11 @@ public:
         cudaEventRecord(b->done, s);
         b->pending = true;
     }
+    // After the pool's stream has drained: the buffers go to the host cache.
     void release() {
         for (Buf& b : bufs_) {
             if (b.done) cudaEventDestroy(b.done);
-            if (b.host) cudaFreeHost(b.host);
+            if (b.host) HostCache::get().give(b.host, b.cap);
         }
         bufs_.clear();
     }
