@@ -298,6 +298,30 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
     // last element and group for their loads and write nothing.
     const long long e = valid ? e_raw : d.elements - 1;
     const long long group = group_raw < d.groups ? group_raw : d.groups - 1;
+    {
+        // This warp's own group record (24 KB of forms) and state into L2 now, with one
+        // bulk prefetch each, and the small per-element rows with a line each.  The loads
+        // of them come after a dependent chain (node ids, node rows, the rotation) that
+        // the registers cannot run ahead of; prefetched, they hit L2 instead of DRAM.
+        // Measured on the 2 M-element panel: 4.24 -> 3.73 ms per element pass.
+        const void* rec = d.forms + (size_t)group * kShellRec4 * 32;
+        const void* st = d.state + (size_t)group * kShellStateQ * 32;
+        if (lane == 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rec), "r"((unsigned)(kShellRec4 * 32 * 16))
+                         : "memory");
+        if (lane == 1)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(st), "r"((unsigned)(kShellStateQ * 32 * 4))
+                         : "memory");
+        const long long e0 = group * 4;  // <= elements - 1
+        if (lane == 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.index + e0 * 8));
+        if (lane == 3) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.slot + e0 * 8));
+        if (lane == 4) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.alpha + e0 * 8));
+        if (lane == 5) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.j0inv + e0 * 9));
+        if (lane == 6) {
+            const long long last = d.elements * 9 - 1, at = e0 * 9 + 32;
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(d.j0inv + (at < last ? at : last)));
+        }
+    }
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const long long s = d.counter[0];
         d.counter[1] = s;
