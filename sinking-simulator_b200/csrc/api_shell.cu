@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -164,8 +165,17 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     if (N == 0 || E == 0) return fail(nullptr, FEMSTEP_EINVAL, "empty mesh");
     if (N >= 0xffffffffu || E * 8 >= 0xffffffffu) return fail(nullptr, FEMSTEP_EINVAL, "mesh too large for 32-bit ids");
     if (!m.rest || !m.index) return fail(nullptr, FEMSTEP_EINVAL, "rest and index are required");
-    for (size_t i = 0; i < E * 8; ++i)
-        if (m.index[i] >= N) return fail(nullptr, FEMSTEP_EINVAL, "element index out of range");
+    {
+        std::atomic<bool> bad{false};
+        fs::parallel_chunks(E * 8, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i)
+                if (m.index[i] >= N) {
+                    bad = true;
+                    return;
+                }
+        });
+        if (bad) return fail(nullptr, FEMSTEP_EINVAL, "element index out of range");
+    }
     if (!m.mass && !(m.density > 0.0)) return fail(nullptr, FEMSTEP_EINVAL, "need a lumped mass or a positive density");
     std::vector<uint32_t> offset, entry;
     if (m.adjacency_offset && m.adjacency_entry) {
@@ -175,15 +185,29 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     } else {
         fs::build_csr(N, E, 8, m.index, offset, entry);
     }
+    // The slot map, node by node: an entry belongs to the one node its corner names, so
+    // the nodes' runs touch disjoint slots and run in parallel.
     std::vector<uint32_t> slot(E * 8, 0xffffffffu);
-    for (size_t n = 0; n < N; ++n) {
-        if (offset[n + 1] < offset[n]) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets decrease");
-        for (uint32_t k = offset[n]; k < offset[n + 1]; ++k) {
-            const uint32_t e = entry[k];
-            if (e >= E * 8 || m.index[e] != n || slot[e] != 0xffffffffu)
-                return fail(nullptr, FEMSTEP_EINVAL, "adjacency is not the node-to-corner map of this mesh");
-            slot[e] = k;
-        }
+    {
+        std::atomic<int> bad{0};
+        fs::parallel_chunks(N, [&](size_t b, size_t e) {
+            for (size_t n = b; n < e && !bad; ++n) {
+                if (offset[n + 1] < offset[n]) {
+                    bad = 1;
+                    return;
+                }
+                for (uint32_t k = offset[n]; k < offset[n + 1]; ++k) {
+                    const uint32_t c = entry[k];
+                    if (c >= E * 8 || m.index[c] != n || slot[c] != 0xffffffffu) {
+                        bad = 2;
+                        return;
+                    }
+                    slot[c] = k;
+                }
+            }
+        });
+        if (bad == 1) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets decrease");
+        if (bad == 2) return fail(nullptr, FEMSTEP_EINVAL, "adjacency is not the node-to-corner map of this mesh");
     }
     const int dev = fs::device_status();
     if (dev != FEMSTEP_OK) return dev;
@@ -241,27 +265,45 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     // position = rest + (u - c): u = fl(x) for the caller's x = position - rest, and c =
     // fl(u - x) carries the part of x that u cannot, so a position read back from this
     // solver (rest + u - c, in double) and handed to a new one continues bit for bit.
-    std::vector<float> disp(N * 3, 0.0f), comp(N * 3, 0.0f), vel(N * 3, 0.0f);
-    if (m.position)
-        for (size_t i = 0; i < N * 3; ++i) {
-            const double x = m.position[i] - m.rest[i];
-            disp[i] = (float)x;
-            comp[i] = (float)((double)disp[i] - x);
-        }
-    if (m.velocity)
-        for (size_t i = 0; i < N * 3; ++i) vel[i] = (float)m.velocity[i];
-    d.disp = A.upload(disp.data(), N * 3);
-    d.disp_c = A.upload(comp.data(), N * 3);
-    d.velocity = A.upload(vel.data(), N * 3);
+    // A node array the caller leaves out starts at zero on the device, not uploaded.
+    if (m.position) {
+        std::vector<float> disp(N * 3), comp(N * 3);
+        fs::parallel_chunks(N * 3, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) {
+                const double x = m.position[i] - m.rest[i];
+                disp[i] = (float)x;
+                comp[i] = (float)((double)disp[i] - x);
+            }
+        });
+        d.disp = A.upload(disp.data(), N * 3);
+        d.disp_c = A.upload(comp.data(), N * 3);
+    } else {
+        d.disp = A.zeros<float>(N * 3);
+        d.disp_c = A.zeros<float>(N * 3);
+    }
+    if (m.velocity) {
+        std::vector<float> vel(N * 3);
+        fs::parallel_chunks(N * 3, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) vel[i] = (float)m.velocity[i];
+        });
+        d.velocity = A.upload(vel.data(), N * 3);
+    } else {
+        d.velocity = A.zeros<float>(N * 3);
+    }
     std::vector<uint8_t>& pin = s->pin;
     pin.assign(N, 0);
     if (m.pinned)
-        for (size_t n = 0; n < N; ++n)
-            pin[n] = (uint8_t)((m.pinned[n * 3] ? 1 : 0) | (m.pinned[n * 3 + 1] ? 2 : 0) | (m.pinned[n * 3 + 2] ? 4 : 0));
+        fs::parallel_chunks(N, [&](size_t b, size_t e) {
+            for (size_t n = b; n < e; ++n)
+                pin[n] = (uint8_t)((m.pinned[n * 3] ? 1 : 0) | (m.pinned[n * 3 + 1] ? 2 : 0) |
+                                   (m.pinned[n * 3 + 2] ? 4 : 0));
+        });
     d.pinned = A.upload(pin.data(), N);
     if (m.load) {
         std::vector<float> load(N * 3);
-        for (size_t i = 0; i < N * 3; ++i) load[i] = (float)m.load[i];
+        fs::parallel_chunks(N * 3, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) load[i] = (float)m.load[i];
+        });
         d.load = A.upload(load.data(), N * 3);
     }
     float* mass = A.alloc<float>(N);
@@ -454,12 +496,16 @@ int femstep_shell_readback(femstep_shell* s, double* position, double* velocity)
             rc = check(s, cudaMemcpy(comp.data(), s->d.disp_c, n3 * sizeof(float), cudaMemcpyDeviceToHost),
                        "readback");
         if (rc) return rc;
-        for (size_t i = 0; i < n3; ++i) position[i] = s->rest[i] + ((double)buf[i] - (double)comp[i]);
+        fs::parallel_chunks(n3, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) position[i] = s->rest[i] + ((double)buf[i] - (double)comp[i]);
+        });
     }
     if (velocity) {
         rc = check(s, cudaMemcpy(buf.data(), s->d.velocity, n3 * sizeof(float), cudaMemcpyDeviceToHost), "readback");
         if (rc) return rc;
-        for (size_t i = 0; i < n3; ++i) velocity[i] = buf[i];
+        fs::parallel_chunks(n3, [&](size_t b, size_t e) {
+            for (size_t i = b; i < e; ++i) velocity[i] = buf[i];
+        });
     }
     return FEMSTEP_OK;
 }

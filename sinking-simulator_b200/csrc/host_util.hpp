@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace fs {
@@ -64,6 +66,24 @@ private:
 // FP64 tet step's rest state, bit-identical to the FP64 oracle's.
 void tet_rest_state64(size_t nodes, size_t tets, const float* position, const uint32_t* index, double density,
                       std::vector<double>& inv, std::vector<double>& vol, std::vector<double>& mass);
+
+// f(begin, end) over [0, n) split into contiguous chunks, one per host core (inline
+// when n is small).  For loops whose iterations are independent.
+template <class F>
+void parallel_chunks(size_t n, F f, size_t min_chunk = size_t(1) << 16) {
+    const size_t cores = std::max(1u, std::thread::hardware_concurrency());
+    const size_t parts = std::min(cores, std::max<size_t>(1, n / min_chunk));
+    if (parts <= 1) {
+        f(size_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t k = 0; k < parts; ++k) {
+        const size_t b = n * k / parts, e = n * (k + 1) / parts;
+        pool.emplace_back([=, &f]() { f(b, e); });
+    }
+    for (auto& t : pool) t.join();
+}
 
 // Node -> incident corner CSR by counting sort, the construction of
 // engine/sim/fem.cpp:147-157 and engine/sim/zone.cpp:739-754.
