@@ -217,7 +217,8 @@ struct femstep_pool {
     PoolTile* d_etiles = nullptr;
     PoolTile* d_ntiles = nullptr;
     int* d_active = nullptr;
-    double* d_block_max = nullptr;  // critical-dt scratch
+    fs::PoolAdmit* d_admit = nullptr;  // [max_meshes]: an admission group's records
+    unsigned long long* d_w2 = nullptr;  // [max_meshes]: the group's element bounds
     cudaGraphExec_t graph = nullptr;
     bool graph_staged = false;  // which element pass the graph was captured with
     long long launches = 0;
@@ -435,7 +436,7 @@ void stage_layout(Placement& pl, size_t base) {
 // reference's order (fem.cpp:147-157), the slot map, the rest positions, pins and load;
 // node and slot ids rebased into the pool.  The FP64 rest state (Dm^-1, volumes, lumped
 // masses; fem.cpp:119-158) is computed on the device from the staged positions
-// (launch_pool_rest_state).  Runs on any host thread; touches nothing but the mesh's
+// (launch_pool_admit).  Runs on any host thread; touches nothing but the mesh's
 // own staging.
 void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
     const long long N = pl.N, T = pl.T;
@@ -606,14 +607,19 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
         }
         std::vector<long long> weight(g1 - g0);
         for (int i = g0; i < g1; ++i) weight[i - g0] = pl[i].T;
+        const int G = g1 - g0;
+        const size_t table = ((size_t)G * sizeof(fs::PoolAdmit) + 255) & ~size_t(255);
         cudaError_t err;
-        Staging::Buf* buf = p->staging.get(bytes, err);
+        Staging::Buf* buf = p->staging.get(bytes + table, err);
         if (!buf) {
             undo();  // earlier groups' copies went to ranges that are free again
             return check(p, err, "pinned staging");
         }
         char* stage = Staging::take(buf, bytes);
+        fs::PoolAdmit* adm = (fs::PoolAdmit*)Staging::take(buf, table);
         parallel_for(g1 - g0, weight, [&](int k) { prepare_mesh(meshes[g0 + k], pl[g0 + k], stage); });
+        long long tets = 0, nodes = 0, parts = 0;
+        bool any_dt = false;
         auto send = [&](void* dst, size_t off, size_t len) {
             cudaMemcpyAsync(dst, stage + off, len, cudaMemcpyHostToDevice, st);
         };
@@ -623,24 +629,12 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
             const long long T = q.T, N = q.N, t0 = q.t0, n0 = q.n0, part0 = q.part0;
             send(d.index + t0, q.idx4, T * sizeof(uint4));
             send(d.slot + t0, q.slot4, T * sizeof(uint4));
-            for (int k = 0; k < 7; ++k) {
-                cudaMemsetAsync(d.plastic + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
-                cudaMemsetAsync(d.plastic_c + (size_t)k * p->tet_cap + t0, 0, T * 4, st);
-            }
             send(d.offset + n0, q.offs, (N + 1) * 4);
             send(d.fixed + n0, q.fixed, N + 1);
             send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
-            cudaMemsetAsync(d.disp + n0, 0, (N + 1) * 16, st);
-            cudaMemsetAsync(d.disp_c + n0, 0, (N + 1) * 16, st);
-            // the rest state from the rest positions, staged in the mesh's velocity rows,
-            // which then start at rest
+            // the rest positions, staged in the mesh's velocity rows for the rest state;
+            // the admission kernels below then start the nodes at rest
             send(d.velocity + n0 * 3, q.pos, (N + 1) * 12);
-            fs::launch_pool_rest_state(d, t0, T, n0, N, m.density, st);
-            cudaMemsetAsync(d.velocity + n0 * 3, 0, (N + 1) * 12, st);
-            cudaMemsetAsync(d.e_diss + part0, 0, q.e_tiles * 8, st);
-            cudaMemsetAsync(d.e_strain + part0, 0, q.e_tiles * 8, st);
-            cudaMemsetAsync(d.n_work + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
-            cudaMemsetAsync(d.n_kin + part0 + q.e_tiles, 0, q.n_tiles * 8, st);
             PoolMesh* pm = (PoolMesh*)(stage + q.rec);
             std::memset(pm, 0, sizeof(PoolMesh));
             const double E = m.youngs_modulus, nu = m.poisson_ratio;
@@ -658,11 +652,31 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
             pm->n_part = part0 + q.e_tiles;
             pm->serial = p->next_serial + i;
             send(d.meshes + q.id, q.rec, sizeof(PoolMesh));
-            // no step given: 0.9 x the FP64 element eigenvalue bound of the uploaded FP32
-            // Dm^-1, computed and stored on the device behind the uploads
-            if (!(m.dt > 0.0))
-                fs::launch_pool_dt(d, q.id, t0, T, E, nu, m.density, 0.9, p->d_block_max, p->d_out + 7, st);
+            // the group's record of this mesh for the admission kernels; no step given:
+            // 0.9 x the FP64 element eigenvalue bound of the stored FP32 Dm^-1, formed
+            // and stored on the device behind the uploads
+            fs::PoolAdmit& a = adm[i - g0];
+            a.t0 = t0;
+            a.T = T;
+            a.n0 = n0;
+            a.N = N;
+            a.part0 = part0;
+            a.parts = q.e_tiles + q.n_tiles;
+            a.tet_first = tets;
+            a.node_first = nodes;
+            a.part_first = parts;
+            a.density = m.density;
+            a.lambda = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+            a.mu = E / (2.0 * (1.0 + nu));
+            a.id = q.id;
+            a.want_dt = m.dt > 0.0 ? 0 : 1;
+            any_dt = any_dt || a.want_dt;
+            tets += T;
+            nodes += N + 1;
+            parts += a.parts;
         }
+        cudaMemcpyAsync(p->d_admit, adm, (size_t)G * sizeof(fs::PoolAdmit), cudaMemcpyHostToDevice, st);
+        fs::launch_pool_admit(d, p->d_admit, G, tets, nodes, parts, any_dt, p->d_w2, st);
         Staging::submit(buf, st);
         g0 = g1;
     }
@@ -758,7 +772,8 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
     p->d_etiles = A.alloc<PoolTile>(p->part_cap);
     p->d_ntiles = A.alloc<PoolTile>(p->part_cap);
     p->d_active = A.zeros<int>(max_meshes);
-    p->d_block_max = A.zeros<double>(Tc / fs::kBlock + 1);
+    p->d_admit = A.alloc<fs::PoolAdmit>(max_meshes);
+    p->d_w2 = A.zeros<unsigned long long>(max_meshes);
     p->d_out = A.zeros<double>(8);
     if (!A.ok()) {
         const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;

@@ -5,8 +5,11 @@
 // (its tiles do nothing) until the host retires it.  The energy partial of a tile goes
 // to the slot its mesh was given at admission, so nothing in a mesh's result depends
 // on what else is in the pool.
+#include <algorithm>
+
 #include "bulk.cuh"
 #include "common.cuh"
+#include "omega.cuh"
 #include "pool.hpp"
 #include "tet.hpp"
 
@@ -196,12 +199,6 @@ __global__ void __launch_bounds__(B, 1024 / B) pool_persistent(PoolDevice d, int
     }
 }
 
-__global__ void pool_set_dt(PoolMesh* meshes, int id, const double* w2, double safety) {
-    const double v = w2[0];
-    const double dt = v > 0.0 ? safety * 2.0 / sqrt(v) : 0.0;
-    meshes[id].dt64 = dt;
-    meshes[id].dt = (float)dt;
-}
 
 }  // namespace
 
@@ -287,9 +284,7 @@ namespace {
 // each corner's force slot (the element pass writes every slot before anything reads
 // it).  The mesh's rest positions are staged in its own velocity rows (indexed by
 // pool node id), which the admission zeroes afterwards.
-__global__ void pool_rest_tets(PoolDevice d, long long t0, long long T, double density) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
+__device__ __forceinline__ void rest_tet(const PoolDevice& d, long long t0, long long t, double density) {
     const float* pos = d.velocity;
     const uint4 id4 = d.index[t0 + t];
     const uint32_t id[4] = {id4.x, id4.y, id4.z, id4.w};
@@ -326,9 +321,7 @@ __global__ void pool_rest_tets(PoolDevice d, long long t0, long long T, double d
 
 // Lumped node masses: the tets' quarters over the node's CSR run, which lists its tets
 // in ascending order -- the order the host loop adds them in.  Then the spare node.
-__global__ void pool_rest_nodes(PoolDevice d, long long n0, long long N) {
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n > N) return;
+__device__ __forceinline__ void rest_node(const PoolDevice& d, long long n0, long long N, long long n) {
     if (n == N) {  // the spare node slot holds the CSR end and has no mass
         d.mass[n0 + N] = 0.0f;
         d.inv_mass[n0 + N] = 0.0f;
@@ -340,20 +333,104 @@ __global__ void pool_rest_nodes(PoolDevice d, long long n0, long long N) {
     d.inv_mass[n0 + n] = m > 0.0 ? (float)(1.0 / m) : 0.0f;
 }
 
+// The group record a thread's item belongs to: the last one whose prefix `first` of the
+// kind given is <= k (records ascend).
+template <long long PoolAdmit::*First>
+__device__ __forceinline__ int admit_of(const PoolAdmit* adm, int G, long long k) {
+    int lo = 0, hi = G - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (adm[mid].*First <= k)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per tet of the group: zero its plastic state, form its rest state.  Per partial
+// slot of the group: zero the four energy partials.
+__global__ void pool_admit_tets(PoolDevice d, const PoolAdmit* adm, int G, long long tets, long long parts) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tets; k += stride) {
+        const PoolAdmit& a = adm[admit_of<&PoolAdmit::tet_first>(adm, G, k)];
+        const long long t = k - a.tet_first;
+        for (int i = 0; i < 7; ++i) {
+            d.plastic[(size_t)i * d.tet_cap + a.t0 + t] = 0.0f;
+            d.plastic_c[(size_t)i * d.tet_cap + a.t0 + t] = 0.0f;
+        }
+        rest_tet(d, a.t0, t, a.density);
+    }
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < parts; k += stride) {
+        const PoolAdmit& a = adm[admit_of<&PoolAdmit::part_first>(adm, G, k)];
+        const long long q = a.part0 + (k - a.part_first);
+        d.e_diss[q] = 0.0;
+        d.e_strain[q] = 0.0;
+        d.n_work[q] = 0.0;
+        d.n_kin[q] = 0.0;
+    }
+}
+
+// Per node of the group (and each mesh's spare slot): its lumped mass from the tets'
+// quarters, then displacement, compensation and velocity at rest (the velocity rows
+// held the staged positions until now).
+__global__ void pool_admit_nodes(PoolDevice d, const PoolAdmit* adm, int G, long long nodes) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nodes; k += stride) {
+        const PoolAdmit& a = adm[admit_of<&PoolAdmit::node_first>(adm, G, k)];
+        const long long n = k - a.node_first;
+        rest_node(d, a.n0, a.N, n);
+        d.disp[a.n0 + n] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        d.disp_c[a.n0 + n] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float* v = d.velocity + (size_t)(a.n0 + n) * 3;
+        v[0] = v[1] = v[2] = 0.0f;
+    }
+}
+
+// Per tet of a mesh that wants its step formed: the element bound from the stored
+// FP32 Dm^-1 (promoted to double), maximised per mesh.  A non-negative double orders
+// as its bit pattern, so the maximum is an integer atomicMax and exact.
+__global__ void pool_admit_omega(PoolDevice d, const PoolAdmit* adm, int G, long long tets,
+                                 unsigned long long* w2) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tets; k += stride) {
+        const int g = admit_of<&PoolAdmit::tet_first>(adm, G, k);
+        const PoolAdmit& a = adm[g];
+        if (!a.want_dt) continue;
+        const long long t = a.t0 + (k - a.tet_first);
+        double gr[4][3];
+        for (int c = 0; c < 3; ++c)
+            for (int r = 0; r < 3; ++r) gr[c + 1][r] = (double)d.rest_inv[(size_t)(r * 3 + c) * d.tet_cap + t];
+        for (int r = 0; r < 3; ++r) gr[0][r] = -(gr[1][r] + gr[2][r] + gr[3][r]);
+        const double v = tet_omega2_one(gr, a.lambda, a.mu, a.density);
+        atomicMax(w2 + g, (unsigned long long)__double_as_longlong(v > 0.0 ? v : 0.0));
+    }
+}
+
+__global__ void pool_admit_dt(PoolMesh* meshes, const PoolAdmit* adm, int G, const unsigned long long* w2) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G || !adm[g].want_dt) return;
+    const double v = __longlong_as_double((long long)w2[g]);
+    const double dt = v > 0.0 ? 0.9 * 2.0 / sqrt(v) : 0.0;  // safety 0.9, as the single-mesh bound
+    meshes[adm[g].id].dt64 = dt;
+    meshes[adm[g].id].dt = (float)dt;
+}
+
 }  // namespace
 
-void launch_pool_rest_state(const PoolDevice& d, long long t0, long long T, long long n0, long long N, double density,
-                            cudaStream_t stream) {
-    pool_rest_tets<<<blocks_for(T, kBlock), kBlock, 0, stream>>>(d, t0, T, density);
-    pool_rest_nodes<<<blocks_for(N + 1, kBlock), kBlock, 0, stream>>>(d, n0, N);
+void launch_pool_admit(const PoolDevice& d, const PoolAdmit* adm, int G, long long tets, long long nodes,
+                       long long parts, bool any_dt, unsigned long long* w2, cudaStream_t stream) {
+    const int cap = sm_count() * 8;
+    auto grid = [&](long long n) { return (int)std::max(1LL, std::min((long long)cap, (n + kBlock - 1) / kBlock)); };
+    pool_admit_tets<<<grid(std::max(tets, parts)), kBlock, 0, stream>>>(d, adm, G, tets, parts);
+    pool_admit_nodes<<<grid(nodes), kBlock, 0, stream>>>(d, adm, G, nodes);
+    if (any_dt) {
+        cudaMemsetAsync(w2, 0, (size_t)G * sizeof(unsigned long long), stream);
+        pool_admit_omega<<<grid(tets), kBlock, 0, stream>>>(d, adm, G, tets, w2);
+        pool_admit_dt<<<(G + 127) / 128, 128, 0, stream>>>(d.meshes, adm, G, w2);
+    }
 }
 
-void launch_pool_dt(const PoolDevice& d, int id, long long t0, long long T, double E, double nu, double rho,
-                    double safety, double* block_max, double* w2, cudaStream_t stream) {
-    const int blocks = blocks_for(T, kBlock);
-    launch_tet_omega2_f32(T, d.rest_inv + t0, d.tet_cap, E, nu, rho, block_max, blocks, stream);
-    launch_reduce_max(block_max, blocks, w2, stream);
-    pool_set_dt<<<1, 1, 0, stream>>>(d.meshes, id, w2, safety);
-}
+
 
 }  // namespace fs

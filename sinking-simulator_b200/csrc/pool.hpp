@@ -95,12 +95,26 @@ int pool_persistent_max_blocks(int tile);
 // meshes[id].dt = safety * 2 / sqrt(max omega^2) of the mesh's tets [t0, t0 + T),
 // from the pool's FP32 Dm^-1; 0 when the bound is not positive.  `block_max` holds
 // ceil(T / 256) doubles and `w2` one double of scratch.
-// An admitted mesh's rest state on the device (fem.cpp:119-158 in FP64): Dm^-1 and
-// volume rows, lumped masses.  Needs the mesh's index, slot map and CSR offsets in
-// place, and its rest positions (float, by pool node id) staged in d.velocity.
-void launch_pool_rest_state(const PoolDevice& d, long long t0, long long T, long long n0, long long N, double density,
-                            cudaStream_t stream);
-void launch_pool_dt(const PoolDevice& d, int id, long long t0, long long T, double E, double nu, double rho,
-                    double safety, double* block_max, double* w2, cudaStream_t stream);
+// One mesh of an admission group, for the group's batched admission kernels: its
+// ranges in the pool, where its tets / nodes / partial slots start among the group's
+// (prefix sums, ascending), its density and elastic constants, and whether its time
+// step is to be formed on the device.
+struct PoolAdmit {
+    long long t0, T, n0, N, part0, parts;
+    long long tet_first, node_first, part_first;  // node_first counts N + 1 per mesh
+    double density, lambda, mu;
+    int id, want_dt;
+};
+
+// The device half of admitting a group of meshes, after their index, slot map, CSR
+// offsets, pins, load, record and rest positions (staged in the velocity rows) are
+// uploaded: zero the plastic state and the energy partials, form the FP64 rest state
+// (Dm^-1, volumes, lumped masses), start the nodes at rest, and, for the meshes that
+// want it, set the time step to 0.9 x the FP64 element bound, 2 / sqrt(max omega^2)
+// over its tets (tet_omega2_one, the single-mesh handle's bound).
+// `adm` (device) holds the G records; `w2` is G scratch words.  Four launches per
+// group, whatever its size.
+void launch_pool_admit(const PoolDevice& d, const PoolAdmit* adm, int G, long long tets, long long nodes,
+                       long long parts, bool any_dt, unsigned long long* w2, cudaStream_t stream);
 
 }  // namespace fs

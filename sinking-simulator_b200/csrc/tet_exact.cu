@@ -18,6 +18,7 @@
 // F64): one thread per tet / per node, SoA element arrays so each warp load is one
 // contiguous 128 B line, node-major force slots so each node's gather is contiguous.
 #include "common.cuh"
+#include "omega.cuh"
 #include "tet.hpp"
 
 namespace fs {
@@ -389,59 +390,7 @@ __global__ void __launch_bounds__(kBlock) tet_omega2(long long tets, const In* r
             for (int a = 0; a < 3; ++a) g[c + 1][a] = (double)rest_inv[(size_t)(a * 3 + c) * stride + t];
 #pragma unroll
         for (int a = 0; a < 3; ++a) g[0][a] = -(g[1][a] + g[2][a] + g[3][a]);
-        double v[12];
-#pragma unroll
-        for (int i = 0; i < 12; ++i) v[i] = 1.0 + 0.37 * i - 0.11 * i * i;
-        double lam = 0.0;
-#pragma unroll 1
-        for (int it = 0; it < 400; ++it) {
-            double e[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-            for (int n = 0; n < 4; ++n) {
-                const double* u = &v[n * 3];
-                e[0] += g[n][0] * u[0];
-                e[1] += g[n][1] * u[1];
-                e[2] += g[n][2] * u[2];
-                e[3] += g[n][1] * u[0] + g[n][0] * u[1];
-                e[4] += g[n][2] * u[1] + g[n][1] * u[2];
-                e[5] += g[n][0] * u[2] + g[n][2] * u[0];
-            }
-            const double tr = e[0] + e[1] + e[2];
-            double s[6];
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                s[i] = lambda * tr + 2.0 * mu * e[i];
-                s[3 + i] = mu * e[3 + i];
-            }
-            double w[12];
-#pragma unroll
-            for (int n = 0; n < 4; ++n) {
-                w[n * 3 + 0] = g[n][0] * s[0] + g[n][1] * s[3] + g[n][2] * s[5];
-                w[n * 3 + 1] = g[n][1] * s[1] + g[n][0] * s[3] + g[n][2] * s[4];
-                w[n * 3 + 2] = g[n][2] * s[2] + g[n][1] * s[4] + g[n][0] * s[5];
-            }
-            double num = 0.0, den = 0.0, norm = 0.0;
-#pragma unroll
-            for (int i = 0; i < 12; ++i) {
-                num += v[i] * w[i];
-                den += v[i] * v[i];
-                norm += w[i] * w[i];
-            }
-            const double next = den > 0.0 ? num / den : 0.0;
-            norm = sqrt(norm);
-            if (!(norm > 0.0)) {
-                lam = 0.0;
-                break;
-            }
-#pragma unroll
-            for (int i = 0; i < 12; ++i) v[i] = w[i] / norm;
-            if (it > 8 && fabs(next - lam) <= 1e-10 * fabs(next)) {
-                lam = next;
-                break;
-            }
-            lam = next;
-        }
-        w2 = 4.0 / rho * lam;
+        w2 = tet_omega2_one(g, lambda, mu, rho);
     }
     smax[threadIdx.x] = w2;
     __syncthreads();
