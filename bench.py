@@ -547,9 +547,10 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
         h2d = sum(b.position.nbytes + b.index.nbytes + b.fixed.nbytes + b.external_force.nbytes for b in built)
         e2e = {"value": T * args.steps / wall, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                "d2h_bytes_per_step": d2h / args.steps, "phases": phases,
-               "note": "create the pool, admit every mesh from host arrays (femstep_pool_admit_many: host rest "
-                       "state on all cores + upload), K steps, read back every mesh's positions and velocities, "
-                       "through the C ABI, wall clock"}
+               "note": "create the pool, admit every mesh from host arrays (femstep_pool_admit_many: CSR and slot "
+                       "map on all host cores, upload, FP64 rest state on the device), K steps, read back every "
+                       "mesh's positions and velocities (femstep_pool_readback_many), destroy; through the C ABI, "
+                       "wall clock"}
     peak, peak_kind = measured_peak()
     achieved = eb / (elem_ms / 1e3) / 1e9
     if rank == 0:

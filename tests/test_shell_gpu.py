@@ -64,6 +64,35 @@ def test_shell_step_against_fp64_oracle(fem, port, compensated, tol):
     assert abs(e[1] - er[1]) < 5e-3 * abs(er[1]) + 1e-12
 
 
+@pytest.mark.parametrize("nx,ny", [(1, 1), (3, 1), (5, 1), (5, 3), (7, 2)])
+def test_ragged_element_counts_against_fp64_oracle(fem, port, nx, ny):
+    """Element counts that do not fill the last warp group of four (1, 3, 5, 15, 14):
+    the tail lanes shadow the last element and write nothing, in the step and in the
+    set-up.  A cantilever strip, clamped at x = 0, bent by a tip load into yield."""
+    rest, index = fem.plate_mesh(0.01 * nx, 0.01 * ny, 0.004, nx, ny, 1)
+    p0 = rest.reshape(-1, 3)
+    pinned = np.repeat(p0[:, 0] < 1e-9, 3).astype(np.uint8)
+    tip = p0[:, 0] > 0.01 * nx - 1e-9
+    load = np.zeros_like(p0)
+    load[tip, 2] = 600.0 * ny / tip.sum()
+    load = load.reshape(-1)
+    mat = O.material(E=206e9, nu=0.3, yield_=355e6, hardening=1e9)
+    ref = O.ShellModel(port, rest, index, pinned, mat, fext=load)
+    s = fem.ShellSolver(rest, index, pinned=pinned, load=load, density=7850.0)
+    dt = s.critical_dt(206e9, 0.3, 7850.0, 0.9)
+    steps, rise = 300, 100 * dt
+    ref.step(dt, steps, rise_time=rise)
+    s.run(steps, dt=dt, rise_time=rise, compensated=True, max_iterations=40, tol_residual=1e-6, tol_work=1e-16)
+    p, _ = s.readback()
+    u, ur = p - rest, ref.position - rest
+    assert np.abs(ur).max() > 1e-6, "the strip must bend"
+    err = np.abs(u - ur).max() / np.abs(ur).max()
+    assert err < 1e-4, err
+    st, sr = s.state(), ref.state.reshape(-1, 129)
+    assert st.shape == sr.shape
+    assert np.abs(st[:, 12:120:15] - sr[:, 12:120:15]).max() <= 1e-3 * max(sr[:, 12:120:15].max(), 1e-12) + 1e-9
+
+
 def test_caller_forms_match_device_forms(fem, port):
     """Forms handed over from the CPU solver (ZoneGpuSolver::initialise's path) give the
     same step as forms built on the device: the same doubles narrowed the same way."""
