@@ -124,3 +124,39 @@ def test_rest_stays_at_rest(fem):
         # by far less than a femtometre.
         tol = 0.0 if mode != "f64" else 1e-14
         assert np.abs(p - pos).max() <= tol and np.abs(v).max() <= tol * 1e5, mode
+
+
+@pytest.mark.parametrize("cells", [(1, 1, 1), (2, 1, 1), (5, 3, 1)])
+def test_tiny_meshes_in_every_mode(fem, port, cells):
+    """Meshes far smaller than a block (6, 12 and 90 tets): the tail threads of the
+    element and node passes do nothing.  The FP64 step is bit-identical to the FP64
+    oracle; the FP32-compensated one within the target tolerance; REF32 bit-identical
+    to the reference's float step restated."""
+    nx, ny, nz = cells
+    pos, idx = fem.box_tet_mesh(0.1 * nx, 0.1 * ny, 0.1 * nz, nx, ny, nz)
+    fixed = (pos[0::3] < 1e-6).astype(np.uint32)
+    tip = pos[0::3] > 0.1 * nx - 1e-6
+    fext = np.zeros(pos.size)
+    fext[2::3][tip] = -2e5 * ny * nz / tip.sum()
+    ref = O.TetMesh64(port, pos, idx, fixed, fext)
+    dt = port.tet64_critical_dt(C.byref(ref._s), 210e9, 0.3, 7850.0, 0.9)
+    ref.step(O.tet64_params(dt=dt, ramp_steps=100), 300)
+    g = fem.TetSolver(pos, idx, mode="f64", fixed=fixed, external_force=fext, density=7850.0)
+    g.run(300, dt=dt, ramp_steps=100)
+    p64, _ = g.readback64()
+    assert np.array_equal(p64, ref.position)
+    k = fem.TetSolver(pos, idx, mode="f32k", fixed=fixed, external_force=fext, density=7850.0)
+    k.run(300, dt=dt, ramp_steps=100)
+    pk, _ = k.readback64()
+    assert np.abs(ref.position - pos).max() > 1e-7, "the mesh must move"
+    assert _rel_disp_error(pk, ref.position, pos.astype(np.float64)) < 1e-5
+    # REF32: the reference's float step (elastic, gravity), restated, bit for bit
+    m = O.TetMesh32(port, pos, idx)
+    m.fixed[:] = fixed
+    m.rest_state(210e9, 0.3, 7850.0)
+    r = fem.TetSolver(pos, idx, mode="ref32", fixed=fixed, mass=m.mass, rest_inv=m.rest_inv,
+                      rest_volume=m.rest_volume, adjacency_offset=m.adj_offset, adjacency_entry=m.adj_entry)
+    m.step(210e9, 0.3, 7850.0, 1e-6, 9.80665, 1.0, 50)
+    r.run(50, youngs=210e9, poisson=0.3, dt=1e-6, gravity=9.80665, damping=1.0)
+    pr, vr = r.readback()
+    assert np.array_equal(pr, m.position) and np.array_equal(vr, m.velocity)
