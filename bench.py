@@ -498,7 +498,9 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
     pool.run(0)
     admit_s = time.perf_counter() - t_admit
     tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=16)
-    pool.run(args.warmup)
+    # W warm-up steps, at least one captured graph's worth (16 steps), so that the graph
+    # the timed chunk replays is built before the timed region
+    pool.run(max(args.warmup, 16))
     barrier()
     with ClockSampler(local) as clocks:
         clocks.wait_first()
