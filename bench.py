@@ -724,7 +724,8 @@ def main():
     s = w.s
     # W warm-up steps, at least one captured graph's worth (32 steps), so the graph the
     # timed run replays is built before the timed region
-    s.run(max(args.warmup, 32), **w.kw)
+    warm = max(args.warmup, 32)
+    s.run(warm, **w.kw)
     barrier()
     with ClockSampler(local) as clocks:
         clocks.wait_first()
@@ -759,7 +760,7 @@ def main():
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "elements": w.units, "nodes": w.nodes,
                        "dt": w.kw["dt"], "element_kernel_ms": elem_ms, "node_kernel_ms": node_ms,
