@@ -113,11 +113,12 @@ def tet_bytes(T, N, mode):
 
 
 def shell_bytes(E, N):
-    """Element kernel: forms 8 x 188 floats + J0^-1 36 + state R/W 2 x 8 x 14 floats +
-    alpha R/W 2 x 32 + index 32 + slot map 32 + corner forces 96, and the node reads
-    (rest 24 + displacement 12) once per node.  Node kernel: offsets 4, forces 12 per
-    slot, displacement and compensation R/W 48, velocity R/W 24, mass 8, pins 1, load 12."""
-    elem = E * (8 * 188 * 4 + 36 + 2 * 8 * 14 * 4 + 2 * 32 + 32 + 32 + 96) + N * (24 + 12)
+    """Element kernel: the element row (J0^-1 and the enhanced-mode scales) 64 + state
+    R/W 2 x 8 x 14 floats + alpha R/W 2 x 32 + index 32 + slot map 32 + corner forces 96,
+    and the node reads (rest 24 + displacement 12) once per node; B and G are formed in
+    the kernel from the rest corners.  Node kernel: offsets 4, forces 12 per slot,
+    displacement and compensation R/W 48, velocity R/W 24, mass 8, pins 1, load 12."""
+    elem = E * (64 + 2 * 8 * 14 * 4 + 2 * 32 + 32 + 32 + 96) + N * (24 + 12)
     node = N * (4 + 48 + 24 + 8 + 1 + 12) + E * 8 * 12
     return elem, node
 

@@ -274,9 +274,12 @@ typedef struct {
     const uint32_t *index;          /* 8E, node order of solid_shell.hpp:115-126 */
     const uint8_t *pinned;          /* 3N (Solver::pinnedDof / HexMesh::fixed), NULL = none */
     const double *load;             /* 3N full-amplitude external nodal load, NULL = none */
-    const double *forms;            /* NULL: formed on the device in FP64.  Else the caller's
-                                       RestForms, 1505 doubles per element in the order of
-                                       engine/gpu/zone_gpu.cpp:28-34 (b, g, weight, J0^-1) */
+    const double *forms;            /* NULL, or the caller's RestForms, 1505 doubles per
+                                       element in the order of engine/gpu/zone_gpu.cpp:28-34
+                                       (b, g, weight, J0^-1).  The step forms B and G in FP32
+                                       from the rest positions itself; given forms must be the
+                                       solid-shell forms of those positions (every weight, and
+                                       all of the first 64 elements, to 1e-9), else EINVAL */
     const double *mass;             /* N lumped mass (Solver::nodalMass), NULL = lumped on device */
     const double *state;            /* 129 doubles per element (zone_gpu.cpp:36-40 layout), NULL = virgin */
     const uint32_t *adjacency_offset; /* N+1 (Solver::adjacencyOffset), NULL = built */

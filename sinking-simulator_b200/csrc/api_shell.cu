@@ -153,6 +153,57 @@ int ensure_factor(femstep_shell* s, const femstep_shell_params& p) {
     return FEMSTEP_OK;
 }
 
+// The caller's RestForms (1505 doubles per element, zone_gpu.cpp:28-34 order) against
+// the device's FP64 forms of the same rest positions: every element's Gauss weights,
+// and all the values of the first 64 elements, each block (B, G, w, J0^-1) to 1e-9 of
+// its largest entry.
+int check_caller_forms(femstep_shell* s, const double* forms, const double* weights) {
+    const size_t E = s->elements;
+    std::vector<double> w(E * 8);
+    int rc = check(s, cudaMemcpy(w.data(), weights, w.size() * sizeof(double), cudaMemcpyDeviceToHost), "forms check");
+    if (rc) return rc;
+    for (size_t e = 0; e < E; ++e)
+        for (int gp = 0; gp < 8; ++gp) {
+            const double mine = w[e * 8 + gp], theirs = forms[e * 1505 + 1488 + gp];
+            if (!(std::fabs(mine - theirs) <= 1e-9 * std::fabs(mine)))
+                return fail(s, FEMSTEP_EINVAL,
+                            "forms: element " + std::to_string(e) + "'s Gauss weights are not those of its rest positions");
+        }
+    const size_t n = std::min<size_t>(E, 64);
+    double* f64 = nullptr;
+    rc = check(s, cudaMalloc(&f64, n * 1507 * sizeof(double)), "forms check");
+    if (rc) return rc;
+    fs::ShellSetupArgs a{};
+    a.elements = (long long)n;
+    a.groups = (long long)((n + 3) / 4);
+    a.rest = s->d.rest;
+    a.index = s->d.index;
+    a.slot = s->d.slot;
+    a.formulation = 2;
+    a.forms64 = f64;
+    fs::launch_shell_setup(a, s->stream);
+    std::vector<double> h(n * 1507);
+    rc = check(s, cudaMemcpyAsync(h.data(), f64, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
+               "forms check");
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "forms check");
+    cudaFree(f64);
+    if (rc) return rc;
+    const size_t block[5] = {0, 1152, 1488, 1496, 1505};
+    for (size_t e = 0; e < n; ++e)
+        for (int b = 0; b < 4; ++b) {
+            const double* mine = h.data() + e * 1507;
+            const double* theirs = forms + e * 1505;
+            double scale = 0.0;
+            for (size_t k = block[b]; k < block[b + 1]; ++k) scale = std::max(scale, std::fabs(mine[k]));
+            for (size_t k = block[b]; k < block[b + 1]; ++k)
+                if (!(std::fabs(mine[k] - theirs[k]) <= 1e-9 * scale))
+                    return fail(s, FEMSTEP_EINVAL,
+                                "forms: element " + std::to_string(e) +
+                                    "'s forms are not the solid-shell forms of its rest positions");
+        }
+    return FEMSTEP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -237,10 +288,8 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.index = A.upload(m.index, E * 8);
     d.slot = A.upload(slot.data(), E * 8);
     d.offset = A.upload(offset.data(), N + 1);
-    float4* forms = A.zeros<float4>((size_t)s->groups * fs::kShellRec4 * 32);
-    d.forms = forms;
-    float* j0 = A.zeros<float>(E * 9);
-    d.j0inv = j0;
+    float4* elem = A.zeros<float4>(E * fs::kShellElemQ);
+    d.elem = elem;
     d.state = A.zeros<float>((size_t)s->groups * fs::kShellStateQ * 32);
     d.alpha = A.zeros<float>(Epad * 8);
     d.state2 = A.zeros<float>((size_t)s->groups * fs::kShellState2Q * 32);
@@ -311,32 +360,20 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.mass = mass;
     d.inv_mass = inv_mass;
 
-    // forms: the caller's (narrowed to float, as zone_gpu.cpp:668-684 does), or formed here
-    if (A.ok() && m.forms) {
-        std::vector<float4> rec((size_t)s->groups * fs::kShellRec4 * 32, make_float4(0, 0, 0, 0));
-        std::vector<float> j(E * 9);
-        for (size_t e = 0; e < E; ++e) {
-            const double* f = m.forms + e * 1505;
-            for (int gp = 0; gp < 8; ++gp) {
-                float r[fs::kShellRec];
-                for (int i = 0; i < 6; ++i)
-                    for (int c = 0; c < 24; ++c) r[i * 24 + c] = (float)f[(gp * 6 + i) * 24 + c];
-                for (int i = 0; i < 6; ++i)
-                    for (int k = 0; k < 7; ++k) r[144 + i * 7 + k] = (float)f[1152 + (gp * 6 + i) * 7 + k];
-                r[186] = (float)f[1488 + gp];
-                r[187] = 0.0f;
-                const size_t base = (e / 4) * fs::kShellRec4 * 32 + (e % 4) * 8 + gp;
-                for (int k = 0; k < fs::kShellRec4; ++k)
-                    rec[base + (size_t)k * 32] = make_float4(r[4 * k], r[4 * k + 1], r[4 * k + 2], r[4 * k + 3]);
-            }
-            for (int k = 0; k < 9; ++k) j[e * 9 + k] = (float)f[1496 + k];
-        }
-        cudaMemcpy(forms, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice);
-        cudaMemcpy(j0, j.data(), j.size() * sizeof(float), cudaMemcpyHostToDevice);
-    }
+    // The element rows (J0^-1, the enhanced modes' scales), and the lumped mass unless
+    // the caller gives it, formed here from the rest positions: the step forms B and G
+    // from them itself.  Forms handed over by the caller (zone_gpu.cpp:668-684 narrows
+    // them for its shaders) must be the solid-shell forms of the same rest positions:
+    // every element's Gauss weights, and the whole forms of the first elements, are
+    // checked against the device's own FP64 forms.
     double* corner_mass = nullptr;
-    if (A.ok() && (!m.forms || !m.mass)) {
+    double* weights = nullptr;
+    if (A.ok()) {
         corner_mass = m.mass ? nullptr : A.zeros<double>(E * 8);
+        if (m.forms && cudaMalloc(&weights, E * 8 * sizeof(double)) != cudaSuccess) {
+            femstep_shell_destroy(s);
+            return fail(nullptr, FEMSTEP_ENOMEM, "device allocation failed");
+        }
         fs::ShellSetupArgs a{};
         a.elements = (long long)E;
         a.groups = s->groups;
@@ -345,13 +382,15 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
         a.slot = d.slot;
         a.formulation = 2;
         a.density = m.density;
-        a.forms = m.forms ? nullptr : forms;
-        a.j0inv = m.forms ? nullptr : j0;
+        a.elem = elem;
         a.corner_mass = corner_mass;
+        a.gauss_volume = weights;
         fs::launch_shell_setup(a, s->stream);
         if (corner_mass) fs::launch_shell_mass((long long)N, d.offset, corner_mass, nullptr, mass, inv_mass, s->stream);
         cudaStreamSynchronize(s->stream);
         rc = check(s, cudaGetLastError(), "rest forms");
+        if (!rc && m.forms) rc = check_caller_forms(s, m.forms, weights);
+        if (weights) cudaFree(weights);
         if (rc) {
             femstep_shell_destroy(s);
             return rc;

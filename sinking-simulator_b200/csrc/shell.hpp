@@ -5,13 +5,13 @@
 // CSR gather and node update (engine/sim/zone.cpp:928-989, 1094-1121, 1200-1202).
 //
 // Work mapping: one element = 8 lanes of a warp, lane g owning Gauss point g, so a
-// warp holds 4 elements.  The per-Gauss-point forms record (B 6x24, G 6x7, w) is
-// stored lane-interleaved in "warp groups" of 4 elements, so every load a warp issues
-// is one contiguous 512-byte run of float4s:
+// warp holds 4 elements.  Each lane forms its point's strain-displacement and
+// enhanced-strain operators in FP32 from the element's rest corners every step
+// (shell_geom.cuh), so per element only a 64-byte row of rest data is stored:
 //
-//   forms   float4 [groups][kRec4][32]     kRec4 = 47 float4 = 188 floats per lane:
-//                                          B[6][24] (144) | G[6][7] (42) | w (1) | pad
-//   j0inv   float  [E][9]                  rest Jacobian inverse at the centre (row-major)
+//   elem    float4 [E][4]                  J0^-1 at the centre (row-major, 9) and the
+//                                          enhanced modes' scales det J0 n_j (7); all
+//                                          zero for an element without valid forms
 //   state   float  [groups][14][32]        per lane: plastic strain (6), eq. plastic
 //                                          strain, and their Kahan compensations (7)
 //   alpha   float  [E][8]                  the seven enhanced parameters (+ pad)
@@ -30,8 +30,7 @@
 
 namespace fs {
 
-constexpr int kShellRec = 188;       // floats per lane record
-constexpr int kShellRec4 = kShellRec / 4;
+constexpr int kShellElemQ = 4;       // float4 per element row: J0^-1 (9), enhanced-mode scales (7)
 constexpr int kShellStateQ = 14;     // floats of state per lane
 constexpr int kShellState2Q = 8;     // back stress (6), damage, failed: the general point law
 constexpr int kShellLanesPerElement = 8;
@@ -39,8 +38,7 @@ constexpr int kShellElementsPerWarp = 4;
 
 struct ShellDevice {
     long long nodes = 0, elements = 0, groups = 0;
-    const float4* forms = nullptr;
-    const float* j0inv = nullptr;
+    const float4* elem = nullptr;  // [E][kShellElemQ]
     float* state = nullptr;
     float* alpha = nullptr;
     const uint32_t* index = nullptr;
@@ -151,11 +149,11 @@ void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t 
 void launch_shell_elastic_factor(const ShellDevice& d, double youngs, double poisson, float* out,
                                  cudaStream_t stream);
 
-// Rest forms in FP64 on the device (solid_shell.cpp:237-375), one thread per
-// element: writes the FP32 lane records and J0^-1, and in double the lumped corner
-// masses (into CSR slots), the Gauss volumes and, if dt_out is non-null, the
-// element's critical step (solid_shell.cpp:1088-1133).  forms64 (optional, 1507
-// doubles per element) receives the double forms for testing.
+// Rest forms in FP64 on the device (solid_shell.cpp:237-375).  The solver's set-up
+// (eight lanes per element) writes the element rows and, in double, the lumped corner
+// masses (into CSR slots) and the Gauss volumes; the per-element form (one thread per
+// element) writes the double forms (forms64, 1507 doubles per element), the masses
+// and, if dt_out is non-null, the element's critical step (solid_shell.cpp:1088-1133).
 struct ShellSetupArgs {
     long long elements, groups;
     const double* rest;        // 3N
@@ -163,8 +161,7 @@ struct ShellSetupArgs {
     const uint32_t* slot;      // 8E
     int formulation;           // 0 displacement, 1 ANS, 2 solid-shell
     double density, youngs, poisson, safety;
-    float4* forms;             // device layout (may be null)
-    float* j0inv;              // [E][9] (may be null)
+    float4* elem;              // [E][kShellElemQ] element rows (may be null)
     double* corner_mass;       // CSR slots (may be null)
     double* gauss_volume;      // [E][8] (may be null)
     double* dt_out;            // [E] (may be null)

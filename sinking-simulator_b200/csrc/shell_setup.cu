@@ -387,25 +387,6 @@ __global__ void __launch_bounds__(64) shell_setup_kernel(ShellSetupArgs a, doubl
         o[1505] = f.eas;
         o[1506] = f.ok;
     }
-    if (a.forms) {
-        // lane record of Gauss point gp of element e: group e/4, lane (e%4)*8 + gp
-        const long long group = e / 4;
-        const int base_lane = (int)(e % 4) * 8;
-        for (int gp = 0; gp < 8; ++gp) {
-            float rec[kShellRec];
-            for (int i = 0; i < 6; ++i)
-                for (int j = 0; j < 24; ++j) rec[i * 24 + j] = f.ok ? (float)f.b[gp][i][j] : 0.0f;
-            for (int i = 0; i < 6; ++i)
-                for (int j = 0; j < 7; ++j) rec[144 + i * 7 + j] = f.ok ? (float)f.g[gp][i][j] : 0.0f;
-            rec[186] = f.ok ? (float)f.w[gp] : 0.0f;
-            rec[187] = 0.0f;
-            float4* dst = a.forms + (size_t)group * kShellRec4 * 32 + base_lane + gp;
-            for (int k = 0; k < kShellRec4; ++k)
-                dst[(size_t)k * 32] = make_float4(rec[4 * k], rec[4 * k + 1], rec[4 * k + 2], rec[4 * k + 3]);
-        }
-    }
-    if (a.j0inv)
-        for (int k = 0; k < 9; ++k) a.j0inv[e * 9 + k] = f.ok ? (float)f.j0[k] : 0.0f;
     if (a.gauss_volume || a.corner_mass || a.dt_out) {
         // gaussVolumes / elementMass (solid_shell.cpp:655-673) run computeForms with
         // the displacement formulation; its weights det J are the ones above (the
@@ -441,13 +422,13 @@ __global__ void __launch_bounds__(64) shell_setup_kernel(ShellSetupArgs a, doubl
     }
 }
 
-// The same forms, lumped corner masses and Gauss volumes with 8 lanes per element
-// (lane = Gauss point), for the solver's set-up: each lane runs compute_forms's
-// operations for its own point in the same order, and the element-wide steps combine
-// the lanes' values in the reference's point order through shuffles -- the EAS column
-// norms (sum over points, then rows), the lumped mass (sum over points), and the
-// element's validity (every point's det J > 0).  Each lane writes its own lane record,
-// so the stores are whole 512-byte runs.  Bit-identical to shell_setup_kernel.
+// The solver's set-up with 8 lanes per element (lane = Gauss point): the element row
+// (J0^-1 and the enhanced modes' scales det J0 n_j), the lumped corner masses and the
+// Gauss volumes.  Each lane runs compute_forms's operations for its own point in the
+// same order, and the element-wide steps combine the lanes' values in the reference's
+// point order through shuffles -- the EAS column norms (sum over points, then rows),
+// the lumped mass (sum over points), and the element's validity (every point's
+// det J > 0).  Bit-identical to shell_setup_kernel's values.
 __global__ void __launch_bounds__(128) shell_setup_lanes(ShellSetupArgs a) {
     const int lane = threadIdx.x & 31, gp = lane & 7;
     const long long e_raw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
@@ -459,7 +440,7 @@ __global__ void __launch_bounds__(128) shell_setup_lanes(ShellSetupArgs a) {
         const uint32_t id = a.index[e * 8 + n];
         for (int i = 0; i < 3; ++i) nodes[n * 3 + i] = a.rest[(size_t)id * 3 + i];
     }
-    const bool ans = a.formulation >= 1, eas = a.formulation >= 2;
+    const bool eas = a.formulation >= 2;
     Point centre;
     evaluate(nodes, 0.0, 0.0, 0.0, centre);
     double a0[3][3];
@@ -468,51 +449,14 @@ __global__ void __launch_bounds__(128) shell_setup_lanes(ShellSetupArgs a) {
     const double xi = (gp & 1) ? q : -q;
     const double eta = (gp & 2) ? q : -q;
     const double zta = (gp & 4) ? q : -q;
-    const int level = (gp & 4) ? 1 : 0;
     Point p;
     evaluate(nodes, xi, eta, zta, p);
     double am[3][3];
     const double det = inv3(p.jac, am);
     // computeForms gives up on the element at the first point with det J <= 0
     const bool ok = (__ballot_sync(0xffffffffu, det0 > 0.0 && det > 0.0) & group_mask) == group_mask;
-    double bn[6][24];
-    for (int r = 0; r < 6; ++r) natural_b_row(p, r, bn[r]);
-    if (ans) {
-        // the assumed strains of this point's level: transverse shear from the edge
-        // midpoints, thickness strain from the corners (solid_shell.cpp:276-334)
-        const double wa = 0.5 * (1.0 - xi), wc = 0.5 * (1.0 + xi);
-        const double wb = 0.5 * (1.0 - eta), wd = 0.5 * (1.0 + eta);
-        double s0[24], s1[24];
-        Point t;
-        evaluate(nodes, kShearSample[0][0], kShearSample[0][1], zta, t);
-        natural_b_row(t, 4, s0);
-        evaluate(nodes, kShearSample[1][0], kShearSample[1][1], zta, t);
-        natural_b_row(t, 4, s1);
-        for (int c = 0; c < 24; ++c) bn[4][c] = wa * s0[c] + wc * s1[c];
-        evaluate(nodes, kShearSample[2][0], kShearSample[2][1], zta, t);
-        natural_b_row(t, 5, s0);
-        evaluate(nodes, kShearSample[3][0], kShearSample[3][1], zta, t);
-        natural_b_row(t, 5, s1);
-        for (int c = 0; c < 24; ++c) bn[5][c] = wb * s0[c] + wd * s1[c];
-        for (int c = 0; c < 24; ++c) bn[2][c] = 0.0;
-        for (int sc = 0; sc < 4; ++sc) {
-            evaluate(nodes, kCornerSample[sc][0], kCornerSample[sc][1], zta, t);
-            natural_b_row(t, 2, s0);
-            const double w = 0.25 * (1.0 + xi * kCornerSample[sc][0]) * (1.0 + eta * kCornerSample[sc][1]);
-            for (int c = 0; c < 24; ++c) bn[2][c] += w * s0[c];
-        }
-    }
-    (void)level;
-    double tm[6][6];
-    voigt_transform(am, tm);
-    float rec[kShellRec];
-    for (int i = 0; i < 6; ++i)
-        for (int c = 0; c < 24; ++c) {
-            double sum = 0.0;
-            for (int k = 0; k < 6; ++k) sum += tm[i][k] * bn[k][c];
-            rec[i * 24 + c] = ok ? (float)sum : 0.0f;
-        }
-    // G: enhancedM mapped by the centre transform and scaled by det J0 / det J
+    // G: enhancedM mapped by the centre transform and scaled by det J0 / det J, for the
+    // modes' norms; the step re-forms G from J0^-1 and the scale det J0 / norm_j
     double g[6][7];
     {
         double t0[6][6];
@@ -535,6 +479,7 @@ __global__ void __launch_bounds__(128) shell_setup_lanes(ShellSetupArgs a) {
                 g[i][j] = eas ? scale * sum : 0.0;
             }
     }
+    double mine = 0.0;  // this lane's mode (gp < 7): det J0 / norm, or det J0 for an unused mode
     if (eas)
         for (int j = 0; j < 7; ++j) {
             // sum over points, then rows, in the reference's order, in every lane alike
@@ -544,14 +489,9 @@ __global__ void __launch_bounds__(128) shell_setup_lanes(ShellSetupArgs a) {
                     const double term = __shfl_sync(0xffffffffu, det * g[i][j] * g[i][j], (lane & 24) + src);
                     norm += term;
                 }
-            if (!(norm > 0.0)) continue;
-            const double inverse = 1.0 / sqrt(norm);
-            for (int i = 0; i < 6; ++i) g[i][j] *= inverse;
+            const double inverse = norm > 0.0 ? 1.0 / sqrt(norm) : 1.0;  // an unused mode stays as it is
+            if (j == gp) mine = det0 * inverse;
         }
-    for (int i = 0; i < 6; ++i)
-        for (int j = 0; j < 7; ++j) rec[144 + i * 7 + j] = ok ? (float)g[i][j] : 0.0f;
-    rec[186] = ok ? (float)det : 0.0f;
-    rec[187] = 0.0f;
     // lumped corner mass (elementMass, solid_shell.cpp:655-663): lane n sums node n over
     // the points in order
     double mass = 0.0;
@@ -562,14 +502,11 @@ __global__ void __launch_bounds__(128) shell_setup_lanes(ShellSetupArgs a) {
         mass += a.density * w * shape;
     }
     if (!valid) return;
-    if (a.forms) {
-        float4* dst = a.forms + (size_t)(e / 4) * kShellRec4 * 32 + lane;
-        for (int k = 0; k < kShellRec4; ++k)
-            dst[(size_t)k * 32] = make_float4(rec[4 * k], rec[4 * k + 1], rec[4 * k + 2], rec[4 * k + 3]);
-    }
-    if (a.j0inv) {
-        a.j0inv[e * 9 + gp] = ok ? (float)a0[gp / 3][gp % 3] : 0.0f;
-        if (gp == 0) a.j0inv[e * 9 + 8] = ok ? (float)a0[2][2] : 0.0f;
+    if (a.elem) {
+        float* row = reinterpret_cast<float*>(a.elem + e * kShellElemQ);
+        row[gp] = ok ? (float)a0[gp / 3][gp % 3] : 0.0f;
+        if (gp == 0) row[8] = ok ? (float)a0[2][2] : 0.0f;
+        if (gp < 7) row[9 + gp] = ok ? (float)mine : 0.0f;
     }
     if (a.gauss_volume) a.gauss_volume[e * 8 + gp] = ok ? det : 0.0;
     if (a.corner_mass) a.corner_mass[a.slot[e * 8 + gp]] = ok ? mass : 0.0;
@@ -590,9 +527,7 @@ __global__ void shell_mass_kernel(long long nodes, const uint32_t* offset, const
 
 void launch_shell_setup(const ShellSetupArgs& a, cudaStream_t stream) {
     if (!a.dt_out && !a.forms64 && !a.ok) {
-        // the solver's set-up: forms, J0^-1, masses, Gauss volumes, 8 lanes per element
-        // (the record layout needs whole groups of 4 elements per warp: the grid starts
-        // at element 0)
+        // the solver's set-up: element rows, masses, Gauss volumes, 8 lanes per element
         shell_setup_lanes<<<blocks_for(a.elements * 8, 128), 128, 0, stream>>>(a);
         return;
     }
@@ -607,12 +542,10 @@ void launch_shell_setup(const ShellSetupArgs& a, cudaStream_t stream) {
         c.elements = n;
         c.index = a.index + first * 8;
         c.slot = a.slot + first * 8;
-        if (a.forms) c.forms = a.forms + (size_t)(first / 4) * kShellRec4 * 32;
         if (a.gauss_volume) c.gauss_volume = a.gauss_volume + first * 8;
         if (a.dt_out) c.dt_out = a.dt_out + first;
         if (a.forms64) c.forms64 = a.forms64 + first * 1507;
         if (a.ok) c.ok = a.ok + first;
-        if (a.j0inv) c.j0inv = a.j0inv + first * 9;
         shell_setup_kernel<<<blocks_for(n, 64), 64, 0, stream>>>(c, scratch);
     }
     if (scratch) cudaFreeAsync(scratch, stream);

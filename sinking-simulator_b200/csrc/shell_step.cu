@@ -25,6 +25,7 @@
 // FP64 only for the per-block energy partials.
 #include "common.cuh"
 #include "shell.hpp"
+#include "shell_geom.cuh"
 
 namespace fs {
 namespace {
@@ -41,6 +42,27 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     const float t = sum + y;
     comp = (t - sum) - y;
     sum = t;
+}
+
+// Element e's rest corners for the element operators: the bottom corners relative to
+// corner 0 and the directors D_c = X_{c+4} - X_c, each difference taken in double and
+// rounded once.  Plain loads: after the step's stores they are read again, not kept.
+__device__ __forceinline__ void shell_rest_corners(const ShellDevice& d, long long e, float Xb[4][3], float D[4][3]) {
+    const uint4 i0 = reinterpret_cast<const uint4*>(d.index)[e * 2];
+    const uint4 i1 = reinterpret_cast<const uint4*>(d.index)[e * 2 + 1];
+    const unsigned nid[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+    const double X0 = d.rest[(size_t)nid[0] * 3], Y0 = d.rest[(size_t)nid[0] * 3 + 1], Z0 = d.rest[(size_t)nid[0] * 3 + 2];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const size_t ob = (size_t)nid[c] * 3, ot = (size_t)nid[c + 4] * 3;
+        const double bx = d.rest[ob], by = d.rest[ob + 1], bz = d.rest[ob + 2];
+        Xb[c][0] = (float)(bx - X0);
+        Xb[c][1] = (float)(by - Y0);
+        Xb[c][2] = (float)(bz - Z0);
+        D[c][0] = (float)(d.rest[ot] - bx);
+        D[c][1] = (float)(d.rest[ot + 1] - by);
+        D[c][2] = (float)(d.rest[ot + 2] - bz);
+    }
 }
 
 // 3x3 row-major inverse with the reference's singular guard
@@ -299,16 +321,11 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
     const long long e = valid ? e_raw : d.elements - 1;
     const long long group = group_raw < d.groups ? group_raw : d.groups - 1;
     {
-        // This warp's own group record (24 KB of forms) and state into L2 now, with one
-        // bulk prefetch each, and the small per-element rows with a line each.  The loads
-        // of them come after a dependent chain (node ids, node rows, the rotation) that
-        // the registers cannot run ahead of; prefetched, they hit L2 instead of DRAM.
-        // Measured on the 2 M-element panel: 4.24 -> 3.73 ms per element pass.
-        const void* rec = d.forms + (size_t)group * kShellRec4 * 32;
+        // This warp's plastic state into L2 now, with one bulk prefetch, and the small
+        // per-element rows with a line each.  The loads of them come after a dependent
+        // chain (node ids, node rows, the rotation) that the registers cannot run ahead
+        // of; prefetched, they hit L2 instead of DRAM.
         const void* st = d.state + (size_t)group * kShellStateQ * 32;
-        if (lane == 0)
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rec), "r"((unsigned)(kShellRec4 * 32 * 16))
-                         : "memory");
         if (lane == 1)
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(st), "r"((unsigned)(kShellStateQ * 32 * 4))
                          : "memory");
@@ -316,10 +333,10 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         if (lane == 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.index + e0 * 8));
         if (lane == 3) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.slot + e0 * 8));
         if (lane == 4) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.alpha + e0 * 8));
-        if (lane == 5) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.j0inv + e0 * 9));
+        if (lane == 5) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.elem + e0 * kShellElemQ));
         if (lane == 6) {
-            const long long last = d.elements * 9 - 1, at = e0 * 9 + 32;
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(d.j0inv + (at < last ? at : last)));
+            const long long last = d.elements * kShellElemQ - 1, at = e0 * kShellElemQ + 8;
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(d.elem + (at < last ? at : last)));
         }
     }
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -332,18 +349,33 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
     const uint4 i0 = reinterpret_cast<const uint4*>(d.index)[e * 2];
     const uint4 i1 = reinterpret_cast<const uint4*>(d.index)[e * 2 + 1];
     const unsigned nid[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
-    float dX[8][3], dd[8][3];
+    // rest geometry: every corner relative to corner 0 (for the rotation), the bottom
+    // corners and the directors D_c = X_{c+4} - X_c (for the element operators), each
+    // difference taken in double and rounded once
+    float dX[8][3], dd[8][3], D[4][3];
     {
         const double X0 = d.rest[(size_t)nid[0] * 3], Y0 = d.rest[(size_t)nid[0] * 3 + 1],
                      Z0 = d.rest[(size_t)nid[0] * 3 + 2];
         const float u0 = d.disp[(size_t)nid[0] * 3], v0 = d.disp[(size_t)nid[0] * 3 + 1],
                     w0 = d.disp[(size_t)nid[0] * 3 + 2];
 #pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const size_t ob = (size_t)nid[c] * 3, ot = (size_t)nid[c + 4] * 3;
+            const double bx = d.rest[ob], by = d.rest[ob + 1], bz = d.rest[ob + 2];
+            const double tx = d.rest[ot], ty = d.rest[ot + 1], tz = d.rest[ot + 2];
+            dX[c][0] = (float)(bx - X0);
+            dX[c][1] = (float)(by - Y0);
+            dX[c][2] = (float)(bz - Z0);
+            dX[c + 4][0] = (float)(tx - X0);
+            dX[c + 4][1] = (float)(ty - Y0);
+            dX[c + 4][2] = (float)(tz - Z0);
+            D[c][0] = (float)(tx - bx);
+            D[c][1] = (float)(ty - by);
+            D[c][2] = (float)(tz - bz);
+        }
+#pragma unroll
         for (int a = 0; a < 8; ++a) {
             const size_t o = (size_t)nid[a] * 3;
-            dX[a][0] = (float)(d.rest[o] - X0);
-            dX[a][1] = (float)(d.rest[o + 1] - Y0);
-            dX[a][2] = (float)(d.rest[o + 2] - Z0);
             dd[a][0] = d.disp[o] - u0;
             dd[a][1] = d.disp[o + 1] - v0;
             dd[a][2] = d.disp[o + 2] - w0;
@@ -363,6 +395,20 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             }
         }
     }
+    // ---- the element row: J0^-1 and the enhanced-mode scales (all zero: no valid forms) ----
+    float j0[9], cm[7];
+    {
+        const float4* row = d.elem + e * kShellElemQ;
+        const float4 r0 = __ldg(row), r1 = __ldg(row + 1), r2 = __ldg(row + 2), r3 = __ldg(row + 3);
+        const float v[16] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+#pragma unroll
+        for (int k = 0; k < 9; ++k) j0[k] = v[k];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) cm[k] = v[9 + k];
+    }
+    bool formed = false;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) formed = formed || j0[k] != 0.0f;
     // ---- rotation: H = (sum_a dN_a(0) (x) dd_a) J0^-1, R = I + Q ----
     float q[9];
     {
@@ -382,9 +428,6 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             jd[i * 3 + 1] = 0.125f * a1;
             jd[i * 3 + 2] = 0.125f * a2;
         }
-        float j0[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) j0[k] = d.j0inv[e * 9 + k];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -432,33 +475,16 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             u[a * 3 + i] = dd[a][i] + (q[0 * 3 + i] * s + q[1 * 3 + i] * t + q[2 * 3 + i] * w);
         }
 
-    // ---- the lane's forms record ----
-    const float4* rec = d.forms + (size_t)group * kShellRec4 * 32 + lane;
+    // ---- the point's operators, formed from the rest geometry ----
+    const ShellLanePoint P = shell_lane_point(gp);
+    float gx[3], gy[3], Ainv[9], w;
+    shell_frame(dX, D, P, formed, gx, gy, Ainv, w);
     float eps_u[6];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        float s = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float4 b = __ldg(rec + (size_t)(i * 6 + k) * 32);
-            s += b.x * u[k * 4] + b.y * u[k * 4 + 1] + b.z * u[k * 4 + 2] + b.w * u[k * 4 + 3];
-        }
-        eps_u[i] = s;
-    }
-    float G[42];
-    float w;
-    {
-        const float4* gr = rec + (size_t)36 * 32;
-#pragma unroll
-        for (int k = 0; k < 11; ++k) {
-            const float4 v = __ldg(gr + (size_t)k * 32);
-            if (4 * k < 42) G[4 * k] = v.x;
-            if (4 * k + 1 < 42) G[4 * k + 1] = v.y;
-            if (4 * k + 2 < 42) G[4 * k + 2] = v.z;
-            if (4 * k + 3 < 42) G[4 * k + 3] = v.w;
-            if (k == 10) w = v.z;
-        }
-    }
+    shell_strain(dX, D, u, P, gx, gy, Ainv, eps_u);
+    // G factored: column j = gc_j T0[:, k_j], k = (0, 1, 2, 2, 2, 3, 3)
+    float T[24], gc[7];
+    shell_t0(j0, T);
+    shell_enhanced_scales(cm, w, P, gc);
     // element volume and the energy scale sigma_y V
     const float volume = sum8(w);
     const float scale = p.yield * volume;
@@ -496,24 +522,25 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
 #pragma unroll 1
     for (int iteration = 0;; ++iteration) {
         float eps[6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) {
-            float s = eps_u[i];
-#pragma unroll
-            for (int k = 0; k < 7; ++k) s += G[i * 7 + k] * alpha[k];
-            eps[i] = s;
-        }
+        shell_enhanced_apply(T, gc, alpha, eps_u, eps);
         if (GENERAL)
             point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
         else
             point_law(eps, ps, p, o);
+        // r_j = sum_g w gc_j (T0[:, k_j] . sigma)
         float r[7];
+        {
+            float tau[4];
 #pragma unroll
-        for (int k = 0; k < 7; ++k) {
-            float s = 0.0f;
+            for (int k = 0; k < 4; ++k) {
+                float s = 0.0f;
 #pragma unroll
-            for (int i = 0; i < 6; ++i) s += G[i * 7 + k] * o.sigma[i];
-            r[k] = sum8(w * s);
+                for (int i = 0; i < 6; ++i) s += T[k * 6 + i] * o.sigma[i];
+                tau[k] = w * s;
+            }
+            const int kj[7] = {0, 1, 2, 2, 2, 3, 3};
+#pragma unroll
+            for (int j = 0; j < 7; ++j) r[j] = sum8(gc[j] * tau[kj[j]]);
         }
         if (!done && !eas_on) {  // no enhanced modes: one evaluation is the update
             converged = true;
@@ -540,22 +567,30 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         float l[28];
         bool spd = true;
         if (__any_sync(0xffffffffu, !elastic_element)) {
-        // K_aa = sum_g w_g G^T C G, lower triangle, one column of C G at a time (six
-        // live values rather than 42: the same products in the same order)
+        // K_aa = sum_g w_g G^T C G, lower triangle: with G factored, the point's part is
+        // gc_a gc_b H[k_a][k_b], H = T0c^T C T0c over T0's four columns (four tangent
+        // applications rather than seven)
         float kaa[28];
+        {
+            float H[10];
 #pragma unroll
-        for (int b = 0; b < 7; ++b) {
-            float g[6], cgb[6];
+            for (int kb = 0; kb < 4; ++kb) {
+                float cg[6];
+                tangent_apply(o, p, &T[kb * 6], cg);
 #pragma unroll
-            for (int i = 0; i < 6; ++i) g[i] = G[i * 7 + b];
-            tangent_apply(o, p, g, cgb);
+                for (int ka = kb; ka < 4; ++ka) {
+                    float s = 0.0f;
 #pragma unroll
-            for (int a = b; a < 7; ++a) {
-                float s = 0.0f;
-#pragma unroll
-                for (int i = 0; i < 6; ++i) s += G[i * 7 + a] * cgb[i];
-                kaa[a * (a + 1) / 2 + b] = sum8(w * s);
+                    for (int i = 0; i < 6; ++i) s += T[ka * 6 + i] * cg[i];
+                    H[ka * (ka + 1) / 2 + kb] = w * s;
+                }
             }
+            const int kj[7] = {0, 1, 2, 2, 2, 3, 3};
+#pragma unroll
+            for (int b = 0; b < 7; ++b)
+#pragma unroll
+                for (int a = b; a < 7; ++a)
+                    kaa[a * (a + 1) / 2 + b] = sum8(gc[a] * gc[b] * H[kj[a] * (kj[a] + 1) / 2 + kj[b]]);
         }
         // Cholesky (solid_shell.cpp:432-457), identical in every lane
         {
@@ -638,13 +673,7 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
                 for (int k = 0; k < 7; ++k) alpha[k] = 0.0f;
             }
             float eps[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-                float s = eps_u[i];
-#pragma unroll
-                for (int k = 0; k < 7; ++k) s += G[i * 7 + k] * alpha[k];
-                eps[i] = s;
-            }
+            shell_enhanced_apply(T, gc, alpha, eps_u, eps);
             point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
         }
     }
@@ -694,23 +723,16 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
     }
 
     // ---- f = -R sum_g w_g B_g^T sigma_g, reduce-scattered so lane a holds node a ----
+    // (the rest corners and the point's frame formed again: cheaper than holding them
+    // in registers through the Newton iterations)
     float f[24];
+#pragma unroll
+    for (int j = 0; j < 24; ++j) f[j] = 0.0f;
     {
-        float ws[6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) ws[i] = w * o.sigma[i];
-#pragma unroll
-        for (int j = 0; j < 24; ++j) f[j] = 0.0f;
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                const float4 b = __ldg(rec + (size_t)(i * 6 + k) * 32);
-                f[k * 4] += b.x * ws[i];
-                f[k * 4 + 1] += b.y * ws[i];
-                f[k * 4 + 2] += b.z * ws[i];
-                f[k * 4 + 3] += b.w * ws[i];
-            }
+        float Xb[4][3], Dr[4][3], fx[3], fy[3], Af[9], wf;
+        shell_rest_corners(d, e, Xb, Dr);
+        shell_frame(Xb, Dr, P, formed, fx, fy, Af, wf);
+        shell_force(Xb, Dr, P, fx, fy, Af, wf, o.sigma, f);
     }
     // round 1 (xor 4): keep nodes 0-3 (bit 2 clear) or 4-7
     const bool hi4 = (gp & 4) != 0, hi2 = (gp & 2) != 0, hi1 = (gp & 1) != 0;
@@ -1073,28 +1095,35 @@ __global__ void __launch_bounds__(kShellPunchBlock) shell_punch(ShellDevice d, S
     }
 }
 
-// The elastic K_aa = sum_g w_g G_g^T C G_g of every element, from the FP32 forms the
-// step uses, accumulated in double, and its Cholesky factor (packed lower triangle,
-// 28 of 32 floats per element, each diagonal entry stored as its reciprocal, as the
-// step's own factorisation keeps it).  A zero first entry marks an element whose
-// elastic K_aa is not positive definite; the step then forms K_aa itself.
+// The elastic K_aa = sum_g w_g G_g^T C G_g of every element, from the FP32 G and
+// weights the step forms (shell_geom.cuh), accumulated in double, and its Cholesky
+// factor (packed lower triangle, 28 of 32 floats per element, each diagonal entry
+// stored as its reciprocal, as the step's own factorisation keeps it).  A zero first
+// entry marks an element whose elastic K_aa is not positive definite; the step then
+// forms K_aa itself.
 __global__ void shell_elastic_factor(ShellDevice d, double lambda, double mu, float* out) {
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= d.elements) return;
-    const float4* base = d.forms + (size_t)(e / 4) * kShellRec4 * 32 + (e % 4) * 8;
+    float Xb[4][3], D[4][3], a0[9], cm[7];
+    shell_rest_corners(d, e, Xb, D);
+    {
+        const float* row = reinterpret_cast<const float*>(d.elem + e * kShellElemQ);
+        for (int k = 0; k < 9; ++k) a0[k] = row[k];
+        for (int k = 0; k < 7; ++k) cm[k] = row[9 + k];
+    }
+    bool formed = false;
+    for (int k = 0; k < 9; ++k) formed = formed || a0[k] != 0.0f;
+    float T[24];
+    shell_t0(a0, T);
     double kaa[7][7];
     for (int a = 0; a < 7; ++a)
         for (int b = 0; b < 7; ++b) kaa[a][b] = 0.0;
     for (int gp = 0; gp < 8; ++gp) {
-        float g[44];
-        for (int k = 0; k < 11; ++k) {
-            const float4 v = base[(size_t)(36 + k) * 32 + gp];
-            g[4 * k] = v.x;
-            g[4 * k + 1] = v.y;
-            g[4 * k + 2] = v.z;
-            g[4 * k + 3] = v.w;
-        }
-        const double w = g[42];
+        const ShellLanePoint P = shell_lane_point(gp);
+        float gx[3], gy[3], A[9], wf, g[42];
+        shell_frame(Xb, D, P, formed, gx, gy, A, wf);
+        shell_enhanced(T, cm, wf, P, g);
+        const double w = wf;
         for (int b = 0; b < 7; ++b) {
             double col[6], cg[6];
             for (int i = 0; i < 6; ++i) col[i] = g[i * 7 + b];
