@@ -124,10 +124,11 @@ def shell_bytes(E, N):
 
 
 # FP32 operations per solid-shell element update, counted by ncu on the shell-sample
-# workload (SASS thread instructions: 2 x FFMA + FADD + FMUL, 13,263 per element; the
-# 449 FP64 operations of the energy account are left out).  The second roofline of the
-# shell element, against the FP32 SIMT peak: SMs x 128 lanes x 2 x the SM clock.
-SHELL_FP32_FLOP_PER_ELEMENT = 13263
+# workload (SASS thread instructions: 2 x FFMA + FADD + FMUL, 17,667 per element with B
+# and G formed in the kernel; the 665 FP64 operations -- rest-corner differences and
+# the energy account -- are left out).  The second roofline of the shell element,
+# against the FP32 SIMT peak: SMs x 128 lanes x 2 x the SM clock.
+SHELL_FP32_FLOP_PER_ELEMENT = 17667
 
 
 def simt_roofline(flop_per_unit, units, kernel_ms, max_mhz):
@@ -749,13 +750,18 @@ def main():
     if not args.no_e2e:
         t0 = time.perf_counter()
         e = w.make()
+        t1 = time.perf_counter()
         e.run(args.steps, **w.kw)
+        t2 = time.perf_counter()
         p_host, v_host = w.readback(e)
+        t3 = time.perf_counter()
         e.close()
-        wall = time.perf_counter() - t0
+        t4 = time.perf_counter()
+        wall = t4 - t0
         e2e = {"value": w.units * args.steps / wall, "unit": UNIT,
                "h2d_bytes_per_step": w.h2d_bytes() / args.steps,
                "d2h_bytes_per_step": (p_host.nbytes + v_host.nbytes) / args.steps,
+               "phases": {"create_s": t1 - t0, "steps_s": t2 - t1, "readback_s": t3 - t2, "destroy_s": t4 - t3},
                "note": "upload + K steps + readback through the C ABI, wall clock"}
 
     if rank == 0:

@@ -297,12 +297,13 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
     for (int i = 3; i < 6; ++i) out[i] = 0.5f * a * g[i] - b * o.n[i];
 }
 
-// Blocks per SM the register budget is sized for.  On the 2 M-element panel: 3 (168
-// registers, 12 warps per SM, no spill) 4.61 ms per step and 1.32x faster than 2 (177
-// registers, 8 warps); 4 (128, 16 warps, ~140 bytes of spill to L1) 4.43 ms; 5 (102,
-// 20 warps, ~400 bytes of spill) 4.60 ms.
+// Blocks per SM the register budget is sized for.  With the operators formed in the
+// kernel the element pass is issue- and latency-bound, and more warps win over fewer
+// spills.  Element pass on the 2 M-element panel: 4 blocks (128 registers, 16 warps per
+// SM, ~30 bytes of spill) 2.49 ms; 5 (102 registers, 20 warps, ~310 bytes of spill to
+// L1) 2.34 ms; 6 (85 registers, ~650 bytes) 2.74 ms.
 #ifndef FEMSTEP_SHELL_MINB
-#define FEMSTEP_SHELL_MINB 4
+#define FEMSTEP_SHELL_MINB 5
 #endif
 
 // GENERAL: the general point law and the element failure rules (ShellParams::general);
@@ -475,6 +476,11 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
             u[a * 3 + i] = dd[a][i] + (q[0 * 3 + i] * s + q[1 * 3 + i] * t + q[2 * 3 + i] * w);
         }
 
+    // the rotation waits in shared memory through the Newton iterations (each lane its
+    // own copy: no synchronisation), freeing nine registers there
+    __shared__ float q_park[9][kShellBlock];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) q_park[k][threadIdx.x] = q[k];
     // ---- the point's operators, formed from the rest geometry ----
     const ShellLanePoint P = shell_lane_point(gp);
     float gx[3], gy[3], Ainv[9], w;
@@ -758,7 +764,11 @@ __global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(
         // lane gp now holds sum over points of node gp's internal force; apply -R
         float* out = d.slots + (size_t)d.slot[e * 8 + gp] * 3;
 #pragma unroll
-        for (int i = 0; i < 3; ++i) out[i] = -(f[i] + (q[i * 3] * f[0] + q[i * 3 + 1] * f[1] + q[i * 3 + 2] * f[2]));
+        float qr[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) qr[k] = q_park[k][threadIdx.x];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[i] = -(f[i] + (qr[i * 3] * f[0] + qr[i * 3 + 1] * f[1] + qr[i * 3 + 2] * f[2]));
     }
     // per-warp partials in fixed shuffle order: no block barrier, so a warp whose
     // elements converge early does not wait for the slowest warp of its block
