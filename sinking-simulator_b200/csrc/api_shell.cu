@@ -283,6 +283,12 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     d.nodes = (long long)N;
     d.elements = (long long)E;
     d.groups = s->groups;
+    {
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+            d.sms = sms;
+    }
     s->rest.assign(m.rest, m.rest + N * 3);
     d.rest = A.upload(m.rest, N * 3);
     d.index = A.upload(m.index, E * 8);

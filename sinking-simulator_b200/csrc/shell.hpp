@@ -38,6 +38,7 @@ constexpr int kShellElementsPerWarp = 4;
 
 struct ShellDevice {
     long long nodes = 0, elements = 0, groups = 0;
+    int sms = 148;                  // the device's SM count (the element pass's launch form)
     const float4* elem = nullptr;  // [E][kShellElemQ]
     float* state = nullptr;
     float* alpha = nullptr;

@@ -297,19 +297,23 @@ __device__ __forceinline__ void tangent_apply(const PointOut& o, const ShellPara
     for (int i = 3; i < 6; ++i) out[i] = 0.5f * a * g[i] - b * o.n[i];
 }
 
-// Blocks per SM the register budget is sized for.  With the operators formed in the
-// kernel the element pass is issue- and latency-bound, and more warps win over fewer
-// spills.  Element pass on the 2 M-element panel: 4 blocks (128 registers, 16 warps per
-// SM, ~30 bytes of spill) 2.49 ms; 5 (102 registers, 20 warps, ~310 bytes of spill to
-// L1) 2.34 ms; 6 (85 registers, ~650 bytes) 2.74 ms.
-#ifndef FEMSTEP_SHELL_MINB
-#define FEMSTEP_SHELL_MINB 5
-#endif
+// Blocks per SM the register budget is sized for, chosen per launch.  With the
+// operators formed in the kernel the element pass is issue- and latency-bound.  A zone
+// that fills the GPU wants warps to hide latency, more than it minds spills: on the
+// 2 M-element panel 4 blocks (128 registers, 16 warps per SM, ~30 bytes of spill)
+// take 2.49 ms per pass, 5 (96 registers, 20 warps, ~310 bytes of spill to L1)
+// 2.34 ms, 6 (85 registers, ~650 bytes) 2.74 ms.  A zone that fits in one wave is
+// bound by one warp's dependent chain, where every spill reload is latency: on the
+// reference's 2,048-element probe zone 3 blocks (168 registers, no spill) take 18.2 us
+// per step, 4 blocks 19.7 us, 5 blocks 24.0 us.
+constexpr int kShellMinbWide = 5;
+constexpr int kShellMinbNarrow = 3;
+constexpr int kShellWarpsNarrow = kShellMinbNarrow * kShellBlock / 32;  // per SM
 
 // GENERAL: the general point law and the element failure rules (ShellParams::general);
 // otherwise the linear law, whose state is only the plastic strain.
-template <bool KAHAN, bool GENERAL>
-__global__ void __launch_bounds__(kShellBlock, FEMSTEP_SHELL_MINB) shell_forces(ShellDevice d, ShellParams p) {
+template <bool KAHAN, bool GENERAL, int MINB>
+__global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d, ShellParams p) {
     // an inertial punch has stopped: the run is over (every thread reads the same flag)
     if (d.halt && *d.halt) return;
     const int lane = threadIdx.x & 31;
@@ -1180,6 +1184,21 @@ void launch_shell_elastic_factor(const ShellDevice& d, double youngs, double poi
     shell_elastic_factor<<<blocks_for(d.elements, 128), 128, 0, stream>>>(d, lambda, mu, out);
 }
 
+template <int MINB>
+static void launch_forces(const ShellDevice& d, const ShellParams& p, int blocks, cudaStream_t stream) {
+    if (p.compensated) {
+        if (p.general)
+            shell_forces<true, true, MINB><<<blocks, kShellBlock, 0, stream>>>(d, p);
+        else
+            shell_forces<true, false, MINB><<<blocks, kShellBlock, 0, stream>>>(d, p);
+    } else {
+        if (p.general)
+            shell_forces<false, true, MINB><<<blocks, kShellBlock, 0, stream>>>(d, p);
+        else
+            shell_forces<false, false, MINB><<<blocks, kShellBlock, 0, stream>>>(d, p);
+    }
+}
+
 void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t stream, int parts) {
     const int eb = blocks_for(d.groups * 32, kShellBlock);
     const int nb = blocks_for(d.nodes, kShellNodeBlock);
@@ -1190,22 +1209,18 @@ void launch_shell_step(const ShellDevice& d, const ShellParams& p, cudaStream_t 
         else
             shell_fibers<false><<<fb, kShellFiberBlock, 0, stream>>>(d, p);
     }
+    // one wave at the narrow budget: the latency-bound form; else the wide one
+    const bool narrow = d.groups <= (long long)d.sms * kShellWarpsNarrow;
+    if (parts & 1) {
+        if (narrow)
+            launch_forces<kShellMinbNarrow>(d, p, eb, stream);
+        else
+            launch_forces<kShellMinbWide>(d, p, eb, stream);
+    }
     if (p.compensated) {
-        if (parts & 1) {
-            if (p.general)
-                shell_forces<true, true><<<eb, kShellBlock, 0, stream>>>(d, p);
-            else
-                shell_forces<true, false><<<eb, kShellBlock, 0, stream>>>(d, p);
-        }
         if (parts & 2) shell_nodes<true><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
         if ((parts & 2) && p.inertial) shell_punch<true><<<1, kShellPunchBlock, 0, stream>>>(d, p);
     } else {
-        if (parts & 1) {
-            if (p.general)
-                shell_forces<false, true><<<eb, kShellBlock, 0, stream>>>(d, p);
-            else
-                shell_forces<false, false><<<eb, kShellBlock, 0, stream>>>(d, p);
-        }
         if (parts & 2) shell_nodes<false><<<nb, kShellNodeBlock, 0, stream>>>(d, p);
         if ((parts & 2) && p.inertial) shell_punch<false><<<1, kShellPunchBlock, 0, stream>>>(d, p);
     }

@@ -64,6 +64,32 @@ def test_shell_step_against_fp64_oracle(fem, port, compensated, tol):
     assert abs(e[1] - er[1]) < 5e-3 * abs(er[1]) + 1e-12
 
 
+def test_wide_launch_form_against_fp64_oracle(fem, port):
+    """A zone of more warps than one wave at the narrow register budget (7,296 elements,
+    1,824 warp groups against 148 SMs x 12 warps): the element pass takes its wide launch
+    form (five blocks per SM), the one the full-size panel runs.  Against the FP64
+    oracle, yielding, 120 steps."""
+    nx, ny = 96, 76
+    rest, index, pinned, load = fem.stiffened_panel(nx=nx, ny=ny, lx=0.01 * nx, ly=0.01 * ny, thickness=0.004,
+                                                    stiffeners=1, imperfection=2e-4, peak_pressure=2e7, radius=0.1)
+    assert index.size // 8 // 4 > 148 * 12
+    mat = O.material(E=206e9, nu=0.3, yield_=355e6, hardening=1e9)
+    ref = O.ShellModel(port, rest, index, pinned, mat, fext=load)
+    s = fem.ShellSolver(rest, index, pinned=pinned, load=load, density=7850.0)
+    dt = s.critical_dt(206e9, 0.3, 7850.0, 0.9)
+    steps, rise = 120, 40 * dt
+    ref.step(dt, steps, rise_time=rise)
+    s.run(steps, dt=dt, rise_time=rise, compensated=True, max_iterations=12)
+    p, _ = s.readback()
+    u, ur = p - rest, ref.position - rest
+    ep_ref = ref.state.reshape(-1, 129)[:, 12:120:15]
+    assert (ep_ref > 0).sum() > 100, "the case must yield"
+    err = np.abs(u - ur).max() / np.abs(ur).max()
+    assert err < 2e-5, err
+    ep = s.state()[:, 12:120:15]
+    assert abs(ep.max() - ep_ref.max()) <= 1e-3 * ep_ref.max()
+
+
 @pytest.mark.parametrize("nx,ny", [(1, 1), (3, 1), (5, 1), (5, 3), (7, 2)])
 def test_ragged_element_counts_against_fp64_oracle(fem, port, nx, ny):
     """Element counts that do not fill the last warp group of four (1, 3, 5, 15, 14):
