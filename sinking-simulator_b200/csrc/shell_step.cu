@@ -438,8 +438,11 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
 #pragma unroll
             for (int j = 0; j < 3; ++j) q[i * 3 + j] = jd[i * 3] * j0[j] + jd[i * 3 + 1] * j0[3 + j] + jd[i * 3 + 2] * j0[6 + j];
         // Higham iteration to convergence in FP32 (the CPU runs it to 1e-16 in double,
-        // solid_shell.cpp:473-487): stop once a step moves Q by no more than a few FP32
-        // ulps of |Q| (2^-21), at most six iterations.
+        // solid_shell.cpp:473-487), at most six iterations.  The iteration converges
+        // quadratically: X = R (I + E) goes to R (I + E^2 / 2), and a step moves Q by
+        // about |E|, so after a step of size s the next would move it by about s^2 / 2.
+        // Stop once that is within an FP32 ulp of |Q| (s^2 <= 2.4e-7 |Q|), or once a
+        // step itself moved Q by no more than a few ulps (4.8e-7 |Q|).
 #pragma unroll 1
         for (int it = 0; it < 6; ++it) {
             float ipq[9], m[9];
@@ -465,7 +468,7 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
                 size = fmaxf(size, fabsf(ipq[k]));
                 q[k] = ipq[k];
             }
-            if (step <= 4.8e-7f * size) break;  // within ~4 ulps: only rounding left to move
+            if (step <= 4.8e-7f * size || step * step <= 2.4e-7f * size) break;
         }
     }
     // ---- co-rotated relative displacement u'_a = Q^T dX_a + dd_a + Q^T dd_a ----
