@@ -136,6 +136,25 @@ def test_caller_forms_match_device_forms(fem, port):
     assert np.array_equal(pa, pb) and np.array_equal(va, vb)
 
 
+def test_caller_forms_of_another_geometry_are_refused(fem, port):
+    """The step forms B and G from the rest positions, so forms a caller hands over are
+    only checked: a Gauss weight, or a B entry of one of the first 64 elements, that is
+    not the solid-shell's of those positions is refused at create."""
+    rest, index, pinned, load = small_plate(fem, nx=6, ny=4)
+    mat = O.material(E=206e9, nu=0.3, yield_=355e6, hardening=1e9)
+    ref = O.ShellModel(port, rest, index, pinned, mat, fext=load)
+    forms = ref.forms.reshape(-1, O.FORMS_LEN)[:, :1505].copy()
+    fem.ShellSolver(rest, index, pinned=pinned, load=load, forms=forms, mass=ref.mass).close()
+    bad = forms.copy()
+    bad[-1, 1488 + 5] *= 1.0 + 1e-6  # the last element's sixth Gauss weight
+    with pytest.raises(fem.FemStepError, match="Gauss weights"):
+        fem.ShellSolver(rest, index, pinned=pinned, load=load, forms=bad, mass=ref.mass)
+    bad = forms.copy()
+    bad[2, 7] += 1e-6 * np.abs(bad[2, :1152]).max()  # one B entry of element 2
+    with pytest.raises(fem.FemStepError, match="solid-shell forms"):
+        fem.ShellSolver(rest, index, pinned=pinned, load=load, forms=bad, mass=ref.mass)
+
+
 def test_rigid_translation_carries_no_force(fem):
     """tests/test_zone.cpp:529: a uniform velocity moves the patch rigidly."""
     rest, index = fem.plate_mesh(0.06, 0.04, 0.012, 6, 4, 1)
