@@ -46,7 +46,7 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
 
 // Element e's rest corners for the element operators: the bottom corners relative to
 // corner 0 and the directors D_c = X_{c+4} - X_c, each difference taken in double and
-// rounded once.  Plain loads: after the step's stores they are read again, not kept.
+// rounded once (the same values the step forms from its own node loads).
 __device__ __forceinline__ void shell_rest_corners(const ShellDevice& d, long long e, float Xb[4][3], float D[4][3]) {
     const uint4 i0 = reinterpret_cast<const uint4*>(d.index)[e * 2];
     const uint4 i1 = reinterpret_cast<const uint4*>(d.index)[e * 2 + 1];
@@ -488,6 +488,19 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     __shared__ float q_park[9][kShellBlock];
 #pragma unroll
     for (int k = 0; k < 9; ++k) q_park[k][threadIdx.x] = q[k];
+    // and the element's rest corners, one copy per element: its eight lanes hold the same
+    // values and each reads back what it wrote itself, so no synchronisation either
+    __shared__ float corner_park[24][kShellBlock / 8];
+    {
+        const int el = threadIdx.x >> 3;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                corner_park[c * 3 + i][el] = dX[c][i];
+                corner_park[12 + c * 3 + i][el] = D[c][i];
+            }
+    }
     // ---- the point's operators, formed from the rest geometry ----
     const ShellLanePoint P = shell_lane_point(gp);
     float gx[3], gy[3], Ainv[9], w;
@@ -736,14 +749,21 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     }
 
     // ---- f = -R sum_g w_g B_g^T sigma_g, reduce-scattered so lane a holds node a ----
-    // (the rest corners and the point's frame formed again: cheaper than holding them
-    // in registers through the Newton iterations)
+    // (the rest corners back from shared memory and the point's frame formed again:
+    // cheaper than holding them in registers through the Newton iterations)
     float f[24];
 #pragma unroll
     for (int j = 0; j < 24; ++j) f[j] = 0.0f;
     {
         float Xb[4][3], Dr[4][3], fx[3], fy[3], Af[9], wf;
-        shell_rest_corners(d, e, Xb, Dr);
+        const int el = threadIdx.x >> 3;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                Xb[c][i] = corner_park[c * 3 + i][el];
+                Dr[c][i] = corner_park[12 + c * 3 + i][el];
+            }
         shell_frame(Xb, Dr, P, formed, fx, fy, Af, wf);
         shell_force(Xb, Dr, P, fx, fy, Af, wf, o.sigma, f);
     }
