@@ -228,18 +228,20 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
         if (bad) return fail(nullptr, FEMSTEP_EINVAL, "element index out of range");
     }
     if (!m.mass && !(m.density > 0.0)) return fail(nullptr, FEMSTEP_EINVAL, "need a lumped mass or a positive density");
-    std::vector<uint32_t> offset, entry;
-    if (m.adjacency_offset && m.adjacency_entry) {
+    // The adjacency: the caller's (zone::Solver's), checked here on the host together with
+    // its slot map; or, without one, built on the device once the index is there
+    // (csr.cu: the same runs as the CPU counting sort).
+    const bool caller_csr = m.adjacency_offset && m.adjacency_entry;
+    std::vector<uint32_t> offset, entry, slot;
+    if (caller_csr) {
         offset.assign(m.adjacency_offset, m.adjacency_offset + N + 1);
         entry.assign(m.adjacency_entry, m.adjacency_entry + E * 8);
         if (offset[0] != 0 || offset[N] != E * 8) return fail(nullptr, FEMSTEP_EINVAL, "adjacency offsets do not span 8E entries");
-    } else {
-        fs::build_csr(N, E, 8, m.index, offset, entry);
+        slot.assign(E * 8, 0xffffffffu);
     }
     // The slot map, node by node: an entry belongs to the one node its corner names, so
     // the nodes' runs touch disjoint slots and run in parallel.
-    std::vector<uint32_t> slot(E * 8, 0xffffffffu);
-    {
+    if (caller_csr) {
         std::atomic<int> bad{0};
         fs::parallel_chunks(N, [&](size_t b, size_t e) {
             for (size_t n = b; n < e && !bad; ++n) {
@@ -292,8 +294,23 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     s->rest.assign(m.rest, m.rest + N * 3);
     d.rest = A.upload(m.rest, N * 3);
     d.index = A.upload(m.index, E * 8);
-    d.slot = A.upload(slot.data(), E * 8);
-    d.offset = A.upload(offset.data(), N + 1);
+    if (caller_csr) {
+        d.slot = A.upload(slot.data(), E * 8);
+        d.offset = A.upload(offset.data(), N + 1);
+    } else {
+        uint32_t* dslot = A.alloc<uint32_t>(E * 8);
+        uint32_t* doffset = A.alloc<uint32_t>(N + 1);
+        d.slot = dslot;
+        d.offset = doffset;
+        if (A.ok()) {
+            rc = check(s, fs::build_csr_device(d.index, (long long)(E * 8), (long long)N, doffset, dslot, s->stream),
+                       "adjacency");
+            if (rc) {
+                femstep_shell_destroy(s);
+                return rc;
+            }
+        }
+    }
     float4* elem = A.zeros<float4>(E * fs::kShellElemQ);
     d.elem = elem;
     d.state = A.zeros<float>((size_t)s->groups * fs::kShellStateQ * 32);

@@ -155,6 +155,31 @@ def test_caller_forms_of_another_geometry_are_refused(fem, port):
         fem.ShellSolver(rest, index, pinned=pinned, load=load, forms=bad, mass=ref.mass)
 
 
+def test_device_adjacency_is_the_counting_sort(fem):
+    """Without a caller's adjacency the solver builds the node -> corner CSR on the
+    device (atomic scatter, then each node's run sorted); with zone::Solver's
+    (element-order counting sort, zone.cpp:739-755) handed over it checks and uploads
+    that one.  The gather order is the CSR order, so the two runs agree bit for bit --
+    on a plate and on a mesh whose elements are shuffled."""
+    rest, index, pinned, load = small_plate(fem)
+    rng = np.random.default_rng(7)
+    shuffled = index.reshape(-1, 8)[rng.permutation(index.size // 8)].reshape(-1)
+    for idx in (index, shuffled):
+        offset, entry = fem.csr(rest.size // 3, idx, 8)
+        a = fem.ShellSolver(rest, idx, pinned=pinned, load=load, density=7850.0)
+        b = fem.ShellSolver(rest, idx, pinned=pinned, load=load, density=7850.0, adjacency_offset=offset,
+                            adjacency_entry=entry)
+        dt = a.critical_dt(206e9, 0.3, 7850.0, 0.9)
+        a.run(60, dt=dt, rise_time=20 * dt)
+        b.run(60, dt=dt, rise_time=20 * dt)
+        pa, va = a.readback()
+        pb, vb = b.readback()
+        assert np.abs(pa - rest).max() > 0
+        assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+        a.close()
+        b.close()
+
+
 def test_rigid_translation_carries_no_force(fem):
     """tests/test_zone.cpp:529: a uniform velocity moves the patch rigidly."""
     rest, index = fem.plate_mesh(0.06, 0.04, 0.012, 6, 4, 1)
