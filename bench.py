@@ -61,7 +61,9 @@ METRIC = "element-updates/s @1 B200 (batched vs plain, % HBM peak); p50/p99 step
 UNIT = "element-updates/s"
 
 WORKLOADS = {
-    "shell-panel": dict(kind="shell", cells=(2000, 1000), sample_cells=(100, 50)),
+    # the configuration's whole run: 5,000 steps, through the pressure pulse's 5 ms rise
+    # (the plating yields as the load comes on); --steps times fewer
+    "shell-panel": dict(kind="shell", cells=(2000, 1000), sample_cells=(100, 50), run_steps=5000),
     # a 2 x 1 m corner of the same panel (20,000 elements, 0.14 GB per step): the size
     # the ncu captures are taken on
     "shell-sample": dict(kind="shell", cells=(200, 100), sample_cells=(100, 50)),
@@ -672,7 +674,7 @@ class Solver:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 100; shell-panel 5000)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet-batched", choices=sorted(WORKLOADS))
@@ -686,6 +688,8 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
+    if args.steps is None:
+        args.steps = wl.get("run_steps", 100)
     if args.impl == "reference":
         return run_reference(args, wl)
 
