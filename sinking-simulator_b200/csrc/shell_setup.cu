@@ -15,6 +15,9 @@
 namespace fs {
 namespace {
 
+// elements per launch of the one-thread-per-element set-up (its stiffness scratch is
+// 576 doubles x this many)
+constexpr long long kSetupChunk = 1 << 16;
 __device__ __constant__ double kXi[8] = {-1, +1, +1, -1, -1, +1, +1, -1};
 __device__ __constant__ double kEta[8] = {-1, -1, +1, +1, -1, -1, +1, +1};
 __device__ __constant__ double kZta[8] = {-1, -1, -1, -1, +1, +1, +1, +1};
@@ -262,7 +265,9 @@ __device__ bool solve_small(const double a[49], int n, double* rhs, int columns)
 
 // elementStiffness from computed forms: computeBlocks (solid_shell.cpp:377-429) and
 // the static condensation (:509-535).
-__device__ void stiffness(const Forms& f, double E, double nu, double* out /*576*/) {
+// out holds the 576 entries at a stride (the scratch is entry-major across elements, so
+// the threads of a warp touch adjacent words).
+__device__ void stiffness(const Forms& f, double E, double nu, double* out /*576 x stride*/, size_t stride) {
     const double lambda = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     const double mu = E / (2.0 * (1.0 + nu));
     double c[6][6];
@@ -274,7 +279,7 @@ __device__ void stiffness(const Forms& f, double E, double nu, double* out /*576
         c[3 + i][3 + i] = mu;
     }
     double kua[24 * 7], kaa[49];
-    for (int i = 0; i < 576; ++i) out[i] = 0.0;
+    for (int i = 0; i < 576; ++i) out[i * stride] = 0.0;
     for (int i = 0; i < 24 * 7; ++i) kua[i] = 0.0;
     for (int i = 0; i < 49; ++i) kaa[i] = 0.0;
     for (int gp = 0; gp < 8; ++gp) {
@@ -290,7 +295,7 @@ __device__ void stiffness(const Forms& f, double E, double nu, double* out /*576
             for (int j = 0; j < 24; ++j) {
                 double s = 0.0;
                 for (int k = 0; k < 6; ++k) s += f.b[gp][k][i] * cb[k][j];
-                out[i * 24 + j] += w * s;
+                out[(i * 24 + j) * stride] += w * s;
             }
         if (f.eas == 0) continue;
         double cg[6][7];
@@ -322,12 +327,12 @@ __device__ void stiffness(const Forms& f, double E, double nu, double* out /*576
         for (int j = 0; j < 24; ++j) {
             double s = 0.0;
             for (int k = 0; k < f.eas; ++k) s += kua[i * 7 + k] * x[k * 24 + j];
-            out[i * 24 + j] -= s;
+            out[(i * 24 + j) * stride] -= s;
         }
 }
 
 // criticalTimestep, solid_shell.cpp:1088-1133
-__device__ double power_dt(const double* k, const double m[8], double safety) {
+__device__ double power_dt(const double* k, size_t stride, const double m[8], double safety) {
     for (int a = 0; a < 8; ++a)
         if (!(m[a] > 0.0)) return 0.0;
     double d[24];
@@ -340,7 +345,7 @@ __device__ double power_dt(const double* k, const double m[8], double safety) {
         double w[24];
         for (int i = 0; i < 24; ++i) {
             double s = 0.0;
-            for (int j = 0; j < 24; ++j) s += k[i * 24 + j] * (d[j] * v[j]);
+            for (int j = 0; j < 24; ++j) s += k[(i * 24 + j) * stride] * (d[j] * v[j]);
             w[i] = d[i] * s;
         }
         double num = 0.0, den = 0.0;
@@ -409,12 +414,12 @@ __global__ void __launch_bounds__(64) shell_setup_kernel(ShellSetupArgs a, doubl
         if (a.corner_mass)
             for (int n = 0; n < 8; ++n) a.corner_mass[a.slot[e * 8 + n]] = m[n];
         if (a.dt_out) {
-            double* k = scratch_k + (size_t)e * 576;
+            double* k = scratch_k + e;  // entry-major: entry i of element e at i * chunk + e
             if (f.ok) {
                 // criticalTimestep builds its own stiffness from the nodes (for the
                 // solid-shell formulation, the same forms as above).
-                stiffness(f, a.youngs, a.poisson, k);
-                a.dt_out[e] = power_dt(k, m, a.safety);
+                stiffness(f, a.youngs, a.poisson, k, kSetupChunk);
+                a.dt_out[e] = power_dt(k, kSetupChunk, m, a.safety);
             } else {
                 a.dt_out[e] = 0.0;
             }
@@ -532,7 +537,7 @@ void launch_shell_setup(const ShellSetupArgs& a, cudaStream_t stream) {
         return;
     }
     double* scratch = nullptr;
-    const long long chunk = 1 << 16;
+    const long long chunk = kSetupChunk;
     if (a.dt_out) cudaMallocAsync(&scratch, (size_t)chunk * 576 * sizeof(double), stream);
     for (long long first = 0; first < a.elements; first += chunk) {
         ShellSetupArgs c = a;
