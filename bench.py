@@ -127,7 +127,7 @@ def shell_bytes(E, N):
 
 # FP32 operations per solid-shell element update, counted by ncu on the shell-sample
 # workload (SASS thread instructions: 2 x FFMA + FADD + FMUL, 16,707 per element with B
-# and G formed in the kernel; the 665 FP64 operations -- rest-corner differences and
+# and G formed in the kernel; the 473 FP64 operations -- rest-corner differences and
 # the energy account -- are left out).  The second roofline of the shell element,
 # against the FP32 SIMT peak: SMs x 128 lanes x 2 x the SM clock.
 SHELL_FP32_FLOP_PER_ELEMENT = 16707
