@@ -38,7 +38,7 @@ Workloads (synthetic and seeded; no dataset is involved):
   tet-serving     Poisson arrivals (40/s) of tet meshes of log-uniform size in
                   [1e3, 5e5] and U[500, 5000] steps, admitted into a pool sized to a
                   150 GB budget as room frees up, with p50/p99 step latency; the trace
-                  lasts --serve-seconds (default 30 s) of arrivals.
+                  lasts --serve-seconds (default 120 s, the configuration's) of arrivals.
 """
 from __future__ import annotations
 
@@ -83,9 +83,9 @@ SHELL_MATERIAL = dict(youngs=206e9, poisson=0.3, yield_strength=355e6, hardening
 # inputs
 
 def tet_beam(nx, ny, nz, length=1.0, width=0.1, depth=0.1, load=20e3):
-    import femstep as F
+    import meshes as M
 
-    pos, idx = F.box_tet_mesh(length, width, depth, nx, ny, nz)
+    pos, idx = M.box_tet_mesh(length, width, depth, nx, ny, nz)
     fixed = (pos[0::3] < 1e-6).astype(np.uint32)
     tip = pos[0::3] > length - 1e-6
     fext = np.zeros(pos.size)
@@ -94,10 +94,10 @@ def tet_beam(nx, ny, nz, length=1.0, width=0.1, depth=0.1, load=20e3):
 
 
 def shell_panel(nx, ny):
-    import femstep as F
+    import meshes as M
 
     # the full panel is 2000 x 1000 cells of 10 mm; a sample keeps the cell size
-    return F.stiffened_panel(nx=nx, ny=ny, lx=20.0 * nx / 2000, ly=10.0 * ny / 1000)
+    return M.stiffened_panel(nx=nx, ny=ny, lx=20.0 * nx / 2000, ly=10.0 * ny / 1000)
 
 
 # ---------------------------------------------------------------------------------
@@ -253,39 +253,16 @@ def cpu_baseline(wl, seconds=15.0):
            node update, on a sub-panel with the full panel's 10 mm cells."""
     import oracle as O
 
-    kind = "reference" if O.have_ref() else "port"
-    o = O.Oracle("ref" if kind == "reference" else "port")
     workers = os.cpu_count() or 1
     if wl["kind"] in ("pool", "serve"):
-        import workloads as W
-
-        specs = batch_specs(wl)[:6]
-        port = o if kind == "port" else O.Oracle("port")  # the FP64 element bound (set-up, untimed)
-        done, spent, sample = 0.0, 0.0, []
-        for sp in specs:
-            b = W.build(sp)
-            m = O.TetMesh64(o, b.position, b.index, b.fixed, b.external_force)
-            dt = port.tet64_critical_dt(C.byref(m._s), W.YOUNGS, W.POISSON, W.DENSITY, 0.9)
-            p = O.tet64_params(dt=dt, ramp_steps=1000, yield_=sp.yield_strength, hardening=sp.hardening)
-            T = sp.tets
-            budget = seconds / len(specs)
-            if kind == "reference":
-                rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), 1, workers)
-                steps = max(1, int(budget * rate / T))
-                rate = o.tet64_time_parallel(C.byref(m._s), C.byref(p), steps, workers)
-                spent += T * steps / rate  # the step loop's own clock (thread start-up excluded)
-            else:
-                t0 = time.perf_counter()
-                m.step(p, 1)
-                steps = max(1, int(budget / max(time.perf_counter() - t0, 1e-9)))
-                t0 = time.perf_counter()
-                m.step(p, steps)
-                spent += time.perf_counter() - t0
-            done += T * steps
-            sample.append(f"{T}x{steps}")
-        return {"value": done / spent, "unit": UNIT, "cores": workers if kind == "reference" else 1, "kind": kind,
-                "sample": "O-tet64 (FP64 J2) on the first %d meshes of the workload, meshes in sequence, tets x "
-                          "steps: %s" % (len(specs), ", ".join(sample))}
+        batch = RefBatch(wl)
+        per_step = batch.time(1, workers)  # warm-up step, and the size of a step
+        steps = max(1, min(20, int(seconds / max(per_step, 1e-9))))
+        spent = batch.time(steps, workers)
+        return {"value": batch.tets * steps / spent, "unit": UNIT, "cores": workers, "kind": batch.kind,
+                "sample": batch.sample(1, steps, workers)}
+    kind = "reference" if O.have_ref() else "port"
+    o = O.Oracle("ref" if kind == "reference" else "port")
     if wl["kind"] == "tet":
         pos, idx, fixed, fext = tet_beam(*wl["cells"], load=wl["load"])
         m = O.TetMesh64(o, pos, idx, fixed, fext)
@@ -331,23 +308,81 @@ def cpu_baseline(wl, seconds=15.0):
     return {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
 
+class RefBatch:
+    """The batched workload's meshes as O-tet64 states for the reference's CPU step:
+    the compiled reference (oracle/_ref) when present, else the C restatement.  Each
+    mesh has its own material, load ramp and time step (0.9 x its FP64 element bound,
+    as on the GPU).  A step is one time step of every mesh, one mesh after another
+    (the reference steps one mesh per solver, fem.cpp:187), each mesh's element loop
+    over the host threads.  Imports neither the product library nor anything that
+    loads it."""
+
+    def __init__(self, wl):
+        import oracle as O
+        import workloads as W
+
+        self.O = O
+        self.kind = "reference" if O.have_ref() else "port"
+        self.o = O.Oracle("ref" if self.kind == "reference" else "port")
+        port = self.o if self.kind == "port" else O.Oracle("port")
+        self.specs = batch_specs(wl)
+        self.meshes, self.params = [], []
+        for sp in self.specs:
+            b = W.build(sp)
+            m = O.TetMesh64(self.o, b.position, b.index, b.fixed, b.external_force)
+            dt = port.tet64_critical_dt(C.byref(m._s), W.YOUNGS, W.POISSON, W.DENSITY, 0.9)
+            self.meshes.append(m)
+            self.params.append(O.tet64_params(dt=dt, ramp_steps=sp.ramp_steps, yield_=sp.yield_strength,
+                                              hardening=sp.hardening))
+        self.tets = sum(sp.tets for sp in self.specs)
+
+    def time(self, steps, workers):
+        """Seconds of `steps` steps of the whole batch (the step loop's own clock)."""
+        O = self.O
+        if self.kind == "reference":
+            arr = (C.POINTER(O.Tet64) * len(self.meshes))(*[C.pointer(m._s) for m in self.meshes])
+            ps = (O.Tet64Params * len(self.params))(*self.params)
+            return self.o.tet64_time_batch(arr, ps, len(self.meshes), steps, workers)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for m, p in zip(self.meshes, self.params):
+                m.step(p, 1, threads=workers)
+        return time.perf_counter() - t0
+
+    def sample(self, warmup, steps, workers):
+        what = "the compiled reference" if self.kind == "reference" else "the C restatement"
+        return (f"all {len(self.specs)} meshes of the workload ({self.tets:,} tets), {warmup} warm-up + {steps} "
+                f"timed steps, each step one mesh after another; O-tet64 (fem.cpp kinematics with "
+                f"plasticity::update in FP64) from {what}, element loop on {workers} host threads")
+
+
 def run_reference(args, wl):
+    """The reference's CPU step on the same workload, W warm-up and K timed steps; rank
+    0 only (the other ranks exit without work)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    for _ in range(min(args.warmup, 1)):
+    workers = os.cpu_count() or 1
+    if wl["kind"] in ("pool", "serve"):
+        batch = RefBatch(wl)
+        batch.time(args.warmup, workers)
+        spent = batch.time(args.steps, workers)
+        value = batch.tets * args.steps / spent
+        base = {"value": value, "unit": UNIT, "cores": workers, "kind": batch.kind,
+                "sample": batch.sample(args.warmup, args.steps, workers)}
+        config = pool_config(args, wl, batch.specs, args.gpus)
+        ms = spent / args.steps * 1e3
+    else:
         cpu_baseline(wl, seconds=2.0)
-    rates = []
-    base = None
-    per = max(2.0, 60.0 / max(args.steps, 1))
-    for _ in range(min(args.steps, 10)):
-        base = cpu_baseline(wl, seconds=per)
-        rates.append(base["value"])
-    value = float(np.median(rates))
-    base["value"] = value
+        rates = [cpu_baseline(wl, seconds=max(2.0, 60.0 / max(args.steps, 1)))["value"]
+                 for _ in range(min(args.steps, 10))]
+        base = cpu_baseline(wl, seconds=2.0)
+        value = base["value"] = float(np.median(rates))
+        config = {"workload": args.workload}
+        ms = None
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": args.workload}, "cpu_baseline": base,
+           "config": config, "cpu_baseline": base,
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -361,6 +396,17 @@ def batch_specs(wl):
     if wl["kind"] == "serve":
         return W.request_trace(rate=wl["rate"], duration=4.0, lo=wl["lo"], hi=wl["hi"])
     return W.batch_meshes(count=wl["count"], lo=wl["lo"], hi=wl["hi"], steps=0, ramp_steps=1000)
+
+
+def pool_config(args, wl, specs, world):
+    """The batched workload's description, the same in both arms' lines."""
+    T = sum(sp.tets for sp in specs)
+    N = sum(sp.nodes for sp in specs)
+    per_step = sum(sum(tet_bytes(sp.tets, sp.nodes, "f32k")) for sp in specs)
+    return {"workload": args.workload, "meshes": len(specs), "elements": T, "nodes": N,
+            "mesh_seed": "workloads.batch_meshes defaults", "load_ramp_steps": 1000,
+            "l2": "no flush: %.2f GB move per step, above the 126 MB L2" % (per_step / 1e9),
+            "parallelism": f"replicas x{world}"}
 
 
 def tet_von_mises(position, rest, index, plastic, mu, kappa):
@@ -487,6 +533,65 @@ def plain_sequential(F, W, built, steps, mode):
     return units / (total_ms / 1e3), total_ms
 
 
+def pool_drift(F, W, specs, steps=2000):
+    """Drift of the batched FP32-compensated step against FP64 on a sample of the
+    batch (workloads.drift_sample: the largest mesh and the smallest plate of each
+    clamped face and load kind), over the 1,000-step load ramp plus 1,000 steps.  The
+    FP64 side is the plain single-mesh FP64 GPU step, which is bit-identical to the FP64
+    oracle (tests/test_tet_gpu.py, tests/test_pool_gpu.py)."""
+    picks = W.drift_sample(specs)
+    built = [W.build(specs[i]) for i in picks]
+    T = sum(b.spec.tets for b in built)
+    N = sum(b.spec.nodes for b in built)
+    pool = F.TetPool(T, N + len(built) + 1, max_meshes=len(built) + 1)
+    mu, kappa = W.YOUNGS / (2 * (1 + W.POISSON)), W.YOUNGS / (3 * (1 - 2 * W.POISSON))
+    ids, refs = [], []
+    for b in built:
+        s = F.TetSolver(b.position, b.index, mode="f64", fixed=b.fixed, external_force=b.external_force,
+                        density=W.DENSITY)
+        dt = s.critical_dt(W.YOUNGS, W.POISSON, W.DENSITY, 0.9)
+        s.run(steps, dt=dt, ramp_steps=b.spec.ramp_steps, yield_strength=b.spec.yield_strength,
+              hardening=b.spec.hardening)
+        p64, _ = s.readback64()
+        refs.append((p64, s.plastic(), s.energy()))
+        s.close()
+        ids.append(pool.admit(steps=steps, dt=dt, **b.admit_kwargs()))
+    pool.run(steps)
+
+    def balance(e):
+        w = e[0] + e[4]
+        return abs(w - (e[1] + e[2] + e[3])) / abs(w)
+
+    rows = []
+    for b, i, (p64, pl64, e64) in zip(built, ids, refs):
+        p, _ = pool.readback(i)
+        pl = pool.plastic(i)
+        e = pool.energy(i)
+        rest = b.position.astype(np.float64)
+        u, u64 = p - rest, p64 - rest
+        vm = tet_von_mises(p, rest, b.index, pl, mu, kappa)
+        vm64 = tet_von_mises(p64, rest, b.index, pl64, mu, kappa)
+        ep, ep64 = pl[:, 6], pl64[:, 6]
+        rows.append({"tets": b.spec.tets, "clamp": b.spec.clamp, "load": b.spec.load_kind,
+                     "yielded_fraction_fp64": float((ep64 > 0).mean()),
+                     "displacement": float(np.abs(u - u64).max() / np.abs(u64).max()),
+                     "von_mises": float(np.abs(vm - vm64).max() / vm64.max()),
+                     "plastic_strain": float(np.abs(ep - ep64).max() / ep64.max()) if ep64.max() > 0 else 0.0,
+                     "energy_balance_fp32k": float(balance(e)), "energy_balance_fp64": float(balance(e64)),
+                     "energy_terms_vs_work": float(np.abs(np.asarray(e[:4]) - np.asarray(e64[:4])).max()
+                                                   / abs(e64[0]))})
+    pool.close()
+    return {"meshes": picks, "steps": steps, "reference": "FP64 GPU step, bit-identical to the FP64 oracle",
+            "max_rel_displacement_error": max(r["displacement"] for r in rows),
+            "max_rel_von_mises_error": max(r["von_mises"] for r in rows),
+            "max_rel_plastic_strain_error": max(r["plastic_strain"] for r in rows),
+            "max_energy_term_error_over_work": max(r["energy_terms_vs_work"] for r in rows),
+            "errors": "max |a - a64| / max |a64| per mesh (displacement over nodes; von Mises from the final "
+                      "state and equivalent plastic strain over tets); energy terms (work, dissipation, strain, "
+                      "kinetic) against FP64, over the external work",
+            "per_mesh": rows}
+
+
 def run_pool(args, wl, rank, world, barrier, dist, local):
     import femstep as F
     import workloads as W
@@ -502,9 +607,10 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
     pool.run(0)
     admit_s = time.perf_counter() - t_admit
     tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=16)
-    # W warm-up steps, at least one captured graph's worth (16 steps), so that the graph
-    # the timed chunk replays is built before the timed region
-    warm = max(args.warmup, 16)
+    # the work list and the schedule's captured graph are built before the warm-up, so
+    # the timed chunk does no set-up whatever W is
+    pool.prepare()
+    warm = args.warmup
     pool.run(warm)
     barrier()
     with ClockSampler(local) as clocks:
@@ -558,6 +664,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
                        "map on all host cores, upload, FP64 rest state on the device), K steps, read back every "
                        "mesh's positions and velocities (femstep_pool_readback_many), destroy; through the C ABI, "
                        "wall clock"}
+    drift = None if args.no_drift else pool_drift(F, W, specs)
     peak, peak_kind = measured_peak()
     achieved = eb / (elem_ms / 1e3) / 1e9
     if rank == 0:
@@ -565,13 +672,14 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "meshes": len(specs), "elements": T, "nodes": N,
-                       "schedule": tune, "element_kernel_ms": elem_ms, "node_kernel_ms": node_ms,
+            "config": pool_config(args, wl, specs, world),
+            "detail": {"schedule": tune, "element_kernel_ms": elem_ms, "node_kernel_ms": node_ms,
                        "step_effective_gbs": (eb + nb) / (ms / args.steps / 1e3) / 1e9,
-                       "l2": "no flush: %.2f GB move per step, above the 126 MB L2" % ((eb + nb) / 1e9),
                        "admit_seconds": admit_s, "device_bytes": info["device_bytes"],
-                       "parallelism": f"replicas x{world}"},
+                       "warmup_note": "the work list and the 16-step graph are built (femstep_pool_prepare) "
+                                      "before the W warm-up steps"},
             "plain": plain,
+            "drift": drift,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
@@ -683,7 +791,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="tet-batched: skip the one-mesh-at-a-time comparison")
     ap.add_argument("--schedule", default=None,
                     help="pool workloads: TILE:graph|persistent|graph-staged instead of the autotuner")
-    ap.add_argument("--serve-seconds", type=float, default=30.0)
+    ap.add_argument("--no-drift", action="store_true", help="tet-batched: skip the drift sample against FP64")
+    ap.add_argument("--serve-seconds", type=float, default=120.0)
     ap.add_argument("--serve-chunk", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -31,7 +31,7 @@ extern "C" {
 #define FEMSTEP_ENOMEM 3    /* device or host allocation failed / over the memory budget */
 #define FEMSTEP_ECUDA 4     /* a CUDA call failed */
 #define FEMSTEP_ESTATE 5    /* call out of order (e.g. run before upload) */
-#define FEMSTEP_ETIMEOUT 6  /* a bounded device-side wait gave up */
+#define FEMSTEP_ETIMEOUT 6  /* a bounded device-side wait gave up; the outputs of that launch are undefined */
 
 /* Text of the last error raised on this thread by a call that has no handle yet. */
 const char *femstep_last_error(void);
@@ -141,10 +141,14 @@ typedef struct {
    its device arrays, and the only scratch, the per-tet corner forces, is a fixed
    library-resident array of 65,536 tets (3 MiB per GPU that loads the library, held
    until the process exits).  Larger meshes are rejected with FEMSTEP_EINVAL.  The
-   first call on a device looks up that array's device address, so make that call
-   before any stream capture.  Every call on a device shares the array: calls whose
-   kernels overlap on the GPU race; calls ordered on one stream do not.  Launches on
-   `stream` (a cudaStream_t, NULL for the legacy default stream) and returns without
+   step is elastic: yield_strength, hardening_modulus and ramp_steps must be 0
+   (FEMSTEP_EINVAL otherwise).  The first call in each CUDA context on a device looks
+   up that array's device address in that context (a new context after
+   cudaDeviceReset gets a new lookup), so make that call before any stream capture.
+   Every call on a device shares the array: calls whose kernels overlap on the GPU
+   race; calls ordered on one stream do not.  A CUDA error pending from before the
+   call is returned as FEMSTEP_ECUDA without launching.  Launches on `stream` (a
+   cudaStream_t, NULL for the legacy default stream) and returns without
    synchronising. */
 int femstep_tet_step_noalloc(const femstep_tet_device_mesh *mesh, int substeps, const femstep_tet_params *params,
                              void *stream);
@@ -217,6 +221,10 @@ int femstep_pool_admit_resume(femstep_pool *pool, const femstep_pool_mesh *mesh,
 /* Queue one chunk: every admitted mesh that has steps left advances by up to `steps`
    steps (meshes that reach their count stop there).  Returns without waiting. */
 int femstep_pool_run_async(femstep_pool *pool, int steps, int mode);
+/* Build what the next chunk launches -- the work list and, in the graph schedules,
+   the captured graph of 16 steps -- without running a step, so that a timed chunk
+   that follows does no set-up.  Waits for the pool's stream. */
+int femstep_pool_prepare(femstep_pool *pool);
 /* Wait for the queued chunk; its device milliseconds (CUDA events). */
 int femstep_pool_wait(femstep_pool *pool, double *gpu_ms);
 /* run_async + wait. */

@@ -12,6 +12,7 @@
 #include "femoracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -572,9 +573,146 @@ void or_tet64_rest_state(or_tet64 *m, double rho) {
     build_csr(m->nodes, m->tets, 4, m->index, m->adj_offset, m->adj_entry);
 }
 
-/* One O-tet64 step: fem.cpp:73-117 in double with the J2 point law at the single
- * point, then fem.cpp:196-214 with the ramped external load added after the gather. */
-void or_tet64_step(or_tet64 *m, const or_tet64_params *p, int steps) {
+/* The element part of one O-tet64 step for tet t: fem.cpp:73-117 in double with the
+ * J2 point law at the single point.  Writes the tet's corner forces and stress, its
+ * plastic state, and its dissipation and strain energy into diss[t] and energy[t]. */
+static void tet64_element(or_tet64 *m, const or_tet64_params *p, const double *mat, double mu, double bulk,
+                          size_t t, double *diss, double *energy) {
+    const uint32_t *idx = &m->index[t * 4];
+    const double *x = m->position;
+    m3d ds, dm_inv;
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a) D3(ds, a, c) = x[(size_t)idx[c + 1] * 3 + a] - x[(size_t)idx[0] * 3 + a];
+    for (int k = 0; k < 9; ++k) dm_inv.m[k] = m->rest_inv[t * 9 + k];
+    const m3d f = m3d_mul(&ds, &dm_inv);
+    const m3d r = m3d_polar(&f, p->polar_fixed);
+    const m3d rt = m3d_tr(&r);
+    const m3d sm = m3d_mul(&rt, &f);
+    double strain[6];
+    strain[0] = 0.5 * (D3(sm, 0, 0) + D3(sm, 0, 0)) - 1.0;
+    strain[1] = 0.5 * (D3(sm, 1, 1) + D3(sm, 1, 1)) - 1.0;
+    strain[2] = 0.5 * (D3(sm, 2, 2) + D3(sm, 2, 2)) - 1.0;
+    strain[3] = 2.0 * (0.5 * (D3(sm, 0, 1) + D3(sm, 1, 0)));
+    strain[4] = 2.0 * (0.5 * (D3(sm, 1, 2) + D3(sm, 2, 1)));
+    strain[5] = 2.0 * (0.5 * (D3(sm, 2, 0) + D3(sm, 0, 2)));
+    double point[OR_POINT_LEN] = {0};
+    double *ps = &m->plastic[t * 7];
+    for (int i = 0; i < 6; ++i) point[i] = ps[i];
+    point[12] = ps[6];
+    double sv[6], inc[OR_INCR_LEN];
+    or_plastic_update(mat, INFINITY, strain, point, sv, NULL, inc);
+    for (int i = 0; i < 6; ++i) ps[i] = point[i];
+    ps[6] = point[12];
+    for (int i = 0; i < 6; ++i) m->stress[t * 6 + i] = sv[i];
+    const double vol = m->rest_volume[t];
+    diss[t] = vol * inc[4];
+    const double pressure = (sv[0] + sv[1] + sv[2]) / 3.0;
+    double density = 0;
+    for (int i = 0; i < 3; ++i) density += 0.5 * sv[i] * ((sv[i] - pressure) / (2.0 * mu) + pressure / (3.0 * bulk));
+    for (int i = 3; i < 6; ++i) density += 0.5 * sv[i] * (sv[i] / mu);
+    energy[t] = vol * density;
+
+    m3d stress;
+    D3(stress, 0, 0) = sv[0];
+    D3(stress, 1, 1) = sv[1];
+    D3(stress, 2, 2) = sv[2];
+    D3(stress, 0, 1) = D3(stress, 1, 0) = sv[3];
+    D3(stress, 1, 2) = D3(stress, 2, 1) = sv[4];
+    D3(stress, 2, 0) = D3(stress, 0, 2) = sv[5];
+    const m3d piola = m3d_mul(&r, &stress);
+    const m3d dmt = m3d_tr(&dm_inv);
+    const m3d h = m3d_mul(&piola, &dmt);
+    const double scale = -vol;
+    double *out = &m->tet_force[t * 12];
+    double f0[3] = {0, 0, 0};
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a) {
+            const double v = scale * D3(h, a, c);
+            out[(c + 1) * 3 + a] = v;
+            f0[a] -= v;
+        }
+    for (int a = 0; a < 3; ++a) out[a] = f0[a];
+}
+
+#define OR_MAX_THREADS 256
+
+/* The node part of one O-tet64 step for node n (fem.cpp:196-214, the ramped external
+ * load added after the gather): its velocity and position, and its contributions to
+ * the external work (per DOF), the kinetic energy (per DOF) and gravity's work. */
+static void tet64_node(or_tet64 *m, const or_tet64_params *p, double lf, size_t n, double *nw, double *nk,
+                       double *ng) {
+    if (m->fixed[n]) {
+        for (int k = 0; k < 3; ++k) m->velocity[n * 3 + k] = 0.0;
+        return;
+    }
+    double force[3] = {0.0, 0.0, -p->gravity * m->mass[n]};
+    for (uint32_t e = m->adj_offset[n]; e < m->adj_offset[n + 1]; ++e) {
+        const uint32_t entry = m->adj_entry[e];
+        const double *fs = &m->tet_force[(size_t)(entry >> 2) * 12 + (entry & 3u) * 3];
+        for (int k = 0; k < 3; ++k) force[k] += fs[k];
+    }
+    double ext[3] = {0.0, 0.0, 0.0};
+    if (m->fext)
+        for (int k = 0; k < 3; ++k) ext[k] = lf * m->fext[n * 3 + k];
+    for (int k = 0; k < 3; ++k) force[k] += ext[k];
+    const double inv_mass = 1.0 / m->mass[n];
+    for (int k = 0; k < 3; ++k) {
+        double v = m->velocity[n * 3 + k] + force[k] * inv_mass * p->dt;
+        v *= p->damping;
+        m->velocity[n * 3 + k] = v;
+        m->position[n * 3 + k] += v * p->dt;
+        nw[n * 3 + k] = ext[k] * v * p->dt;
+        nk[n * 3 + k] = 0.5 * m->mass[n] * v * v;
+    }
+    ng[n] = -p->gravity * m->mass[n] * m->velocity[n * 3 + 2] * p->dt;
+}
+
+typedef struct {
+    or_tet64 *m;
+    const or_tet64_params *p;
+    const double *mat;
+    double mu, bulk, lf;
+    size_t begin, end;
+    double *diss, *energy, *nw, *nk, *ng;
+    int nodes; /* 0: tets [begin, end); 1: nodes [begin, end) */
+} tet64_range;
+
+static void *tet64_range_run(void *arg) {
+    const tet64_range *r = (const tet64_range *)arg;
+    for (size_t i = r->begin; i < r->end; ++i) {
+        if (r->nodes)
+            tet64_node(r->m, r->p, r->lf, i, r->nw, r->nk, r->ng);
+        else
+            tet64_element(r->m, r->p, r->mat, r->mu, r->bulk, i, r->diss, r->energy);
+    }
+    return NULL;
+}
+
+/* The element loop (nodes = 0) or the node loop (nodes = 1) of one step, over
+ * `threads` host threads in contiguous ranges, or serially. */
+static void tet64_loop(or_tet64 *m, const or_tet64_params *p, const double *mat, double mu, double bulk, double lf,
+                       int threads, double *diss, double *energy, double *nw, double *nk, double *ng, int nodes) {
+    const size_t count = nodes ? m->nodes : m->tets;
+    const int n = threads < 1 ? 1 : (threads < OR_MAX_THREADS ? threads : OR_MAX_THREADS);
+    tet64_range job[OR_MAX_THREADS];
+    pthread_t tid[OR_MAX_THREADS];
+    for (int k = 0; k < n; ++k)
+        job[k] = (tet64_range){m, p, mat, mu, bulk, lf, count * k / n, count * (k + 1) / n, diss, energy, nw, nk, ng,
+                               nodes};
+    if (n == 1) {
+        tet64_range_run(&job[0]);
+        return;
+    }
+    for (int k = 0; k < n; ++k)
+        if (pthread_create(&tid[k], NULL, tet64_range_run, &job[k])) abort();
+    for (int k = 0; k < n; ++k) pthread_join(tid[k], NULL);
+}
+
+/* Steps of O-tet64: the element loop (tet64_element), then the node loop
+ * (tet64_node), each over `threads` host threads when threads > 1.  The per-tet and
+ * per-node energy terms are summed afterwards in tet and node order, as the serial
+ * loops add them, so every thread count gives the same bits. */
+static void tet64_steps(or_tet64 *m, const or_tet64_params *p, int steps, int threads) {
     double mat[OR_MAT_LEN] = {0};
     mat[0] = p->E;
     mat[1] = p->nu;
@@ -582,99 +720,52 @@ void or_tet64_step(or_tet64 *m, const or_tet64_params *p, int steps) {
     mat[3] = p->hardening;
     const double mu = p->E / (2.0 * (1.0 + p->nu));
     const double bulk = p->E / (3.0 * (1.0 - 2.0 * p->nu));
+    double *diss = malloc((m->tets + 1) * sizeof(double));
+    double *energy = malloc((m->tets + 1) * sizeof(double));
+    double *nw = malloc((m->nodes * 3 + 1) * sizeof(double));
+    double *nk = malloc((m->nodes * 3 + 1) * sizeof(double));
+    double *ng = malloc((m->nodes + 1) * sizeof(double));
+    if (!diss || !energy || !nw || !nk || !ng) abort();
     for (int s = 0; s < steps; ++s) {
         const double lf = p->ramp_steps > 0 ? dmin((double)(m->step + 1) / (double)p->ramp_steps, 1.0) : 1.0;
-        double strain_energy = 0.0, dissipation = 0.0;
-        for (size_t t = 0; t < m->tets; ++t) {
-            const uint32_t *idx = &m->index[t * 4];
-            const double *x = m->position;
-            m3d ds, dm_inv;
-            for (int c = 0; c < 3; ++c)
-                for (int a = 0; a < 3; ++a) D3(ds, a, c) = x[(size_t)idx[c + 1] * 3 + a] - x[(size_t)idx[0] * 3 + a];
-            for (int k = 0; k < 9; ++k) dm_inv.m[k] = m->rest_inv[t * 9 + k];
-            const m3d f = m3d_mul(&ds, &dm_inv);
-            const m3d r = m3d_polar(&f, p->polar_fixed);
-            const m3d rt = m3d_tr(&r);
-            const m3d sm = m3d_mul(&rt, &f);
-            double strain[6];
-            strain[0] = 0.5 * (D3(sm, 0, 0) + D3(sm, 0, 0)) - 1.0;
-            strain[1] = 0.5 * (D3(sm, 1, 1) + D3(sm, 1, 1)) - 1.0;
-            strain[2] = 0.5 * (D3(sm, 2, 2) + D3(sm, 2, 2)) - 1.0;
-            strain[3] = 2.0 * (0.5 * (D3(sm, 0, 1) + D3(sm, 1, 0)));
-            strain[4] = 2.0 * (0.5 * (D3(sm, 1, 2) + D3(sm, 2, 1)));
-            strain[5] = 2.0 * (0.5 * (D3(sm, 2, 0) + D3(sm, 0, 2)));
-            double point[OR_POINT_LEN] = {0};
-            double *ps = &m->plastic[t * 7];
-            for (int i = 0; i < 6; ++i) point[i] = ps[i];
-            point[12] = ps[6];
-            double sv[6], inc[OR_INCR_LEN];
-            or_plastic_update(mat, INFINITY, strain, point, sv, NULL, inc);
-            for (int i = 0; i < 6; ++i) ps[i] = point[i];
-            ps[6] = point[12];
-            for (int i = 0; i < 6; ++i) m->stress[t * 6 + i] = sv[i];
-            const double vol = m->rest_volume[t];
-            dissipation += vol * inc[4];
-            const double pressure = (sv[0] + sv[1] + sv[2]) / 3.0;
-            double density = 0;
-            for (int i = 0; i < 3; ++i) density += 0.5 * sv[i] * ((sv[i] - pressure) / (2.0 * mu) + pressure / (3.0 * bulk));
-            for (int i = 3; i < 6; ++i) density += 0.5 * sv[i] * (sv[i] / mu);
-            strain_energy += vol * density;
-
-            m3d stress;
-            D3(stress, 0, 0) = sv[0];
-            D3(stress, 1, 1) = sv[1];
-            D3(stress, 2, 2) = sv[2];
-            D3(stress, 0, 1) = D3(stress, 1, 0) = sv[3];
-            D3(stress, 1, 2) = D3(stress, 2, 1) = sv[4];
-            D3(stress, 2, 0) = D3(stress, 0, 2) = sv[5];
-            const m3d piola = m3d_mul(&r, &stress);
-            const m3d dmt = m3d_tr(&dm_inv);
-            const m3d h = m3d_mul(&piola, &dmt);
-            const double scale = -vol;
-            double *out = &m->tet_force[t * 12];
-            double f0[3] = {0, 0, 0};
-            for (int c = 0; c < 3; ++c)
-                for (int a = 0; a < 3; ++a) {
-                    const double v = scale * D3(h, a, c);
-                    out[(c + 1) * 3 + a] = v;
-                    f0[a] -= v;
-                }
-            for (int a = 0; a < 3; ++a) out[a] = f0[a];
-        }
+        tet64_loop(m, p, mat, mu, bulk, lf, threads, diss, energy, nw, nk, ng, 0);
+        tet64_loop(m, p, mat, mu, bulk, lf, threads, diss, energy, nw, nk, ng, 1);
+        /* the energy terms in node order, DOF by DOF, as the serial loop adds them */
         double work = 0.0, gwork = 0.0, kinetic = 0.0;
         for (size_t n = 0; n < m->nodes; ++n) {
-            if (m->fixed[n]) {
-                for (int k = 0; k < 3; ++k) m->velocity[n * 3 + k] = 0.0;
-                continue;
-            }
-            double force[3] = {0.0, 0.0, -p->gravity * m->mass[n]};
-            for (uint32_t e = m->adj_offset[n]; e < m->adj_offset[n + 1]; ++e) {
-                const uint32_t entry = m->adj_entry[e];
-                const double *fs = &m->tet_force[(size_t)(entry >> 2) * 12 + (entry & 3u) * 3];
-                for (int k = 0; k < 3; ++k) force[k] += fs[k];
-            }
-            double ext[3] = {0.0, 0.0, 0.0};
-            if (m->fext)
-                for (int k = 0; k < 3; ++k) ext[k] = lf * m->fext[n * 3 + k];
-            for (int k = 0; k < 3; ++k) force[k] += ext[k];
-            const double inv_mass = 1.0 / m->mass[n];
+            if (m->fixed[n]) continue;
             for (int k = 0; k < 3; ++k) {
-                double v = m->velocity[n * 3 + k] + force[k] * inv_mass * p->dt;
-                v *= p->damping;
-                m->velocity[n * 3 + k] = v;
-                m->position[n * 3 + k] += v * p->dt;
-                work += ext[k] * v * p->dt;
-                kinetic += 0.5 * m->mass[n] * v * v;
+                work += nw[n * 3 + k];
+                kinetic += nk[n * 3 + k];
             }
-            gwork += -p->gravity * m->mass[n] * m->velocity[n * 3 + 2] * p->dt;
+            gwork += ng[n];
         }
         m->energy[0] += work;
+        double dissipation = 0.0, strain_energy = 0.0;
+        for (size_t t = 0; t < m->tets; ++t) {
+            dissipation += diss[t];
+            strain_energy += energy[t];
+        }
         m->energy[1] += dissipation;
         m->energy[2] = strain_energy;
         m->energy[3] = kinetic;
         m->energy[4] += gwork;
         ++m->step;
     }
+    free(diss);
+    free(energy);
+    free(nw);
+    free(nk);
+    free(ng);
+}
+
+/* Steps of O-tet64, serial. */
+void or_tet64_step(or_tet64 *m, const or_tet64_params *p, int steps) { tet64_steps(m, p, steps, 1); }
+
+/* The same steps with the element loop over `threads` host threads: bit-identical to
+ * or_tet64_step, for the larger meshes the GPU tests check. */
+void or_tet64_step_threads(or_tet64 *m, const or_tet64_params *p, int steps, int threads) {
+    tet64_steps(m, p, steps, threads);
 }
 
 /* Element eigenvalue bound for a lumped-mass linear tet.  The element's mass matrix
@@ -1543,33 +1634,72 @@ static double fiber_forces(or_shell *m, const double *mat, double *force) {
     return dissipation;
 }
 
-void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int steps) {
+/* The element part of one shell step for element e (zone.cpp:964-973): its forces,
+ * stresses and state, and its dissipation into diss[e] (0 for a torn element). */
+static void shell_element(or_shell *m, const double *mat, size_t e, double *diss) {
+    double rest[24], current[24];
+    for (int a = 0; a < 8; ++a)
+        for (int i = 0; i < 3; ++i) {
+            rest[a * 3 + i] = m->rest[(size_t)m->index[e * 8 + a] * 3 + i];
+            current[a * 3 + i] = m->position[(size_t)m->index[e * 8 + a] * 3 + i];
+        }
+    double *st = m->state + e * OR_SHELL_STATE_LEN;
+    double *out = m->element_force + e * 24;
+    double *stress = m->stress + e * 48;
+    diss[e] = 0.0;
+    if (st[128] != 0.0) {
+        for (int i = 0; i < 24; ++i) out[i] = 0.0;
+        for (int i = 0; i < 48; ++i) stress[i] = 0.0;
+        return;
+    }
+    double info[7];
+    or_shell_plastic_update(m->forms + e * OR_FORMS_LEN, rest, current, mat, st, out, stress, info);
+    diss[e] = info[4];
+}
+
+typedef struct {
+    or_shell *m;
+    const double *mat;
+    size_t begin, end;
+    double *diss;
+} shell_range;
+
+static void *shell_range_run(void *arg) {
+    const shell_range *r = (const shell_range *)arg;
+    for (size_t e = r->begin; e < r->end; ++e) shell_element(r->m, r->mat, e, r->diss);
+    return NULL;
+}
+
+/* Steps of the composed shell step: the element loop (shell_element), over `threads`
+ * host threads when threads > 1, then the gather and the node update.  The element
+ * dissipations are summed in element order, skipping torn elements as the serial loop
+ * does, so every thread count gives the same bits. */
+static void shell_steps(or_shell *m, const double *mat, const or_shell_params *p, int steps, int threads) {
     /* the velocity each driven-edge DOF would have taken had nothing held it */
     double *edge_free = m->prescribed ? (double *)calloc(m->nodes * 3, sizeof(double)) : NULL;
     double *gathered = (double *)malloc(m->nodes * 3 * sizeof(double));
+    double *diss = (double *)malloc((m->elements + 1) * sizeof(double));
+    unsigned char *torn = (unsigned char *)malloc(m->elements + 1);
+    if (!gathered || !diss || !torn) abort();
     for (int s = 0; s < steps && !m->arrested; ++s) {
         const double time = (double)(m->step + 1) * p->dt;
         const double lf = p->rise_time > 0 ? dmin(time / p->rise_time, 1.0) : 1.0;
-        double dissipation = 0.0;
-        for (size_t e = 0; e < m->elements; ++e) {
-            double rest[24], current[24];
-            for (int a = 0; a < 8; ++a)
-                for (int i = 0; i < 3; ++i) {
-                    rest[a * 3 + i] = m->rest[(size_t)m->index[e * 8 + a] * 3 + i];
-                    current[a * 3 + i] = m->position[(size_t)m->index[e * 8 + a] * 3 + i];
-                }
-            double *st = m->state + e * OR_SHELL_STATE_LEN;
-            double *out = m->element_force + e * 24;
-            double *stress = m->stress + e * 48;
-            if (st[128] != 0.0) {
-                for (int i = 0; i < 24; ++i) out[i] = 0.0;
-                for (int i = 0; i < 48; ++i) stress[i] = 0.0;
-                continue;
+        for (size_t e = 0; e < m->elements; ++e) torn[e] = m->state[e * OR_SHELL_STATE_LEN + 128] != 0.0;
+        if (threads > 1) {
+            pthread_t tid[OR_MAX_THREADS];
+            shell_range job[OR_MAX_THREADS];
+            const int n = threads < OR_MAX_THREADS ? threads : OR_MAX_THREADS;
+            for (int k = 0; k < n; ++k) {
+                job[k] = (shell_range){m, mat, m->elements * k / n, m->elements * (k + 1) / n, diss};
+                if (pthread_create(&tid[k], NULL, shell_range_run, &job[k])) abort();
             }
-            double info[7];
-            or_shell_plastic_update(m->forms + e * OR_FORMS_LEN, rest, current, mat, st, out, stress, info);
-            dissipation += info[4];
+            for (int k = 0; k < n; ++k) pthread_join(tid[k], NULL);
+        } else {
+            for (size_t e = 0; e < m->elements; ++e) shell_element(m, mat, e, diss);
         }
+        double dissipation = 0.0;
+        for (size_t e = 0; e < m->elements; ++e)
+            if (!torn[e]) dissipation += diss[e];
         /* the gather (zone.cpp:976-989), then the stiffeners' forces through their ties,
            in fibre order (zone.cpp:990-1002) */
         for (size_t node = 0; node < m->nodes; ++node) {
@@ -1677,6 +1807,19 @@ void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int
     }
     free(edge_free);
     free(gathered);
+    free(diss);
+    free(torn);
+}
+
+/* Steps of the composed shell step (zone.cpp:1086-1252), serial. */
+void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int steps) {
+    shell_steps(m, mat, p, steps, 1);
+}
+
+/* The same steps with the element loop over `threads` host threads: bit-identical to
+ * or_shell_step, for the larger panels the GPU checks use. */
+void or_shell_step_threads(or_shell *m, const double *mat, const or_shell_params *p, int steps, int threads) {
+    shell_steps(m, mat, p, steps, threads);
 }
 
 /* accumulateEnergy, zone.cpp:1014-1044 */

@@ -122,6 +122,7 @@ typedef struct {
 /* Rest state in double from float positions promoted: Dm^-1, |det|/6, rho V/4. */
 void or_tet64_rest_state(or_tet64 *m, double rho);
 void or_tet64_step(or_tet64 *m, const or_tet64_params *p, int steps);
+void or_tet64_step_threads(or_tet64 *m, const or_tet64_params *p, int steps, int threads);
 /* Element eigenvalue bound (lumped mass): largest omega^2 of the element, FP64.
    dt = safety * 2 / sqrt(max). */
 double or_tet64_critical_dt(const or_tet64 *m, double E, double nu, double rho, double safety);
@@ -254,6 +255,7 @@ typedef struct {
 
 void or_shell_setup(or_shell *m, const double *mat, double density);
 void or_shell_step(or_shell *m, const double *mat, const or_shell_params *p, int steps);
+void or_shell_step_threads(or_shell *m, const double *mat, const or_shell_params *p, int steps, int threads);
 void or_shell_energy(or_shell *m, const double *mat);
 
 #ifdef __cplusplus

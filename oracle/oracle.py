@@ -170,11 +170,15 @@ class Oracle:
         if which == "port":
             g("tet64_critical_dt", C.c_double, [C.POINTER(Tet64), C.c_double, C.c_double, C.c_double,
                                                 C.c_double])
+            g("tet64_step_threads", None, [C.POINTER(Tet64), C.POINTER(Tet64Params), C.c_int, C.c_int])
+            g("shell_step_threads", None, [C.POINTER(Shell), f64p, C.POINTER(ShellParams), C.c_int, C.c_int])
         else:
             g("shell_time_parallel", C.c_double, [C.POINTER(Shell), f64p, C.POINTER(ShellParams), C.c_int,
                                                   C.c_int])
             g("default_workers", C.c_uint, [])
             g("tet64_time_parallel", C.c_double, [C.POINTER(Tet64), C.POINTER(Tet64Params), C.c_int, C.c_int])
+            g("tet64_time_batch", C.c_double, [C.POINTER(C.POINTER(Tet64)), C.POINTER(Tet64Params), C.c_size_t,
+                                               C.c_int, C.c_int])
             g("tet32_time", C.c_double, [C.POINTER(Tet32), C.c_float, C.c_float, C.c_float, C.c_float, C.c_int])
             g("zone_sizes", C.c_int, [C.POINTER(ZoneCase), C.POINTER(C.c_size_t)])
             g("zone_run", C.c_int, [C.POINTER(ZoneCase), C.POINTER(ZoneOut)])
@@ -325,8 +329,13 @@ class TetMesh64:
         s.step = 0
         return s
 
-    def step(self, params: Tet64Params, steps: int):
-        self.o.tet64_step(C.byref(self._s), C.byref(params), steps)
+    def step(self, params: Tet64Params, steps: int, threads: int = 1):
+        """`steps` steps; with threads > 1 the element loop runs on that many host
+        threads (restatement only), bit-identical to the serial step."""
+        if threads > 1:
+            self.o.tet64_step_threads(C.byref(self._s), C.byref(params), steps, threads)
+        else:
+            self.o.tet64_step(C.byref(self._s), C.byref(params), steps)
         self.energy[:] = list(self._s.energy)
         self.steps = self._s.step
 
@@ -447,13 +456,40 @@ class ShellModel:
     def punch_work(self):
         return self._s.energy[4]
 
-    def step(self, dt, steps, damping=1.0, rise_time=0.0, punch_speed=0.0, punch_ramp=0.0):
+    def step(self, dt, steps, damping=1.0, rise_time=0.0, punch_speed=0.0, punch_ramp=0.0, threads=1):
+        """`steps` steps; with threads > 1 the element loop runs on that many host
+        threads (restatement only), bit-identical to the serial step."""
         p = ShellParams(dt, damping, rise_time, punch_speed, punch_ramp)
-        self.o.shell_step(C.byref(self._s), self.mat, C.byref(p), steps)
+        if threads > 1:
+            self.o.shell_step_threads(C.byref(self._s), self.mat, C.byref(p), steps, threads)
+        else:
+            self.o.shell_step(C.byref(self._s), self.mat, C.byref(p), steps)
 
     def compute_energy(self):
         self.o.shell_energy(C.byref(self._s), self.mat)
         return self.energy
+
+    def von_mises(self, position, state):
+        """Von Mises stress at each Gauss point, (elements, 8), of a state (positions and
+        the 129-double ElementPlasticState per element) of this model's mesh: the element
+        update (elementPlasticUpdate) run on a copy of each element's state at those
+        positions, so any two states go through the same routine."""
+        pos = np.ascontiguousarray(position, np.float64).reshape(-1, 3)
+        st = np.ascontiguousarray(state, np.float64).reshape(self.elements, -1)
+        idx = self.index.reshape(-1, 8).astype(np.int64)
+        rest = self.rest.reshape(-1, 3)
+        out = np.empty((self.elements, 8))
+        force, stress, info = np.zeros(24), np.zeros(48), np.zeros(7)
+        for e in range(self.elements):
+            cur = np.ascontiguousarray(pos[idx[e]].reshape(-1))
+            r = np.ascontiguousarray(rest[idx[e]].reshape(-1))
+            copy = st[e].copy()
+            self.o.shell_plastic_update(self.forms[e * FORMS_LEN:(e + 1) * FORMS_LEN], r, cur, self.mat, copy, force,
+                                        stress, info)
+            sv = stress.reshape(8, 6)
+            out[e] = np.sqrt(0.5 * ((sv[:, 0] - sv[:, 1]) ** 2 + (sv[:, 1] - sv[:, 2]) ** 2 +
+                                    (sv[:, 2] - sv[:, 0]) ** 2) + 3.0 * (sv[:, 3:] ** 2).sum(1))
+        return out
 
     def time_parallel(self, dt, steps, workers=0, rise_time=0.0):
         p = ShellParams(dt, 1.0, rise_time, 0.0, 0.0)

@@ -413,98 +413,130 @@ void ref_tet64_step(or_tet64* m, const or_tet64_params* p, int steps) {
     }
 }
 
-// The same O-tet64 step with the element loop spread over `workers` host threads by
-// the reference's own core::JobSystem::parallelFor (as zone.cpp:967-973 spreads its
+// One O-tet64 step of mesh m with the element loop spread over the workers of `jobs`
+// by the reference's own core::JobSystem::parallelFor (as zone.cpp:967-973 spreads its
 // element loop) and the node loop serial in CSR order (fem.cpp:196-214).  Per-tet
-// energies go to arrays and are summed in element order, so the result is the same
-// for every worker count.  Returns tets x steps / second.
-double ref_tet64_time_parallel(or_tet64* m, const or_tet64_params* p, int steps, int workers) {
+// energies go to `diss` and are summed in element order, so the result is the same for
+// every worker count.
+static void tet64_parallel_step(or_tet64* m, const or_tet64_params* p, const pl::Material& mat,
+                                core::JobSystem& jobs, std::vector<double>& diss) {
+    const double lf =
+        p->ramp_steps > 0
+            ? std::min(static_cast<double>(m->step + 1) / static_cast<double>(p->ramp_steps), 1.0)
+            : 1.0;
+    jobs.parallelFor(0, m->tets, 256, [&](std::size_t b, std::size_t e_end) {
+        for (std::size_t t = b; t < e_end; ++t) {
+            const uint32_t* idx = &m->index[t * 4];
+            const double* x = m->position;
+            M3d ds{};
+            for (int c = 0; c < 3; ++c)
+                for (int a = 0; a < 3; ++a) ds(a, c) = x[idx[c + 1] * 3 + a] - x[idx[0] * 3 + a];
+            M3d dmInv{};
+            for (int k = 0; k < 9; ++k) dmInv.m[k] = m->rest_inv[t * 9 + k];
+            const M3d f = mul(ds, dmInv);
+            const M3d r = polar(f, p->polar_fixed);
+            const M3d sm = mul(tr(r), f);
+            double strain[6];
+            strain[0] = 0.5 * (sm(0, 0) + sm(0, 0)) - 1.0;
+            strain[1] = 0.5 * (sm(1, 1) + sm(1, 1)) - 1.0;
+            strain[2] = 0.5 * (sm(2, 2) + sm(2, 2)) - 1.0;
+            strain[3] = 2.0 * (0.5 * (sm(0, 1) + sm(1, 0)));
+            strain[4] = 2.0 * (0.5 * (sm(1, 2) + sm(2, 1)));
+            strain[5] = 2.0 * (0.5 * (sm(2, 0) + sm(0, 2)));
+            pl::State st;
+            double* ps = &m->plastic[t * 7];
+            for (int i = 0; i < 6; ++i) st.plasticStrain[i] = ps[i];
+            st.equivalentPlasticStrain = ps[6];
+            double sv[6];
+            const pl::Increment inc = pl::update(mat, pl::kNeverFails, strain, st, sv);
+            for (int i = 0; i < 6; ++i) ps[i] = st.plasticStrain[i];
+            ps[6] = st.equivalentPlasticStrain;
+            diss[t] = m->rest_volume[t] * inc.dissipation;
+            M3d stress{};
+            stress(0, 0) = sv[0];
+            stress(1, 1) = sv[1];
+            stress(2, 2) = sv[2];
+            stress(0, 1) = stress(1, 0) = sv[3];
+            stress(1, 2) = stress(2, 1) = sv[4];
+            stress(2, 0) = stress(0, 2) = sv[5];
+            const M3d h = mul(mul(r, stress), tr(dmInv));
+            const double scale = -m->rest_volume[t];
+            double* out = &m->tet_force[t * 12];
+            double f0[3] = {0, 0, 0};
+            for (int c = 0; c < 3; ++c)
+                for (int a = 0; a < 3; ++a) {
+                    const double v = scale * h(a, c);
+                    out[(c + 1) * 3 + a] = v;
+                    f0[a] -= v;
+                }
+            for (int a = 0; a < 3; ++a) out[a] = f0[a];
+        }
+    });
+    for (size_t t = 0; t < m->tets; ++t) m->energy[1] += diss[t];
+    for (size_t n = 0; n < m->nodes; ++n) {
+        if (m->fixed[n]) {
+            for (int k = 0; k < 3; ++k) m->velocity[n * 3 + k] = 0.0;
+            continue;
+        }
+        double force[3] = {0.0, 0.0, -p->gravity * m->mass[n]};
+        for (uint32_t e = m->adj_offset[n]; e < m->adj_offset[n + 1]; ++e) {
+            const uint32_t entry = m->adj_entry[e];
+            const double* fs = &m->tet_force[(entry >> 2) * 12 + (entry & 3u) * 3];
+            for (int k = 0; k < 3; ++k) force[k] += fs[k];
+        }
+        if (m->fext)
+            for (int k = 0; k < 3; ++k) force[k] += lf * m->fext[n * 3 + k];
+        const double invMass = 1.0 / m->mass[n];
+        for (int k = 0; k < 3; ++k) {
+            double v = m->velocity[n * 3 + k] + force[k] * invMass * p->dt;
+            v *= p->damping;
+            m->velocity[n * 3 + k] = v;
+            m->position[n * 3 + k] += v * p->dt;
+        }
+    }
+    ++m->step;
+}
+
+static pl::Material tet64_material(const or_tet64_params* p) {
     pl::Material mat;
     mat.youngsModulus = p->E;
     mat.poissonRatio = p->nu;
     mat.flow = pl::linearHardening(p->yield, p->hardening);
+    return mat;
+}
+
+// `steps` O-tet64 steps of one mesh over `workers` host threads.  Returns tets x steps
+// / second of the step loop's own clock (thread start-up excluded).
+double ref_tet64_time_parallel(or_tet64* m, const or_tet64_params* p, int steps, int workers) {
+    const pl::Material mat = tet64_material(p);
     core::JobSystem jobs(workers > 1 ? static_cast<unsigned>(workers - 1) : 0u);
     std::vector<double> diss(m->tets);
     const auto begin = std::chrono::steady_clock::now();
-    for (int s = 0; s < steps; ++s) {
-        const double lf =
-            p->ramp_steps > 0
-                ? std::min(static_cast<double>(m->step + 1) / static_cast<double>(p->ramp_steps), 1.0)
-                : 1.0;
-        jobs.parallelFor(0, m->tets, 256, [&](std::size_t b, std::size_t e_end) {
-            for (std::size_t t = b; t < e_end; ++t) {
-                const uint32_t* idx = &m->index[t * 4];
-                const double* x = m->position;
-                M3d ds{};
-                for (int c = 0; c < 3; ++c)
-                    for (int a = 0; a < 3; ++a) ds(a, c) = x[idx[c + 1] * 3 + a] - x[idx[0] * 3 + a];
-                M3d dmInv{};
-                for (int k = 0; k < 9; ++k) dmInv.m[k] = m->rest_inv[t * 9 + k];
-                const M3d f = mul(ds, dmInv);
-                const M3d r = polar(f, p->polar_fixed);
-                const M3d sm = mul(tr(r), f);
-                double strain[6];
-                strain[0] = 0.5 * (sm(0, 0) + sm(0, 0)) - 1.0;
-                strain[1] = 0.5 * (sm(1, 1) + sm(1, 1)) - 1.0;
-                strain[2] = 0.5 * (sm(2, 2) + sm(2, 2)) - 1.0;
-                strain[3] = 2.0 * (0.5 * (sm(0, 1) + sm(1, 0)));
-                strain[4] = 2.0 * (0.5 * (sm(1, 2) + sm(2, 1)));
-                strain[5] = 2.0 * (0.5 * (sm(2, 0) + sm(0, 2)));
-                pl::State st;
-                double* ps = &m->plastic[t * 7];
-                for (int i = 0; i < 6; ++i) st.plasticStrain[i] = ps[i];
-                st.equivalentPlasticStrain = ps[6];
-                double sv[6];
-                const pl::Increment inc = pl::update(mat, pl::kNeverFails, strain, st, sv);
-                for (int i = 0; i < 6; ++i) ps[i] = st.plasticStrain[i];
-                ps[6] = st.equivalentPlasticStrain;
-                diss[t] = m->rest_volume[t] * inc.dissipation;
-                M3d stress{};
-                stress(0, 0) = sv[0];
-                stress(1, 1) = sv[1];
-                stress(2, 2) = sv[2];
-                stress(0, 1) = stress(1, 0) = sv[3];
-                stress(1, 2) = stress(2, 1) = sv[4];
-                stress(2, 0) = stress(0, 2) = sv[5];
-                const M3d h = mul(mul(r, stress), tr(dmInv));
-                const double scale = -m->rest_volume[t];
-                double* out = &m->tet_force[t * 12];
-                double f0[3] = {0, 0, 0};
-                for (int c = 0; c < 3; ++c)
-                    for (int a = 0; a < 3; ++a) {
-                        const double v = scale * h(a, c);
-                        out[(c + 1) * 3 + a] = v;
-                        f0[a] -= v;
-                    }
-                for (int a = 0; a < 3; ++a) out[a] = f0[a];
-            }
-        });
-        for (size_t t = 0; t < m->tets; ++t) m->energy[1] += diss[t];
-        for (size_t n = 0; n < m->nodes; ++n) {
-            if (m->fixed[n]) {
-                for (int k = 0; k < 3; ++k) m->velocity[n * 3 + k] = 0.0;
-                continue;
-            }
-            double force[3] = {0.0, 0.0, -p->gravity * m->mass[n]};
-            for (uint32_t e = m->adj_offset[n]; e < m->adj_offset[n + 1]; ++e) {
-                const uint32_t entry = m->adj_entry[e];
-                const double* fs = &m->tet_force[(entry >> 2) * 12 + (entry & 3u) * 3];
-                for (int k = 0; k < 3; ++k) force[k] += fs[k];
-            }
-            if (m->fext)
-                for (int k = 0; k < 3; ++k) force[k] += lf * m->fext[n * 3 + k];
-            const double invMass = 1.0 / m->mass[n];
-            for (int k = 0; k < 3; ++k) {
-                double v = m->velocity[n * 3 + k] + force[k] * invMass * p->dt;
-                v *= p->damping;
-                m->velocity[n * 3 + k] = v;
-                m->position[n * 3 + k] += v * p->dt;
-            }
-        }
-        ++m->step;
-    }
+    for (int s = 0; s < steps; ++s) tet64_parallel_step(m, p, mat, jobs, diss);
     const auto end = std::chrono::steady_clock::now();
     return static_cast<double>(m->tets) * steps / std::chrono::duration<double>(end - begin).count();
+}
+
+// `steps` steps of a batch of independent meshes, as the reference solves them: one
+// mesh at a time (it steps one mesh per solver, fem.cpp:187), each mesh's element loop
+// over `workers` host threads.  Step s of every mesh is taken before step s + 1 of any,
+// so one timed step is one time step of the whole batch.  Returns the seconds of the
+// step loop's own clock (thread start-up excluded).
+double ref_tet64_time_batch(or_tet64* const* meshes, const or_tet64_params* params, size_t count, int steps,
+                            int workers) {
+    std::vector<pl::Material> mats;
+    size_t most = 0;
+    for (size_t i = 0; i < count; ++i) {
+        mats.push_back(tet64_material(&params[i]));
+        most = std::max(most, meshes[i]->tets);
+    }
+    core::JobSystem jobs(workers > 1 ? static_cast<unsigned>(workers - 1) : 0u);
+    std::vector<double> diss(most);
+    const auto begin = std::chrono::steady_clock::now();
+    for (int s = 0; s < steps; ++s)
+        for (size_t i = 0; i < count; ++i) tet64_parallel_step(meshes[i], &params[i], mats[i], jobs, diss);
+    const auto end = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(end - begin).count();
 }
 
 // --- solid-shell -------------------------------------------------------------

@@ -295,6 +295,24 @@ int rebuild(femstep_pool* p) {
     return check(p, cudaGetLastError(), "work list upload");
 }
 
+// The graph of kGraphSteps steps over the current work list, captured once (nothing
+// runs while it is captured).
+int ensure_graph(femstep_pool* p, bool staged) {
+    if (p->graph && p->graph_staged != staged) drop_graph(p);
+    if (p->graph) return FEMSTEP_OK;
+    cudaGraph_t g = nullptr;
+    int rc = check(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "capture");
+    if (rc) return rc;
+    fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream, staged);
+    rc = check(p, cudaStreamEndCapture(p->stream, &g), "capture end");
+    if (rc) return rc;
+    rc = check(p, cudaGraphInstantiate(&p->graph, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    if (rc) return rc;
+    p->graph_staged = staged;
+    return FEMSTEP_OK;
+}
+
 int launch_chunk(femstep_pool* p, int steps, int mode) {
     if (steps <= 0 || p->d.n_etiles == 0) return FEMSTEP_OK;
     const bool staged = mode == FEMSTEP_POOL_GRAPH_STAGED;
@@ -309,18 +327,8 @@ int launch_chunk(femstep_pool* p, int steps, int mode) {
     }
     int left = steps;
     if (left >= kGraphSteps) {
-        if (!p->graph) {
-            cudaGraph_t g = nullptr;
-            int rc = check(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "capture");
-            if (rc) return rc;
-            fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream, staged);
-            rc = check(p, cudaStreamEndCapture(p->stream, &g), "capture end");
-            if (rc) return rc;
-            rc = check(p, cudaGraphInstantiate(&p->graph, g, 0), "graph instantiate");
-            cudaGraphDestroy(g);
-            if (rc) return rc;
-            p->graph_staged = staged;
-        }
+        const int rc = ensure_graph(p, staged);
+        if (rc) return rc;
         for (; left >= kGraphSteps; left -= kGraphSteps) {
             const int rc = check(p, cudaGraphLaunch(p->graph, p->stream), "graph launch");
             if (rc) return rc;
@@ -386,8 +394,12 @@ int wait_chunk(femstep_pool* p, double* gpu_ms) {
     int rc = check(p, cudaEventSynchronize(p->ev1), "pool step");
     if (rc) return rc;
     if (*p->h_error) {
+        // a grid barrier or a staged tile's copies gave up: the launch's outputs are
+        // undefined, so the pool takes no further step
         p->broken = true;
-        return fail(p, FEMSTEP_ETIMEOUT, "a grid barrier of the persistent launch gave up waiting");
+        return fail(p, FEMSTEP_ETIMEOUT, "a device-side wait gave up (a grid barrier of the persistent launch, or a "
+                                         "staged tile's copies); the pool's state is undefined and it takes no "
+                                         "further step");
     }
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, p->ev0, p->ev1);
@@ -957,6 +969,18 @@ int femstep_pool_run_async(femstep_pool* p, int steps, int mode) {
     if (rc) return rc;
     p->in_flight = true;
     return FEMSTEP_OK;
+}
+
+int femstep_pool_prepare(femstep_pool* p) {
+    if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
+    if (p->broken) return fail(p, FEMSTEP_ESTATE, "the pool stopped after a device wait gave up");
+    if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
+    int rc = rebuild(p);
+    if (rc) return rc;
+    if (p->d.n_etiles > 0 && p->mode != FEMSTEP_POOL_PERSISTENT)
+        rc = ensure_graph(p, p->mode == FEMSTEP_POOL_GRAPH_STAGED);
+    if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "prepare");
+    return rc;
 }
 
 int femstep_pool_wait(femstep_pool* p, double* gpu_ms) {

@@ -22,6 +22,13 @@
 // race on it; calls on one stream are ordered and safe.  It keeps the last call's
 // contents; nothing needs clearing because each step writes every tet's twelve slots
 // before the node pass reads them.
+//
+// The array's device address belongs to one CUDA context.  The first call in a
+// context looks it up (cudaGetSymbolAddress, with that context's device current) and
+// keeps it keyed on the context's process-unique id, so a new context on the same
+// device -- after cudaDeviceReset, or a caller's own driver-API context -- gets its
+// own lookup.  Make that first call outside any stream capture.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,10 +48,14 @@ namespace {
 constexpr long long kNoAllocMaxTets = 65536;
 constexpr int kMaxDevices = 64;
 
-// Device address of g_force_scratch per device, looked up once with that device
-// current.  In host code the symbol is only a host-side stand-in and must never be
-// handed to a kernel.
-float* g_scratch_ptr[kMaxDevices] = {};
+// Device address of g_force_scratch per device, looked up with that device current
+// and kept with the id of the context it belongs to.  In host code the symbol is only
+// a host-side stand-in and must never be handed to a kernel.
+struct ScratchAddress {
+    unsigned long long context = 0;  // cuCtxGetId of the context the address is valid in
+    float* ptr = nullptr;
+};
+ScratchAddress g_scratch[kMaxDevices];
 std::mutex g_scratch_mutex;
 
 __device__ __forceinline__ M3<float> polar4(const M3<float>& f) {
@@ -136,6 +147,32 @@ __global__ void __launch_bounds__(kBlock) noalloc_nodes(femstep_tet_device_mesh 
     }
 }
 
+// The id of the current context, through the driver's entry points as the runtime
+// hands them out (no link to the driver library).  0 when there is none.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(fn);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
 int scratch_for_current_device(float** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -147,17 +184,23 @@ int scratch_for_current_device(float** out) {
         set_last_error("device ordinal beyond the no-allocation entry point's table");
         return FEMSTEP_EINVAL;
     }
+    // Before the runtime's first use of the device there is no current context (id 0):
+    // the lookup then brings it up, and the address is kept under its id.  If the
+    // context cannot be named at all, the address is looked up on every call.
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
+    ScratchAddress& slot = g_scratch[dev];
+    if (!slot.ptr || ctx == 0 || slot.context != ctx) {
         float* p = nullptr;
         e = cudaGetSymbolAddress((void**)&p, ::g_force_scratch);
         if (e != cudaSuccess || !p) {
             set_last_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             return FEMSTEP_ECUDA;
         }
-        g_scratch_ptr[dev] = p;
+        slot.ptr = p;
+        slot.context = ctx ? ctx : current_context_id();
     }
-    *out = g_scratch_ptr[dev];
+    *out = slot.ptr;
     return FEMSTEP_OK;
 }
 
@@ -187,8 +230,21 @@ int femstep_tet_step_noalloc(const femstep_tet_device_mesh* mesh, int substeps, 
         fs::set_last_error("negative step count or non-positive dt");
         return FEMSTEP_EINVAL;
     }
+    if (params->yield_strength > 0.0 || params->hardening_modulus != 0.0 || params->ramp_steps != 0) {
+        fs::set_last_error("femstep_tet_step_noalloc is the elastic REF32 step: yield_strength, hardening_modulus "
+                           "and ramp_steps must be 0");
+        return FEMSTEP_EINVAL;
+    }
     const int dev = fs::device_status();
     if (dev != FEMSTEP_OK) return dev;
+    // an error left by an earlier call on this thread is reported as such, not as this
+    // call's launch failure
+    const cudaError_t pending = cudaGetLastError();
+    if (pending != cudaSuccess) {
+        fs::set_last_error(std::string("a CUDA error from before this call was pending: ") +
+                           cudaGetErrorString(pending));
+        return FEMSTEP_ECUDA;
+    }
     float* scratch = nullptr;
     const int rc = fs::scratch_for_current_device(&scratch);
     if (rc) return rc;

@@ -71,7 +71,8 @@ class Server:
     """Continuous batching over `pool` (a femstep.TetPool or anything with its face).
 
     clock: seconds since an arbitrary origin (time.perf_counter by default).
-    keep_results: read each finished solve back (positions, velocities) before release.
+    keep_results: read each finished solve back before release: (positions, velocities),
+                  and its plastic state where the pool keeps one.
     full_error: the exception the pool raises when a mesh does not fit now.
     """
 
@@ -184,6 +185,8 @@ class Server:
                     continue
                 if self.keep_results:
                     r.result = self.pool.readback(mid)
+                    if hasattr(self.pool, "plastic"):
+                        r.result = tuple(r.result) + (self.pool.plastic(mid),)
                 self.pool.release(mid)
                 r.finished = now()
                 report.completed += 1

@@ -1,7 +1,10 @@
 """Seeded synthetic tet meshes for the batched and the served step.
 
+This module loads no native library (numpy only), so the CPU baselines can build the
+workload without the GPU library.
+
 No dataset is involved: every mesh is a Kuhn-split box (fem::makeBoxTetMesh,
-engine/sim/fem.cpp:217-263, restated in femstep.box_tet_mesh) of steel, shaped as a
+engine/sim/fem.cpp:217-263, restated in meshes.box_tet_mesh) of steel, shaped as a
 beam or a plate, with a seeded size, material, clamped face and load.
 
   batch_meshes     many meshes with tet counts log-uniform in [lo, hi], yield uniform
@@ -18,11 +21,17 @@ from dataclasses import dataclass
 
 import numpy as np
 
-import femstep as F
+import meshes as M
 
 DENSITY = 7850.0
 YOUNGS = 210e9
 POISSON = 0.3
+# The Kuhn tet meshes here first yield at about 2.5 times the load that yields a beam
+# of the same section (FP64 oracle, 1,000-step ramp plus 1,000 steps: plates at 2x the
+# beam's load stay elastic or nearly so, at 4x a fifth to a half of their tets yield;
+# beams yield from about 1.5x).  Scaled by U[0.5, 2], the batch then runs from
+# elastic meshes to meshes with most of their tets yielded.
+LOCKING = 2.5
 
 
 @dataclass
@@ -100,7 +109,7 @@ def random_spec(rng: np.random.Generator, lo: float, hi: float, seed: int) -> Me
 def build(spec: MeshSpec) -> BuiltMesh:
     nx, ny, nz = spec.cells
     lx, ly, lz = spec.size
-    pos, idx = F.box_tet_mesh(lx, ly, lz, nx, ny, nz)
+    pos, idx = M.box_tet_mesh(lx, ly, lz, nx, ny, nz)
     p = pos.reshape(-1, 3).astype(np.float64)
     axis = 0 if spec.clamp[0] == "x" else 1
     at_max = spec.clamp[1] == "1"
@@ -108,9 +117,11 @@ def build(spec: MeshSpec) -> BuiltMesh:
     eps = 1e-6 * extent
     clamped = (p[:, axis] > extent - eps) if at_max else (p[:, axis] < eps)
     fixed = clamped.astype(np.uint32)
-    # first-yield load of the clamped section, as a cantilever of span `extent`
+    # first-yield load of the clamped section, as a cantilever of span `extent`, times
+    # the mesh's stiffening: linear tets one to a few cells deep are several times
+    # stiffer in bending than the beam, so their clamped section yields later
     width = (ly, lx)[axis]
-    m_yield = spec.yield_strength * width * lz * lz / 6.0  # yield x elastic section modulus
+    m_yield = LOCKING * spec.yield_strength * width * lz * lz / 6.0  # yield x elastic section modulus
     fext = np.zeros_like(p)
     if spec.load_kind == "tip":
         tip = (p[:, axis] < eps) if at_max else (p[:, axis] > extent - eps)
@@ -132,6 +143,24 @@ def batch_meshes(count=256, lo=2e3, hi=2e5, seed=20261203, steps=0, ramp_steps=1
         s.steps, s.ramp_steps = steps, ramp_steps
         specs.append(s)
     return specs
+
+
+def drift_sample(specs):
+    """Indices of eight meshes of a batch that between them cover its variety: the
+    largest, and the smallest plate of each clamped face and load kind (x0, x1, y0, y1;
+    tip and pressure) whose load factor is above 1.2, so that most of them yield.  The
+    precision checks of the batched step run these."""
+    def plate(s):
+        return s.cells[1] > s.cells[2]
+
+    picks = [max(range(len(specs)), key=lambda i: specs[i].tets)]
+    for clamp, kind in (("x0", "tip"), ("x0", "pressure"), ("x1", "tip"), ("y0", "tip"), ("y0", "pressure"),
+                        ("y1", "tip"), ("y1", "pressure")):
+        c = [i for i, s in enumerate(specs) if plate(s) and s.clamp == clamp and s.load_kind == kind
+             and s.load_factor > 1.2 and i not in picks]
+        if c:
+            picks.append(min(c, key=lambda i: specs[i].tets))
+    return picks
 
 
 def request_trace(rate=40.0, duration=120.0, lo=1e3, hi=5e5, steps=(500, 5000), seed=20261204):

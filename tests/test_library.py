@@ -82,3 +82,19 @@ def test_plate_mesher_matches_reference_generator(fem, port):
             ref = np.zeros(a[0].size)
             port.plate_pressure_load(b[0], b[1], b[0].size // 3, b[1].size // 8, 2.5e5, ref)
             assert np.allclose(load, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def test_workload_builders_load_no_gpu_library():
+    """The workload generators and the oracle's batch (the CPU baselines' inputs) never
+    load libfemstep.so, so the reference arm of the benchmark runs without it."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.path[:0] = [%r, %r, %r]\n"
+            "import workloads as W, meshes, oracle\n"
+            "b = W.build(W.batch_meshes(3)[0]); meshes.stiffened_panel(nx=4, ny=3, lx=0.04, ly=0.03)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'femstep' not in sys.modules and 'libfemstep' not in maps\n"
+            "print('clean')\n") % (os.path.join(ROOT, "sinking-simulator_b200"), os.path.join(ROOT, "oracle"), ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "clean" in r.stdout, r.stderr

@@ -181,3 +181,34 @@ def test_port_matches_compiled_reference(port, ref):
             for x, y in zip(o, r):
                 assert np.array_equal(x, y)
             assert np.array_equal(sa, sb)
+
+
+def test_threaded_steps_are_the_serial_steps(port):
+    """The restatement's threaded O-tet64 and shell steps (element and node loops over
+    host threads, energy terms summed in element and node order) give the serial
+    steps' bits: the GPU tests use them for their larger meshes."""
+    import meshes as M
+
+    pos, idx = M.box_tet_mesh(0.4, 0.1, 0.05, 16, 4, 2)
+    fixed = (pos[0::3] < 1e-6).astype(np.uint32)
+    tip = pos[0::3] > 0.4 - 1e-6
+    fext = np.zeros(pos.size)
+    fext[2::3][tip] = -2.5e5 / tip.sum()
+    a, b = (O.TetMesh64(port, pos, idx, fixed, fext) for _ in range(2))
+    dt = port.tet64_critical_dt(C.byref(a._s), 210e9, 0.3, 7850.0, 0.9)
+    p = O.tet64_params(dt=dt, ramp_steps=100, gravity=9.81)
+    a.step(p, 300)
+    b.step(p, 300, threads=5)
+    assert (a.plastic.reshape(-1, 7)[:, 6] > 0).any(), "the case must yield"
+    assert np.array_equal(a.position, b.position) and np.array_equal(a.velocity, b.velocity)
+    assert np.array_equal(a.plastic, b.plastic) and np.array_equal(a.energy, b.energy)
+
+    rest, index, pinned, load = M.stiffened_panel(nx=12, ny=8, lx=0.12, ly=0.08, thickness=0.004, stiffeners=1,
+                                                  imperfection=2e-4, peak_pressure=6e7, radius=0.02)
+    mat = O.material(E=206e9, nu=0.3, yield_=355e6, hardening=1e9)
+    s, t = (O.ShellModel(port, rest, index, pinned, mat, fext=load) for _ in range(2))
+    s.step(5e-7, 400, rise_time=1e-4)
+    t.step(5e-7, 400, rise_time=1e-4, threads=3)
+    assert (s.state.reshape(-1, 129)[:, 12:120:15] > 0).any(), "the case must yield"
+    assert np.array_equal(s.position, t.position) and np.array_equal(s.velocity, t.velocity)
+    assert np.array_equal(s.state, t.state, equal_nan=True) and np.array_equal(s.energy, t.energy)

@@ -8,6 +8,7 @@ reference's tet kinematics with plasticity::update, in double) each mesh keeps t
 target tolerance: 1e-5 relative displacement and energy within 0.5 %.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -236,6 +237,54 @@ def test_pool_meshes_against_fp64_oracle(fem, port, k):
     assert abs(e[0] - er[0]) / er[0] < 5e-3
     for j in (1, 2, 3):
         assert abs(e[j] - er[j]) <= 5e-3 * er[0]
+
+
+def test_workload_meshes_against_fp64_oracle(fem, port):
+    """Eight meshes of the batched workload itself (workloads.batch_meshes as the bench
+    draws it; workloads.drift_sample picks them): the largest, a 197,106-tet beam under
+    pressure, and the smallest plate of each clamped face and load kind -- x0, x1, y0,
+    y1, tip and pressure -- all in one pool for the 1,000-step ramp plus 1,000 steps.
+    Each against O-tet64 (in double, on all host cores): 1e-5 relative displacement, and
+    every energy term within 0.5 % of the external work."""
+    import workloads as W
+
+    specs = W.batch_meshes(256)
+    picks = W.drift_sample(specs)
+    assert len(picks) == 8
+    chosen = [specs[i] for i in picks]
+    assert {s.clamp for s in chosen} == {"x0", "x1", "y0", "y1"}
+    assert sum(s.load_kind == "pressure" and s.cells[1] > s.cells[2] for s in chosen) >= 2
+    assert max(s.tets for s in chosen) > 190000
+    built = [W.build(sp) for sp in chosen]
+    threads = os.cpu_count() or 1
+    refs, dts = [], []
+    for b in built:
+        r = O.TetMesh64(port, b.position, b.index, b.fixed, b.external_force)
+        dt = port.tet64_critical_dt(C.byref(r._s), W.YOUNGS, W.POISSON, W.DENSITY, 0.9)
+        r.step(O.tet64_params(dt=dt, ramp_steps=1000, yield_=b.spec.yield_strength, hardening=b.spec.hardening),
+               2000, threads=threads)
+        refs.append(r)
+        dts.append(dt)
+    T = sum(sp.tets for sp in chosen)
+    N = sum(sp.nodes for sp in chosen)
+    pool = fem.TetPool(T, N + len(chosen) + 1, max_meshes=len(chosen) + 1)
+    ids = [pool.admit(steps=2000, dt=dt, **b.admit_kwargs()) for b, dt in zip(built, dts)]
+    for chunk in (1000, 7, 993):
+        pool.run(chunk)
+    yielded = []
+    for b, r, i in zip(built, refs, ids):
+        assert pool.status(i)[0] == 2000
+        p, _ = pool.readback(i)
+        rest = b.position.astype(np.float64)
+        u, ur = p - rest, r.position - rest
+        err = np.abs(u - ur).max() / np.abs(ur).max()
+        assert err < 1e-5, (b.spec, err)
+        e, er = pool.energy(i), r.energy
+        for j in (0, 1, 2, 3):
+            assert abs(e[j] - er[j]) <= 5e-3 * er[0], (b.spec, j, e, er)
+        yielded.append((r.plastic.reshape(-1, 7)[:, 6] > 0).mean())
+    assert sum(y > 0.01 for y in yielded) >= 5, yielded
+    pool.close()
 
 
 def test_evict_and_resume_is_bit_identical(fem):
