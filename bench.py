@@ -559,7 +559,7 @@ def pool_drift(F, W, specs, steps=2000):
     pool.run(steps)
 
     def balance(e):
-        w = e[0] + e[4]
+        w = e[0] + (e[4] if len(e) > 4 else 0.0)  # external work, and gravity's where it is kept
         return abs(w - (e[1] + e[2] + e[3])) / abs(w)
 
     rows = []

@@ -315,7 +315,9 @@ typedef struct {
     double dt, damping;                        /* SolveParams::timestep / damping (zone.hpp:698-699) */
     double rise_time;                          /* load factor min((step+1) dt / rise, 1); 0 = full */
     int max_iterations;                        /* EAS Newton cap (CPU: 40) */
-    double tol_residual, tol_work;             /* Newton stops on ||r|| or |delta.r| below tol * sigma_y V */
+    double tol_residual, tol_work;             /* Newton stops on ||r|| or |delta.r| below tol * sigma_y V
+                                                  (0: the reference's 1e-12 and 1e-16), or once ||r|| is at
+                                                  FP32 rounding (16 ulps of the magnitude of its terms) */
     int compensated;                           /* 1: Kahan-compensated displacement and plastic strain */
     const femstep_shell_material *material;    /* NULL: the linear law, no back stress, no damage;
                                                   else the general law and the element failure rules

@@ -97,8 +97,9 @@ ShellParams make_params(const femstep_shell_params& p) {
     q.damping64 = p.damping;
     q.rise_time = p.rise_time;
     q.max_iterations = p.max_iterations > 0 ? p.max_iterations : 12;
-    q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 5e-5);
-    q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-13);
+    // the reference's tolerances (solid_shell.cpp:939, 988) unless the caller gives its own
+    q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 1e-12);
+    q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-16);
     q.compensated = p.compensated;
     // the fibres' law in double: the same material, linear unless the curve is Swift
     q.fiber.youngs = E;

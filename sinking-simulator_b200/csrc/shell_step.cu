@@ -30,6 +30,10 @@
 namespace fs {
 namespace {
 
+// The EAS residual's rounding floor in FP32, relative to the magnitude of its terms:
+// sixteen ulps of 1.
+constexpr float kResidualFloor = 16.0f * 1.1920929e-7f;
+
 __device__ __forceinline__ float sum8(float v) {
     v += __shfl_xor_sync(0xffffffffu, v, 1);
     v += __shfl_xor_sync(0xffffffffu, v, 2);
@@ -514,6 +518,11 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     // element volume and the energy scale sigma_y V
     const float volume = sum8(w);
     const float scale = p.yield * volume;
+    // the size of this point's enhanced operator, for the residual's rounding floor
+    float gnorm = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 7; ++j) gnorm += gc[j] * gc[j];
+    gnorm = sqrtf(gnorm);
 
     // ---- start-of-step state ----
     const size_t sbase = (size_t)group * kShellStateQ * 32 + lane;
@@ -568,6 +577,17 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
 #pragma unroll
             for (int j = 0; j < 7; ++j) r[j] = sum8(gc[j] * tau[kj[j]]);
         }
+        // The rounding floor of the residual in FP32: a few ulps of the magnitude of its
+        // terms, sum_g w |sigma_g| |gc_g| (T0's columns are unit vectors).  A residual
+        // there is as converged as single precision allows; the tolerances below are
+        // the reference's, scaled by sigma_y V, and reach far below it at low stress.
+        float rfloor;
+        {
+            float sn = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) sn += o.sigma[i] * o.sigma[i];
+            rfloor = kResidualFloor * sum8(w * sqrtf(sn) * gnorm);
+        }
         if (!done && !eas_on) {  // no enhanced modes: one evaluation is the update
             converged = true;
             done = true;
@@ -576,7 +596,7 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             float rn = 0.0f;
 #pragma unroll
             for (int k = 0; k < 7; ++k) rn += r[k] * r[k];
-            if (sqrtf(rn) <= p.tol_residual * scale) {
+            if (sqrtf(rn) <= fmaxf(p.tol_residual * scale, rfloor)) {
                 converged = true;
                 done = true;
             } else if (iteration + 1 >= p.max_iterations) {

@@ -337,7 +337,7 @@ class ShellSolver:
             _raise(rc, _sh_error(self._h))
 
     def params(self, youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9, dt=1e-7, damping=1.0,
-               rise_time=0.0, max_iterations=12, tol_residual=5e-5, tol_work=1e-13, compensated=True, material=None):
+               rise_time=0.0, max_iterations=12, tol_residual=1e-12, tol_work=1e-16, compensated=True, material=None):
         """material: None (the linear law) or a dict of femstep_shell_material fields
         (hardening=SHELL_SWIFT|SHELL_LINEAR, strength_coefficient, reference_strain,
         hardening_exponent, kinematic_modulus, triaxiality_sensitivity,

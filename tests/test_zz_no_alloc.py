@@ -208,15 +208,17 @@ state = (g["start"].astype(np.float32), np.zeros(g["start"].size, np.float32))
 state = run_in_current_context(10, state)
 ref.run(10, youngs=210e9, poisson=0.3, dt=dt, gravity=9.80665, damping=1.0)
 assert all(np.array_equal(a, b) for a, b in zip(state, ref.readback())), "primary context"
-# 2: a context of the caller's own
+# 2: a context of the caller's own, current while the entry point runs; the allocating
+# handle lives in the library's context, so that one is current again for it
 ctx = C.c_void_p()
 ok(cu.cuCtxCreate_v2(C.byref(ctx), 0, dev), "cuCtxCreate")
 state = run_in_current_context(10, state)
+old = C.c_void_p()
+ok(cu.cuCtxPopCurrent_v2(C.byref(old)), "cuCtxPopCurrent")
+assert old.value == ctx.value
 ref.run(10, youngs=210e9, poisson=0.3, dt=dt, gravity=9.80665, damping=1.0)
 assert all(np.array_equal(a, b) for a, b in zip(state, ref.readback())), "caller's context"
 # 3: back in the primary context
-old = C.c_void_p()
-ok(cu.cuCtxPopCurrent_v2(C.byref(old)), "cuCtxPopCurrent")
 state = run_in_current_context(10, state)
 ok(cu.cuCtxDestroy_v2(ctx), "cuCtxDestroy")
 ref.run(10, youngs=210e9, poisson=0.3, dt=dt, gravity=9.80665, damping=1.0)
