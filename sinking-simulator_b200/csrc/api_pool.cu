@@ -734,6 +734,7 @@ int femstep_pool_create(size_t tet_capacity, size_t node_capacity, int max_meshe
     if (tile != 128 && tile != 256 && tile != 512) return fail(nullptr, FEMSTEP_EINVAL, "tile must be 128, 256 or 512");
     const int dev = fs::device_status();
     if (dev != FEMSTEP_OK) return dev;
+    fs::pool_kernels_setup();
     femstep_pool* p = new femstep_pool();
     // rows of 4-byte per-tet data start on 16-byte boundaries (bulk copies need them)
     tet_capacity = (tet_capacity + 3) & ~size_t(3);

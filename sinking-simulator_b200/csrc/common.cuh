@@ -37,12 +37,18 @@ __device__ __forceinline__ double block_sum(double v, double* scratch /* >= 32 *
 
 // Two deterministic block sums in one pass (one pair of barriers): the same order as
 // block_sum for each.  scratch >= 64 doubles.
+// The warp part of block_sum2: each of a and b summed over the warp into lane 0.
+__device__ __forceinline__ void warp_sum2(double& a, double& b) {
+    // a warp whose `a` values are all zero (no tet yielded) has the sum zero already
+    if (__any_sync(0xffffffffu, a != 0.0)) {
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    }
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_down_sync(0xffffffffu, b, o);
+}
+
 __device__ __forceinline__ void block_sum2(double& a, double& b, double* scratch) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-    }
+    warp_sum2(a, b);
     if (lane == 0) {
         scratch[warp] = a;
         scratch[32 + warp] = b;

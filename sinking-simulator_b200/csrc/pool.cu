@@ -76,67 +76,113 @@ __global__ void __launch_bounds__(B, 1024 / B) pool_elements(PoolDevice d, int s
     element_tile<false>(d, blockIdx.x, sub, scratch, blockIdx.x + wave);
 }
 
-// The element pass with each tile's own rows staged in shared memory: one thread arms
-// an mbarrier and issues 19 bulk copies (node ids, slot map, 9 rows of Dm^-1, volume,
-// 7 rows of plastic state); the block then reads them from shared memory.  The 4-byte
-// rows are copied from the tile's first tet rounded down to a multiple of 4 (the pool's
-// row stride is a multiple of 4, so every copy starts on a 16-byte boundary) to its last
-// rounded up; the extra tets are never used.  The wait is bounded: a tile whose copies
-// do not land in time sets the pool's error flag, waits (bounded) for its copies to
-// finish, and is skipped.  B is 128 or 256 (static shared memory).
+// The bound on a wait for a tile's staged rows: a few million polls (seconds), far
+// beyond any copy's time; a wait that runs out is reported, never waited out.
 constexpr uint32_t kStageWaitPolls = 1u << 22;
 
+// The element pass on a persistent grid with each tile's own rows staged into shared
+// memory one tile ahead: block b takes tiles b, b + grid, b + 2 grid, ...  While the
+// block computes one tile, its thread 0 has already queued the bulk copies of the next
+// tile's rows (node ids, slot map, Dm^-1, volume, plastic state: the 19 copies of
+// stage_tile_rows) into the other of two buffers, completed on that buffer's mbarrier.
+// So the rows' DRAM latency runs behind a whole tile's arithmetic, and a tet finds its
+// own rows in shared memory; only the corner displacements are read from global
+// memory (mostly L1 hits: the tets of a tile share their nodes).  A buffer is refilled
+// only after the barrier that ends the tile which read it.  Waits are bounded: a tile
+// whose copies do not land sets the pool's error flag and is skipped, and the launch
+// still ends (the host then reports FEMSTEP_ETIMEOUT and retires the pool).  The
+// arithmetic is tet_element_f32's, so the results are the plain pass's to the bit.
 template <int B>
-__global__ void __launch_bounds__(B, 1024 / B) pool_elements_staged(PoolDevice d, int sub, int wave) {
-    constexpr int kPitch = B + 4;
-    __shared__ double scratch[64];
-    __shared__ __align__(16) uint4 s_idx[B];
-    __shared__ __align__(16) uint4 s_slot[B];
-    __shared__ __align__(16) float s_rows[17 * kPitch];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_ok;
-    {
-        const int ahead = blockIdx.x + wave;
-        if (ahead < d.n_etiles) {
-            const PoolTile nx = d.etiles[ahead];
-            prefetch_tet_rows(element_refs(d), nx.begin, nx.end);
-        }
-    }
-    const PoolTile tl = d.etiles[blockIdx.x];
+struct RingStage {
+    static constexpr int kPitch = B + 4;
+    uint4 idx[B];
+    uint4 slot[B];
+    float rows[17 * kPitch];
+};
+
+// Thread 0: queue the copies of `tile`'s rows into stage `st` (or arrive with nothing,
+// for a frozen mesh's tile).
+template <int B>
+__device__ __forceinline__ void stage_tile_rows(const PoolDevice& d, int tile, int sub, RingStage<B>& st,
+                                                uint64_t* bar) {
+    const PoolTile tl = d.etiles[tile];
     const PoolMesh& m = d.meshes[tl.mesh];
-    const bool live = m.step + sub < m.target;  // the same in every thread of the block
-    double diss = 0.0, energy = 0.0;
+    if (!(m.step + sub < m.target)) {
+        mbar_arrive(bar);
+        return;
+    }
     const long long first = tl.begin, n = tl.end - tl.begin;
     const long long base = first & ~3LL, last4 = (tl.end + 3) & ~3LL;
-    if (live) {
-        if (threadIdx.x == 0) {
-            const uint32_t row_bytes = (uint32_t)((last4 - base) * 4);
-            mbar_init(&bar, 1);
-            mbar_arrive_expect_tx(&bar, 2u * (uint32_t)n * 16u + 17u * row_bytes);
-            bulk_copy_g2s(s_idx, d.index + first, (uint32_t)n * 16u, &bar);
-            bulk_copy_g2s(s_slot, d.slot + first, (uint32_t)n * 16u, &bar);
-            for (int k = 0; k < 9; ++k)
-                bulk_copy_g2s(s_rows + k * kPitch, d.rest_inv + (size_t)k * d.tet_cap + base, row_bytes, &bar);
-            bulk_copy_g2s(s_rows + 9 * kPitch, d.rest_vol + base, row_bytes, &bar);
-            for (int i = 0; i < 7; ++i)
-                bulk_copy_g2s(s_rows + (10 + i) * kPitch, d.plastic + (size_t)i * d.tet_cap + base, row_bytes, &bar);
-            bool ok = mbar_wait_bounded(&bar, 0, kStageWaitPolls);
-            if (!ok) {
-                atomicExch(d.error, 1);
-                mbar_wait_bounded(&bar, 0, kStageWaitPolls);  // let the copies in flight finish
-            }
-            s_ok = ok ? 1 : 0;
-        }
-        __syncthreads();
-        const long long t = first + threadIdx.x;
-        if (s_ok && t < tl.end)
-            tet_element_f32<true, false, SharedRows>(element_refs(d), SharedRows{s_idx, s_slot, s_rows, kPitch, first, base},
-                                                     t, m.mat, diss, energy);
+    const uint32_t row_bytes = (uint32_t)((last4 - base) * 4);
+    mbar_arrive_expect_tx(bar, 2u * (uint32_t)n * 16u + 17u * row_bytes);
+    bulk_copy_g2s(st.idx, d.index + first, (uint32_t)n * 16u, bar);
+    bulk_copy_g2s(st.slot, d.slot + first, (uint32_t)n * 16u, bar);
+    for (int k = 0; k < 9; ++k)
+        bulk_copy_g2s(st.rows + k * RingStage<B>::kPitch, d.rest_inv + (size_t)k * d.tet_cap + base, row_bytes, bar);
+    bulk_copy_g2s(st.rows + 9 * RingStage<B>::kPitch, d.rest_vol + base, row_bytes, bar);
+    for (int i = 0; i < 7; ++i)
+        bulk_copy_g2s(st.rows + (10 + i) * RingStage<B>::kPitch, d.plastic + (size_t)i * d.tet_cap + base, row_bytes,
+                      bar);
+}
+
+// MINB: the blocks per SM the register budget is set for.
+template <int B, int MINB>
+__global__ void __launch_bounds__(B, MINB) pool_elements_ring(PoolDevice d, int sub) {
+    __shared__ double scratch[64];
+    __shared__ __align__(8) uint64_t bar[2];
+    extern __shared__ __align__(16) unsigned char ring_smem[];  // two RingStage<B>
+    RingStage<B>* stage = reinterpret_cast<RingStage<B>*>(ring_smem);
+    const TetElementRefs r = element_refs(d);
+    const int stride = (int)gridDim.x;
+    int tile = blockIdx.x;
+    if (tile >= d.n_etiles) return;  // the whole block (the grid is at most the tile count)
+    uint32_t issued[2] = {0u, 0u};   // thread 0: the phases it queued on each buffer
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        stage_tile_rows<B>(d, tile, sub, stage[0], &bar[0]);
+        issued[0] = 1;
     }
-    block_sum2(diss, energy, scratch);  // valid in thread 0
-    if (live && threadIdx.x == 0 && s_ok) {
-        d.e_diss[tl.part] += diss;
-        d.e_strain[tl.part] = energy;
+    __syncthreads();  // the barriers are set up before anyone waits on them
+    for (int k = 0;; ++k) {
+        const int b = k & 1;
+        const int next = tile + stride;
+        // once a wait anywhere has given up, nothing more is staged or waited for
+        const bool failed = *(volatile int*)d.error != 0;
+        // the other buffer was last read by the tile before this one, which the
+        // previous iteration's closing barrier has finished
+        if (threadIdx.x == 0 && next < d.n_etiles && !failed) {
+            stage_tile_rows<B>(d, next, sub, stage[b ^ 1], &bar[b ^ 1]);
+            ++issued[b ^ 1];
+        }
+        const PoolTile tl = d.etiles[tile];
+        const PoolMesh& m = d.meshes[tl.mesh];
+        const bool live = m.step + sub < m.target;
+        // buffer b's (k / 2)-th phase holds this tile
+        const bool ok = !failed && mbar_wait_bounded(&bar[b], (uint32_t)((k >> 1) & 1), kStageWaitPolls);
+        if (!ok && !failed) atomicExch(d.error, 1);
+        double diss = 0.0, energy = 0.0;
+        const long long t = tl.begin + threadIdx.x;
+        if (ok && live && t < tl.end) {
+            const long long base = tl.begin & ~3LL;
+            tet_element_f32<true, false, SharedRows>(
+                r, SharedRows{stage[b].idx, stage[b].slot, stage[b].rows, RingStage<B>::kPitch, tl.begin, base}, t,
+                m.mat, diss, energy);
+        }
+        block_sum2(diss, energy, scratch);  // valid in thread 0; also the closing barrier
+        if (threadIdx.x == 0 && live && ok) {
+            d.e_diss[tl.part] += diss;
+            d.e_strain[tl.part] = energy;
+        }
+        if (next >= d.n_etiles) break;
+        tile = next;
+    }
+    // after a wait gave up, copies may still be in flight into this block's shared
+    // memory: thread 0 lets the last phase of each buffer land (bounded) before the
+    // block, and with it its shared memory, retires
+    if (threadIdx.x == 0 && *(volatile int*)d.error != 0) {
+        for (int b = 0; b < 2; ++b)
+            if (issued[b]) mbar_wait_bounded(&bar[b], (issued[b] - 1) & 1, kStageWaitPolls);
     }
 }
 
@@ -202,17 +248,52 @@ __global__ void __launch_bounds__(B, 1024 / B) pool_persistent(PoolDevice d, int
 
 }  // namespace
 
+// The staged pass's two stages in dynamic shared memory (52 KB for tiles of 256, above
+// the 48 KB a launch gets without asking), and its persistent grid: as many blocks as
+// fit on the GPU at once, at most one per tile.
+template <int B>
+static size_t ring_smem_bytes() {
+    return 2 * sizeof(RingStage<B>);
+}
+
+// Eight blocks of 128 per SM (four of 256): 64 registers per thread and 32 warps.  A
+// budget of six blocks (80 registers, no spill) measured 7 % slower: the warps hide
+// more latency than the spilled registers cost.
+template <int B>
+constexpr int kRingBlocks = 1024 / B;
+
+template <int B>
+static int ring_grid(int tiles) {
+    static int per_sm = -1;
+    if (per_sm < 0) {
+        cudaFuncSetAttribute(pool_elements_ring<B, kRingBlocks<B>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ring_smem_bytes<B>());
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pool_elements_ring<B, kRingBlocks<B>>, B,
+                                                      ring_smem_bytes<B>());
+        per_sm = n > 0 ? n : 1;
+    }
+    return std::min(tiles, per_sm * sm_count());
+}
+
+void pool_kernels_setup() {
+    ring_grid<128>(1);
+    ring_grid<256>(1);
+}
+
 void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream, bool staged) {
     if (!d.n_etiles) return;
-    const int wave = sm_count() * (1024 / tile);
     if (staged && tile == 128) {
-        pool_elements_staged<128><<<d.n_etiles, 128, 0, stream>>>(d, sub, wave);
+        pool_elements_ring<128, kRingBlocks<128>>
+            <<<ring_grid<128>(d.n_etiles), 128, ring_smem_bytes<128>(), stream>>>(d, sub);
         return;
     }
     if (staged && tile == 256) {
-        pool_elements_staged<256><<<d.n_etiles, 256, 0, stream>>>(d, sub, wave);
+        pool_elements_ring<256, kRingBlocks<256>>
+            <<<ring_grid<256>(d.n_etiles), 256, ring_smem_bytes<256>(), stream>>>(d, sub);
         return;
     }
+    const int wave = sm_count() * (1024 / tile);
     switch (tile) {
         case 128: pool_elements<128><<<d.n_etiles, 128, 0, stream>>>(d, sub, wave); break;
         case 256: pool_elements<256><<<d.n_etiles, 256, 0, stream>>>(d, sub, wave); break;

@@ -92,6 +92,9 @@ void launch_pool_advance(const PoolDevice& d, int steps, cudaStream_t stream);
 // then the advance.
 cudaError_t launch_pool_persistent(const PoolDevice& d, int tile, int steps, int blocks, cudaStream_t stream);
 int pool_persistent_max_blocks(int tile);
+// One-time set-up of the pool's kernels on the current device (the staged pass's
+// shared-memory size and grid); call outside any stream capture.
+void pool_kernels_setup();
 // meshes[id].dt = safety * 2 / sqrt(max omega^2) of the mesh's tets [t0, t0 + T),
 // from the pool's FP32 Dm^-1; 0 when the bound is not positive.  `block_max` holds
 // ceil(T / 256) doubles and `w2` one double of scratch.

@@ -17,7 +17,9 @@
 //     deviation from identity Q = R - I, never on F = I + H and R themselves, so the
 //     strain R^T F - I = H + Q^T + Q^T H is formed from small terms with no
 //     cancellation.  The Higham iteration R <- (R + R^-T)/2 is carried in Q:
-//     Q <- (Q - (M Q)^T)/2 with M = (I + Q)^-1 (fem.cpp:62-69, four iterations);
+//     Q <- (Q - (M Q)^T)/2 with M = (I + Q)^-1 (fem.cpp:62-69), for as many steps as
+//     FP32 needs at the tet's stretch (two for elastic steel, up to the reference's
+//     four);
 //   * the plastic strain is accumulated with Kahan compensation in the compensated
 //     variant.
 //
@@ -99,13 +101,14 @@ struct TetElementRefs {
 
 struct J2f {
     float mu, kappa, yield, hardening;
-    // for the FP64 strain-energy density: 1 / (2 mu), 1 / (3 kappa)
-    double inv_2mu, inv_3kappa;
+    // for the strain-energy density: 1 / (2 mu), 1 / (3 kappa)
+    float inv_2mu_f, inv_3kappa_f;
 };
 
 // The material record of the FP32 J2 tet from the FP64 constants.
 __host__ __device__ inline J2f make_j2f(double mu, double kappa, double yield, double hardening) {
-    return J2f{(float)mu, (float)kappa, (float)yield, (float)hardening, 1.0 / (2.0 * mu), 1.0 / (3.0 * kappa)};
+    return J2f{(float)mu, (float)kappa, (float)yield, (float)hardening, (float)(1.0 / (2.0 * mu)),
+               (float)(1.0 / (3.0 * kappa))};
 }
 
 // L2 prefetch of the per-tet rows of tets [begin, end) -- one 128-byte line per thread
@@ -123,6 +126,10 @@ __device__ __forceinline__ void prefetch_tet_rows(const TetElementRefs& d, long 
     const long long n = end - begin;
     const int wide = (int)((n * 16 + 127) >> 7);   // lines of a 16-byte row
     const int narrow = (int)((n * 4 + 127) >> 7);  // lines of a 4-byte row
+    // each 4-byte row gets a power-of-two count of threads (no integer division);
+    // threads past the row's last line issue nothing
+    const int span = narrow <= 1 ? 1 : 1 << (32 - __clz(narrow - 1));
+    const int shift = 31 - __clz(span);
     int k = x;
     if (k < wide) {
         prefetch_l2(reinterpret_cast<const char*>(d.index + begin) + ((long long)k << 7));
@@ -134,7 +141,8 @@ __device__ __forceinline__ void prefetch_tet_rows(const TetElementRefs& d, long 
         return;
     }
     k -= wide;
-    const int row = k / narrow, line = k - row * narrow;
+    const int row = k >> shift, line = k & (span - 1);
+    if (line >= narrow) return;
     const float* base;
     if (row < 9)
         base = d.rest_inv + (size_t)row * d.stride;
@@ -179,18 +187,12 @@ struct SharedRows {
 // One tet: forces into the node-major slots, plastic state advanced; returns the
 // dissipation and strain energy of the element (FP64, for the energy account).  The
 // arithmetic is the same whichever `Rows` supplies the tet's own rows.
-template <bool KAHAN, bool CG = false, class Rows = GlobalRows>
-__device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const Rows& rows, long long t, const J2f& m,
-                                                double& diss, double& energy) {
-    const uint4 idx = rows.index(t);
-    const unsigned nid[4] = {idx.x, idx.y, idx.z, idx.w};
-    float4 un[4], cn[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) un[c] = ldg_coherent4<CG>(d.disp + nid[c]);
-    if (KAHAN) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) cn[c] = ldg_coherent4<CG>(d.disp_c + nid[c]);
-    }
+// One tet from its four corners' displacements un (and compensations cn), however
+// they were fetched: forces into the node-major slots, plastic state advanced.
+template <bool KAHAN, class Rows>
+__device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d, const Rows& rows, long long t,
+                                                        const J2f& m, const float4 (&un)[4], const float4 (&cn)[4],
+                                                        double& diss, double& energy) {
     M3<float> du, dm_inv;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -206,10 +208,17 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const R
 #pragma unroll
     for (int k = 0; k < 9; ++k) dm_inv.m[k] = rows.inv(k, t);
     const M3<float> h = mul_fma(du, dm_inv);  // displacement gradient
-    // rotation deviation Q = R - I by the Higham iteration on F = I + H
+    // rotation deviation Q = R - I by the Higham iteration on F = I + H.  Each step
+    // squares the stretch error and halves it (F = R (I + E) goes to R (I + E^2 / 2)),
+    // starting from about |sym H|, so the steps to reach FP32's relative precision of
+    // the strain itself are known before the first: two up to |sym H| = 8e-3, three up
+    // to 0.1, the reference's four beyond (fem.cpp:62-69 always takes four).
+    const float e0 = fmaxf(fmaxf(fmaxf(fabsf(h(0, 0)), fabsf(h(1, 1))), fmaxf(fabsf(h(2, 2)), fabsf(h(0, 1) + h(1, 0)))),
+                           fmaxf(fabsf(h(1, 2) + h(2, 1)), fabsf(h(2, 0) + h(0, 2))));
+    const int higham_steps = e0 <= 8e-3f ? 2 : (e0 <= 0.1f ? 3 : 4);
     M3<float> q = h;
 #pragma unroll 1
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < higham_steps; ++it) {
         M3<float> ipq = q;
         ipq(0, 0) += 1.0f;
         ipq(1, 1) += 1.0f;
@@ -299,17 +308,17 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const R
             sv[3 + i] = trial[3 + i];
         }
     }
-    const double vol = (double)rows.vol(t);
-    diss *= vol;
+    const float volf = rows.vol(t);
+    diss *= (double)volf;
     {
-        const double s0 = sv[0], s1 = sv[1], s2 = sv[2], s3 = sv[3], s4 = sv[4], s5 = sv[5];
         // 1/2 sigma : C^-1 : sigma = 1/2 [s_dev : s_dev / (2 mu) + p tr(sigma) / (3 kappa)]
-        // with p = tr(sigma) / 3, the engineering shears counted twice
-        const double tr = s0 + s1 + s2;
-        const double pr = tr * (1.0 / 3.0);
-        const double d0 = s0 - pr, d1 = s1 - pr, d2 = s2 - pr;
-        const double dev = d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (s3 * s3 + s4 * s4 + s5 * s5);
-        energy = vol * 0.5 * (dev * m.inv_2mu + pr * tr * m.inv_3kappa);
+        // with p = tr(sigma) / 3, the engineering shears counted twice; the density in
+        // FP32 (a relative error of a few ulps per tet), the account summed in FP64
+        const float tr = sv[0] + sv[1] + sv[2];
+        const float pr = tr * (1.0f / 3.0f);
+        const float d0 = sv[0] - pr, d1 = sv[1] - pr, d2 = sv[2] - pr;
+        const float dev = d0 * d0 + d1 * d1 + d2 * d2 + 2.0f * (sv[3] * sv[3] + sv[4] * sv[4] + sv[5] * sv[5]);
+        energy = (double)(volf * 0.5f * (dev * m.inv_2mu_f + pr * tr * m.inv_3kappa_f));
     }
     // P = R sigma = sigma + Q sigma; nodal forces f_c = -V (P Dm^-T) column c
     M3<float> sig;
@@ -323,7 +332,7 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const R
 #pragma unroll
     for (int k = 0; k < 9; ++k) sig.m[k] += qs.m[k];
     const M3<float> hf = mul_fma(sig, transpose(dm_inv));
-    const float scale = -rows.vol(t);
+    const float scale = -volf;
     const uint4 sl = rows.slot(t);
     const unsigned sid[4] = {sl.x, sl.y, sl.z, sl.w};
     float f0[3] = {0.0f, 0.0f, 0.0f};
@@ -338,6 +347,21 @@ __device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const R
         d.slots[sid[c + 1]] = make_float4(v[0], v[1], v[2], 0.0f);  // one 16-byte store
     }
     d.slots[sid[0]] = make_float4(f0[0], f0[1], f0[2], 0.0f);
+}
+
+template <bool KAHAN, bool CG = false, class Rows = GlobalRows>
+__device__ __forceinline__ void tet_element_f32(const TetElementRefs& d, const Rows& rows, long long t, const J2f& m,
+                                                double& diss, double& energy) {
+    const uint4 idx = rows.index(t);
+    const unsigned nid[4] = {idx.x, idx.y, idx.z, idx.w};
+    float4 un[4], cn[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) un[c] = ldg_coherent4<CG>(d.disp + nid[c]);
+    if (KAHAN) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cn[c] = ldg_coherent4<CG>(d.disp_c + nid[c]);
+    }
+    tet_element_f32_corners<KAHAN, Rows>(d, rows, t, m, un, cn, diss, energy);
 }
 
 template <bool KAHAN, bool CG = false>
