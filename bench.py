@@ -653,6 +653,8 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
                        "mesh's positions and velocities (femstep_pool_readback_many), destroy; through the C ABI, "
                        "wall clock"}
     drift = None if args.no_drift else pool_drift(F, W, specs)
+    element_kernel = {"graph": "pool_elements", "graph-staged": "pool_elements_ring",
+                      "persistent": "pool_persistent"}[tune["mode"]]
     peak, peak_kind = measured_peak()
     achieved = eb / (elem_ms / 1e3) / 1e9
     if rank == 0:
@@ -672,7 +674,8 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": ncu_traffic(args.workload), "kernel": "pool_elements (tet element pass)",
+                         "traffic": ncu_traffic(f"{args.workload}:{element_kernel}"),
+                         "kernel": f"{element_kernel} (tet element pass, the {tune['mode']} schedule's)",
                          "peak_source": peak_kind},
         }
         if not args.no_cpu_baseline:

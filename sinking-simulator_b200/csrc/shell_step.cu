@@ -10,14 +10,16 @@
 //      a small rotation is lost to the identity;
 //   2. co-rotated displacement relative to corner 0 (B annihilates a translation):
 //      u'_a = R^T (dX_a + dd_a) - dX_a = Q^T dX_a + dd_a + Q^T dd_a;
-//   3. strain at the lane's point eps_u = B_g u' (B streamed from HBM);
+//   3. strain at the lane's point eps_u = B_g u', with B_g formed in the kernel from
+//      the element's rest corners (shell_geom.cuh);
 //   4. EAS Newton on r(alpha) = sum_g w_g G_g^T sigma_g = 0: every iterate restarts
 //      the point law from the step's start state (plasticity.cpp:319-505, linear
 //      isotropic hardening), the residual and K_aa = sum_g w_g G_g^T C_g G_g are warp
 //      butterfly sums over the element's 8 lanes (fixed order, identical bits in every
 //      lane), and each lane runs the same 7x7 Cholesky (solid_shell.cpp:432);
-//      convergence on the correction's energy |delta . r| against sigma_y V
-//      (solid_shell.cpp:963-988), with an FP32 tolerance and iteration cap;
+//      convergence on ||r|| or on the correction's energy |delta . r| against
+//      sigma_y V with the reference's tolerances (solid_shell.cpp:939, 963-988), or on
+//      ||r|| at FP32's rounding floor, with an iteration cap;
 //   5. commit the state of the last evaluation, f = -R sum_g w_g B_g^T sigma_g: a
 //      3-round reduce-scatter leaves node a's force in lane a, which writes it to the
 //      node-major CSR slot.

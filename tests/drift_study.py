@@ -7,7 +7,7 @@
 Each study prints one JSON line: the errors of the GPU results against the FP64 CPU
 oracle (oracle/femoracle.c, pinned bit for bit to the reference), over
   tet-precision  the precision-study beam: 200 x 20 x 20 cells x 6 Kuhn tets (480,000
-                 tets), 130 kN tip load ramped over 10,000 steps, 20,000 steps at 0.9 x
+                 tets), 165 kN tip load ramped over 10,000 steps, 20,000 steps at 0.9 x
                  the FP64 element bound; GPU FP32, FP32-compensated and FP64;
   shell-bay      a bay of the single-large-mesh panel (its 10 mm cells, 12 mm plating,
                  1 mm seeded imperfection, 0.5 MPa Gaussian pulse of 1.5 m with a 5 ms
@@ -124,7 +124,7 @@ def digest(*arrays, **scalars):
 # ---------------------------------------------------------------------------------
 
 def tet_precision(args, cache):
-    cells, load, ramp, steps = (200, 20, 20), 130e3, 10000, 20000
+    cells, load, ramp, steps = (200, 20, 20), 165e3, 10000, 20000
     pos, idx = M.box_tet_mesh(1.0, 0.1, 0.1, *cells)
     fixed = (pos[0::3] < 1e-6).astype(np.uint32)
     tip = pos[0::3] > 1.0 - 1e-6
