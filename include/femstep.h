@@ -323,6 +323,12 @@ typedef struct {
                                                   else the general law and the element failure rules
                                                   (no enhanced modes after a point fails, one retry
                                                   without them, torn when all eight points have) */
+    int eas_fp64;                              /* how much of the enhanced-strain block runs in FP64
+                                                  (gpu::EasPrecision, zone_gpu.hpp:153-162): 0 none;
+                                                  1 the 7x7 factor and substitutions; 2 also K_aa and
+                                                  the residual summed in double; 3 also alpha, its
+                                                  correction and its stored state.  1-3 need the
+                                                  compensated step and a material */
 } femstep_shell_params;
 
 typedef struct femstep_shell femstep_shell;

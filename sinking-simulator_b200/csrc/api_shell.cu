@@ -38,6 +38,9 @@ struct femstep_shell {
     ShellParams graph_params{};
     long long launches = 0;
     float* fail_strain = nullptr;  // [E] per-element failure strain (+inf: never fails)
+    // alpha in double for the EAS64 = 3 variant, allocated on its first run; `alpha64_live`:
+    // it holds the current alpha (else the float copy does, and it is reloaded from it)
+    bool alpha64_live = false;
     // the punch (femstep_shell_set_punch) and its host-side account, as the reference's
     // GPU zone step keeps it (zone_gpu.cpp:889-919)
     uint8_t* driven = nullptr;     // [N]
@@ -101,6 +104,7 @@ ShellParams make_params(const femstep_shell_params& p) {
     q.tol_residual = (float)(p.tol_residual > 0 ? p.tol_residual : 1e-12);
     q.tol_work = (float)(p.tol_work > 0 ? p.tol_work : 1e-16);
     q.compensated = p.compensated;
+    q.eas64 = p.eas_fp64;
     // the fibres' law in double: the same material, linear unless the curve is Swift
     q.fiber.youngs = E;
     q.fiber.yield = p.yield_strength;
@@ -480,7 +484,34 @@ int femstep_shell_run(femstep_shell* s, int substeps, const femstep_shell_params
     if (!s || !params) return fail(s, FEMSTEP_EINVAL, "null solver or params");
     if (substeps < 0) return fail(s, FEMSTEP_EINVAL, "negative step count");
     if (!(params->dt > 0.0) || !std::isfinite(params->dt)) return fail(s, FEMSTEP_EINVAL, "dt must be positive");
+    if (params->eas_fp64 < 0 || params->eas_fp64 > 3) return fail(s, FEMSTEP_EINVAL, "eas_fp64 must be 0-3");
+    if (params->eas_fp64 > 0 && (!params->compensated || !params->material))
+        return fail(s, FEMSTEP_EINVAL, "the FP64 enhanced-block variants run the compensated step with a material");
     ShellParams q = make_params(*params);
+    if (params->eas_fp64 == 3 && !s->alpha64_live) {
+        // alpha into double from its float copy, on this variant's first run
+        const size_t n = (size_t)s->groups * 4 * 8;
+        if (!s->d.alpha64) {
+            s->d.alpha64 = s->arena.alloc<double>(n);
+            if (!s->arena.ok()) return fail(s, FEMSTEP_ENOMEM, "alpha in double");
+        }
+        std::vector<float> af(n);
+        std::vector<double> ad(n);
+        int rc0 = check(s, cudaMemcpyAsync(af.data(), s->d.alpha, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
+                        "alpha");
+        if (!rc0) rc0 = check(s, cudaStreamSynchronize(s->stream), "alpha");
+        for (size_t i = 0; i < n && !rc0; ++i) ad[i] = af[i];
+        if (!rc0)
+            rc0 = check(s, cudaMemcpyAsync(s->d.alpha64, ad.data(), n * sizeof(double), cudaMemcpyHostToDevice,
+                                           s->stream), "alpha");
+        if (!rc0) rc0 = check(s, cudaStreamSynchronize(s->stream), "alpha");
+        if (rc0) return rc0;
+        if (s->graph) {  // a captured graph holds the old device record
+            cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+        }
+    }
+    s->alpha64_live = params->eas_fp64 == 3;
     q.edge_ramp = s->edge_ramp;
     if (s->punch) {
         q.punch_speed = (float)s->punch_speed;
@@ -872,6 +903,13 @@ int femstep_shell_state(femstep_shell* s, double* state) {
                    "readback");
     if (!rc) rc = check(s, cudaMemcpy(fs_.data(), s->fail_strain, E * sizeof(float), cudaMemcpyDeviceToHost), "readback");
     if (rc) return rc;
+    std::vector<double> a64;
+    if (s->alpha64_live) {  // the EAS64 = 3 variant keeps alpha in double
+        a64.resize(al.size());
+        rc = check(s, cudaMemcpy(a64.data(), s->d.alpha64, a64.size() * sizeof(double), cudaMemcpyDeviceToHost),
+                   "readback");
+        if (rc) return rc;
+    }
     for (size_t e = 0; e < E; ++e) {
         double* x = state + e * 129;
         std::fill(x, x + 129, 0.0);
@@ -886,7 +924,7 @@ int femstep_shell_state(femstep_shell* s, double* state) {
             x[gp * 15 + 13] = st2[b2 + (size_t)6 * 32];
             x[gp * 15 + 14] = st2[b2 + (size_t)7 * 32];
         }
-        for (int k = 0; k < 7; ++k) x[120 + k] = al[e * 8 + k];
+        for (int k = 0; k < 7; ++k) x[120 + k] = a64.empty() ? (double)al[e * 8 + k] : a64[e * 8 + k];
         x[127] = fs_[e];
         x[128] = al[e * 8 + 7];
     }
@@ -1123,6 +1161,7 @@ int femstep_shell_restore(femstep_shell* s, const void* buffer, size_t bytes) {
     s->punch_time = h.punch_time;
     s->punch_penetration = h.punch_penetration;
     s->punch_steps = h.punch_steps;
+    s->alpha64_live = false;  // the float alpha restored is the current one
     return FEMSTEP_OK;
 }
 

@@ -42,6 +42,7 @@ struct ShellDevice {
     const float4* elem = nullptr;  // [E][kShellElemQ]
     float* state = nullptr;
     float* alpha = nullptr;
+    double* alpha64 = nullptr;         // [E][8]: alpha in double (the EAS64 = 3 variant only)
     const uint32_t* index = nullptr;
     const uint32_t* slot = nullptr;
     const double* rest = nullptr;
@@ -138,6 +139,7 @@ struct ShellParams {
     int max_iterations;                   // EAS Newton cap
     float tol_residual, tol_work;         // relative to sigma_y V
     int compensated;                      // Kahan on displacement and plastic strain
+    int eas64;                            // FP64 in the enhanced-strain block: 0-3 (shell_forces)
 };
 
 constexpr int kShellBlock = 128;          // 16 elements per block

@@ -43,6 +43,26 @@ __device__ __forceinline__ float sum8(float v) {
     return v;
 }
 
+__device__ __forceinline__ double sum8d(double v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    return v;
+}
+
+// The enhanced strain with alpha in double: the enhanced part summed in double, then
+// added to the compatible strain and rounded once.
+__device__ __forceinline__ void shell_enhanced_apply64(const float T[24], const float gc[7], const double alpha[7],
+                                                       const float base[6], float out[6]) {
+    const double b0 = (double)gc[0] * alpha[0], b1 = (double)gc[1] * alpha[1];
+    const double b2 = (double)gc[2] * alpha[2] + (double)gc[3] * alpha[3] + (double)gc[4] * alpha[4];
+    const double b3 = (double)gc[5] * alpha[5] + (double)gc[6] * alpha[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+        out[i] = (float)((double)base[i] + (double)T[i] * b0 + (double)T[6 + i] * b1 + (double)T[12 + i] * b2 +
+                         (double)T[18 + i] * b3);
+}
+
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
     const float y = x - comp;
     const float t = sum + y;
@@ -318,7 +338,10 @@ constexpr int kShellWarpsNarrow = kShellMinbNarrow * kShellBlock / 32;  // per S
 
 // GENERAL: the general point law and the element failure rules (ShellParams::general);
 // otherwise the linear law, whose state is only the plastic strain.
-template <bool KAHAN, bool GENERAL, int MINB>
+// EAS64: how much of the enhanced-strain block runs in FP64 (ShellParams::eas64): 0
+// none; 1 the 7x7 factor and its substitutions; 2 also K_aa and the residual summed in
+// double; 3 also alpha, its correction and its stored state (d.alpha64).
+template <bool KAHAN, bool GENERAL, int MINB, int EAS64 = 0>
 __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d, ShellParams p) {
     // an inertial punch has stopped: the run is over (every thread reads the same flag)
     if (d.halt && *d.halt) return;
@@ -547,8 +570,14 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     float alpha[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) alpha[k] = eas_on ? d.alpha[e * 8 + k] : 0.0f;
-    // the elastic K_aa factor of this element is usable (formed, and positive definite)
-    const bool have_factor = d.kaa_factor != nullptr && __ldg(d.kaa_factor + e * 32) > 0.0f;
+    double alpha64[7];
+    if constexpr (EAS64 >= 3) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) alpha64[k] = eas_on ? d.alpha64[e * 8 + k] : 0.0;
+    }
+    // the elastic K_aa factor of this element is usable (formed, and positive definite);
+    // the FP64 variants form and factor K_aa every time
+    const bool have_factor = EAS64 == 0 && d.kaa_factor != nullptr && __ldg(d.kaa_factor + e * 32) > 0.0f;
 
     // ---- EAS Newton ----
     // The four elements of a warp iterate together (the shuffles need the whole warp):
@@ -559,7 +588,10 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
 #pragma unroll 1
     for (int iteration = 0;; ++iteration) {
         float eps[6];
-        shell_enhanced_apply(T, gc, alpha, eps_u, eps);
+        if constexpr (EAS64 >= 3)
+            shell_enhanced_apply64(T, gc, alpha64, eps_u, eps);
+        else
+            shell_enhanced_apply(T, gc, alpha, eps_u, eps);
         if (GENERAL)
             point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
         else
@@ -578,6 +610,23 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             const int kj[7] = {0, 1, 2, 2, 2, 3, 3};
 #pragma unroll
             for (int j = 0; j < 7; ++j) r[j] = sum8(gc[j] * tau[kj[j]]);
+        }
+        double r64[7];
+        if constexpr (EAS64 >= 2) {  // the residual summed in double
+            double tau[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                double s = 0.0;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) s += (double)T[k * 6 + i] * (double)o.sigma[i];
+                tau[k] = (double)w * s;
+            }
+            const int kj[7] = {0, 1, 2, 2, 2, 3, 3};
+#pragma unroll
+            for (int j = 0; j < 7; ++j) r64[j] = sum8d((double)gc[j] * tau[kj[j]]);
+        } else if constexpr (EAS64 == 1) {
+#pragma unroll
+            for (int j = 0; j < 7; ++j) r64[j] = (double)r[j];
         }
         // The rounding floor of the residual in FP32: a few ulps of the magnitude of its
         // terms, sum_g w |sigma_g| |gc_g| (T0's columns are unit vectors).  A residual
@@ -598,6 +647,12 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             float rn = 0.0f;
 #pragma unroll
             for (int k = 0; k < 7; ++k) rn += r[k] * r[k];
+            if constexpr (EAS64 >= 2) {
+                double rn64 = 0.0;
+#pragma unroll
+                for (int k = 0; k < 7; ++k) rn64 += r64[k] * r64[k];
+                rn = (float)rn64;
+            }
             if (sqrtf(rn) <= fmaxf(p.tol_residual * scale, rfloor)) {
                 converged = true;
                 done = true;
@@ -606,6 +661,7 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             }
         }
         if (__all_sync(0xffffffffu, done)) break;
+        if constexpr (EAS64 == 0) {
         // An element whose eight points are all elastic at this iterate has the
         // elastic K_aa, whose Cholesky factor is formed once per material
         // (shell_elastic_factor).  The warp builds K_aa itself only when one of its
@@ -703,6 +759,110 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
                 for (int k = 0; k < 7; ++k) alpha[k] += delta[k];
             }
         }
+        } else {
+            // The enhanced block with FP64 in it: K_aa (from the FP32 tangent, summed in
+            // double from EAS64 = 2), its factor and the correction in double.
+            double kaa64[28];
+            {
+                const int kj[7] = {0, 1, 2, 2, 2, 3, 3};
+                if constexpr (EAS64 >= 2) {
+                    double H[10];
+#pragma unroll
+                    for (int kb = 0; kb < 4; ++kb) {
+                        float cg[6];
+                        tangent_apply(o, p, &T[kb * 6], cg);
+#pragma unroll
+                        for (int ka = kb; ka < 4; ++ka) {
+                            double s = 0.0;
+#pragma unroll
+                            for (int i = 0; i < 6; ++i) s += (double)T[ka * 6 + i] * (double)cg[i];
+                            H[ka * (ka + 1) / 2 + kb] = (double)w * s;
+                        }
+                    }
+#pragma unroll
+                    for (int b = 0; b < 7; ++b)
+#pragma unroll
+                        for (int a = b; a < 7; ++a)
+                            kaa64[a * (a + 1) / 2 + b] =
+                                sum8d((double)gc[a] * (double)gc[b] * H[kj[a] * (kj[a] + 1) / 2 + kj[b]]);
+                } else {
+                    float H[10];
+#pragma unroll
+                    for (int kb = 0; kb < 4; ++kb) {
+                        float cg[6];
+                        tangent_apply(o, p, &T[kb * 6], cg);
+#pragma unroll
+                        for (int ka = kb; ka < 4; ++ka) {
+                            float s = 0.0f;
+#pragma unroll
+                            for (int i = 0; i < 6; ++i) s += T[ka * 6 + i] * cg[i];
+                            H[ka * (ka + 1) / 2 + kb] = w * s;
+                        }
+                    }
+#pragma unroll
+                    for (int b = 0; b < 7; ++b)
+#pragma unroll
+                        for (int a = b; a < 7; ++a)
+                            kaa64[a * (a + 1) / 2 + b] =
+                                (double)sum8(gc[a] * gc[b] * H[kj[a] * (kj[a] + 1) / 2 + kj[b]]);
+                }
+            }
+            // Cholesky (solid_shell.cpp:432-457) in double, the diagonal kept as its reciprocal
+            double l64[28];
+            bool spd = true;
+            {
+                int t = 0;
+#pragma unroll
+                for (int i = 0; i < 7; ++i) {
+#pragma unroll
+                    for (int j = 0; j <= i; ++j) {
+                        double s = kaa64[t];
+#pragma unroll
+                        for (int k = 0; k < j; ++k) s -= l64[i * (i + 1) / 2 + k] * l64[j * (j + 1) / 2 + k];
+                        if (i == j) {
+                            spd = spd && (s > 0.0);
+                            l64[t] = 1.0 / sqrt(fmax(s, 1e-300));
+                        } else {
+                            l64[t] = s * l64[j * (j + 1) / 2 + j];
+                        }
+                        ++t;
+                    }
+                }
+            }
+            double delta64[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) {
+                double s = -r64[i];
+#pragma unroll
+                for (int k = 0; k < i; ++k) s -= l64[i * (i + 1) / 2 + k] * delta64[k];
+                delta64[i] = s * l64[i * (i + 1) / 2 + i];
+            }
+#pragma unroll
+            for (int i = 6; i >= 0; --i) {
+                double s = delta64[i];
+#pragma unroll
+                for (int k = i + 1; k < 7; ++k) s -= l64[k * (k + 1) / 2 + i] * delta64[k];
+                delta64[i] = s * l64[i * (i + 1) / 2 + i];
+            }
+            double work = 0.0;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) work += delta64[k] * r64[k];
+            if (!done) {
+                if (!spd) {
+                    done = true;
+                } else if (fabs(work) <= (double)p.tol_work * (double)scale) {
+                    converged = true;  // stop before applying, as solid_shell.cpp:983-988
+                    done = true;
+                } else if constexpr (EAS64 >= 3) {
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) alpha64[k] += delta64[k];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) alpha[k] += (float)delta64[k];
+                }
+            }
+        }
+
     }
 
     // A point that failed in this step's Newton sends its element round once more
@@ -719,9 +879,16 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
                 converged = true;
 #pragma unroll
                 for (int k = 0; k < 7; ++k) alpha[k] = 0.0f;
+                if constexpr (EAS64 >= 3) {
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) alpha64[k] = 0.0;
+                }
             }
             float eps[6];
-            shell_enhanced_apply(T, gc, alpha, eps_u, eps);
+            if constexpr (EAS64 >= 3)
+                shell_enhanced_apply64(T, gc, alpha64, eps_u, eps);
+            else
+                shell_enhanced_apply(T, gc, alpha, eps_u, eps);
             point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
         }
     }
@@ -757,6 +924,12 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
                 d.state2[sbase2 + (size_t)6 * 32] = o.damage;
                 d.state2[sbase2 + (size_t)7 * 32] = o.failed ? 1.0f : 0.0f;
             }
+        }
+        if constexpr (EAS64 >= 3) {
+            // alpha in double; its FP32 copy is what the rest of the solver reads
+#pragma unroll
+            for (int k = 0; k < 7; ++k) alpha[k] = (float)alpha64[k];
+            if (gp < 7) d.alpha64[e * 8 + gp] = alpha64[gp];
         }
         if (gp < 7) d.alpha[e * 8 + gp] = alpha[gp];
         const double s0 = o.sigma[0], s1 = o.sigma[1], s2 = o.sigma[2], s3 = o.sigma[3], s4 = o.sigma[4],
@@ -1231,6 +1404,20 @@ void launch_shell_elastic_factor(const ShellDevice& d, double youngs, double poi
 
 template <int MINB>
 static void launch_forces(const ShellDevice& d, const ShellParams& p, int blocks, cudaStream_t stream) {
+    // the FP64 enhanced-block variants: compensated state and the general law only (the
+    // host checks), at the narrow register budget
+    if (p.eas64 == 1) {
+        shell_forces<true, true, kShellMinbNarrow, 1><<<blocks, kShellBlock, 0, stream>>>(d, p);
+        return;
+    }
+    if (p.eas64 == 2) {
+        shell_forces<true, true, kShellMinbNarrow, 2><<<blocks, kShellBlock, 0, stream>>>(d, p);
+        return;
+    }
+    if (p.eas64 == 3) {
+        shell_forces<true, true, kShellMinbNarrow, 3><<<blocks, kShellBlock, 0, stream>>>(d, p);
+        return;
+    }
     if (p.compensated) {
         if (p.general)
             shell_forces<true, true, MINB><<<blocks, kShellBlock, 0, stream>>>(d, p);

@@ -254,7 +254,8 @@ class ShellParamsC(C.Structure):
     _fields_ = [("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double), ("yield_strength", C.c_double),
                 ("hardening_modulus", C.c_double), ("dt", C.c_double), ("damping", C.c_double),
                 ("rise_time", C.c_double), ("max_iterations", C.c_int), ("tol_residual", C.c_double),
-                ("tol_work", C.c_double), ("compensated", C.c_int), ("material", C.c_void_p)]
+                ("tol_work", C.c_double), ("compensated", C.c_int), ("material", C.c_void_p),
+                ("eas_fp64", C.c_int)]
 
 
 _sh_create = _sig("femstep_shell_create", C.c_int, [C.POINTER(ShellMeshC), C.POINTER(C.c_void_p)])
@@ -337,13 +338,15 @@ class ShellSolver:
             _raise(rc, _sh_error(self._h))
 
     def params(self, youngs=206e9, poisson=0.3, yield_strength=355e6, hardening=1e9, dt=1e-7, damping=1.0,
-               rise_time=0.0, max_iterations=12, tol_residual=1e-12, tol_work=1e-16, compensated=True, material=None):
-        """material: None (the linear law) or a dict of femstep_shell_material fields
+               rise_time=0.0, max_iterations=12, tol_residual=1e-12, tol_work=1e-16, compensated=True, material=None,
+               eas_fp64=0):
+        """eas_fp64: how much of the enhanced-strain block runs in FP64 (0-3, needs a material).
+        material: None (the linear law) or a dict of femstep_shell_material fields
         (hardening=SHELL_SWIFT|SHELL_LINEAR, strength_coefficient, reference_strain,
         hardening_exponent, kinematic_modulus, triaxiality_sensitivity,
         reference_triaxiality, cutoff_triaxiality)."""
         p = ShellParamsC(youngs, poisson, yield_strength, hardening, dt, damping, rise_time, int(max_iterations),
-                         tol_residual, tol_work, int(bool(compensated)), None)
+                         tol_residual, tol_work, int(bool(compensated)), None, int(eas_fp64))
         if material is not None:
             m = dict(hardening=SHELL_LINEAR, strength_coefficient=0.0, reference_strain=0.0, hardening_exponent=1.0,
                      kinematic_modulus=0.0, triaxiality_sensitivity=1.5, reference_triaxiality=1.0 / 3.0,
