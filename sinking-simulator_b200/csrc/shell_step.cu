@@ -587,15 +587,18 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     bool converged = false, done = false;
 #pragma unroll 1
     for (int iteration = 0;; ++iteration) {
-        float eps[6];
-        if constexpr (EAS64 >= 3)
-            shell_enhanced_apply64(T, gc, alpha64, eps_u, eps);
-        else
-            shell_enhanced_apply(T, gc, alpha, eps_u, eps);
-        if (GENERAL)
-            point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
-        else
-            point_law(eps, ps, p, o);
+        // a finished element keeps its point state: the one at its final alpha
+        if (!done) {
+            float eps[6];
+            if constexpr (EAS64 >= 3)
+                shell_enhanced_apply64(T, gc, alpha64, eps_u, eps);
+            else
+                shell_enhanced_apply(T, gc, alpha, eps_u, eps);
+            if (GENERAL)
+                point_law_general(eps, ps, back0, damage0, failed0, fstrain, p, o);
+            else
+                point_law(eps, ps, p, o);
+        }
         // r_j = sum_g w gc_j (T0[:, k_j] . sigma)
         float r[7];
         {
@@ -668,6 +671,22 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
         // elements has a yielded point; the shuffles need the whole warp.
         const unsigned yielded_mask = __ballot_sync(0xffffffffu, o.yielded);
         const bool elastic_element = have_factor && ((yielded_mask >> (lane & 24)) & 0xffu) == 0u;
+        if constexpr (EAS64 == 0) {
+            // The work gate without the solve: |delta . r| = r^T K^-1 r <= trace(K^-1) |r|^2
+            // for the elastic K_aa, so where the bound is under the gate the correction
+            // would be turned down (as solid_shell.cpp:983-988 turns it down) and need not
+            // be formed.  The element's factor is then not even read.
+            if (!done && elastic_element) {
+                float rn = 0.0f;
+#pragma unroll
+                for (int k = 0; k < 7; ++k) rn += r[k] * r[k];
+                if (__ldg(d.kaa_factor + e * 32 + 28) * rn <= p.tol_work * scale) {
+                    converged = true;
+                    done = true;
+                }
+            }
+            if (__all_sync(0xffffffffu, done)) break;
+        }
         float l[28];
         bool spd = true;
         if (__any_sync(0xffffffffu, !elastic_element)) {
@@ -717,7 +736,7 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             }
         }
         }
-        if (elastic_element) {
+        if (elastic_element && !done) {
             const float4* lf = reinterpret_cast<const float4*>(d.kaa_factor + e * 32);
 #pragma unroll
             for (int k = 0; k < 7; ++k) {
@@ -748,6 +767,13 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
         float work = 0.0f;
 #pragma unroll
         for (int k = 0; k < 7; ++k) work += delta[k] * r[k];
+        // An element whose eight points are elastic, corrected with the exact elastic
+        // factor, has its residual at zero to rounding after the correction: its stress
+        // is linear in alpha, so the point state at the new alpha is the old one plus
+        // C G delta, with no second evaluation, unless that stress would yield at a point
+        // (then the iteration goes on as usual).  Linear law only.
+        bool linear_try = false, linear_elastic = false;
+        float sn[6];
         if (!done) {
             if (!spd) {
                 done = true;  // no stiffness left in the enhanced modes: report, do not iterate
@@ -757,6 +783,34 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             } else {
 #pragma unroll
                 for (int k = 0; k < 7; ++k) alpha[k] += delta[k];
+                if (!GENERAL && elastic_element) {
+                    const float zero[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    float de[6];
+                    shell_enhanced_apply(T, gc, delta, zero, de);
+                    const float dv = de[0] + de[1] + de[2];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        sn[i] = o.sigma[i] + (p.kappa * dv + 2.0f * p.mu * (de[i] - dv * (1.0f / 3.0f)));
+                        sn[3 + i] = o.sigma[3 + i] + p.mu * de[3 + i];
+                    }
+                    const float pr = (sn[0] + sn[1] + sn[2]) * (1.0f / 3.0f);
+                    const float s0 = sn[0] - pr, s1 = sn[1] - pr, s2 = sn[2] - pr;
+                    const float norm =
+                        sqrtf(s0 * s0 + s1 * s1 + s2 * s2 + 2.0f * (sn[3] * sn[3] + sn[4] * sn[4] + sn[5] * sn[5]));
+                    const float radius = 0.81649658092772603f * (p.yield + p.hardening * fmaxf(ps[6], 0.0f));
+                    linear_try = true;
+                    linear_elastic = norm <= radius;
+                }
+            }
+        }
+        if (!GENERAL) {
+            // every lane takes part in the ballot; the decision is the element's
+            const unsigned elastic_mask = __ballot_sync(0xffffffffu, linear_try && linear_elastic);
+            if (linear_try && ((elastic_mask >> (lane & 24)) & 0xffu) == 0xffu) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) o.sigma[i] = sn[i];
+                converged = true;
+                done = true;
             }
         }
         } else {
@@ -1387,7 +1441,18 @@ __global__ void shell_elastic_factor(ShellDevice d, double lambda, double mu, fl
         }
     for (int k = 0; k < 28; ++k) l[k] = (float)ld[k];
     for (int i = 0; i < 7; ++i) l[i * (i + 1) / 2 + i] = (float)(1.0 / ld[i * (i + 1) / 2 + i]);  // as the step keeps it
-    l[28] = l[29] = l[30] = l[31] = 0.0f;
+    // trace(K^-1) = |L^-1|_F^2, a bound on |K^-1|: the step decides the work gate
+    // |delta . r| = r^T K^-1 r <= trace(K^-1) |r|^2 from it without solving, where it can
+    double inv[28], trace = 0.0;
+    for (int j = 0; j < 7; ++j)
+        for (int i = j; i < 7; ++i) {
+            double v = i == j ? 1.0 : 0.0;
+            for (int k = j; k < i; ++k) v -= ld[i * (i + 1) / 2 + k] * inv[k * (k + 1) / 2 + j];
+            inv[i * (i + 1) / 2 + j] = v / ld[i * (i + 1) / 2 + i];
+            trace += inv[i * (i + 1) / 2 + j] * inv[i * (i + 1) / 2 + j];
+        }
+    l[28] = spd ? (float)(trace * (1.0 + 1e-4)) : 0.0f;  // a little over, for the rounding
+    l[29] = l[30] = l[31] = 0.0f;
     if (!spd) l[0] = 0.0f;
     float4* o = reinterpret_cast<float4*>(out + e * 32);
     for (int k = 0; k < 8; ++k) o[k] = make_float4(l[4 * k], l[4 * k + 1], l[4 * k + 2], l[4 * k + 3]);
