@@ -17,6 +17,29 @@ thread_local std::string g_last_error;
 void set_last_error(const std::string& what) { g_last_error = what; }
 const char* last_error() { return g_last_error.c_str(); }
 
+cudaError_t device_alloc(void** p, size_t bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    // once per device: keep freed memory up to the retained size
+    static bool configured[64] = {};
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = kRetainedDeviceBytes;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        configured[dev] = true;
+    }
+    e = cudaMallocAsync(p, bytes, cudaStreamLegacy);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(cudaStreamLegacy);
+}
+
+void device_free(void* p) {
+    if (p) cudaFreeAsync(p, cudaStreamLegacy);
+}
+
 int device_status() {
     int count = 0;
     const cudaError_t e = cudaGetDeviceCount(&count);

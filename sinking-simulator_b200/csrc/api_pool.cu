@@ -373,7 +373,7 @@ int snapshot(femstep_pool* p, Snapshot& s, bool restore) {
         s.spans.push_back({p->d.n_kin, (size_t)pmax * 8});
         size_t total = 0;
         for (auto& sp : s.spans) total += sp.second;
-        const int rc = check(p, cudaMalloc(&s.buf, total ? total : 1), "snapshot");
+        const int rc = check(p, fs::device_alloc((void**)&s.buf, total ? total : 1), "snapshot");
         if (rc) return rc;
     }
     size_t off = 0;
@@ -1196,7 +1196,7 @@ int femstep_pool_autotune(femstep_pool* p, int steps, int* tile_out, int* mode_o
                 best_mode = modes[mi];
             }
         }
-    cudaFree(snap.buf);
+    fs::device_free(snap.buf);
     p->tile = best_tile;
     p->mode = best_mode;
     p->dirty = true;

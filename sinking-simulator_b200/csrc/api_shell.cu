@@ -176,7 +176,7 @@ int check_caller_forms(femstep_shell* s, const double* forms, const double* weig
         }
     const size_t n = std::min<size_t>(E, 64);
     double* f64 = nullptr;
-    rc = check(s, cudaMalloc(&f64, n * 1507 * sizeof(double)), "forms check");
+    rc = check(s, fs::device_alloc((void**)&f64, n * 1507 * sizeof(double)), "forms check");
     if (rc) return rc;
     fs::ShellSetupArgs a{};
     a.elements = (long long)n;
@@ -191,7 +191,7 @@ int check_caller_forms(femstep_shell* s, const double* forms, const double* weig
     rc = check(s, cudaMemcpyAsync(h.data(), f64, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream),
                "forms check");
     if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "forms check");
-    cudaFree(f64);
+    fs::device_free(f64);
     if (rc) return rc;
     const size_t block[5] = {0, 1152, 1488, 1496, 1505};
     for (size_t e = 0; e < n; ++e)
@@ -398,7 +398,7 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
     double* weights = nullptr;
     if (A.ok()) {
         corner_mass = m.mass ? nullptr : A.zeros<double>(E * 8);
-        if (m.forms && cudaMalloc(&weights, E * 8 * sizeof(double)) != cudaSuccess) {
+        if (m.forms && fs::device_alloc((void**)&weights, E * 8 * sizeof(double)) != cudaSuccess) {
             femstep_shell_destroy(s);
             return fail(nullptr, FEMSTEP_ENOMEM, "device allocation failed");
         }
@@ -418,7 +418,7 @@ int femstep_shell_create(const femstep_shell_mesh* mesh, femstep_shell** out) {
         cudaStreamSynchronize(s->stream);
         rc = check(s, cudaGetLastError(), "rest forms");
         if (!rc && m.forms) rc = check_caller_forms(s, m.forms, weights);
-        if (weights) cudaFree(weights);
+        if (weights) fs::device_free(weights);
         if (rc) {
             femstep_shell_destroy(s);
             return rc;
@@ -969,7 +969,7 @@ int femstep_shell_critical_dt(femstep_shell* s, double youngs, double poisson, d
                               double* dt) {
     if (!s || !dt) return fail(s, FEMSTEP_EINVAL, "null argument");
     double* per = nullptr;
-    int rc = check(s, cudaMalloc(&per, s->elements * sizeof(double)), "alloc");
+    int rc = check(s, fs::device_alloc((void**)&per, s->elements * sizeof(double)), "alloc");
     if (rc) return rc;
     fs::ShellSetupArgs a{};
     a.elements = (long long)s->elements;
@@ -987,7 +987,7 @@ int femstep_shell_critical_dt(femstep_shell* s, double youngs, double poisson, d
     std::vector<double> h(s->elements);
     rc = check(s, cudaMemcpyAsync(h.data(), per, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "readback");
     if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "critical dt");
-    cudaFree(per);
+    fs::device_free(per);
     if (rc) return rc;
     // smallest positive element step (solid_shell.cpp:1187-1198)
     double best = INFINITY;

@@ -446,17 +446,17 @@ int femstep_tet_critical_dt(femstep_tet* s, double youngs, double poisson, doubl
             const std::vector<double> a = soa(s->rest_inv64.data(), T, 9);
             host = a;
         }
-        rc = check(s, cudaMalloc(&tmp, host.size() * sizeof(double)), "alloc");
+        rc = check(s, fs::device_alloc((void**)&tmp, host.size() * sizeof(double)), "alloc");
         if (rc) return rc;
         rc = check(s, cudaMemcpy(tmp, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
         if (rc) {
-            cudaFree(tmp);
+            fs::device_free(tmp);
             return rc;
         }
         inv = tmp;
     }
     double* block_max = nullptr;
-    rc = check(s, cudaMalloc(&block_max, sizeof(double) * s->eblocks), "alloc");
+    rc = check(s, fs::device_alloc((void**)&block_max, sizeof(double) * s->eblocks), "alloc");
     if (!rc) {
         fs::launch_tet_omega2((long long)T, inv, youngs, poisson, density, block_max, s->eblocks, s->stream);
         fs::launch_reduce_max(block_max, s->eblocks, s->d_out + 7, s->stream);
@@ -465,8 +465,8 @@ int femstep_tet_critical_dt(femstep_tet* s, double youngs, double poisson, doubl
         if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "critical dt");
         *dt = w2 > 0.0 ? safety * 2.0 / std::sqrt(w2) : 0.0;
     }
-    cudaFree(block_max);
-    if (tmp) cudaFree(tmp);
+    fs::device_free(block_max);
+    if (tmp) fs::device_free(tmp);
     return rc;
 }
 

@@ -19,6 +19,16 @@ const char* last_error();
 // when there is none -- the reference's "degrade, not abort" (fem_gpu.hpp:21-22).
 int device_status();
 
+// Device memory from the current device's stream-ordered pool (cudaMallocAsync on the
+// legacy stream, then a wait for it, so the memory is ready for any stream).  Memory a
+// handle frees stays with the process for the next handle, up to kRetainedDeviceBytes
+// kept across synchronisations, instead of going back to the driver: a pool or solver
+// created after another one was destroyed maps no new memory, and a destroy never waits
+// in the driver's unmapping.
+constexpr size_t kRetainedDeviceBytes = size_t(16) << 30;
+cudaError_t device_alloc(void** p, size_t bytes);
+void device_free(void* p);
+
 // Every device allocation a handle makes, freed together.  Upload failures are sticky
 // so a constructor can do all its uploads and check once.
 class DeviceArena {
@@ -28,7 +38,7 @@ public:
         if (status_ != cudaSuccess) return nullptr;
         void* p = nullptr;
         const size_t bytes = count ? count * sizeof(T) : sizeof(T);
-        status_ = cudaMalloc(&p, bytes);
+        status_ = device_alloc(&p, bytes);
         if (status_ != cudaSuccess) return nullptr;
         ptrs_.push_back(p);
         bytes_ += bytes;
@@ -50,7 +60,7 @@ public:
     cudaError_t status() const { return status_; }
     size_t bytes() const { return bytes_; }
     void release() {
-        for (void* p : ptrs_) cudaFree(p);
+        for (void* p : ptrs_) device_free(p);
         ptrs_.clear();
         bytes_ = 0;
     }
