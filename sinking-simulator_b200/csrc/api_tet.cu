@@ -16,6 +16,7 @@
 #include "../../include/femstep.h"
 #include "common.cuh"
 #include "host_util.hpp"
+#include "shell.hpp"
 #include "tet.hpp"
 
 using fs::TetDevice;
@@ -29,7 +30,8 @@ struct femstep_tet {
     TetDevice<float> d32;
     TetDevice<double> d64;
     std::vector<float> rest;          // FP32 J2 modes: rest positions for readback
-    std::vector<double> rest_inv64;   // J2 modes: Dm^-1 in double (critical dt)
+    std::vector<double> rest_inv64;   // J2 modes given an adjacency: Dm^-1 in double (critical dt)
+    double* inv64 = nullptr;          // J2 FP32 modes built on the device: Dm^-1 in double, SoA
     int eblocks = 0, nblocks = 0;
     double* d_out = nullptr;          // 8 doubles of reduction output
     double* d_scratch = nullptr;      // per-block maxima for the critical step
@@ -102,6 +104,135 @@ void launch_step(femstep_tet* s, const TetParams& q, int parts = fs::kWholeStep)
 
 constexpr int kGraphSteps = 32;
 
+// femstep_tet_create for the J2 modes when the caller gives no adjacency (the mesh is
+// already checked): everything from the caller's node positions and node ids on the
+// device.  The CSR and slot map of csr.cu (counting-sort order), and computeRestState
+// (fem.cpp:119-158) in FP64 by tet_exact.cu's kernels, bit-identical to the host's
+// tet_rest_state64; the FP32 modes' float copies rounded once from it.
+int create_on_device(const femstep_tet_mesh& m, int mode, femstep_tet** out) {
+    const int dev = fs::device_status();
+    if (dev != FEMSTEP_OK) return dev;
+    const size_t N = m.nodes, T = m.tets;
+    femstep_tet* s = new femstep_tet();
+    s->mode = mode;
+    s->nodes = N;
+    s->tets = T;
+    s->eblocks = fs::blocks_for((long long)T, fs::kBlock);
+    s->nblocks = fs::blocks_for((long long)N, fs::kBlock);
+    int rc = check(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    if (rc == FEMSTEP_OK) rc = check(s, cudaEventCreate(&s->ev0), "event");
+    if (rc == FEMSTEP_OK) rc = check(s, cudaEventCreate(&s->ev1), "event");
+    if (rc != FEMSTEP_OK) {
+        femstep_tet_destroy(s);
+        return rc;
+    }
+    fs::DeviceArena& A = s->arena;
+    std::vector<uint8_t> fixed(N, 0);
+    if (m.fixed)
+        for (size_t n = 0; n < N; ++n) fixed[n] = m.fixed[n] ? 1 : 0;
+    const uint32_t* index = A.upload(m.index, T * 4);
+    const float* pos32 = A.upload(m.position, N * 3);
+    uint32_t* offset = A.alloc<uint32_t>(N + 1);
+    uint32_t* slot = A.alloc<uint32_t>(T * 4);
+    // the FP64 rest state: Dm^-1 (SoA) and volumes per tet, lumped masses per node
+    double* inv64 = A.alloc<double>(T * 9);
+    double* vol64 = A.alloc<double>(T);
+    double* mass64 = A.alloc<double>(N);
+    if (!A.ok()) {
+        const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;
+        fail(s, code, std::string("device upload failed: ") + cudaGetErrorString(A.status()));
+        femstep_tet_destroy(s);
+        return code;
+    }
+    uint32_t* entry = nullptr;
+    double* quarter = nullptr;
+    rc = check(s, fs::device_alloc((void**)&entry, T * 4 * sizeof(uint32_t)), "alloc");
+    if (!rc) rc = check(s, fs::device_alloc((void**)&quarter, T * sizeof(double)), "alloc");
+    if (!rc) rc = check(s, fs::build_csr_device(index, (long long)T * 4, (long long)N, offset, slot, s->stream, entry),
+                        "adjacency");
+    if (!rc) {
+        fs::launch_tet_rest64(pos32, index, (long long)T, m.density, inv64, vol64, quarter, s->stream);
+        fs::launch_tet_mass64(offset, entry, (long long)N, quarter, mass64, s->stream);
+        rc = check(s, cudaGetLastError(), "rest state");
+    }
+
+    auto common = [&](auto& d) {
+        d.nodes = (long long)N;
+        d.tets = (long long)T;
+        d.index = reinterpret_cast<const uint4*>(index);
+        d.slot = reinterpret_cast<const uint4*>(slot);
+        d.fixed = A.upload(fixed.data(), N);
+        d.offset = offset;
+        d.counter = A.zeros<long long>(2);
+        d.e_diss = A.zeros<double>(s->eblocks);
+        d.e_strain = A.zeros<double>(s->eblocks);
+        d.n_work = A.zeros<double>(s->nblocks);
+        d.n_kin = A.zeros<double>(s->nblocks);
+        d.n_grav = A.zeros<double>(s->nblocks);
+    };
+    if (!rc && mode == FEMSTEP_TET_J2_F64) {
+        TetDevice<double>& d = s->d64;
+        common(d);
+        double* pos = A.alloc<double>(N * 3);
+        if (pos) fs::launch_widen(pos32, (long long)N * 3, pos, s->stream);
+        d.position = pos;
+        std::vector<double> vel(N * 3, 0.0);
+        if (m.velocity)
+            for (size_t i = 0; i < N * 3; ++i) vel[i] = m.velocity[i];
+        d.velocity = A.upload(vel.data(), N * 3);
+        d.mass = mass64;
+        d.rest_inv = inv64;
+        d.rest_vol = vol64;
+        d.plastic = A.zeros<double>(T * 7);
+        if (m.external_force) d.ext = A.upload(m.external_force, N * 3);
+        d.slots = A.zeros<double>(T * 4 * 3 + 2);
+    } else if (!rc) {
+        TetDevice<float>& d = s->d32;
+        common(d);
+        std::vector<float> vel(N * 3, 0.0f);
+        if (m.velocity) std::memcpy(vel.data(), m.velocity, sizeof(float) * N * 3);
+        d.velocity = A.upload(vel.data(), N * 3);
+        d.slots = A.zeros<float>(T * 4 * 4 + 4);  // a padded float4 per corner
+        s->rest.assign(m.position, m.position + N * 3);
+        d.rest = pos32;
+        d.disp = A.zeros<float>(N * 4);
+        if (mode == FEMSTEP_TET_J2_F32K) d.disp_c = A.zeros<float>(N * 4);
+        float* inv32 = A.alloc<float>(T * 9);
+        float* vol32 = A.alloc<float>(T);
+        float* mass32 = A.alloc<float>(N);
+        float* inv_mass32 = A.alloc<float>(N);
+        if (A.ok())
+            fs::launch_tet_rest_f32(inv64, vol64, (long long)T, mass64, (long long)N, inv32, vol32, mass32, inv_mass32,
+                                    s->stream);
+        d.rest_inv = inv32;
+        d.rest_vol = vol32;
+        d.mass = mass32;
+        d.inv_mass = inv_mass32;
+        d.plastic = A.zeros<float>(T * 7);
+        if (mode == FEMSTEP_TET_J2_F32K) d.plastic_c = A.zeros<float>(T * 7);
+        if (m.external_force) {
+            std::vector<float> ext(N * 3);
+            for (size_t i = 0; i < N * 3; ++i) ext[i] = (float)m.external_force[i];
+            d.ext = A.upload(ext.data(), N * 3);
+        }
+        s->inv64 = inv64;
+    }
+    s->d_out = A.zeros<double>(8);
+    if (!rc) rc = check(s, cudaStreamSynchronize(s->stream), "set-up");
+    fs::device_free(entry);
+    fs::device_free(quarter);
+    if (!rc && !A.ok()) {
+        const int code = A.status() == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA;
+        rc = fail(s, code, std::string("device upload failed: ") + cudaGetErrorString(A.status()));
+    }
+    if (rc) {
+        femstep_tet_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return FEMSTEP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -121,6 +252,10 @@ int femstep_tet_create(const femstep_tet_mesh* mesh, int mode, femstep_tet** out
         return fail(nullptr, FEMSTEP_EINVAL, "REF32 needs the caller's mass, rest_inv and rest_volume");
     if (mode != FEMSTEP_TET_REF32 && !(m.density > 0.0))
         return fail(nullptr, FEMSTEP_EINVAL, "J2 modes need a positive density");
+
+    // The J2 modes without a caller adjacency are set up on the device: the CSR (the
+    // counting sort's order), the slot map and the FP64 rest state.
+    if (mode != FEMSTEP_TET_REF32 && !(m.adjacency_offset && m.adjacency_entry)) return create_on_device(m, mode, out);
 
     // CSR: the caller's (validated), or built by counting sort as fem.cpp:147-157.
     std::vector<uint32_t> offset, entry;
@@ -435,6 +570,8 @@ int femstep_tet_critical_dt(femstep_tet* s, double youngs, double poisson, doubl
     int rc = FEMSTEP_OK;
     if (s->mode == FEMSTEP_TET_J2_F64) {
         inv = s->d64.rest_inv;
+    } else if (s->inv64) {
+        inv = s->inv64;  // formed on the device at create
     } else {
         std::vector<double> host(T * 9);
         if (s->mode == FEMSTEP_TET_REF32) {

@@ -50,13 +50,13 @@ __global__ void csr_slots(const uint32_t* entry, long long total, uint32_t* slot
 }  // namespace
 
 cudaError_t build_csr_device(const uint32_t* index, long long total, long long nodes, uint32_t* offset, uint32_t* slot,
-                             cudaStream_t stream) {
-    uint32_t *count = nullptr, *entry = nullptr;
+                             cudaStream_t stream, uint32_t* entry_out) {
+    uint32_t *count = nullptr, *entry = entry_out;
     void* temp = nullptr;
     size_t temp_bytes = 0;
     cudaError_t err = cub::DeviceScan::InclusiveSum(nullptr, temp_bytes, count, offset + 1, (int)nodes, stream);
     if (err == cudaSuccess) err = cudaMallocAsync(&count, (size_t)nodes * sizeof(uint32_t), stream);
-    if (err == cudaSuccess) err = cudaMallocAsync(&entry, (size_t)total * sizeof(uint32_t), stream);
+    if (err == cudaSuccess && !entry) err = cudaMallocAsync(&entry, (size_t)total * sizeof(uint32_t), stream);
     if (err == cudaSuccess) err = cudaMallocAsync(&temp, temp_bytes, stream);
     if (err == cudaSuccess) {
         const int grid = 148 * 8;
@@ -75,7 +75,7 @@ cudaError_t build_csr_device(const uint32_t* index, long long total, long long n
         err = cudaGetLastError();
     }
     if (temp) cudaFreeAsync(temp, stream);
-    if (entry) cudaFreeAsync(entry, stream);
+    if (entry && entry != entry_out) cudaFreeAsync(entry, stream);
     if (count) cudaFreeAsync(count, stream);
     return err;
 }

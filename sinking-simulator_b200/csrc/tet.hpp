@@ -92,6 +92,18 @@ void launch_tet_omega2(long long tets, const double* rest_inv, double E, double 
 // the first tet), promoted to double: the matrix the FP32 element kernels use.
 void launch_tet_omega2_f32(long long tets, const float* rest_inv, long long stride, double E, double nu, double rho,
                            double* per_block_max, int blocks, cudaStream_t stream);
+// The single mesh's rest state on the device, bit-identical to tet_rest_state64:
+// per tet Dm^-1 (SoA, `tets` per row), volume and quarter mass; per node the lumped
+// mass summed over the node's CSR run (`entry`: corner ids, ascending per node).
+void launch_tet_rest64(const float* position, const uint32_t* index, long long tets, double density, double* inv,
+                       double* vol, double* quarter, cudaStream_t stream);
+void launch_tet_mass64(const uint32_t* offset, const uint32_t* entry, long long nodes, const double* quarter,
+                       double* mass, cudaStream_t stream);
+// The FP32 modes' rest state from it: Dm^-1, volume, mass and 1 / mass, rounded once.
+void launch_tet_rest_f32(const double* inv, const double* vol, long long tets, const double* mass, long long nodes,
+                         float* inv32, float* vol32, float* mass32, float* inv_mass32, cudaStream_t stream);
+// out[i] = (double)in[i].
+void launch_widen(const float* in, long long n, double* out, cudaStream_t stream);
 // Fixed-order FP64 sum / max of `n` doubles into out[0] (one block).
 void launch_reduce_sum(const double* in, long long n, double* out, cudaStream_t stream);
 void launch_reduce_max(const double* in, long long n, double* out, cudaStream_t stream);

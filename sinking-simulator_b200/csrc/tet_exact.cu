@@ -422,7 +422,96 @@ __global__ void __launch_bounds__(1024) reduce_max(const double* in, long long n
     if (threadIdx.x == 0) out[0] = smax[0];
 }
 
+// computeRestState (fem.cpp:119-158) in FP64 on the device, with the host's operations
+// in the host's order (tet_rest_state64 in api_common.cu, compiled without contraction
+// as this file is): per tet Dm^-1 (SoA rows of `tets`), |det| / 6 and its quarter of
+// the lumped mass.
+__global__ void tet_rest64_kernel(const float* position, const uint32_t* index, long long tets, double density,
+                                  double* inv, double* vol, double* quarter) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tets) return;
+    const uint32_t* idx = index + t * 4;
+    double a[9];  // column-major
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r)
+            a[c * 3 + r] = (double)position[(size_t)idx[c + 1] * 3 + r] - (double)position[(size_t)idx[0] * 3 + r];
+#define A(r, c) a[(c) * 3 + (r)]
+    const double det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
+                       A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                       A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+    const double volume = fabs(det / 6.0);
+    const double id = fabs(det) > 1e-300 ? 1.0 / det : 0.0;
+    double r[9];
+#define R(rr, cc) r[(cc) * 3 + (rr)]
+    R(0, 0) = (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) * id;
+    R(0, 1) = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * id;
+    R(0, 2) = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * id;
+    R(1, 0) = (A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2)) * id;
+    R(1, 1) = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * id;
+    R(1, 2) = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * id;
+    R(2, 0) = (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0)) * id;
+    R(2, 1) = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * id;
+    R(2, 2) = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * id;
+#undef R
+#undef A
+    for (int k = 0; k < 9; ++k) inv[(size_t)k * tets + t] = r[k];
+    vol[t] = volume;
+    quarter[t] = density * volume * 0.25;
+}
+
+// Each node's lumped mass: its tets' quarters summed over its CSR run, which lists its
+// corners in ascending tet order -- the order the host's loop adds them in.
+__global__ void tet_mass64_kernel(const uint32_t* offset, const uint32_t* entry, long long nodes, const double* quarter,
+                                  double* mass) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nodes) return;
+    double m = 0.0;
+    for (uint32_t k = offset[n]; k < offset[n + 1]; ++k) m += quarter[entry[k] >> 2];
+    mass[n] = m;
+}
+
+// The FP32 modes' copies of the FP64 rest state, rounded once.
+__global__ void tet_rest_f32_kernel(const double* inv, const double* vol, long long tets, float* inv32, float* vol32) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tets) return;
+    for (int k = 0; k < 9; ++k) inv32[(size_t)k * tets + t] = (float)inv[(size_t)k * tets + t];
+    vol32[t] = (float)vol[t];
+}
+
+__global__ void tet_mass_f32_kernel(const double* mass, long long nodes, float* mass32, float* inv_mass32) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nodes) return;
+    mass32[n] = (float)mass[n];
+    inv_mass32[n] = mass[n] > 0.0 ? (float)(1.0 / mass[n]) : 0.0f;
+}
+
+__global__ void widen_kernel(const float* in, long long n, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)in[i];
+}
+
 }  // namespace
+
+void launch_tet_rest64(const float* position, const uint32_t* index, long long tets, double density, double* inv,
+                       double* vol, double* quarter, cudaStream_t stream) {
+    tet_rest64_kernel<<<blocks_for(tets, kBlock), kBlock, 0, stream>>>(position, index, tets, density, inv, vol,
+                                                                       quarter);
+}
+
+void launch_tet_mass64(const uint32_t* offset, const uint32_t* entry, long long nodes, const double* quarter,
+                       double* mass, cudaStream_t stream) {
+    tet_mass64_kernel<<<blocks_for(nodes, kBlock), kBlock, 0, stream>>>(offset, entry, nodes, quarter, mass);
+}
+
+void launch_tet_rest_f32(const double* inv, const double* vol, long long tets, const double* mass, long long nodes,
+                         float* inv32, float* vol32, float* mass32, float* inv_mass32, cudaStream_t stream) {
+    tet_rest_f32_kernel<<<blocks_for(tets, kBlock), kBlock, 0, stream>>>(inv, vol, tets, inv32, vol32);
+    tet_mass_f32_kernel<<<blocks_for(nodes, kBlock), kBlock, 0, stream>>>(mass, nodes, mass32, inv_mass32);
+}
+
+void launch_widen(const float* in, long long n, double* out, cudaStream_t stream) {
+    widen_kernel<<<blocks_for(n, kBlock), kBlock, 0, stream>>>(in, n, out);
+}
 
 void launch_ref32_step(const TetDevice<float>& d, const TetParams& p, cudaStream_t stream, int parts) {
     const float lambda = (float)p.lambda, mu = (float)p.mu;

@@ -160,3 +160,25 @@ def test_tiny_meshes_in_every_mode(fem, port, cells):
     r.run(50, youngs=210e9, poisson=0.3, dt=1e-6, gravity=9.80665, damping=1.0)
     pr, vr = r.readback()
     assert np.array_equal(pr, m.position) and np.array_equal(vr, m.velocity)
+
+
+@pytest.mark.parametrize("mode", ["f64", "f32k", "f32"])
+def test_device_set_up_is_the_host_set_up(fem, mode):
+    """A J2 mesh given without an adjacency is set up on the device (CSR, slot map and
+    the FP64 rest state); given with one, on the host.  The two must be the same to the
+    bit: the same critical step, and the same state after a yielding run."""
+    pos, idx, fixed, fext = cantilever(fem, 24, 3, 3, load=300e3)
+    offset, entry = fem.csr(pos.size // 3, idx, 4)
+    dev = fem.TetSolver(pos, idx, mode=mode, fixed=fixed, external_force=fext, density=7850.0)
+    host = fem.TetSolver(pos, idx, mode=mode, fixed=fixed, external_force=fext, density=7850.0,
+                         adjacency_offset=offset, adjacency_entry=entry)
+    dt = dev.critical_dt(210e9, 0.3, 7850.0, 0.9)
+    assert dt == host.critical_dt(210e9, 0.3, 7850.0, 0.9)
+    for s in (dev, host):
+        s.run(400, dt=dt, ramp_steps=200)
+    pd, vd = dev.readback64()
+    ph, vh = host.readback64()
+    assert np.array_equal(pd, ph) and np.array_equal(vd, vh)
+    assert np.array_equal(dev.plastic(), host.plastic())
+    assert (host.plastic()[:, 6] > 0).any(), "the case must yield"
+    assert np.array_equal(dev.energy(), host.energy())
