@@ -29,6 +29,7 @@
 #include "common.cuh"
 #include "host_util.hpp"
 #include "pool.hpp"
+#include "shell.hpp"
 #include "tet.hpp"
 
 using fs::PoolDevice;
@@ -110,7 +111,7 @@ public:
     }
 
 private:
-    static constexpr size_t kHostCacheBytes = size_t(512) << 20;
+    static constexpr size_t kHostCacheBytes = size_t(1) << 30;
     std::mutex mu_;
     std::multimap<size_t, char*> free_;
     size_t total_ = 0;
@@ -483,6 +484,32 @@ void prepare_mesh(const femstep_pool_mesh& m, Placement& pl, char* stage) {
     ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
 }
 
+// The host part of admitting one mesh of a group whose meshes sit in consecutive tet and
+// node ranges (group_prepare / the device CSR): its node ids local to the group's node
+// span, rest positions, pins and load, each into the group's section for it.  No CSR
+// here: the device builds the group's (build_csr_device).
+void prepare_mesh_sections(const femstep_pool_mesh& m, const Placement& pl, long long t_first, long long n_first,
+                           char* idx_sec, char* pos_sec, char* fix_sec, char* ext_sec) {
+    const long long N = pl.N, T = pl.T;
+    const uint32_t shift = (uint32_t)(pl.n0 - n_first);
+    uint32_t* idx = (uint32_t*)idx_sec + (pl.t0 - t_first) * 4;
+    for (long long i = 0; i < T * 4; ++i) idx[i] = m.index[i] + shift;
+    const long long at = pl.n0 - n_first;
+    float* pos = (float*)pos_sec + at * 3;
+    std::memcpy(pos, m.position, (size_t)N * 12);
+    uint8_t* fixed = (uint8_t*)fix_sec + at;
+    float* ext = (float*)ext_sec + at * 3;
+    for (long long n = 0; n < N; ++n) fixed[n] = m.fixed && m.fixed[n] ? 1 : 0;
+    if (m.external_force)
+        for (long long i = 0; i < N * 3; ++i) ext[i] = (float)m.external_force[i];
+    else
+        std::memset(ext, 0, (size_t)N * 12);
+    // the spare node slot: holds the CSR end; massless (set on the device), fixed, unloaded
+    pos[N * 3] = pos[N * 3 + 1] = pos[N * 3 + 2] = 0.0f;
+    fixed[N] = 1;
+    ext[N * 3] = ext[N * 3 + 1] = ext[N * 3 + 2] = 0.0f;
+}
+
 // Whether some tet of the mesh has a non-zero volume (computeRestState's guard leaves
 // a degenerate tet without stiffness; a mesh of them only has no time step).
 bool any_volume(const femstep_pool_mesh& m) {
@@ -620,6 +647,29 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
         std::vector<long long> weight(g1 - g0);
         for (int i = g0; i < g1; ++i) weight[i - g0] = pl[i].T;
         const int G = g1 - g0;
+        // A group in consecutive tet and node ranges, in order (always so in a pool that
+        // was empty): staged by section and uploaded in one copy per section, its CSR
+        // and slot map built on the device over the whole group -- the per-mesh
+        // counting sorts, since every corner of a mesh names only that mesh's nodes.
+        // Otherwise each mesh is prepared on the host and sent by its own copies.
+        bool contig = true;
+        for (int i = g0 + 1; i < g1; ++i)
+            contig = contig && pl[i].t0 == pl[i - 1].t0 + pl[i - 1].T && pl[i].n0 == pl[i - 1].n0 + pl[i - 1].N + 1;
+        long long tets_g = 0, nodes_g = 0;
+        for (int i = g0; i < g1; ++i) {
+            tets_g += pl[i].T;
+            nodes_g += pl[i].N + 1;
+        }
+        size_t sec_idx = 0, sec_pos = 0, sec_fix = 0, sec_ext = 0, sec_rec = 0;
+        if (contig) {
+            size_t o = 0;
+            sec_idx = o, o += align256((size_t)tets_g * 16);
+            sec_pos = o, o += align256((size_t)nodes_g * 12);
+            sec_fix = o, o += align256((size_t)nodes_g);
+            sec_ext = o, o += align256((size_t)nodes_g * 12);
+            sec_rec = o, o += align256((size_t)G * sizeof(PoolMesh));
+            bytes = o;
+        }
         const size_t table = ((size_t)G * sizeof(fs::PoolAdmit) + 255) & ~size_t(255);
         cudaError_t err;
         Staging::Buf* buf = p->staging.get(bytes + table, err);
@@ -629,25 +679,59 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
         }
         char* stage = Staging::take(buf, bytes);
         fs::PoolAdmit* adm = (fs::PoolAdmit*)Staging::take(buf, table);
-        parallel_for(g1 - g0, weight, [&](int k) { prepare_mesh(meshes[g0 + k], pl[g0 + k], stage); });
+        const long long t_first = pl[g0].t0, n_first = pl[g0].n0;
+        if (contig) {
+            parallel_for(g1 - g0, weight, [&](int k) {
+                prepare_mesh_sections(meshes[g0 + k], pl[g0 + k], t_first, n_first, stage + sec_idx, stage + sec_pos,
+                                      stage + sec_fix, stage + sec_ext);
+                // the host copy of the rest positions, for the readback
+                p->meshes[pl[g0 + k].id].rest.assign(meshes[g0 + k].position,
+                                                     meshes[g0 + k].position + pl[g0 + k].N * 3);
+            });
+        } else {
+            parallel_for(g1 - g0, weight, [&](int k) {
+                prepare_mesh(meshes[g0 + k], pl[g0 + k], stage);
+                p->meshes[pl[g0 + k].id].rest.assign(meshes[g0 + k].position,
+                                                     meshes[g0 + k].position + pl[g0 + k].N * 3);
+            });
+        }
         long long tets = 0, nodes = 0, parts = 0;
         bool any_dt = false;
         auto send = [&](void* dst, size_t off, size_t len) {
             cudaMemcpyAsync(dst, stage + off, len, cudaMemcpyHostToDevice, st);
         };
+        if (contig) {
+            send(d.index + t_first, sec_idx, (size_t)tets_g * 16);
+            send(d.velocity + n_first * 3, sec_pos, (size_t)nodes_g * 12);
+            send(d.fixed + n_first, sec_fix, (size_t)nodes_g);
+            send(d.ext + n_first * 3, sec_ext, (size_t)nodes_g * 12);
+            // the group's last node is its last mesh's spare slot, which holds the CSR end
+            const cudaError_t ce = fs::build_csr_device(reinterpret_cast<const uint32_t*>(d.index + t_first),
+                                                        tets_g * 4, nodes_g - 1, d.offset + n_first,
+                                                        reinterpret_cast<uint32_t*>(d.slot + t_first), st, nullptr,
+                                                        (uint32_t)(4 * t_first));
+            if (ce != cudaSuccess) {
+                undo();
+                return check(p, ce, "group adjacency");
+            }
+            fs::launch_pool_rebase(d.index + t_first, tets_g, (uint32_t)n_first, st);
+        }
         for (int i = g0; i < g1; ++i) {
             const femstep_pool_mesh& m = meshes[i];
             const Placement& q = pl[i];
             const long long T = q.T, N = q.N, t0 = q.t0, n0 = q.n0, part0 = q.part0;
-            send(d.index + t0, q.idx4, T * sizeof(uint4));
-            send(d.slot + t0, q.slot4, T * sizeof(uint4));
-            send(d.offset + n0, q.offs, (N + 1) * 4);
-            send(d.fixed + n0, q.fixed, N + 1);
-            send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
-            // the rest positions, staged in the mesh's velocity rows for the rest state;
-            // the admission kernels below then start the nodes at rest
-            send(d.velocity + n0 * 3, q.pos, (N + 1) * 12);
-            PoolMesh* pm = (PoolMesh*)(stage + q.rec);
+            if (!contig) {
+                send(d.index + t0, q.idx4, T * sizeof(uint4));
+                send(d.slot + t0, q.slot4, T * sizeof(uint4));
+                send(d.offset + n0, q.offs, (N + 1) * 4);
+                send(d.fixed + n0, q.fixed, N + 1);
+                send(d.ext + n0 * 3, q.ext, (N + 1) * 12);
+                // the rest positions, staged in the mesh's velocity rows for the rest
+                // state; the admission kernels below then start the nodes at rest
+                send(d.velocity + n0 * 3, q.pos, (N + 1) * 12);
+            }
+            const size_t rec_at = contig ? sec_rec + (size_t)(i - g0) * sizeof(PoolMesh) : q.rec;
+            PoolMesh* pm = (PoolMesh*)(stage + rec_at);
             std::memset(pm, 0, sizeof(PoolMesh));
             const double E = m.youngs_modulus, nu = m.poisson_ratio;
             // plasticity::Material::shearModulus / bulkModulus (plasticity.hpp:226-227)
@@ -663,7 +747,7 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
             pm->e_part = part0;
             pm->n_part = part0 + q.e_tiles;
             pm->serial = p->next_serial + i;
-            send(d.meshes + q.id, q.rec, sizeof(PoolMesh));
+            send(d.meshes + q.id, rec_at, sizeof(PoolMesh));
             // the group's record of this mesh for the admission kernels; no step given:
             // 0.9 x the FP64 element eigenvalue bound of the stored FP32 Dm^-1, formed
             // and stored on the device behind the uploads
@@ -711,7 +795,6 @@ int admit_meshes(femstep_pool* p, const femstep_pool_mesh* meshes, const long lo
         h.n_tiles = q.n_tiles;
         h.target = steps[i];
         h.serial = p->next_serial + i;
-        h.rest.assign(meshes[i].position, meshes[i].position + q.N * 3);
         ids[i] = q.id;
     }
     p->next_serial += n;

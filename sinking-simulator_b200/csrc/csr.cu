@@ -42,15 +42,20 @@ __global__ void csr_sort_runs(const uint32_t* offset, long long nodes, uint32_t*
     }
 }
 
-__global__ void csr_slots(const uint32_t* entry, long long total, uint32_t* slot) {
+__global__ void csr_slots(const uint32_t* entry, long long total, uint32_t* slot, uint32_t base) {
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
-        slot[entry[k]] = (uint32_t)k;
+        slot[entry[k]] = base + (uint32_t)k;
+}
+
+__global__ void csr_add_base(uint32_t* offset, long long n, uint32_t base) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        offset[i] += base;
 }
 
 }  // namespace
 
 cudaError_t build_csr_device(const uint32_t* index, long long total, long long nodes, uint32_t* offset, uint32_t* slot,
-                             cudaStream_t stream, uint32_t* entry_out) {
+                             cudaStream_t stream, uint32_t* entry_out, uint32_t base) {
     uint32_t *count = nullptr, *entry = entry_out;
     void* temp = nullptr;
     size_t temp_bytes = 0;
@@ -71,7 +76,8 @@ cudaError_t build_csr_device(const uint32_t* index, long long total, long long n
         const int grid = 148 * 8;
         csr_scatter<<<grid, 256, 0, stream>>>(index, total, count, entry);
         csr_sort_runs<<<blocks_for(nodes, 256), 256, 0, stream>>>(offset, nodes, entry);
-        csr_slots<<<grid, 256, 0, stream>>>(entry, total, slot);
+        csr_slots<<<grid, 256, 0, stream>>>(entry, total, slot, base);
+        if (base) csr_add_base<<<grid, 256, 0, stream>>>(offset, nodes + 1, base);
         err = cudaGetLastError();
     }
     if (temp) cudaFreeAsync(temp, stream);

@@ -499,6 +499,23 @@ __global__ void pool_admit_dt(PoolMesh* meshes, const PoolAdmit* adm, int G, con
 
 }  // namespace
 
+namespace {
+__global__ void pool_rebase(uint4* index, long long tets, uint32_t add) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tets; t += (long long)gridDim.x * blockDim.x) {
+        uint4 v = index[t];
+        v.x += add;
+        v.y += add;
+        v.z += add;
+        v.w += add;
+        index[t] = v;
+    }
+}
+}  // namespace
+
+void launch_pool_rebase(uint4* index, long long tets, uint32_t add, cudaStream_t stream) {
+    if (tets > 0) pool_rebase<<<std::min<long long>(blocks_for(tets, 256), 148 * 16), 256, 0, stream>>>(index, tets, add);
+}
+
 void launch_pool_admit(const PoolDevice& d, const PoolAdmit* adm, int G, long long tets, long long nodes,
                        long long parts, bool any_dt, unsigned long long* w2, cudaStream_t stream) {
     const int cap = sm_count() * 8;

@@ -119,5 +119,8 @@ struct PoolAdmit {
 // group, whatever its size.
 void launch_pool_admit(const PoolDevice& d, const PoolAdmit* adm, int G, long long tets, long long nodes,
                        long long parts, bool any_dt, unsigned long long* w2, cudaStream_t stream);
+// index[0 .. tets) += (add, add, add, add): node ids of a group uploaded local to its
+// span, rebased into the pool after the group's CSR was built from them.
+void launch_pool_rebase(uint4* index, long long tets, uint32_t add, cudaStream_t stream);
 
 }  // namespace fs

@@ -174,9 +174,10 @@ struct ShellSetupArgs {
 void launch_shell_setup(const ShellSetupArgs& a, cudaStream_t stream);
 // The node -> corner adjacency in element order and the corner -> CSR slot map, on the
 // device (csr.cu): offset [nodes + 1], slot [total]; index values must be < nodes.
-// `entry_out` [total], if given, receives the adjacency entries themselves.
+// `entry_out` [total], if given, receives the adjacency entries themselves; `base` is
+// added to every offset and slot (a CSR placed at that position of a larger one).
 cudaError_t build_csr_device(const uint32_t* index, long long total, long long nodes, uint32_t* offset, uint32_t* slot,
-                             cudaStream_t stream, uint32_t* entry_out = nullptr);
+                             cudaStream_t stream, uint32_t* entry_out = nullptr, uint32_t base = 0);
 // Sum the CSR corner masses per node in CSR order (the element order zone.cpp:709-712
 // accumulates them in), then the FP32 mass and 1/mass.
 void launch_shell_mass(long long nodes, const uint32_t* offset, const double* corner_mass, double* mass64,
