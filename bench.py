@@ -650,12 +650,12 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
                       "destroy_s": wall - (t4 - t0)}
             return T * args.steps / wall, phases, d2h
 
-        cold, cold_phases, _ = job()
-        warm, phases, d2h = job()
+        cold_rate, cold_phases, _ = job()
+        warm_rate, phases, d2h = job()
         h2d = sum(b.position.nbytes + b.index.nbytes + b.fixed.nbytes + b.external_force.nbytes for b in built)
-        e2e = {"value": warm, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+        e2e = {"value": warm_rate, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                "d2h_bytes_per_step": d2h / args.steps, "phases": phases,
-               "cold_value": cold, "cold_phases": cold_phases,
+               "cold_value": cold_rate, "cold_phases": cold_phases,
                "note": "one whole job through the C ABI, wall clock: create the pool, admit every mesh from host "
                        "arrays (femstep_pool_admit_many: node ids, positions, pins and loads staged on all host "
                        "cores and uploaded; CSR, slot map and the FP64 rest state on the device), K steps, read back "
