@@ -338,3 +338,34 @@ def test_readback_many_is_readback(fem):
         assert np.array_equal(p, pe) and np.array_equal(v, ve)
     assert np.abs(many[1][0] - meshes[1]["position"]).max() > 0
     pool.close()
+
+
+def test_many_workload_meshes_same_bits_in_every_schedule(fem):
+    """A pool of 48 of the batched workload's own meshes (uneven sizes, every clamp face,
+    tip and pressure loads), admitted together: more element tiles than the staged
+    pass's persistent grid holds at once, so its blocks walk several tiles each.  Every
+    mesh's state and FP64 energy account are the same in every schedule, over chunks
+    that straddle the meshes' step counts."""
+    import workloads as W
+
+    specs = W.batch_meshes(count=48, lo=2e3, hi=3e4, seed=77)
+    built = [W.build(s) for s in specs]
+    kw = [dict(m.admit_kwargs(), ramp_steps=40) for m in built]
+    steps = [60 + 7 * (k % 5) for k in range(len(kw))]
+    tets = sum(m.index.size // 4 for m in built)
+    nodes = sum(m.position.size // 3 + 1 for m in built)
+    out = []
+    for mode in (fem.POOL_GRAPH, fem.POOL_GRAPH_STAGED, fem.POOL_PERSISTENT):
+        pool = fem.TetPool(tets + 1000, nodes + 1000, max_meshes=64, tile=128)
+        ids = pool.admit_many(kw, steps)
+        assert len(ids) == len(kw)
+        for chunk in (25, 41, 3, 30):  # 99 steps: every mesh reaches its count (60 to 88)
+            pool.run(chunk, mode)
+        out.append([(pool.readback(i), pool.plastic(i), pool.energy(i), pool.status(i)) for i in ids])
+        pool.close()
+    for other in out[1:]:
+        for (ra, pa, ea, sa), (rb, pb, eb, sb) in zip(out[0], other):
+            assert sa == sb and sa[0] == sa[1]
+            assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[1], rb[1])
+            assert np.array_equal(pa, pb)
+            assert np.array_equal(ea, eb)
