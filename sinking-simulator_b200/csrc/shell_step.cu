@@ -379,55 +379,59 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
         d.counter[0] = s + 1;
     }
 
-    // ---- nodes of the element (every lane reads all eight: broadcast loads) ----
-    const uint4 i0 = reinterpret_cast<const uint4*>(d.index)[e * 2];
-    const uint4 i1 = reinterpret_cast<const uint4*>(d.index)[e * 2 + 1];
-    const unsigned nid[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
-    // rest geometry: every corner relative to corner 0 (for the rotation), the bottom
-    // corners and the directors D_c = X_{c+4} - X_c (for the element operators), each
-    // difference taken in double and rounded once
-    float dX[8][3], dd[8][3], D[4][3];
+    // ---- the element's corners: lane g reads node g alone ----
+    // Each lane forms its own corner's rest difference to corner 0 and displacement
+    // difference to corner 0 (and, for a bottom corner, its director), each difference
+    // taken as before: rest positions in double, rounded once; the compensated
+    // displacement as a double-float.  The corners are parked in shared memory, one copy
+    // per element (`geo`), where the element's eight lanes read them back.  One node read
+    // per lane instead of eight, and no corner arrays held in registers.
+    __shared__ __align__(16) float geo_park[kShellBlock / 8][kShellGeo];
+    float* geo = geo_park[threadIdx.x >> 3];
+    float dXg[3], ddg[3];
     {
-        const double X0 = d.rest[(size_t)nid[0] * 3], Y0 = d.rest[(size_t)nid[0] * 3 + 1],
-                     Z0 = d.rest[(size_t)nid[0] * 3 + 2];
-        const float u0 = d.disp[(size_t)nid[0] * 3], v0 = d.disp[(size_t)nid[0] * 3 + 1],
-                    w0 = d.disp[(size_t)nid[0] * 3 + 2];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const size_t ob = (size_t)nid[c] * 3, ot = (size_t)nid[c + 4] * 3;
-            const double bx = d.rest[ob], by = d.rest[ob + 1], bz = d.rest[ob + 2];
-            const double tx = d.rest[ot], ty = d.rest[ot + 1], tz = d.rest[ot + 2];
-            dX[c][0] = (float)(bx - X0);
-            dX[c][1] = (float)(by - Y0);
-            dX[c][2] = (float)(bz - Z0);
-            dX[c + 4][0] = (float)(tx - X0);
-            dX[c + 4][1] = (float)(ty - Y0);
-            dX[c + 4][2] = (float)(tz - Z0);
-            D[c][0] = (float)(tx - bx);
-            D[c][1] = (float)(ty - by);
-            D[c][2] = (float)(tz - bz);
-        }
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            const size_t o = (size_t)nid[a] * 3;
-            dd[a][0] = d.disp[o] - u0;
-            dd[a][1] = d.disp[o + 1] - v0;
-            dd[a][2] = d.disp[o + 2] - w0;
-        }
+        const int c0l = lane & 24;  // the lane of the element's corner 0
+        const size_t og = (size_t)d.index[e * 8 + gp] * 3;
+        const double Xg = d.rest[og], Yg = d.rest[og + 1], Zg = d.rest[og + 2];
+        const float ug = d.disp[og], vg = d.disp[og + 1], wg = d.disp[og + 2];
+        const double X0 = __shfl_sync(0xffffffffu, Xg, c0l), Y0 = __shfl_sync(0xffffffffu, Yg, c0l),
+                     Z0 = __shfl_sync(0xffffffffu, Zg, c0l);
+        // this corner's top node (bottom corners 0-3 use it for their director)
+        const int topl = c0l + ((gp + 4) & 7);
+        const double Xt = __shfl_sync(0xffffffffu, Xg, topl), Yt = __shfl_sync(0xffffffffu, Yg, topl),
+                     Zt = __shfl_sync(0xffffffffu, Zg, topl);
+        const float u0 = __shfl_sync(0xffffffffu, ug, c0l), v0 = __shfl_sync(0xffffffffu, vg, c0l),
+                    w0 = __shfl_sync(0xffffffffu, wg, c0l);
+        dXg[0] = (float)(Xg - X0);
+        dXg[1] = (float)(Yg - Y0);
+        dXg[2] = (float)(Zg - Z0);
+        ddg[0] = ug - u0;
+        ddg[1] = vg - v0;
+        ddg[2] = wg - w0;
         if (KAHAN) {
             // the compensated displacement u - c as a double-float: the differences above
             // are exact (neighbouring values within a factor of two), and the difference
             // of the compensations restores the low bits u alone has lost
-            const float c0 = d.disp_c[(size_t)nid[0] * 3], c1 = d.disp_c[(size_t)nid[0] * 3 + 1],
-                        c2 = d.disp_c[(size_t)nid[0] * 3 + 2];
-#pragma unroll
-            for (int a = 1; a < 8; ++a) {
-                const size_t o = (size_t)nid[a] * 3;
-                dd[a][0] -= d.disp_c[o] - c0;
-                dd[a][1] -= d.disp_c[o + 1] - c1;
-                dd[a][2] -= d.disp_c[o + 2] - c2;
+            const float cg0 = d.disp_c[og], cg1 = d.disp_c[og + 1], cg2 = d.disp_c[og + 2];
+            const float c0 = __shfl_sync(0xffffffffu, cg0, c0l), c1 = __shfl_sync(0xffffffffu, cg1, c0l),
+                        c2 = __shfl_sync(0xffffffffu, cg2, c0l);
+            if (gp != 0) {
+                ddg[0] -= cg0 - c0;
+                ddg[1] -= cg1 - c1;
+                ddg[2] -= cg2 - c2;
             }
         }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            geo[kGeoX + gp * 3 + i] = dXg[i];
+            geo[kGeoDd + gp * 3 + i] = ddg[i];
+        }
+        if (gp < 4) {
+            geo[kGeoD + gp * 3] = (float)(Xt - Xg);
+            geo[kGeoD + gp * 3 + 1] = (float)(Yt - Yg);
+            geo[kGeoD + gp * 3 + 2] = (float)(Zt - Zg);
+        }
+        __syncwarp();
     }
     // ---- the element row: J0^-1 and the enhanced-mode scales (all zero: no valid forms) ----
     float j0[9], cm[7];
@@ -454,9 +458,10 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
-                a0 += sx[a] * dd[a][i];
-                a1 += sy[a] * dd[a][i];
-                a2 += sz[a] * dd[a][i];
+                const float v = geo[kGeoDd + a * 3 + i];
+                a0 += sx[a] * v;
+                a1 += sy[a] * v;
+                a2 += sz[a] * v;
             }
             jd[i * 3] = 0.125f * a0;
             jd[i * 3 + 1] = 0.125f * a1;
@@ -500,36 +505,26 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
             if (step <= 4.8e-7f * size || step * step <= 2.4e-7f * size) break;
         }
     }
-    // ---- co-rotated relative displacement u'_a = Q^T dX_a + dd_a + Q^T dd_a ----
-    float u[24];
+    // ---- co-rotated relative displacement u'_a = Q^T dX_a + dd_a + Q^T dd_a, lane a's
+    // corner formed by lane a and parked beside the others ----
+    {
+        const float sx = dXg[0] + ddg[0];
+        const float ty = dXg[1] + ddg[1];
+        const float wz = dXg[2] + ddg[2];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const float s = dX[a][0] + dd[a][0];
-            const float t = dX[a][1] + dd[a][1];
-            const float w = dX[a][2] + dd[a][2];
-            u[a * 3 + i] = dd[a][i] + (q[0 * 3 + i] * s + q[1 * 3 + i] * t + q[2 * 3 + i] * w);
-        }
+        for (int i = 0; i < 3; ++i)
+            geo[kGeoU + gp * 3 + i] = ddg[i] + (q[0 * 3 + i] * sx + q[1 * 3 + i] * ty + q[2 * 3 + i] * wz);
+        __syncwarp();
+    }
+    const float(*dX)[3] = reinterpret_cast<const float(*)[3]>(geo + kGeoX);
+    const float(*D)[3] = reinterpret_cast<const float(*)[3]>(geo + kGeoD);
+    const float* u = geo + kGeoU;
 
     // the rotation waits in shared memory through the Newton iterations (each lane its
     // own copy: no synchronisation), freeing nine registers there
     __shared__ float q_park[9][kShellBlock];
 #pragma unroll
     for (int k = 0; k < 9; ++k) q_park[k][threadIdx.x] = q[k];
-    // and the element's rest corners, one copy per element: its eight lanes hold the same
-    // values and each reads back what it wrote itself, so no synchronisation either
-    __shared__ float corner_park[24][kShellBlock / 8];
-    {
-        const int el = threadIdx.x >> 3;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                corner_park[c * 3 + i][el] = dX[c][i];
-                corner_park[12 + c * 3 + i][el] = D[c][i];
-            }
-    }
     // ---- the point's operators, formed from the rest geometry ----
     const ShellLanePoint P = shell_lane_point(gp);
     float gx[3], gy[3], Ainv[9], w;
@@ -1004,17 +999,9 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
 #pragma unroll
     for (int j = 0; j < 24; ++j) f[j] = 0.0f;
     {
-        float Xb[4][3], Dr[4][3], fx[3], fy[3], Af[9], wf;
-        const int el = threadIdx.x >> 3;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                Xb[c][i] = corner_park[c * 3 + i][el];
-                Dr[c][i] = corner_park[12 + c * 3 + i][el];
-            }
-        shell_frame(Xb, Dr, P, formed, fx, fy, Af, wf);
-        shell_force(Xb, Dr, P, fx, fy, Af, wf, o.sigma, f);
+        float fx[3], fy[3], Af[9], wf;
+        shell_frame(dX, D, P, formed, fx, fy, Af, wf);
+        shell_force(dX, D, P, fx, fy, Af, wf, o.sigma, f);
     }
     // round 1 (xor 4): keep nodes 0-3 (bit 2 clear) or 4-7
     const bool hi4 = (gp & 4) != 0, hi2 = (gp & 2) != 0, hi1 = (gp & 1) != 0;
@@ -1039,7 +1026,6 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     if (valid) {
         // lane gp now holds sum over points of node gp's internal force; apply -R
         float* out = d.slots + (size_t)d.slot[e * 8 + gp] * 3;
-#pragma unroll
         float qr[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) qr[k] = q_park[k][threadIdx.x];
