@@ -186,6 +186,11 @@ typedef struct femstep_pool femstep_pool;
 #define FEMSTEP_POOL_PERSISTENT 2  /* one cooperative launch per chunk, grid barriers */
 #define FEMSTEP_POOL_GRAPH_STAGED 3 /* GRAPH, each tile's per-tet rows staged in shared memory by
                                        bulk async copies (tiles of 128 and 256) */
+#define FEMSTEP_POOL_GRAPH_TILED 4  /* GRAPH, tiles of 128: a tile gathers its distinct nodes once and
+                                       writes one force partial per (tile, node); the node pass sums a
+                                       node's partials in tile order.  Same bits alone or in the mix;
+                                       the per-tile association differs from the other schedules' in
+                                       rounding */
 
 /* A pool holding up to `tet_capacity` tets and `node_capacity` nodes (each mesh also
    takes one spare node slot) of at most `max_meshes` meshes; tile = threads per block
@@ -253,7 +258,8 @@ int femstep_pool_dt(femstep_pool *pool, int id, double *dt);
    `steps` steps on the pool as it is, restores the pool's state after each trial (so
    tuning does not change any result), keeps the fastest, and reports it. */
 int femstep_pool_autotune(femstep_pool *pool, int steps, int *tile, int *mode, double *ms_per_step);
-/* Set the schedule by hand (tile 128 / 256 / 512; GRAPH, PERSISTENT or GRAPH_STAGED). */
+/* Set the schedule by hand (tile 128 / 256 / 512; GRAPH, PERSISTENT, GRAPH_STAGED, or
+   GRAPH_TILED at tile 128). */
 int femstep_pool_set_schedule(femstep_pool *pool, int tile, int mode);
 /* Mean device milliseconds per launch of [0] the element pass and [1] the node pass,
    over `steps` steps taken one launch at a time (the steps count as taken). */

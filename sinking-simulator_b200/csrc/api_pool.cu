@@ -25,6 +25,8 @@
 #include <thread>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
+
 #include "../../include/femstep.h"
 #include "common.cuh"
 #include "host_util.hpp"
@@ -221,7 +223,20 @@ struct femstep_pool {
     fs::PoolAdmit* d_admit = nullptr;  // [max_meshes]: an admission group's records
     unsigned long long* d_w2 = nullptr;  // [max_meshes]: the group's element bounds
     cudaGraphExec_t graph = nullptr;
-    bool graph_staged = false;  // which element pass the graph was captured with
+    fs::PoolPasses graph_passes = fs::PoolPasses::kDirect;  // what the graph was captured with
+    // the tiled schedule's tables for the current work list, allocated at first use
+    struct Tiled {
+        bool valid = false;
+        uint32_t *count = nullptr, *off = nullptr, *part_off = nullptr;
+        ushort4* lidx = nullptr;
+        uint16_t* inv = nullptr;
+        uint32_t *node_tab = nullptr, *part_slot = nullptr;
+        uint16_t* inv_start = nullptr;
+        size_t entries_cap = 0;
+        void* scan_tmp = nullptr;
+        size_t scan_bytes = 0;
+        uint32_t* h_total = nullptr;  // pinned: [0] last tile's offset, [1] its count
+    } tiled;
     long long launches = 0;
     bool in_flight = false;
     bool broken = false;
@@ -243,6 +258,11 @@ int check(femstep_pool* p, cudaError_t e, const char* what) {
     if (e == cudaSuccess) return FEMSTEP_OK;
     return fail(p, e == cudaErrorMemoryAllocation ? FEMSTEP_ENOMEM : FEMSTEP_ECUDA,
                 std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+bool valid_mode(int mode) {
+    return mode == FEMSTEP_POOL_GRAPH || mode == FEMSTEP_POOL_PERSISTENT || mode == FEMSTEP_POOL_GRAPH_STAGED ||
+           mode == FEMSTEP_POOL_GRAPH_TILED;
 }
 
 bool valid_id(const femstep_pool* p, int id) { return p && id >= 0 && id < p->max_meshes && p->meshes[id].used; }
@@ -292,32 +312,118 @@ int rebuild(femstep_pool* p) {
     p->d.active = p->d_active;
     p->d.n_active = (int)active.size();
     p->dirty = false;
+    p->tiled.valid = false;
     drop_graph(p);
     return check(p, cudaGetLastError(), "work list upload");
 }
 
+fs::PoolPasses passes_of(int mode) {
+    return mode == FEMSTEP_POOL_GRAPH_STAGED  ? fs::PoolPasses::kStaged
+           : mode == FEMSTEP_POOL_GRAPH_TILED ? fs::PoolPasses::kTiled
+                                              : fs::PoolPasses::kDirect;
+}
+
+void free_tiled(femstep_pool* p) {
+    auto& t = p->tiled;
+    for (void* q : {(void*)t.count, (void*)t.off, (void*)t.part_off, (void*)t.lidx, (void*)t.inv, (void*)t.node_tab,
+                    (void*)t.part_slot, (void*)t.inv_start, t.scan_tmp})
+        fs::device_free(q);
+    if (t.h_total) cudaFreeHost(t.h_total);
+    t = femstep_pool::Tiled{};
+}
+
+// The tiled schedule's tables for the current work list (tiles of 128): per tile its
+// distinct nodes, counted, scanned and filled on the device, then the node -> (tile,
+// node) CSR of the partials.  Waits once for the total count, to size the per-entry
+// arrays.
+int ensure_tiled(femstep_pool* p) {
+    auto& t = p->tiled;
+    if (t.valid) return FEMSTEP_OK;
+    if (p->tile != 128) return fail(p, FEMSTEP_EINVAL, "the tiled schedule runs tiles of 128");
+    PoolDevice& d = p->d;
+    const int G = d.n_etiles;
+    if (G == 0) return FEMSTEP_OK;
+    cudaError_t e = cudaSuccess;
+    if (!t.count) {
+        e = fs::device_alloc((void**)&t.count, (size_t)p->part_cap * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.off, (size_t)p->part_cap * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.part_off, (size_t)(p->node_cap + 1) * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.lidx, (size_t)p->tet_cap * sizeof(ushort4));
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.inv, (size_t)p->tet_cap * 4 * sizeof(uint16_t));
+        if (e == cudaSuccess)
+            e = cub::DeviceScan::ExclusiveSum(nullptr, t.scan_bytes, t.count, t.off, (int)p->part_cap, p->stream);
+        if (e == cudaSuccess) e = fs::device_alloc(&t.scan_tmp, t.scan_bytes ? t.scan_bytes : 1);
+        if (e == cudaSuccess) e = cudaHostAlloc((void**)&t.h_total, 2 * sizeof(uint32_t), cudaHostAllocPortable);
+        if (e != cudaSuccess) {
+            free_tiled(p);
+            return check(p, e, "tiled tables");
+        }
+    }
+    fs::launch_pool_tile_count(d, t.count, p->stream);
+    e = cub::DeviceScan::ExclusiveSum(t.scan_tmp, t.scan_bytes, t.count, t.off, G, p->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t.h_total, t.off + (G - 1), 4, cudaMemcpyDeviceToHost, p->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t.h_total + 1, t.count + (G - 1), 4, cudaMemcpyDeviceToHost, p->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) return check(p, e, "tiled tables");
+    const size_t total = (size_t)t.h_total[0] + t.h_total[1];
+    if (total > t.entries_cap) {
+        fs::device_free(t.node_tab);
+        fs::device_free(t.part_slot);
+        fs::device_free(t.inv_start);
+        t.node_tab = t.part_slot = nullptr;
+        t.inv_start = nullptr;
+        const size_t cap = total + total / 4 + 1024;
+        e = fs::device_alloc((void**)&t.node_tab, cap * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.part_slot, cap * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.inv_start, cap * 2);
+        if (e != cudaSuccess) {
+            t.entries_cap = 0;
+            return check(p, e, "tiled tables");
+        }
+        t.entries_cap = cap;
+    }
+    fs::launch_pool_tile_fill(d, t.off, t.node_tab, t.inv_start, t.lidx, t.inv, p->stream);
+    long long nmax = 0;
+    for (const HostMesh& m : p->meshes)
+        if (m.used) nmax = std::max(nmax, m.n0 + m.N + 1);
+    e = fs::build_csr_device(t.node_tab, (long long)total, nmax, t.part_off, t.part_slot, p->stream, nullptr, 0);
+    if (e != cudaSuccess) return check(p, e, "tiled partial CSR");
+    d.tab_off = t.off;
+    d.tab_count = t.count;
+    d.node_tab = t.node_tab;
+    d.inv_start = t.inv_start;
+    d.part_slot = t.part_slot;
+    d.lidx = t.lidx;
+    d.inv = t.inv;
+    d.part_off = t.part_off;
+    t.valid = true;
+    return check(p, cudaGetLastError(), "tiled tables");
+}
+
 // The graph of kGraphSteps steps over the current work list, captured once (nothing
 // runs while it is captured).
-int ensure_graph(femstep_pool* p, bool staged) {
-    if (p->graph && p->graph_staged != staged) drop_graph(p);
+int ensure_graph(femstep_pool* p, fs::PoolPasses passes) {
+    if (p->graph && p->graph_passes != passes) drop_graph(p);
+    if (passes == fs::PoolPasses::kTiled) {
+        const int rc = ensure_tiled(p);
+        if (rc) return rc;
+    }
     if (p->graph) return FEMSTEP_OK;
     cudaGraph_t g = nullptr;
     int rc = check(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "capture");
     if (rc) return rc;
-    fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream, staged);
+    fs::launch_pool_steps(p->d, p->tile, kGraphSteps, p->stream, passes);
     rc = check(p, cudaStreamEndCapture(p->stream, &g), "capture end");
     if (rc) return rc;
     rc = check(p, cudaGraphInstantiate(&p->graph, g, 0), "graph instantiate");
     cudaGraphDestroy(g);
     if (rc) return rc;
-    p->graph_staged = staged;
+    p->graph_passes = passes;
     return FEMSTEP_OK;
 }
 
 int launch_chunk(femstep_pool* p, int steps, int mode) {
     if (steps <= 0 || p->d.n_etiles == 0) return FEMSTEP_OK;
-    const bool staged = mode == FEMSTEP_POOL_GRAPH_STAGED;
-    if (p->graph && p->graph_staged != staged) drop_graph(p);
     if (mode == FEMSTEP_POOL_PERSISTENT) {
         const int blocks = std::min(fs::pool_persistent_max_blocks(p->tile), p->d.n_etiles);
         if (blocks <= 0) return fail(p, FEMSTEP_ECUDA, "no co-resident blocks for the persistent launch");
@@ -326,9 +432,14 @@ int launch_chunk(femstep_pool* p, int steps, int mode) {
         p->launches += 2;
         return rc;
     }
+    const fs::PoolPasses passes = passes_of(mode);
+    if (passes == fs::PoolPasses::kTiled) {
+        const int rc = ensure_tiled(p);
+        if (rc) return rc;
+    }
     int left = steps;
     if (left >= kGraphSteps) {
-        const int rc = ensure_graph(p, staged);
+        const int rc = ensure_graph(p, passes);
         if (rc) return rc;
         for (; left >= kGraphSteps; left -= kGraphSteps) {
             const int rc = check(p, cudaGraphLaunch(p->graph, p->stream), "graph launch");
@@ -337,7 +448,7 @@ int launch_chunk(femstep_pool* p, int steps, int mode) {
         }
     }
     if (left > 0) {
-        fs::launch_pool_steps(p->d, p->tile, left, p->stream, staged);
+        fs::launch_pool_steps(p->d, p->tile, left, p->stream, passes);
         p->launches += 2 * left + 1;
     }
     return check(p, cudaGetLastError(), "kernel launch");
@@ -1039,8 +1150,9 @@ int femstep_pool_run_async(femstep_pool* p, int steps, int mode) {
     if (steps < 0) return fail(p, FEMSTEP_EINVAL, "negative step count");
     if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is already running: wait for it first");
     if (mode == FEMSTEP_POOL_AUTO) mode = p->mode;
-    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT && mode != FEMSTEP_POOL_GRAPH_STAGED)
-        return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (!valid_mode(mode)) return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (mode == FEMSTEP_POOL_GRAPH_TILED && p->tile != 128)
+        return fail(p, FEMSTEP_EINVAL, "the tiled schedule runs tiles of 128");
     int rc = rebuild(p);
     if (rc) return rc;
     p->launches = 0;
@@ -1062,7 +1174,7 @@ int femstep_pool_prepare(femstep_pool* p) {
     int rc = rebuild(p);
     if (rc) return rc;
     if (p->d.n_etiles > 0 && p->mode != FEMSTEP_POOL_PERSISTENT)
-        rc = ensure_graph(p, p->mode == FEMSTEP_POOL_GRAPH_STAGED);
+        rc = ensure_graph(p, passes_of(p->mode));
     if (!rc) rc = check(p, cudaStreamSynchronize(p->stream), "prepare");
     return rc;
 }
@@ -1259,13 +1371,15 @@ int femstep_pool_autotune(femstep_pool* p, int steps, int* tile_out, int* mode_o
     int rc = snapshot(p, snap, false);
     if (rc) return rc;
     const int tiles[3] = {128, 256, 512};
-    const int modes[3] = {FEMSTEP_POOL_GRAPH, FEMSTEP_POOL_PERSISTENT, FEMSTEP_POOL_GRAPH_STAGED};
+    const int modes[4] = {FEMSTEP_POOL_GRAPH, FEMSTEP_POOL_PERSISTENT, FEMSTEP_POOL_GRAPH_STAGED,
+                          FEMSTEP_POOL_GRAPH_TILED};
     const int tile0 = p->tile, mode0 = p->mode;
     double best = INFINITY;
     int best_tile = tile0, best_mode = mode0;
     for (int ti = 0; ti < 3 && !rc; ++ti)
         for (int mi = 0; mi < 3 && !rc; ++mi) {
             if (modes[mi] == FEMSTEP_POOL_GRAPH_STAGED && tiles[ti] == 512) continue;  // staged: 128, 256
+            if (modes[mi] == FEMSTEP_POOL_GRAPH_TILED && tiles[ti] != 128) continue;   // tiled: 128
             p->tile = tiles[ti];
             p->dirty = true;
             double ms = 0.0;
@@ -1300,8 +1414,9 @@ int femstep_pool_set_schedule(femstep_pool* p, int tile, int mode) {
     if (!p) return fail(p, FEMSTEP_EINVAL, "null pool");
     if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
     if (tile != 128 && tile != 256 && tile != 512) return fail(p, FEMSTEP_EINVAL, "tile must be 128, 256 or 512");
-    if (mode != FEMSTEP_POOL_GRAPH && mode != FEMSTEP_POOL_PERSISTENT && mode != FEMSTEP_POOL_GRAPH_STAGED)
-        return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (!valid_mode(mode)) return fail(p, FEMSTEP_EINVAL, "bad mode");
+    if (mode == FEMSTEP_POOL_GRAPH_TILED && tile != 128)
+        return fail(p, FEMSTEP_EINVAL, "the tiled schedule runs tiles of 128");
     if (mode == FEMSTEP_POOL_GRAPH_STAGED && tile == 512)
         return fail(p, FEMSTEP_EINVAL, "the staged element pass runs tiles of 128 or 256");
     if (tile != p->tile) {
@@ -1321,14 +1436,22 @@ int femstep_pool_profile(femstep_pool* p, int steps, double out[2]) {
     if (p->in_flight) return fail(p, FEMSTEP_ESTATE, "a chunk is running: wait for it first");
     int rc = rebuild(p);
     if (rc) return rc;
+    const bool tiled = p->mode == FEMSTEP_POOL_GRAPH_TILED;
+    if (tiled) rc = ensure_tiled(p);
+    if (rc) return rc;
+    PoolDevice dn = p->d;
+    if (tiled) dn.offset = const_cast<uint32_t*>(p->d.part_off);
     cudaEvent_t ev[3];
     for (auto& e : ev) cudaEventCreate(&e);
     double te = 0.0, tn = 0.0;
     for (int s = 0; s < steps && !rc; ++s) {
         cudaEventRecord(ev[0], p->stream);
-        fs::launch_pool_element_pass(p->d, p->tile, s, p->stream, p->mode == FEMSTEP_POOL_GRAPH_STAGED);
+        if (tiled)
+            fs::launch_pool_tiled_element_pass(p->d, s, p->stream);
+        else
+            fs::launch_pool_element_pass(p->d, p->tile, s, p->stream, p->mode == FEMSTEP_POOL_GRAPH_STAGED);
         cudaEventRecord(ev[1], p->stream);
-        fs::launch_pool_node_pass(p->d, p->tile, s, p->stream);
+        fs::launch_pool_node_pass(dn, p->tile, s, p->stream);
         cudaEventRecord(ev[2], p->stream);
         rc = check(p, cudaEventSynchronize(ev[2]), "profile");
         float a = 0.0f, b = 0.0f;
@@ -1374,6 +1497,7 @@ void femstep_pool_destroy(femstep_pool* p) {
     if (!p) return;
     if (p->stream) cudaStreamSynchronize(p->stream);
     drop_graph(p);
+    free_tiled(p);
     p->arena.release();
     p->staging.release();
     if (p->h_meshes) cudaFreeHost(p->h_meshes);

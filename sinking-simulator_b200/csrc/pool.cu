@@ -310,11 +310,17 @@ void launch_pool_node_pass(const PoolDevice& d, int tile, int sub, cudaStream_t 
     }
 }
 
-void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream, bool staged) {
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream, PoolPasses passes) {
     if (d.n_etiles == 0 || steps <= 0) return;
+    // the tiled node pass gathers the per-tile partials through their own CSR
+    PoolDevice dn = d;
+    if (passes == PoolPasses::kTiled) dn.offset = const_cast<uint32_t*>(d.part_off);
     for (int s = 0; s < steps; ++s) {
-        launch_pool_element_pass(d, tile, s, stream, staged);
-        launch_pool_node_pass(d, tile, s, stream);
+        if (passes == PoolPasses::kTiled)
+            launch_pool_tiled_element_pass(d, s, stream);
+        else
+            launch_pool_element_pass(d, tile, s, stream, passes == PoolPasses::kStaged);
+        launch_pool_node_pass(dn, tile, s, stream);
     }
     pool_advance<<<blocks_for(d.n_active, 256), 256, 0, stream>>>(d, steps);
 }

@@ -75,14 +75,32 @@ struct PoolDevice {
     double* e_strain = nullptr;
     double* n_work = nullptr;
     double* n_kin = nullptr;
+    // The tiled schedule's tables (built for the work list at tile 128; null otherwise).
+    // Per element tile g: its distinct nodes, ascending, at node_tab[tab_off[g] ..
+    // tab_off[g] + tab_count[g]); per tet its corners' places in that list (lidx, four
+    // 16-bit ids); per corner of the tile, the tile's corners sorted by node and then by
+    // corner (inv, 16-bit corner numbers 4 x tet-in-tile + c, at 4 x the tet's pool
+    // index); per listed node the start of its corners in inv (inv_start) and the slot
+    // of its per-tile force partial (part_slot).  part_off: the node-major CSR over those
+    // partials, ascending tile within each node's run; the partials go in `slots`.
+    const uint32_t* tab_off = nullptr;
+    const uint32_t* tab_count = nullptr;
+    const uint32_t* node_tab = nullptr;
+    const uint16_t* inv_start = nullptr;
+    const uint32_t* part_slot = nullptr;
+    const ushort4* lidx = nullptr;
+    const uint16_t* inv = nullptr;
+    const uint32_t* part_off = nullptr;
     unsigned int* barrier = nullptr;  // [0] arrivals, [1] generation
     int* error = nullptr;             // set by a grid barrier that gave up waiting
 };
 
+// How a step's element pass runs: direct; with each tile's rows staged in shared
+// memory by bulk async copies (tiles of 128 and 256; a 512 tile runs the direct pass);
+// or tiled (tiles of 128: per-tile node gather and per-(tile, node) force partials).
+enum class PoolPasses { kDirect, kStaged, kTiled };
 // Two launches per step (element, node), `steps` times, then the advance, on `stream`.
-// staged: the element pass stages each tile's rows in shared memory by bulk async
-// copies (tiles of 128 and 256; a 512 tile runs the direct pass).
-void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream, bool staged);
+void launch_pool_steps(const PoolDevice& d, int tile, int steps, cudaStream_t stream, PoolPasses passes);
 // The passes one at a time (per-kernel timing): element or node pass of sub-step
 // `sub`, and the advance by `steps`.
 void launch_pool_element_pass(const PoolDevice& d, int tile, int sub, cudaStream_t stream, bool staged);
@@ -92,6 +110,24 @@ void launch_pool_advance(const PoolDevice& d, int steps, cudaStream_t stream);
 // then the advance.
 cudaError_t launch_pool_persistent(const PoolDevice& d, int tile, int steps, int blocks, cudaStream_t stream);
 int pool_persistent_max_blocks(int tile);
+// The tiled schedule (tiles of 128 tets): per element tile, its distinct nodes'
+// displacements are gathered once into shared memory, each tet's corner forces are
+// summed per node inside the tile (in tet order), and one partial per (tile, node) is
+// written; the node pass sums a node's partials in ascending tile order.
+//
+// Building the tables for the current work list (d.etiles), in two passes over the
+// tiles: pool_tile_count writes each tile's distinct-node count into `count`; after
+// the caller's exclusive scan of the counts into `off` (and with the arrays sized for
+// the total), pool_tile_fill writes node_tab, inv_start, lidx and inv.  The partial
+// slots and part_off are then the node -> (tile, node) CSR of node_tab
+// (build_csr_device).
+void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, cudaStream_t stream);
+void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, uint32_t* node_tab, uint16_t* inv_start,
+                           ushort4* lidx, uint16_t* inv, cudaStream_t stream);
+// The element pass of the tiled schedule (one block of 128 threads per element tile);
+// its node pass is launch_pool_node_pass over part_off and the partials.
+void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream);
+
 // One-time set-up of the pool's kernels on the current device (the staged pass's
 // shared-memory size and grid); call outside any stream capture.
 void pool_kernels_setup();

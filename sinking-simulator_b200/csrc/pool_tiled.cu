@@ -1,0 +1,296 @@
+// pool_tiled.cu -- the pool's tiled schedule: per-tile node gathers and per-(tile, node)
+// force partials.
+//
+// In the other schedules every tet writes its four corner forces to node-major slots
+// (64 B per tet) and the node pass reads them back (64 B per tet): half of a step's
+// HBM traffic.  Here a block takes one element tile (up to 128 consecutive tets of one
+// mesh) and:
+//   1. gathers the displacements (and compensations) of the tile's distinct nodes once
+//      into shared memory -- about 90 nodes for the 512 corners of a Kuhn box mesh;
+//   2. evaluates each tet from its corners there, with the arithmetic of every other
+//      schedule (tet_element_f32_eval), its corner forces into shared memory;
+//   3. sums, for each distinct node, the corner forces of the tile's tets that name
+//      it, in ascending tet order, and writes that one partial to the node's run of
+//      the per-(tile, node) CSR;
+// and the node pass sums a node's partials in ascending tile order (the other
+// schedules' node kernel over this CSR).  Per tet, the slot traffic falls from 128 B to
+// twice 16 B per (tile, node) pair -- about 22 B.
+//
+// A node's force is then (partial of its first tile) + (partial of the next) + ...,
+// each partial summed in tet order: the same terms as the other schedules' single
+// ascending run, associated per tile.  Tiles are aligned to their mesh's first tet, so
+// the association, and with it every bit of a mesh's result, does not depend on where
+// the mesh sits in the pool or what else is there; it differs from the other
+// schedules' in rounding only.
+//
+// The tables are built on the device for each work list: per tile, its corners are
+// sorted by (node, corner) in shared memory (a bitonic sort of 512 keys), which gives
+// the distinct nodes in ascending order, each corner's place in that list and, per
+// node, its corners in ascending order.
+#include <cub/block/block_scan.cuh>
+
+#include "common.cuh"
+#include "pool.hpp"
+#include "tet_f32.cuh"
+
+namespace fs {
+namespace {
+
+constexpr int kTiledTile = 128;              // tets per tile
+constexpr int kTiledCorners = 4 * kTiledTile;  // 512
+
+// The tile's corners, sorted: key = node << 9 | corner (corner = 4 x tet-in-tile + c);
+// slots past the tile's corners hold ~0 and sort last.  All 128 threads call it.
+__device__ __forceinline__ void sort_tile_corners(const PoolDevice& d, const PoolTile& tl,
+                                                  unsigned long long* key) {
+    const int corners = 4 * (int)(tl.end - tl.begin);
+    for (int i = threadIdx.x; i < kTiledCorners; i += kTiledTile) {
+        unsigned long long k = ~0ull;
+        if (i < corners) {
+            const uint4 id = d.index[tl.begin + (i >> 2)];
+            const uint32_t c = i & 3;
+            const uint32_t node = c == 0 ? id.x : (c == 1 ? id.y : (c == 2 ? id.z : id.w));
+            k = ((unsigned long long)node << 9) | (unsigned long long)i;
+        }
+        key[i] = k;
+    }
+    __syncthreads();
+    for (int size = 2; size <= kTiledCorners; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < kTiledCorners; i += kTiledTile) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const unsigned long long a = key[i], b = key[j];
+                    const bool up = (i & size) == 0;
+                    if ((a > b) == up) {
+                        key[i] = b;
+                        key[j] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// The sorted position i starts a new node (and is a real corner).
+__device__ __forceinline__ bool starts_node(const unsigned long long* key, int i) {
+    if (key[i] == ~0ull) return false;
+    return i == 0 || (key[i] >> 9) != (key[i - 1] >> 9);
+}
+
+using TileScan = cub::BlockScan<int, kTiledTile>;
+
+// Each thread takes four consecutive sorted positions; returns the thread's exclusive
+// prefix of node starts, and the tile's total in `total`.
+__device__ __forceinline__ int scan_node_starts(const unsigned long long* key, int (&flag)[4], int& total,
+                                                typename TileScan::TempStorage& tmp) {
+    int mine = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        flag[q] = starts_node(key, 4 * threadIdx.x + q) ? 1 : 0;
+        mine += flag[q];
+    }
+    int before = 0;
+    TileScan(tmp).ExclusiveSum(mine, before, total);
+    return before;
+}
+
+__global__ void __launch_bounds__(kTiledTile) pool_tile_count(PoolDevice d, uint32_t* count) {
+    __shared__ unsigned long long key[kTiledCorners];
+    __shared__ typename TileScan::TempStorage tmp;
+    const PoolTile tl = d.etiles[blockIdx.x];
+    sort_tile_corners(d, tl, key);
+    int flag[4], total = 0;
+    scan_node_starts(key, flag, total, tmp);
+    if (threadIdx.x == 0) count[blockIdx.x] = (uint32_t)total;
+}
+
+__global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const uint32_t* off, uint32_t* node_tab,
+                                                              uint16_t* inv_start, ushort4* lidx, uint16_t* inv) {
+    __shared__ unsigned long long key[kTiledCorners];
+    __shared__ uint16_t local[kTiledCorners];  // by corner: its node's place in the list
+    __shared__ typename TileScan::TempStorage tmp;
+    const PoolTile tl = d.etiles[blockIdx.x];
+    sort_tile_corners(d, tl, key);
+    int flag[4], total = 0;
+    int at = scan_node_starts(key, flag, total, tmp) - 1;  // the node of position 4 x thread - 1
+    const uint32_t base = off[blockIdx.x];
+    const long long c0 = 4 * tl.begin;  // the tile's corners in the per-corner arrays
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int i = 4 * threadIdx.x + q;
+        const unsigned long long k = key[i];
+        if (k == ~0ull) continue;
+        if (flag[q]) {
+            ++at;
+            node_tab[base + at] = (uint32_t)(k >> 9);
+            inv_start[base + at] = (uint16_t)i;
+        }
+        const int corner = (int)(k & 511ull);
+        inv[c0 + i] = (uint16_t)corner;
+        local[corner] = (uint16_t)at;
+    }
+    __syncthreads();
+    const long long t = tl.begin + threadIdx.x;
+    if (t < tl.end) {
+        const int c = 4 * threadIdx.x;
+        lidx[t] = make_ushort4(local[c], local[c + 1], local[c + 2], local[c + 3]);
+    }
+}
+
+// L2 prefetch of the rows the tiled pass reads for tets [begin, end): the corner places
+// (8 B per tet), Dm^-1 (9 rows of 4 B), the volume and the plastic state (7 rows); one
+// 128-byte line per thread of the block, every address inside its row's range.
+__device__ __forceinline__ void prefetch_tiled_rows(const PoolDevice& d, long long begin, long long end) {
+    if (end <= begin) return;
+    const int x = threadIdx.x;
+    const long long n = end - begin;
+    const int wide = (int)((n * 8 + 127) >> 7);
+    const int narrow = (int)((n * 4 + 127) >> 7);
+    const int span = narrow <= 1 ? 1 : 1 << (32 - __clz(narrow - 1));
+    const int shift = 31 - __clz(span);
+    int k = x;
+    if (k < wide) {
+        prefetch_l2(reinterpret_cast<const char*>(d.lidx + begin) + ((long long)k << 7));
+        return;
+    }
+    k -= wide;
+    const int row = k >> shift, line = k & (span - 1);
+    if (line >= narrow) return;
+    const float* rowp;
+    if (row < 9)
+        rowp = d.rest_inv + (size_t)row * d.tet_cap;
+    else if (row == 9)
+        rowp = d.rest_vol;
+    else if (row < 17)
+        rowp = d.plastic + (size_t)(row - 10) * d.tet_cap;
+    else
+        return;
+    prefetch_l2(reinterpret_cast<const char*>(rowp + begin) + ((long long)line << 7));
+}
+
+// A tet's own rows, loaded into registers before the tile's gather (so their latency
+// runs alongside it), handed to tet_element_f32_eval as its `Rows`.
+struct RegRows {
+    float dm[9], v, pl[7];
+    __device__ __forceinline__ float inv(int k, long long) const { return dm[k]; }
+    __device__ __forceinline__ float vol(long long) const { return v; }
+    __device__ __forceinline__ float plastic(int i, long long) const { return pl[i]; }
+};
+
+// The element pass, one block per element tile.  Shared memory: the distinct nodes'
+// displacement and compensation (up to 512 each; the tets' corner forces take the
+// displacements' place once every tet holds its corners), and the tile's tables (its
+// corners sorted by node, and per node the start of its corners and its partial's
+// slot): 20.5 KB, so eight blocks fit on an SM.
+__global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_tiled(PoolDevice d, int sub, int wave) {
+    __shared__ float4 su[kTiledCorners], sc[kTiledCorners];
+    float4* sf = su;  // corner c of tet i at c x 128 + i (no bank conflicts), after the corners are read
+    __shared__ uint16_t s_inv[kTiledCorners], s_start[kTiledCorners + 1];
+    __shared__ uint32_t s_slot[kTiledCorners];
+    __shared__ double scratch[64];
+    const int g = blockIdx.x;
+    const PoolTile tl = d.etiles[g];
+    const uint32_t base = d.tab_off[g];
+    const uint32_t count = d.tab_count[g];
+    const PoolMesh& m = d.meshes[tl.mesh];
+    const bool live = m.step + sub < m.target;  // the same in every thread
+    // the rows of the tile one wave later into L2, as the direct pass does
+    if (g + wave < d.n_etiles) {
+        const PoolTile nx = d.etiles[g + wave];
+        prefetch_tiled_rows(d, nx.begin, nx.end);
+        // and its tables: node list, corner starts, partial slots (first line of each,
+        // a tile's lists being a few hundred bytes), its sorted corners (1 KB)
+        const uint32_t ob = d.tab_off[g + wave];
+        if (threadIdx.x == 0) prefetch_l2(d.node_tab + ob);
+        if (threadIdx.x == 1) prefetch_l2(d.part_slot + ob);
+        if (threadIdx.x == 2) prefetch_l2(d.inv_start + ob);
+        if (threadIdx.x >= 3 && threadIdx.x < 11) {
+            const long long c = 4 * nx.begin + 64LL * (threadIdx.x - 3);
+            if (c < 4 * nx.end) prefetch_l2(d.inv + c);
+        }
+    }
+    const long long t = tl.begin + threadIdx.x;
+    const bool mine = live && t < tl.end;
+    // this tet's rows first: nothing below waits on them until the evaluation
+    RegRows rr;
+    ushort4 l = make_ushort4(0, 0, 0, 0);
+    if (mine) {
+        l = d.lidx[t];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) rr.dm[k] = d.rest_inv[(size_t)k * d.tet_cap + t];
+        rr.v = d.rest_vol[t];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) rr.pl[i] = d.plastic[(size_t)i * d.tet_cap + t];
+    }
+    const int k = live ? (int)count : 0;
+    const int corners = live ? 4 * (int)(tl.end - tl.begin) : 0;
+    const long long c0 = 4 * tl.begin;
+    // 1. the tile's nodes once each, and its tables
+    for (int j = threadIdx.x; j < k; j += kTiledTile) {
+        const uint32_t n = d.node_tab[base + j];
+        su[j] = d.disp[n];
+        sc[j] = d.disp_c[n];
+        s_start[j] = d.inv_start[base + j];
+        s_slot[j] = d.part_slot[base + j];
+    }
+    for (int i = threadIdx.x; i < corners; i += kTiledTile) s_inv[i] = d.inv[c0 + i];
+    if (threadIdx.x == 0) s_start[k] = (uint16_t)corners;
+    __syncthreads();
+    // 2. each tet from its corners in shared memory
+    float4 un[4], cn[4];
+    if (mine) {
+        un[0] = su[l.x], un[1] = su[l.y], un[2] = su[l.z], un[3] = su[l.w];
+        cn[0] = sc[l.x], cn[1] = sc[l.y], cn[2] = sc[l.z], cn[3] = sc[l.w];
+    }
+    __syncthreads();  // every tet holds its corners: the forces may overwrite them
+    double diss = 0.0, energy = 0.0;
+    if (mine) {
+        const TetElementRefs r{d.index,     d.slot, d.rest_inv, d.rest_vol, d.plastic,
+                               d.plastic_c, d.disp, d.disp_c,   d.slots,    d.tet_cap};
+        float4 fc[4];
+        tet_element_f32_eval<true, RegRows>(r, rr, t, m.mat, un, cn, diss, energy, fc);
+        sf[threadIdx.x] = fc[0];
+        sf[kTiledTile + threadIdx.x] = fc[1];
+        sf[2 * kTiledTile + threadIdx.x] = fc[2];
+        sf[3 * kTiledTile + threadIdx.x] = fc[3];
+    }
+    __syncthreads();
+    // 3. per node of the tile, its corners' forces in ascending tet order
+    for (int j = threadIdx.x; j < k; j += kTiledTile) {
+        const int b = s_start[j], e = s_start[j + 1];
+        int cr = s_inv[b];  // corner 4 x tet-in-tile + c
+        float4 f = sf[(cr & 3) * kTiledTile + (cr >> 2)];
+        for (int q = b + 1; q < e; ++q) {
+            cr = s_inv[q];
+            const float4 h = sf[(cr & 3) * kTiledTile + (cr >> 2)];
+            f.x += h.x;
+            f.y += h.y;
+            f.z += h.z;
+        }
+        d.slots[s_slot[j]] = make_float4(f.x, f.y, f.z, 0.0f);
+    }
+    block_sum2(diss, energy, scratch);  // valid in thread 0
+    if (live && threadIdx.x == 0) {
+        d.e_diss[tl.part] += diss;
+        d.e_strain[tl.part] = energy;
+    }
+}
+
+}  // namespace
+
+void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream) {
+    if (!d.n_etiles) return;
+    pool_elements_tiled<<<d.n_etiles, kTiledTile, 0, stream>>>(d, sub, sm_count() * (1024 / kTiledTile));
+}
+
+void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, cudaStream_t stream) {
+    if (d.n_etiles) pool_tile_count<<<d.n_etiles, kTiledTile, 0, stream>>>(d, count);
+}
+
+void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, uint32_t* node_tab, uint16_t* inv_start,
+                           ushort4* lidx, uint16_t* inv, cudaStream_t stream) {
+    if (d.n_etiles) pool_tile_fill<<<d.n_etiles, kTiledTile, 0, stream>>>(d, off, node_tab, inv_start, lidx, inv);
+}
+
+}  // namespace fs

@@ -145,8 +145,9 @@ struct ShellParams {
 constexpr int kShellBlock = 128;          // 16 elements per block
 // The step's per-element corner record in shared memory (floats): the corners' rest
 // differences to corner 0 (8 x 3), the bottom corners' directors (4 x 3), the
-// displacement differences to corner 0 (8 x 3) and the co-rotated displacements (8 x 3).
-constexpr int kGeoX = 0, kGeoD = 24, kGeoDd = 36, kGeoU = 60, kShellGeo = 84;
+// displacement differences to corner 0 (8 x 3), the co-rotated displacements (8 x 3)
+// and the centre's Voigt transform T0 (4 columns x 6).
+constexpr int kGeoX = 0, kGeoD = 24, kGeoDd = 36, kGeoU = 60, kGeoT = 84, kShellGeo = 108;
 constexpr int kShellNodeBlock = 256;
 constexpr int kShellPunchBlock = 256;   // the inertial punch: one block
 constexpr int kShellFiberBlock = 128;

@@ -532,8 +532,18 @@ __global__ void __launch_bounds__(kShellBlock, MINB) shell_forces(ShellDevice d,
     float eps_u[6];
     shell_strain(dX, D, u, P, gx, gy, Ainv, eps_u);
     // G factored: column j = gc_j T0[:, k_j], k = (0, 1, 2, 2, 2, 3, 3)
-    float T[24], gc[7];
-    shell_t0(j0, T);
+    // T0 is the element's, the same in its eight lanes: one copy in the element's record
+    // in shared memory rather than 24 registers in every lane through the Newton loop
+    float gc[7];
+    {
+        float T0[24];
+        shell_t0(j0, T0);
+        float4* t4 = reinterpret_cast<float4*>(geo + kGeoT);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t4[k] = make_float4(T0[4 * k], T0[4 * k + 1], T0[4 * k + 2], T0[4 * k + 3]);
+        __syncwarp();
+    }
+    const float* T = geo + kGeoT;
     shell_enhanced_scales(cm, w, P, gc);
     // element volume and the energy scale sigma_y V
     const float volume = sum8(w);

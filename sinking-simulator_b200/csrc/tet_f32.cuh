@@ -184,15 +184,15 @@ struct SharedRows {
     }
 };
 
-// One tet: forces into the node-major slots, plastic state advanced; returns the
-// dissipation and strain energy of the element (FP64, for the energy account).  The
-// arithmetic is the same whichever `Rows` supplies the tet's own rows.
 // One tet from its four corners' displacements un (and compensations cn), however
-// they were fetched: forces into the node-major slots, plastic state advanced.
+// they were fetched: its four corner forces into fc (x, y, z, 0), its plastic state
+// advanced; the dissipation and strain energy of the element in diss / energy (FP64,
+// for the energy account).  The arithmetic is the same whichever `Rows` supplies the
+// tet's own rows.
 template <bool KAHAN, class Rows>
-__device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d, const Rows& rows, long long t,
-                                                        const J2f& m, const float4 (&un)[4], const float4 (&cn)[4],
-                                                        double& diss, double& energy) {
+__device__ __forceinline__ void tet_element_f32_eval(const TetElementRefs& d, const Rows& rows, long long t,
+                                                     const J2f& m, const float4 (&un)[4], const float4 (&cn)[4],
+                                                     double& diss, double& energy, float4 (&fc)[4]) {
     M3<float> du, dm_inv;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -243,13 +243,9 @@ __device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d,
     // radial return, linear isotropic hardening (plasticity.cpp:333-456); for a linear
     // curve the consistency condition is affine in dgamma and its root is the closed
     // form below, which the CPU's Newton reaches in one step.
-    float ps[7], pc[7];
+    float ps[7];
 #pragma unroll
     for (int i = 0; i < 7; ++i) ps[i] = rows.plastic(i, t);
-    if (KAHAN) {
-#pragma unroll
-        for (int i = 0; i < 7; ++i) pc[i] = d.plastic_c[(size_t)i * d.stride + t];
-    }
     float el[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) el[i] = strain[i] - ps[i];
@@ -289,6 +285,10 @@ __device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d,
         diss = (double)dsum;
         const float deq = root23 * gamma;
         if (KAHAN) {
+            // the compensation is read only where the state changes
+            float pc[7];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) pc[i] = d.plastic_c[(size_t)i * d.stride + t];
 #pragma unroll
             for (int i = 0; i < 6; ++i) kahan_add(ps[i], pc[i], dp[i]);
             kahan_add(ps[6], pc[6], deq);
@@ -333,8 +333,6 @@ __device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d,
     for (int k = 0; k < 9; ++k) sig.m[k] += qs.m[k];
     const M3<float> hf = mul_fma(sig, transpose(dm_inv));
     const float scale = -volf;
-    const uint4 sl = rows.slot(t);
-    const unsigned sid[4] = {sl.x, sl.y, sl.z, sl.w};
     float f0[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -344,9 +342,24 @@ __device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d,
             v[a] = scale * hf(a, c);
             f0[a] -= v[a];
         }
-        d.slots[sid[c + 1]] = make_float4(v[0], v[1], v[2], 0.0f);  // one 16-byte store
+        fc[c + 1] = make_float4(v[0], v[1], v[2], 0.0f);
     }
-    d.slots[sid[0]] = make_float4(f0[0], f0[1], f0[2], 0.0f);
+    fc[0] = make_float4(f0[0], f0[1], f0[2], 0.0f);
+}
+
+// The same with the corner forces written to the node-major slots (one 16-byte store
+// each).
+template <bool KAHAN, class Rows>
+__device__ __forceinline__ void tet_element_f32_corners(const TetElementRefs& d, const Rows& rows, long long t,
+                                                        const J2f& m, const float4 (&un)[4], const float4 (&cn)[4],
+                                                        double& diss, double& energy) {
+    float4 fc[4];
+    tet_element_f32_eval<KAHAN, Rows>(d, rows, t, m, un, cn, diss, energy, fc);
+    const uint4 sl = rows.slot(t);
+    d.slots[sl.y] = fc[1];
+    d.slots[sl.z] = fc[2];
+    d.slots[sl.w] = fc[3];
+    d.slots[sl.x] = fc[0];
 }
 
 template <bool KAHAN, bool CG = false, class Rows = GlobalRows>

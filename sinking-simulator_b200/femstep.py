@@ -500,8 +500,9 @@ def shell_forms(nodes, formulation=2, youngs=206e9, poisson=0.3, density=7850.0,
 # Pool of many tet meshes: the batched and the served step (no reference counterpart:
 # the reference steps one mesh at a time, fem.cpp:187).
 
-POOL_AUTO, POOL_GRAPH, POOL_PERSISTENT, POOL_GRAPH_STAGED = 0, 1, 2, 3
-POOL_MODE_NAMES = {POOL_GRAPH: "graph", POOL_PERSISTENT: "persistent", POOL_GRAPH_STAGED: "graph-staged"}
+POOL_AUTO, POOL_GRAPH, POOL_PERSISTENT, POOL_GRAPH_STAGED, POOL_GRAPH_TILED = 0, 1, 2, 3, 4
+POOL_MODE_NAMES = {POOL_GRAPH: "graph", POOL_PERSISTENT: "persistent", POOL_GRAPH_STAGED: "graph-staged",
+                   POOL_GRAPH_TILED: "graph-tiled"}
 
 
 class PoolMeshC(C.Structure):

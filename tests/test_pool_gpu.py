@@ -212,20 +212,23 @@ def test_device_critical_dt_matches_single_mesh_bound(fem):
     assert abs(pool.dt(i) / crit(fem, m) - 1.0) < 1e-6
 
 
-@pytest.mark.parametrize("k", [0, 1, 2])
-def test_pool_meshes_against_fp64_oracle(fem, port, k):
+@pytest.mark.parametrize("k,mode", [(0, "graph"), (1, "graph"), (2, "graph"), (0, "graph-tiled"),
+                                    (1, "graph-tiled")])
+def test_pool_meshes_against_fp64_oracle(fem, port, k, mode):
     """Per-mesh materials, 2,000 steps, against O-tet64 (fem.cpp kinematics with the
-    J2 return in double): 1e-5 relative displacement; energy account within 0.5 %."""
+    J2 return in double): 1e-5 relative displacement; energy account within 0.5 %.  In
+    the graph schedule and in the tiled one (its own association of the node sums)."""
     loads = [200e3, 260e3, 230e3]
     m = beam(fem, 40, 4, 4, load=loads[k], clamp_end=k % 2)
     ref = O.TetMesh64(port, m["position"], m["index"], m["fixed"], m["external_force"])
     dt = port.tet64_critical_dt(C.byref(ref._s), 210e9, 0.3, 7850.0, 0.9)
     ref.step(O.tet64_params(dt=dt, ramp_steps=1000, yield_=MATS[k]["yield_strength"],
                             hardening=MATS[k]["hardening"]), 2000)
-    pool = fem.TetPool(100000, 30000, max_meshes=4)
+    code = {v: c for c, v in fem.POOL_MODE_NAMES.items()}[mode]
+    pool = fem.TetPool(100000, 30000, max_meshes=4, tile=128)
     pool.admit(steps=2000, dt=dt, **beam(fem, 8, 2, 2))  # a neighbour, so the mesh runs in a mix
     i = pool.admit(steps=2000, dt=dt, ramp_steps=1000, **MATS[k], **m)
-    pool.run(2000)
+    pool.run(2000, code)
     p, _ = pool.readback(i)
     rest = m["position"].astype(np.float64)
     u, ur = p - rest, ref.position - rest
@@ -369,3 +372,67 @@ def test_many_workload_meshes_same_bits_in_every_schedule(fem):
             assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[1], rb[1])
             assert np.array_equal(pa, pb)
             assert np.array_equal(ea, eb)
+
+
+def test_tiled_schedule_same_bits_alone_in_the_mix_and_resumed(fem):
+    """The tiled schedule associates each node's force sum per tile; its tiles are
+    aligned to the mesh's first tet, so a mesh's bits do not depend on its place in the
+    pool, its neighbours, the chunking or an eviction in between."""
+    a = beam(fem, 30, 3, 3, load=400e3)
+    others = [beam(fem, 16, 2, 2, load=80e3), beam(fem, 50, 4, 4, length=2.0, load=120e3)]
+    T = fem.POOL_GRAPH_TILED
+    alone = fem.TetPool(100000, 30000, max_meshes=4, tile=128)
+    ia = alone.admit(steps=1500, ramp_steps=500, **MATS[0], **a)
+    alone.run(1500, T)
+    pa, va = alone.readback(ia)
+    ea, pla = alone.energy(ia), alone.plastic(ia)
+    assert (pla[:, 6] > 0).mean() > 0.05, "the case must exercise plasticity"
+    mix = fem.TetPool(300000, 90000, max_meshes=8, tile=128)
+    j0 = mix.admit(steps=3000, ramp_steps=300, **MATS[1], **others[0])
+    mix.run(37, T)
+    ib = mix.admit(steps=1500, ramp_steps=500, **MATS[0], **a)  # mid-run, at another place
+    mix.run(400, T)
+    ck = mix.checkpoint(ib)
+    mix.release(ib)
+    j1 = mix.admit(steps=3000, ramp_steps=300, **MATS[2], **others[1])
+    mix.run(29, T)
+    ic = mix.admit_resume(ck, 1500, ramp_steps=500, **MATS[0], **a)
+    for chunk in (3, 64, 500, 533, 100):
+        mix.run(chunk, T)
+    assert mix.status(ic)[0] == 1500
+    pc, vc = mix.readback(ic)
+    assert np.array_equal(pa, pc) and np.array_equal(va, vc)
+    assert np.array_equal(pla, mix.plastic(ic))
+    assert np.array_equal(ea, mix.energy(ic))
+    assert mix.status(j0)[0] > 1500 and mix.status(j1)[0] > 1000
+
+
+def test_tiled_schedule_against_graph_on_workload_meshes(fem):
+    """48 of the batched workload's meshes (every clamp face, tip and pressure loads,
+    uneven sizes) in the tiled schedule against the graph schedule, after the ramp has
+    yielded several of them: the two sum the same terms in a different association, so
+    they agree to rounding -- 1e-6 of each mesh's largest displacement -- and their
+    energy accounts to 1e-6 of the external work."""
+    import workloads as W
+
+    specs = W.batch_meshes(count=48, lo=2e3, hi=3e4, seed=77)
+    built = [W.build(s) for s in specs]
+    kw = [dict(m.admit_kwargs(), ramp_steps=200) for m in built]
+    tets = sum(m.index.size // 4 for m in built)
+    nodes = sum(m.position.size // 3 + 1 for m in built)
+    out = []
+    for mode in (fem.POOL_GRAPH, fem.POOL_GRAPH_TILED):
+        pool = fem.TetPool(tets + 1000, nodes + 1000, max_meshes=64, tile=128)
+        ids = pool.admit_many(kw, [400] * len(kw))
+        pool.run(400, mode)
+        out.append([(pool.readback(i)[0], pool.energy(i), pool.plastic(i)) for i in ids])
+        pool.close()
+    yielded = 0
+    for b, (pg, eg, plg), (pt, et, plt) in zip(built, *out):
+        rest = b.position.astype(np.float64)
+        ug, ut = pg - rest, pt - rest
+        assert np.abs(ug - ut).max() <= 1e-6 * np.abs(ug).max(), b.spec
+        for j in (0, 1, 2, 3):
+            assert abs(eg[j] - et[j]) <= 1e-6 * abs(eg[0]), (b.spec, j)
+        yielded += (plg[:, 6] > 0).any()
+    assert yielded >= 5, yielded
