@@ -25,6 +25,7 @@
 #include <thread>
 #include <vector>
 
+#include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "../../include/femstep.h"
@@ -227,7 +228,7 @@ struct femstep_pool {
     // the tiled schedule's tables for the current work list, allocated at first use
     struct Tiled {
         bool valid = false;
-        uint32_t *count = nullptr, *off = nullptr, *part_off = nullptr;
+        uint32_t *count = nullptr, *span = nullptr, *off = nullptr, *part_off = nullptr, *kmax = nullptr;
         ushort4* lidx = nullptr;
         uint16_t* inv = nullptr;
         uint32_t *node_tab = nullptr, *part_slot = nullptr;
@@ -235,7 +236,8 @@ struct femstep_pool {
         size_t entries_cap = 0;
         void* scan_tmp = nullptr;
         size_t scan_bytes = 0;
-        uint32_t* h_total = nullptr;  // pinned: [0] last tile's offset, [1] its count
+        uint32_t* h_total = nullptr;  // pinned: [0] last tile's offset, [1] its span, [2] the largest count
+        int max_nodes = 0;            // distinct nodes of the largest tile
     } tiled;
     long long launches = 0;
     bool in_flight = false;
@@ -325,8 +327,8 @@ fs::PoolPasses passes_of(int mode) {
 
 void free_tiled(femstep_pool* p) {
     auto& t = p->tiled;
-    for (void* q : {(void*)t.count, (void*)t.off, (void*)t.part_off, (void*)t.lidx, (void*)t.inv, (void*)t.node_tab,
-                    (void*)t.part_slot, (void*)t.inv_start, t.scan_tmp})
+    for (void* q : {(void*)t.count, (void*)t.span, (void*)t.off, (void*)t.part_off, (void*)t.kmax, (void*)t.lidx,
+                    (void*)t.inv, (void*)t.node_tab, (void*)t.part_slot, (void*)t.inv_start, t.scan_tmp})
         fs::device_free(q);
     if (t.h_total) cudaFreeHost(t.h_total);
     t = femstep_pool::Tiled{};
@@ -346,26 +348,37 @@ int ensure_tiled(femstep_pool* p) {
     cudaError_t e = cudaSuccess;
     if (!t.count) {
         e = fs::device_alloc((void**)&t.count, (size_t)p->part_cap * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.span, (size_t)p->part_cap * 4);
         if (e == cudaSuccess) e = fs::device_alloc((void**)&t.off, (size_t)p->part_cap * 4);
-        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.part_off, (size_t)(p->node_cap + 1) * 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.kmax, 4);
+        if (e == cudaSuccess) e = fs::device_alloc((void**)&t.part_off, (size_t)(p->node_cap + 2) * 4);
         if (e == cudaSuccess) e = fs::device_alloc((void**)&t.lidx, (size_t)p->tet_cap * sizeof(ushort4));
         if (e == cudaSuccess) e = fs::device_alloc((void**)&t.inv, (size_t)p->tet_cap * 4 * sizeof(uint16_t));
+        size_t reduce_bytes = 0;
         if (e == cudaSuccess)
-            e = cub::DeviceScan::ExclusiveSum(nullptr, t.scan_bytes, t.count, t.off, (int)p->part_cap, p->stream);
+            e = cub::DeviceScan::ExclusiveSum(nullptr, t.scan_bytes, t.span, t.off, (int)p->part_cap, p->stream);
+        if (e == cudaSuccess)
+            e = cub::DeviceReduce::Max(nullptr, reduce_bytes, t.count, t.kmax, (int)p->part_cap, p->stream);
+        t.scan_bytes = std::max(t.scan_bytes, reduce_bytes);
         if (e == cudaSuccess) e = fs::device_alloc(&t.scan_tmp, t.scan_bytes ? t.scan_bytes : 1);
-        if (e == cudaSuccess) e = cudaHostAlloc((void**)&t.h_total, 2 * sizeof(uint32_t), cudaHostAllocPortable);
+        if (e == cudaSuccess) e = cudaHostAlloc((void**)&t.h_total, 3 * sizeof(uint32_t), cudaHostAllocPortable);
         if (e != cudaSuccess) {
             free_tiled(p);
             return check(p, e, "tiled tables");
         }
     }
-    fs::launch_pool_tile_count(d, t.count, p->stream);
-    e = cub::DeviceScan::ExclusiveSum(t.scan_tmp, t.scan_bytes, t.count, t.off, G, p->stream);
+    fs::launch_pool_tile_count(d, t.count, t.span, p->stream);
+    size_t tmp_bytes = t.scan_bytes;
+    e = cub::DeviceScan::ExclusiveSum(t.scan_tmp, tmp_bytes, t.span, t.off, G, p->stream);
+    tmp_bytes = t.scan_bytes;
+    if (e == cudaSuccess) e = cub::DeviceReduce::Max(t.scan_tmp, tmp_bytes, t.count, t.kmax, G, p->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(t.h_total, t.off + (G - 1), 4, cudaMemcpyDeviceToHost, p->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(t.h_total + 1, t.count + (G - 1), 4, cudaMemcpyDeviceToHost, p->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t.h_total + 1, t.span + (G - 1), 4, cudaMemcpyDeviceToHost, p->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t.h_total + 2, t.kmax, 4, cudaMemcpyDeviceToHost, p->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
     if (e != cudaSuccess) return check(p, e, "tiled tables");
     const size_t total = (size_t)t.h_total[0] + t.h_total[1];
+    t.max_nodes = (int)t.h_total[2];
     if (total > t.entries_cap) {
         fs::device_free(t.node_tab);
         fs::device_free(t.part_slot);
@@ -382,11 +395,12 @@ int ensure_tiled(femstep_pool* p) {
         }
         t.entries_cap = cap;
     }
-    fs::launch_pool_tile_fill(d, t.off, t.node_tab, t.inv_start, t.lidx, t.inv, p->stream);
     long long nmax = 0;
     for (const HostMesh& m : p->meshes)
         if (m.used) nmax = std::max(nmax, m.n0 + m.N + 1);
-    e = fs::build_csr_device(t.node_tab, (long long)total, nmax, t.part_off, t.part_slot, p->stream, nullptr, 0);
+    // the padding entries name node nmax, past every mesh: its run is never read
+    fs::launch_pool_tile_fill(d, t.off, t.node_tab, t.inv_start, t.lidx, t.inv, (uint32_t)nmax, p->stream);
+    e = fs::build_csr_device(t.node_tab, (long long)total, nmax + 1, t.part_off, t.part_slot, p->stream, nullptr, 0);
     if (e != cudaSuccess) return check(p, e, "tiled partial CSR");
     d.tab_off = t.off;
     d.tab_count = t.count;
@@ -396,6 +410,7 @@ int ensure_tiled(femstep_pool* p) {
     d.lidx = t.lidx;
     d.inv = t.inv;
     d.part_off = t.part_off;
+    d.tab_kcap = std::max(8, (t.max_nodes + 7) / 8 * 8);
     t.valid = true;
     return check(p, cudaGetLastError(), "tiled tables");
 }

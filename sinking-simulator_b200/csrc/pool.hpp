@@ -77,12 +77,14 @@ struct PoolDevice {
     double* n_kin = nullptr;
     // The tiled schedule's tables (built for the work list at tile 128; null otherwise).
     // Per element tile g: its distinct nodes, ascending, at node_tab[tab_off[g] ..
-    // tab_off[g] + tab_count[g]); per tet its corners' places in that list (lidx, four
-    // 16-bit ids); per corner of the tile, the tile's corners sorted by node and then by
-    // corner (inv, 16-bit corner numbers 4 x tet-in-tile + c, at 4 x the tet's pool
-    // index); per listed node the start of its corners in inv (inv_start) and the slot
-    // of its per-tile force partial (part_slot).  part_off: the node-major CSR over those
-    // partials, ascending tile within each node's run; the partials go in `slots`.
+    // tab_off[g] + tab_count[g]) (each tile's list padded to a multiple of 8 entries, so
+    // it starts on a 16-byte boundary); per tet its corners' places in that list (lidx,
+    // four 16-bit ids); the tile's corners sorted by node and then by tet (inv, at 4 x
+    // the tet's pool index, each given as its place c x 128 + i in the element pass's
+    // force buffer, corner c of tet i of the tile); per listed node the start of its
+    // corners in inv (inv_start) and the slot of its per-tile force partial (part_slot).
+    // part_off: the node-major CSR over those partials, ascending tile within each
+    // node's run; the partials go in `slots`.
     const uint32_t* tab_off = nullptr;
     const uint32_t* tab_count = nullptr;
     const uint32_t* node_tab = nullptr;
@@ -91,6 +93,7 @@ struct PoolDevice {
     const ushort4* lidx = nullptr;
     const uint16_t* inv = nullptr;
     const uint32_t* part_off = nullptr;
+    int tab_kcap = 0;  // the staged tiled pass's stage size: the largest tile's node count, to a multiple of 8
     unsigned int* barrier = nullptr;  // [0] arrivals, [1] generation
     int* error = nullptr;             // set by a grid barrier that gave up waiting
 };
@@ -121,9 +124,11 @@ int pool_persistent_max_blocks(int tile);
 // the total), pool_tile_fill writes node_tab, inv_start, lidx and inv.  The partial
 // slots and part_off are then the node -> (tile, node) CSR of node_tab
 // (build_csr_device).
-void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, cudaStream_t stream);
+// `span`: each tile's list length padded to a multiple of 8 (what `off` scans); the
+// padding entries name node `dump`, one past every mesh's nodes.
+void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span, cudaStream_t stream);
 void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, uint32_t* node_tab, uint16_t* inv_start,
-                           ushort4* lidx, uint16_t* inv, cudaStream_t stream);
+                           ushort4* lidx, uint16_t* inv, uint32_t dump, cudaStream_t stream);
 // The element pass of the tiled schedule (one block of 128 threads per element tile);
 // its node pass is launch_pool_node_pass over part_off and the partials.
 void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream);

@@ -27,6 +27,8 @@
 // sorted by (node, corner) in shared memory (a bitonic sort of 512 keys), which gives
 // the distinct nodes in ascending order, each corner's place in that list and, per
 // node, its corners in ascending order.
+#include <algorithm>
+
 #include <cub/block/block_scan.cuh>
 
 #include "common.cuh"
@@ -95,18 +97,28 @@ __device__ __forceinline__ int scan_node_starts(const unsigned long long* key, i
     return before;
 }
 
-__global__ void __launch_bounds__(kTiledTile) pool_tile_count(PoolDevice d, uint32_t* count) {
+// A tile's lists are padded to a multiple of 8 entries, so each starts on a 16-byte
+// boundary (for the staged pass's asynchronous copies).
+constexpr int kTablePad = 8;
+
+__global__ void __launch_bounds__(kTiledTile) pool_tile_count(PoolDevice d, uint32_t* count, uint32_t* span) {
     __shared__ unsigned long long key[kTiledCorners];
     __shared__ typename TileScan::TempStorage tmp;
     const PoolTile tl = d.etiles[blockIdx.x];
     sort_tile_corners(d, tl, key);
     int flag[4], total = 0;
     scan_node_starts(key, flag, total, tmp);
-    if (threadIdx.x == 0) count[blockIdx.x] = (uint32_t)total;
+    if (threadIdx.x == 0) {
+        count[blockIdx.x] = (uint32_t)total;
+        span[blockIdx.x] = (uint32_t)((total + kTablePad - 1) / kTablePad * kTablePad);
+    }
 }
 
+// `dump`: the node id the padding entries name (one past every mesh's nodes), so that
+// the partials' CSR counts them under a node no tile reads.
 __global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const uint32_t* off, uint32_t* node_tab,
-                                                              uint16_t* inv_start, ushort4* lidx, uint16_t* inv) {
+                                                              uint16_t* inv_start, ushort4* lidx, uint16_t* inv,
+                                                              uint32_t dump) {
     __shared__ unsigned long long key[kTiledCorners];
     __shared__ uint16_t local[kTiledCorners];  // by corner: its node's place in the list
     __shared__ typename TileScan::TempStorage tmp;
@@ -127,8 +139,15 @@ __global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const
             inv_start[base + at] = (uint16_t)i;
         }
         const int corner = (int)(k & 511ull);
-        inv[c0 + i] = (uint16_t)corner;
+        // stored as the corner's place in the element pass's force buffer, corner c of
+        // tet i at c x 128 + i
+        inv[c0 + i] = (uint16_t)((corner & 3) * kTiledTile + (corner >> 2));
         local[corner] = (uint16_t)at;
+    }
+    const int padded = (total + kTablePad - 1) / kTablePad * kTablePad;
+    if (threadIdx.x < padded - total) {
+        node_tab[base + total + threadIdx.x] = dump;
+        inv_start[base + total + threadIdx.x] = 0;
     }
     __syncthreads();
     const long long t = tl.begin + threadIdx.x;
@@ -259,11 +278,9 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
     // 3. per node of the tile, its corners' forces in ascending tet order
     for (int j = threadIdx.x; j < k; j += kTiledTile) {
         const int b = s_start[j], e = s_start[j + 1];
-        int cr = s_inv[b];  // corner 4 x tet-in-tile + c
-        float4 f = sf[(cr & 3) * kTiledTile + (cr >> 2)];
+        float4 f = sf[s_inv[b]];
         for (int q = b + 1; q < e; ++q) {
-            cr = s_inv[q];
-            const float4 h = sf[(cr & 3) * kTiledTile + (cr >> 2)];
+            const float4 h = sf[s_inv[q]];
             f.x += h.x;
             f.y += h.y;
             f.z += h.z;
@@ -277,20 +294,181 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
     }
 }
 
+// ---- the staged form: a persistent block walks its tiles, and while it computes one,
+// the next one's node gather and tables are already on their way into the other of two
+// shared-memory stages (cp.async, per thread, completed by wait_group and a barrier).
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// One stage for tiles of up to `kcap` distinct nodes (a multiple of 8): the nodes'
+// displacement and compensation, the tile's corner starts and partial slots (padded
+// lists, copied whole), its corners sorted by node.
+struct TiledStage {
+    float4* su;
+    float4* sc;
+    uint32_t* slot;
+    uint16_t* start;
+    uint16_t* inv;
+    __device__ __forceinline__ TiledStage(unsigned char* p, int kcap) {
+        su = reinterpret_cast<float4*>(p);
+        sc = su + kcap;
+        slot = reinterpret_cast<uint32_t*>(sc + kcap);
+        start = reinterpret_cast<uint16_t*>(slot + kcap);
+        inv = start + kcap;
+    }
+    __host__ __device__ static size_t bytes(int kcap) {
+        return (size_t)kcap * 32 + (size_t)kcap * 4 + (size_t)kcap * 2 + (size_t)kTiledCorners * 2;
+    }
+};
+
+// Queue the copies of tile g's gather and tables into `st` (every thread its share).
+__device__ __forceinline__ void tiled_fill(const PoolDevice& d, int g, int sub, const TiledStage& st) {
+    const PoolTile tl = d.etiles[g];
+    const PoolMesh& m = d.meshes[tl.mesh];
+    if (!(m.step + sub < m.target)) return;  // a frozen mesh's tile reads nothing
+    const uint32_t base = d.tab_off[g];
+    const int k = (int)d.tab_count[g];
+    const int kp = (k + kTablePad - 1) / kTablePad * kTablePad;
+    for (int j = threadIdx.x; j < k; j += kTiledTile) {
+        const uint32_t n = d.node_tab[base + j];
+        cp_async16(st.su + j, d.disp + n);
+        cp_async16(st.sc + j, d.disp_c + n);
+    }
+    // the padded lists from their 16-byte aligned starts: 4 slots, or 8 starts, a copy
+    for (int q = threadIdx.x; q < kp / 4; q += kTiledTile) cp_async16(st.slot + 4 * q, d.part_slot + base + 4 * q);
+    for (int q = threadIdx.x; q < kp / 8; q += kTiledTile)
+        cp_async16(st.start + 8 * q, d.inv_start + base + 8 * q);
+    // the sorted corners: four of them (8 bytes) per tet
+    const int n = (int)(tl.end - tl.begin);
+    if ((int)threadIdx.x < n) cp_async8(st.inv + 4 * threadIdx.x, d.inv + 4 * (tl.begin + threadIdx.x));
+}
+
+__global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_tiled_ring(PoolDevice d, int sub,
+                                                                                          int kcap) {
+    extern __shared__ __align__(16) unsigned char tiled_smem[];
+    __shared__ float4 sf[kTiledCorners];  // corner c of tet i at c x 128 + i
+    __shared__ double scratch[64];
+    const int G = (int)gridDim.x;
+    int g = blockIdx.x;
+    if (g >= d.n_etiles) return;
+    const TiledStage st0(tiled_smem, kcap), st1(tiled_smem + TiledStage::bytes(kcap), kcap);
+    tiled_fill(d, g, sub, st0);
+    cp_async_commit();
+    for (int it = 0;; ++it) {
+        const TiledStage& cur = (it & 1) ? st1 : st0;
+        const TiledStage& oth = (it & 1) ? st0 : st1;
+        const int nxt = g + G;
+        // the tile after next into L2: its rows and tables
+        if (nxt + G < d.n_etiles) {
+            const PoolTile nx = d.etiles[nxt + G];
+            prefetch_tiled_rows(d, nx.begin, nx.end);
+            const uint32_t ob = d.tab_off[nxt + G];
+            if (threadIdx.x == 0) prefetch_l2(d.node_tab + ob);
+            if (threadIdx.x == 1) prefetch_l2(d.part_slot + ob);
+            if (threadIdx.x == 2) prefetch_l2(d.inv_start + ob);
+        }
+        const PoolTile tl = d.etiles[g];
+        const PoolMesh& m = d.meshes[tl.mesh];
+        const bool live = m.step + sub < m.target;
+        const long long t = tl.begin + threadIdx.x;
+        const bool mine = live && t < tl.end;
+        // this tet's rows and corner places into registers (their latency overlaps the wait)
+        RegRows rr;
+        ushort4 l = make_ushort4(0, 0, 0, 0);
+        if (mine) {
+            l = d.lidx[t];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) rr.dm[q] = d.rest_inv[(size_t)q * d.tet_cap + t];
+            rr.v = d.rest_vol[t];
+#pragma unroll
+            for (int i = 0; i < 7; ++i) rr.pl[i] = d.plastic[(size_t)i * d.tet_cap + t];
+        }
+        // the next tile's copies go out now; this tile's have landed once all but the
+        // newest group are done, in every thread
+        if (nxt < d.n_etiles) tiled_fill(d, nxt, sub, oth);
+        cp_async_commit();
+        cp_async_wait_one();
+        __syncthreads();
+        double diss = 0.0, energy = 0.0;
+        if (mine) {
+            const float4 un[4] = {cur.su[l.x], cur.su[l.y], cur.su[l.z], cur.su[l.w]};
+            const float4 cn[4] = {cur.sc[l.x], cur.sc[l.y], cur.sc[l.z], cur.sc[l.w]};
+            const TetElementRefs r{d.index,     d.slot, d.rest_inv, d.rest_vol, d.plastic,
+                                   d.plastic_c, d.disp, d.disp_c,   d.slots,    d.tet_cap};
+            float4 fc[4];
+            tet_element_f32_eval<true, RegRows>(r, rr, t, m.mat, un, cn, diss, energy, fc);
+            sf[threadIdx.x] = fc[0];
+            sf[kTiledTile + threadIdx.x] = fc[1];
+            sf[2 * kTiledTile + threadIdx.x] = fc[2];
+            sf[3 * kTiledTile + threadIdx.x] = fc[3];
+        }
+        __syncthreads();
+        if (live) {
+            const int k = (int)d.tab_count[g];
+            const int corners = 4 * (int)(tl.end - tl.begin);
+            for (int j = threadIdx.x; j < k; j += kTiledTile) {
+                const int b = cur.start[j], e = j + 1 < k ? cur.start[j + 1] : corners;
+                float4 f = sf[cur.inv[b]];
+                for (int q = b + 1; q < e; ++q) {
+                    const float4 h = sf[cur.inv[q]];
+                    f.x += h.x;
+                    f.y += h.y;
+                    f.z += h.z;
+                }
+                d.slots[cur.slot[j]] = make_float4(f.x, f.y, f.z, 0.0f);
+            }
+        }
+        block_sum2(diss, energy, scratch);  // valid in thread 0; also ends the stage's reads
+        if (live && threadIdx.x == 0) {
+            d.e_diss[tl.part] += diss;
+            d.e_strain[tl.part] = energy;
+        }
+        if (nxt >= d.n_etiles) break;
+        g = nxt;
+    }
+    cp_async_wait_all();
+}
+
 }  // namespace
 
 void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream) {
     if (!d.n_etiles) return;
-    pool_elements_tiled<<<d.n_etiles, kTiledTile, 0, stream>>>(d, sub, sm_count() * (1024 / kTiledTile));
+    if (d.tab_kcap <= 0) {  // no stage size known: the one-block-per-tile form
+        pool_elements_tiled<<<d.n_etiles, kTiledTile, 0, stream>>>(d, sub, sm_count() * (1024 / kTiledTile));
+        return;
+    }
+    // the persistent staged form: as many blocks as fit with two stages of kcap nodes
+    static int cached_kcap = -1, per_sm = 1;
+    const size_t dyn = 2 * TiledStage::bytes(d.tab_kcap);
+    if (cached_kcap != d.tab_kcap) {
+        cudaFuncSetAttribute(pool_elements_tiled_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pool_elements_tiled_ring, kTiledTile, dyn);
+        per_sm = n > 0 ? n : 1;
+        cached_kcap = d.tab_kcap;
+    }
+    const int grid = std::min(d.n_etiles, per_sm * sm_count());
+    pool_elements_tiled_ring<<<grid, kTiledTile, dyn, stream>>>(d, sub, d.tab_kcap);
 }
 
-void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, cudaStream_t stream) {
-    if (d.n_etiles) pool_tile_count<<<d.n_etiles, kTiledTile, 0, stream>>>(d, count);
+void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span, cudaStream_t stream) {
+    if (d.n_etiles) pool_tile_count<<<d.n_etiles, kTiledTile, 0, stream>>>(d, count, span);
 }
 
 void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, uint32_t* node_tab, uint16_t* inv_start,
-                           ushort4* lidx, uint16_t* inv, cudaStream_t stream) {
-    if (d.n_etiles) pool_tile_fill<<<d.n_etiles, kTiledTile, 0, stream>>>(d, off, node_tab, inv_start, lidx, inv);
+                           ushort4* lidx, uint16_t* inv, uint32_t dump, cudaStream_t stream) {
+    if (d.n_etiles)
+        pool_tile_fill<<<d.n_etiles, kTiledTile, 0, stream>>>(d, off, node_tab, inv_start, lidx, inv, dump);
 }
 
 }  // namespace fs
