@@ -595,7 +595,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
     assert len(ids) == len(built)
     pool.run(0)
     admit_s = time.perf_counter() - t_admit
-    tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=16)
+    tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=48)
     # the work list and the schedule's captured graph are built before the warm-up, so
     # the timed chunk does no set-up whatever W is
     pool.prepare()
@@ -664,14 +664,14 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
                        "one left in the library's caches, as in a serving process; `cold_value` is the first"}
     drift = None if args.no_drift else pool_drift(F, W, specs)
     element_kernel = {"graph": "pool_elements", "graph-staged": "pool_elements_ring",
-                      "persistent": "pool_persistent", "graph-tiled": "pool_elements_tiled"}[tune["mode"]]
+                      "persistent": "pool_persistent", "graph-tiled": "pool_elements_tiled_ring"}[tune["mode"]]
     peak, peak_kind = measured_peak()
     if tune["mode"] == "graph-tiled":
         # the tiled schedule moves fewer bytes than the formula counts (per-(tile, node)
         # partials instead of per-corner slots): the step's formula bytes over the step's
         # time, an effective bandwidth that can exceed the copy peak
         achieved = (eb + nb) / (ms / args.steps / 1e3) / 1e9
-        kernel_label = ("pool_elements_tiled + pool_nodes (the whole step of the tiled schedule; effective "
+        kernel_label = ("pool_elements_tiled_ring + pool_nodes (the whole step of the tiled schedule; effective "
                         "bandwidth: the formula's bytes, slot exchange included, over the step's time)")
     else:
         achieved = eb / (elem_ms / 1e3) / 1e9
@@ -711,7 +711,7 @@ def run_serving(args, wl, rank, world, barrier, dist, local):
     pool = F.TetPool.for_budget(wl["budget"], nodes_per_tet=0.25, max_meshes=4096)
     # the schedule, tuned once on a representative mix
     warm = pool.admit_many([W.build(sp).admit_kwargs() for sp in trace[:48]], [10 ** 6] * 48)
-    tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=16)
+    tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=48)
     for i in warm:
         pool.release(i)
     reqs = [S.Request(key=k, arrival=sp.arrival, tets=sp.tets, steps=sp.steps,
