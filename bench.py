@@ -712,6 +712,11 @@ def run_serving(args, wl, rank, world, barrier, dist, local):
     # the schedule, tuned once on a representative mix
     warm = pool.admit_many([W.build(sp).admit_kwargs() for sp in trace[:48]], [10 ** 6] * 48)
     tune = fixed_schedule(F, pool, args.schedule) or pool.autotune(steps=48)
+    if not args.schedule and tune["mode"] == "graph-tiled":
+        # the tiled schedule rebuilds its tables whenever the mix changes, which a serving
+        # loop does at every chunk: serve with the staged pass at the same tile instead
+        pool.set_schedule(tune["tile"], F.POOL_GRAPH_STAGED)
+        tune = dict(tune, mode="graph-staged", note="the autotuner's graph-tiled replaced for serving")
     for i in warm:
         pool.release(i)
     reqs = [S.Request(key=k, arrival=sp.arrival, tets=sp.tets, steps=sp.steps,

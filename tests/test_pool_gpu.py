@@ -436,3 +436,23 @@ def test_tiled_schedule_against_graph_on_workload_meshes(fem):
             assert abs(eg[j] - et[j]) <= 1e-6 * abs(eg[0]), (b.spec, j)
         yielded += (plg[:, 6] > 0).any()
     assert yielded >= 5, yielded
+
+
+def test_tiled_schedule_refuses_other_tile_sizes(fem):
+    """The tiled schedule's tables are built for tiles of 128 tets: asking for it at
+    another tile size is refused with FEMSTEP_EINVAL, by set_schedule and by run, and the
+    pool keeps working in the schedules it has."""
+    m = beam(fem, 12, 2, 2, load=50e3)
+    pool = fem.TetPool(20000, 6000, max_meshes=2, tile=256)
+    pool.admit(steps=20, ramp_steps=10, **MATS[0], **m)
+    with pytest.raises(fem.FemStepError) as e:
+        pool.set_schedule(256, fem.POOL_GRAPH_TILED)
+    assert e.value.code == fem.EINVAL
+    with pytest.raises(fem.FemStepError) as e:
+        pool.run(5, fem.POOL_GRAPH_TILED)
+    assert e.value.code == fem.EINVAL
+    pool.run(5, fem.POOL_GRAPH)
+    pool.set_schedule(128, fem.POOL_GRAPH_TILED)
+    pool.run(15)
+    assert pool.status(0) == (20, 20)
+    pool.close()
