@@ -157,6 +157,9 @@ __global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const
     }
 }
 
+// Dm^-1 (9 rows), the volume and the plastic state (7 rows)
+constexpr int kRowsPrefetched = 17;
+
 // L2 prefetch of the rows the tiled pass reads for tets [begin, end): the corner places
 // (8 B per tet), Dm^-1 (9 rows of 4 B), the volume and the plastic state (7 rows); one
 // 128-byte line per thread of the block, every address inside its row's range.
@@ -196,6 +199,23 @@ struct RegRows {
     __device__ __forceinline__ float vol(long long) const { return v; }
     __device__ __forceinline__ float plastic(int i, long long) const { return pl[i]; }
 };
+
+// The same prefetch issued by one warp (lane 0..31), a few lines per lane.
+__device__ __forceinline__ void prefetch_tiled_rows_warp(const PoolDevice& d, long long begin, long long end,
+                                                         int lane) {
+    if (end <= begin) return;
+    const long long n = end - begin;
+    const int wide = (int)((n * 8 + 127) >> 7);
+    const int narrow = (int)((n * 4 + 127) >> 7);
+    for (int k = lane; k < wide; k += 32)
+        prefetch_l2(reinterpret_cast<const char*>(d.lidx + begin) + ((long long)k << 7));
+    for (int k = lane; k < kRowsPrefetched * narrow; k += 32) {
+        const int row = k / narrow, line = k - row * narrow;
+        const float* rowp = row < 9 ? d.rest_inv + (size_t)row * d.tet_cap
+                                    : (row == 9 ? d.rest_vol : d.plastic + (size_t)(row - 10) * d.tet_cap);
+        prefetch_l2(reinterpret_cast<const char*>(rowp + begin) + ((long long)line << 7));
+    }
+}
 
 // The element pass, one block per element tile.  Shared memory: the distinct nodes'
 // displacement and compensation (up to 512 each; the tets' corner forces take the
@@ -331,13 +351,24 @@ struct TiledStage {
     }
 };
 
-// Queue the copies of tile g's gather and tables into `st` (every thread its share).
-__device__ __forceinline__ void tiled_fill(const PoolDevice& d, int g, int sub, const TiledStage& st) {
+// What a block needs of its tile, kept in shared memory by the fill that loaded it.
+struct TiledInfo {
+    long long begin, end;
+    uint32_t base;
+    int k, mesh, part, live;
+};
+
+// Queue the copies of tile g's gather and tables into `st` (every thread its share);
+// thread 0 records the tile in `info`.
+__device__ __forceinline__ void tiled_fill(const PoolDevice& d, int g, int sub, const TiledStage& st,
+                                           TiledInfo& info) {
     const PoolTile tl = d.etiles[g];
     const PoolMesh& m = d.meshes[tl.mesh];
-    if (!(m.step + sub < m.target)) return;  // a frozen mesh's tile reads nothing
+    const bool live = m.step + sub < m.target;
     const uint32_t base = d.tab_off[g];
     const int k = (int)d.tab_count[g];
+    if (threadIdx.x == 0) info = TiledInfo{tl.begin, tl.end, base, k, tl.mesh, tl.part, live ? 1 : 0};
+    if (!live) return;  // a frozen mesh's tile reads nothing
     const int kp = (k + kTablePad - 1) / kTablePad * kTablePad;
     for (int j = threadIdx.x; j < k; j += kTiledTile) {
         const uint32_t n = d.node_tab[base + j];
@@ -358,30 +389,35 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
     extern __shared__ __align__(16) unsigned char tiled_smem[];
     __shared__ float4 sf[kTiledCorners];  // corner c of tet i at c x 128 + i
     __shared__ double scratch[64];
+    __shared__ TiledInfo info[2];
     const int G = (int)gridDim.x;
     int g = blockIdx.x;
     if (g >= d.n_etiles) return;
     const TiledStage st0(tiled_smem, kcap), st1(tiled_smem + TiledStage::bytes(kcap), kcap);
-    tiled_fill(d, g, sub, st0);
+    tiled_fill(d, g, sub, st0, info[0]);
     cp_async_commit();
     for (int it = 0;; ++it) {
         const TiledStage& cur = (it & 1) ? st1 : st0;
         const TiledStage& oth = (it & 1) ? st0 : st1;
         const int nxt = g + G;
-        // the tile after next into L2: its rows and tables
-        if (nxt + G < d.n_etiles) {
+        // the tile after next into L2, its rows and tables, by the last warp alone
+        if (threadIdx.x >= kTiledTile - 32 && nxt + G < d.n_etiles) {
             const PoolTile nx = d.etiles[nxt + G];
-            prefetch_tiled_rows(d, nx.begin, nx.end);
+            const int lane = threadIdx.x - (kTiledTile - 32);
+            prefetch_tiled_rows_warp(d, nx.begin, nx.end, lane);
             const uint32_t ob = d.tab_off[nxt + G];
-            if (threadIdx.x == 0) prefetch_l2(d.node_tab + ob);
-            if (threadIdx.x == 1) prefetch_l2(d.part_slot + ob);
-            if (threadIdx.x == 2) prefetch_l2(d.inv_start + ob);
+            if (lane == 0) prefetch_l2(d.node_tab + ob);
+            if (lane == 1) prefetch_l2(d.part_slot + ob);
+            if (lane == 2) prefetch_l2(d.inv_start + ob);
         }
-        const PoolTile tl = d.etiles[g];
-        const PoolMesh& m = d.meshes[tl.mesh];
-        const bool live = m.step + sub < m.target;
-        const long long t = tl.begin + threadIdx.x;
-        const bool mine = live && t < tl.end;
+        // this tile, as its fill recorded it (the barrier that ended the tile before, or
+        // the one below for the first, has made it visible)
+        if (it == 0) __syncthreads();
+        const TiledInfo& ti = info[it & 1];
+        const PoolMesh& m = d.meshes[ti.mesh];
+        const bool live = ti.live != 0;
+        const long long t = ti.begin + threadIdx.x;
+        const bool mine = live && t < ti.end;
         // this tet's rows and corner places into registers (their latency overlaps the wait)
         RegRows rr;
         ushort4 l = make_ushort4(0, 0, 0, 0);
@@ -395,7 +431,7 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
         }
         // the next tile's copies go out now; this tile's have landed once all but the
         // newest group are done, in every thread
-        if (nxt < d.n_etiles) tiled_fill(d, nxt, sub, oth);
+        if (nxt < d.n_etiles) tiled_fill(d, nxt, sub, oth, info[(it & 1) ^ 1]);
         cp_async_commit();
         cp_async_wait_one();
         __syncthreads();
@@ -414,8 +450,8 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
         }
         __syncthreads();
         if (live) {
-            const int k = (int)d.tab_count[g];
-            const int corners = 4 * (int)(tl.end - tl.begin);
+            const int k = ti.k;
+            const int corners = 4 * (int)(ti.end - ti.begin);
             for (int j = threadIdx.x; j < k; j += kTiledTile) {
                 const int b = cur.start[j], e = j + 1 < k ? cur.start[j + 1] : corners;
                 float4 f = sf[cur.inv[b]];
@@ -430,8 +466,8 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
         }
         block_sum2(diss, energy, scratch);  // valid in thread 0; also ends the stage's reads
         if (live && threadIdx.x == 0) {
-            d.e_diss[tl.part] += diss;
-            d.e_strain[tl.part] = energy;
+            d.e_diss[ti.part] += diss;
+            d.e_strain[ti.part] = energy;
         }
         if (nxt >= d.n_etiles) break;
         g = nxt;
