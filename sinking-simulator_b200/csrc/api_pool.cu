@@ -367,7 +367,7 @@ int ensure_tiled(femstep_pool* p) {
             return check(p, e, "tiled tables");
         }
     }
-    fs::launch_pool_tile_count(d, t.count, t.span, p->stream);
+    fs::launch_pool_tile_count(d, t.count, t.span, t.lidx, t.inv, p->stream);
     size_t tmp_bytes = t.scan_bytes;
     e = cub::DeviceScan::ExclusiveSum(t.scan_tmp, tmp_bytes, t.span, t.off, G, p->stream);
     tmp_bytes = t.scan_bytes;
@@ -398,9 +398,11 @@ int ensure_tiled(femstep_pool* p) {
     long long nmax = 0;
     for (const HostMesh& m : p->meshes)
         if (m.used) nmax = std::max(nmax, m.n0 + m.N + 1);
-    // the padding entries name node nmax, past every mesh: its run is never read
-    fs::launch_pool_tile_fill(d, t.off, t.node_tab, t.inv_start, t.lidx, t.inv, (uint32_t)nmax, p->stream);
-    e = fs::build_csr_device(t.node_tab, (long long)total, nmax + 1, t.part_off, t.part_slot, p->stream, nullptr, 0);
+    // the padding entries name node nmax, past every mesh, which the CSR leaves out
+    d.lidx = t.lidx;
+    d.inv = t.inv;
+    fs::launch_pool_tile_fill(d, t.off, t.count, t.node_tab, t.inv_start, (uint32_t)nmax, p->stream);
+    e = fs::build_csr_device(t.node_tab, (long long)total, nmax, t.part_off, t.part_slot, p->stream, nullptr, 0);
     if (e != cudaSuccess) return check(p, e, "tiled partial CSR");
     d.tab_off = t.off;
     d.tab_count = t.count;
@@ -1392,7 +1394,7 @@ int femstep_pool_autotune(femstep_pool* p, int steps, int* tile_out, int* mode_o
     double best = INFINITY;
     int best_tile = tile0, best_mode = mode0;
     for (int ti = 0; ti < 3 && !rc; ++ti)
-        for (int mi = 0; mi < 3 && !rc; ++mi) {
+        for (int mi = 0; mi < 4 && !rc; ++mi) {
             if (modes[mi] == FEMSTEP_POOL_GRAPH_STAGED && tiles[ti] == 512) continue;  // staged: 128, 256
             if (modes[mi] == FEMSTEP_POOL_GRAPH_TILED && tiles[ti] != 128) continue;   // tiled: 128
             p->tile = tiles[ti];

@@ -9,6 +9,8 @@
 // independent of the scatter's order and identical to the CPU counting sort.  Runs are
 // short (eight for an interior node of a hex mesh), so each node sorts its own run by
 // insertion.  The slot map inverts the entries: slot[corner] = its position in the CSR.
+// An entry naming a node id >= `nodes` is left out (no run, no slot): the pool's tiled
+// tables pad their lists with such entries.
 #include <cub/device/device_scan.cuh>
 
 #include "common.cuh"
@@ -17,14 +19,15 @@
 namespace fs {
 namespace {
 
-__global__ void csr_count(const uint32_t* index, long long total, uint32_t* count) {
+__global__ void csr_count(const uint32_t* index, long long total, long long nodes, uint32_t* count) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
-        atomicAdd(&count[index[i]], 1u);
+        if (index[i] < nodes) atomicAdd(&count[index[i]], 1u);
 }
 
-__global__ void csr_scatter(const uint32_t* index, long long total, uint32_t* cursor, uint32_t* entry) {
+__global__ void csr_scatter(const uint32_t* index, long long total, long long nodes, uint32_t* cursor,
+                            uint32_t* entry) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
-        entry[atomicAdd(&cursor[index[i]], 1u)] = (uint32_t)i;
+        if (index[i] < nodes) entry[atomicAdd(&cursor[index[i]], 1u)] = (uint32_t)i;
 }
 
 __global__ void csr_sort_runs(const uint32_t* offset, long long nodes, uint32_t* entry) {
@@ -42,7 +45,9 @@ __global__ void csr_sort_runs(const uint32_t* offset, long long nodes, uint32_t*
     }
 }
 
-__global__ void csr_slots(const uint32_t* entry, long long total, uint32_t* slot, uint32_t base) {
+// over the entries counted: offset[nodes] of them (before the base is added)
+__global__ void csr_slots(const uint32_t* entry, const uint32_t* counted, uint32_t* slot, uint32_t base) {
+    const long long total = *counted;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
         slot[entry[k]] = base + (uint32_t)k;
 }
@@ -67,16 +72,16 @@ cudaError_t build_csr_device(const uint32_t* index, long long total, long long n
         const int grid = 148 * 8;
         cudaMemsetAsync(count, 0, (size_t)nodes * sizeof(uint32_t), stream);
         cudaMemsetAsync(offset, 0, sizeof(uint32_t), stream);
-        csr_count<<<grid, 256, 0, stream>>>(index, total, count);
+        csr_count<<<grid, 256, 0, stream>>>(index, total, nodes, count);
         err = cub::DeviceScan::InclusiveSum(temp, temp_bytes, count, offset + 1, (int)nodes, stream);
     }
     if (err == cudaSuccess) {
         // the cursors start at each run's first position: offset[0 .. nodes)
         cudaMemcpyAsync(count, offset, (size_t)nodes * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
         const int grid = 148 * 8;
-        csr_scatter<<<grid, 256, 0, stream>>>(index, total, count, entry);
+        csr_scatter<<<grid, 256, 0, stream>>>(index, total, nodes, count, entry);
         csr_sort_runs<<<blocks_for(nodes, 256), 256, 0, stream>>>(offset, nodes, entry);
-        csr_slots<<<grid, 256, 0, stream>>>(entry, total, slot, base);
+        csr_slots<<<grid, 256, 0, stream>>>(entry, offset + nodes, slot, base);
         if (base) csr_add_base<<<grid, 256, 0, stream>>>(offset, nodes + 1, base);
         err = cudaGetLastError();
     }

@@ -119,16 +119,17 @@ int pool_persistent_max_blocks(int tile);
 // written; the node pass sums a node's partials in ascending tile order.
 //
 // Building the tables for the current work list (d.etiles), in two passes over the
-// tiles: pool_tile_count writes each tile's distinct-node count into `count`; after
-// the caller's exclusive scan of the counts into `off` (and with the arrays sized for
-// the total), pool_tile_fill writes node_tab, inv_start, lidx and inv.  The partial
-// slots and part_off are then the node -> (tile, node) CSR of node_tab
-// (build_csr_device).
-// `span`: each tile's list length padded to a multiple of 8 (what `off` scans); the
-// padding entries name node `dump`, one past every mesh's nodes.
-void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span, cudaStream_t stream);
-void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, uint32_t* node_tab, uint16_t* inv_start,
-                           ushort4* lidx, uint16_t* inv, uint32_t dump, cudaStream_t stream);
+// tiles with the caller's exclusive scan of the spans into `off` between them (and the
+// arrays sized for the total); the partial slots and part_off are then the node ->
+// (tile, node) CSR of node_tab (build_csr_device).
+// Pass 1 sorts each tile's corners and writes `count` (distinct nodes), `span` (that,
+// padded to a multiple of 8: what `off` scans), `lidx` and `inv`.  Pass 2, with d.lidx
+// set, writes node_tab and inv_start at the scanned offsets; the padding entries name
+// node `dump`, one past every mesh's nodes.
+void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span, ushort4* lidx, uint16_t* inv,
+                            cudaStream_t stream);
+void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, const uint32_t* count, uint32_t* node_tab,
+                           uint16_t* inv_start, uint32_t dump, cudaStream_t stream);
 // The element pass of the tiled schedule (one block of 128 threads per element tile);
 // its node pass is launch_pool_node_pass over part_off and the partials.
 void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream);

@@ -101,24 +101,11 @@ __device__ __forceinline__ int scan_node_starts(const unsigned long long* key, i
 // boundary (for the staged pass's asynchronous copies).
 constexpr int kTablePad = 8;
 
-__global__ void __launch_bounds__(kTiledTile) pool_tile_count(PoolDevice d, uint32_t* count, uint32_t* span) {
-    __shared__ unsigned long long key[kTiledCorners];
-    __shared__ typename TileScan::TempStorage tmp;
-    const PoolTile tl = d.etiles[blockIdx.x];
-    sort_tile_corners(d, tl, key);
-    int flag[4], total = 0;
-    scan_node_starts(key, flag, total, tmp);
-    if (threadIdx.x == 0) {
-        count[blockIdx.x] = (uint32_t)total;
-        span[blockIdx.x] = (uint32_t)((total + kTablePad - 1) / kTablePad * kTablePad);
-    }
-}
-
-// `dump`: the node id the padding entries name (one past every mesh's nodes), so that
-// the partials' CSR counts them under a node no tile reads.
-__global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const uint32_t* off, uint32_t* node_tab,
-                                                              uint16_t* inv_start, ushort4* lidx, uint16_t* inv,
-                                                              uint32_t dump) {
+// Pass 1: per tile, its corners sorted; the distinct-node count (and its padded
+// span), and the two tables that need no global offset: the sorted corners (inv) and
+// each tet's corner places in the tile's node list (lidx).
+__global__ void __launch_bounds__(kTiledTile) pool_tile_count(PoolDevice d, uint32_t* count, uint32_t* span,
+                                                               ushort4* lidx, uint16_t* inv) {
     __shared__ unsigned long long key[kTiledCorners];
     __shared__ uint16_t local[kTiledCorners];  // by corner: its node's place in the list
     __shared__ typename TileScan::TempStorage tmp;
@@ -126,34 +113,80 @@ __global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const
     sort_tile_corners(d, tl, key);
     int flag[4], total = 0;
     int at = scan_node_starts(key, flag, total, tmp) - 1;  // the node of position 4 x thread - 1
-    const uint32_t base = off[blockIdx.x];
     const long long c0 = 4 * tl.begin;  // the tile's corners in the per-corner arrays
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int i = 4 * threadIdx.x + q;
         const unsigned long long k = key[i];
         if (k == ~0ull) continue;
-        if (flag[q]) {
-            ++at;
-            node_tab[base + at] = (uint32_t)(k >> 9);
-            inv_start[base + at] = (uint16_t)i;
-        }
+        if (flag[q]) ++at;
         const int corner = (int)(k & 511ull);
         // stored as the corner's place in the element pass's force buffer, corner c of
         // tet i at c x 128 + i
         inv[c0 + i] = (uint16_t)((corner & 3) * kTiledTile + (corner >> 2));
         local[corner] = (uint16_t)at;
     }
-    const int padded = (total + kTablePad - 1) / kTablePad * kTablePad;
-    if (threadIdx.x < padded - total) {
-        node_tab[base + total + threadIdx.x] = dump;
-        inv_start[base + total + threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        count[blockIdx.x] = (uint32_t)total;
+        span[blockIdx.x] = (uint32_t)((total + kTablePad - 1) / kTablePad * kTablePad);
     }
     __syncthreads();
     const long long t = tl.begin + threadIdx.x;
     if (t < tl.end) {
         const int c = 4 * threadIdx.x;
         lidx[t] = make_ushort4(local[c], local[c + 1], local[c + 2], local[c + 3]);
+    }
+}
+
+// Pass 2, after the scan of the spans into `off`: the node list and, per node, the
+// start of its corners in the sorted list -- from the corner places alone, without a
+// second sort: a node's start is the number of the tile's corners whose nodes come
+// before it in the list.  Padding entries name node `dump`, one past every mesh's
+// nodes, so that the partials' CSR counts them under a node no tile reads.
+__global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const uint32_t* off, const uint32_t* count,
+                                                              uint32_t* node_tab, uint16_t* inv_start,
+                                                              uint32_t dump) {
+    __shared__ int hist[kTiledCorners];
+    __shared__ typename TileScan::TempStorage tmp;
+    const PoolTile tl = d.etiles[blockIdx.x];
+    const uint32_t base = off[blockIdx.x];
+    const int total = (int)count[blockIdx.x];
+    for (int j = threadIdx.x; j < kTiledCorners; j += kTiledTile) hist[j] = 0;
+    __syncthreads();
+    const long long t = tl.begin + threadIdx.x;
+    if (t < tl.end) {
+        const ushort4 l = d.lidx[t];
+        const uint4 id = d.index[t];
+        atomicAdd(&hist[l.x], 1);
+        atomicAdd(&hist[l.y], 1);
+        atomicAdd(&hist[l.z], 1);
+        atomicAdd(&hist[l.w], 1);
+        // every corner of a node writes the same id
+        node_tab[base + l.x] = id.x;
+        node_tab[base + l.y] = id.y;
+        node_tab[base + l.z] = id.z;
+        node_tab[base + l.w] = id.w;
+    }
+    __syncthreads();
+    // exclusive scan of the per-node corner counts: four consecutive nodes a thread
+    int v[4], mine = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        v[q] = hist[4 * threadIdx.x + q];
+        mine += v[q];
+    }
+    int before = 0, all = 0;
+    TileScan(tmp).ExclusiveSum(mine, before, all);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = 4 * threadIdx.x + q;
+        if (j < total) inv_start[base + j] = (uint16_t)before;
+        before += v[q];
+    }
+    const int padded = (total + kTablePad - 1) / kTablePad * kTablePad;
+    if ((int)threadIdx.x < padded - total) {
+        node_tab[base + total + threadIdx.x] = dump;
+        inv_start[base + total + threadIdx.x] = 0;
     }
 }
 
@@ -497,14 +530,15 @@ void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t s
     pool_elements_tiled_ring<<<grid, kTiledTile, dyn, stream>>>(d, sub, d.tab_kcap);
 }
 
-void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span, cudaStream_t stream) {
-    if (d.n_etiles) pool_tile_count<<<d.n_etiles, kTiledTile, 0, stream>>>(d, count, span);
+void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span, ushort4* lidx, uint16_t* inv,
+                            cudaStream_t stream) {
+    if (d.n_etiles) pool_tile_count<<<d.n_etiles, kTiledTile, 0, stream>>>(d, count, span, lidx, inv);
 }
 
-void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, uint32_t* node_tab, uint16_t* inv_start,
-                           ushort4* lidx, uint16_t* inv, uint32_t dump, cudaStream_t stream) {
+void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, const uint32_t* count, uint32_t* node_tab,
+                           uint16_t* inv_start, uint32_t dump, cudaStream_t stream) {
     if (d.n_etiles)
-        pool_tile_fill<<<d.n_etiles, kTiledTile, 0, stream>>>(d, off, node_tab, inv_start, lidx, inv, dump);
+        pool_tile_fill<<<d.n_etiles, kTiledTile, 0, stream>>>(d, off, count, node_tab, inv_start, dump);
 }
 
 }  // namespace fs
