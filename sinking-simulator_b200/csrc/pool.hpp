@@ -130,8 +130,9 @@ void launch_pool_tile_count(const PoolDevice& d, uint32_t* count, uint32_t* span
                             cudaStream_t stream);
 void launch_pool_tile_fill(const PoolDevice& d, const uint32_t* off, const uint32_t* count, uint32_t* node_tab,
                            uint16_t* inv_start, uint32_t dump, cudaStream_t stream);
-// The element pass of the tiled schedule (one block of 128 threads per element tile);
-// its node pass is launch_pool_node_pass over part_off and the partials.
+// The element pass of the tiled schedule: a persistent grid of blocks of 128 threads,
+// each walking its tiles with the next tile's node gather and tables in flight; its
+// node pass is launch_pool_node_pass over part_off and the partials.
 void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream);
 
 // One-time set-up of the pool's kernels on the current device (the staged pass's

@@ -28,6 +28,7 @@
 // the distinct nodes in ascending order, each corner's place in that list and, per
 // node, its corners in ascending order.
 #include <algorithm>
+#include <mutex>
 
 #include <cub/block/block_scan.cuh>
 
@@ -193,47 +194,9 @@ __global__ void __launch_bounds__(kTiledTile) pool_tile_fill(PoolDevice d, const
 // Dm^-1 (9 rows), the volume and the plastic state (7 rows)
 constexpr int kRowsPrefetched = 17;
 
-// L2 prefetch of the rows the tiled pass reads for tets [begin, end): the corner places
-// (8 B per tet), Dm^-1 (9 rows of 4 B), the volume and the plastic state (7 rows); one
-// 128-byte line per thread of the block, every address inside its row's range.
-__device__ __forceinline__ void prefetch_tiled_rows(const PoolDevice& d, long long begin, long long end) {
-    if (end <= begin) return;
-    const int x = threadIdx.x;
-    const long long n = end - begin;
-    const int wide = (int)((n * 8 + 127) >> 7);
-    const int narrow = (int)((n * 4 + 127) >> 7);
-    const int span = narrow <= 1 ? 1 : 1 << (32 - __clz(narrow - 1));
-    const int shift = 31 - __clz(span);
-    int k = x;
-    if (k < wide) {
-        prefetch_l2(reinterpret_cast<const char*>(d.lidx + begin) + ((long long)k << 7));
-        return;
-    }
-    k -= wide;
-    const int row = k >> shift, line = k & (span - 1);
-    if (line >= narrow) return;
-    const float* rowp;
-    if (row < 9)
-        rowp = d.rest_inv + (size_t)row * d.tet_cap;
-    else if (row == 9)
-        rowp = d.rest_vol;
-    else if (row < 17)
-        rowp = d.plastic + (size_t)(row - 10) * d.tet_cap;
-    else
-        return;
-    prefetch_l2(reinterpret_cast<const char*>(rowp + begin) + ((long long)line << 7));
-}
-
-// A tet's own rows, loaded into registers before the tile's gather (so their latency
-// runs alongside it), handed to tet_element_f32_eval as its `Rows`.
-struct RegRows {
-    float dm[9], v, pl[7];
-    __device__ __forceinline__ float inv(int k, long long) const { return dm[k]; }
-    __device__ __forceinline__ float vol(long long) const { return v; }
-    __device__ __forceinline__ float plastic(int i, long long) const { return pl[i]; }
-};
-
-// The same prefetch issued by one warp (lane 0..31), a few lines per lane.
+// L2 prefetch, by one warp (lane 0..31, a few lines each), of the rows the tiled pass
+// reads for tets [begin, end): the corner places (8 B per tet), Dm^-1 (9 rows of 4 B),
+// the volume and the plastic state (7 rows); every line starts inside its row's range.
 __device__ __forceinline__ void prefetch_tiled_rows_warp(const PoolDevice& d, long long begin, long long end,
                                                          int lane) {
     if (end <= begin) return;
@@ -250,102 +213,14 @@ __device__ __forceinline__ void prefetch_tiled_rows_warp(const PoolDevice& d, lo
     }
 }
 
-// The element pass, one block per element tile.  Shared memory: the distinct nodes'
-// displacement and compensation (up to 512 each; the tets' corner forces take the
-// displacements' place once every tet holds its corners), and the tile's tables (its
-// corners sorted by node, and per node the start of its corners and its partial's
-// slot): 20.5 KB, so eight blocks fit on an SM.
-__global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_tiled(PoolDevice d, int sub, int wave) {
-    __shared__ float4 su[kTiledCorners], sc[kTiledCorners];
-    float4* sf = su;  // corner c of tet i at c x 128 + i (no bank conflicts), after the corners are read
-    __shared__ uint16_t s_inv[kTiledCorners], s_start[kTiledCorners + 1];
-    __shared__ uint32_t s_slot[kTiledCorners];
-    __shared__ double scratch[64];
-    const int g = blockIdx.x;
-    const PoolTile tl = d.etiles[g];
-    const uint32_t base = d.tab_off[g];
-    const uint32_t count = d.tab_count[g];
-    const PoolMesh& m = d.meshes[tl.mesh];
-    const bool live = m.step + sub < m.target;  // the same in every thread
-    // the rows of the tile one wave later into L2, as the direct pass does
-    if (g + wave < d.n_etiles) {
-        const PoolTile nx = d.etiles[g + wave];
-        prefetch_tiled_rows(d, nx.begin, nx.end);
-        // and its tables: node list, corner starts, partial slots (first line of each,
-        // a tile's lists being a few hundred bytes), its sorted corners (1 KB)
-        const uint32_t ob = d.tab_off[g + wave];
-        if (threadIdx.x == 0) prefetch_l2(d.node_tab + ob);
-        if (threadIdx.x == 1) prefetch_l2(d.part_slot + ob);
-        if (threadIdx.x == 2) prefetch_l2(d.inv_start + ob);
-        if (threadIdx.x >= 3 && threadIdx.x < 11) {
-            const long long c = 4 * nx.begin + 64LL * (threadIdx.x - 3);
-            if (c < 4 * nx.end) prefetch_l2(d.inv + c);
-        }
-    }
-    const long long t = tl.begin + threadIdx.x;
-    const bool mine = live && t < tl.end;
-    // this tet's rows first: nothing below waits on them until the evaluation
-    RegRows rr;
-    ushort4 l = make_ushort4(0, 0, 0, 0);
-    if (mine) {
-        l = d.lidx[t];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) rr.dm[k] = d.rest_inv[(size_t)k * d.tet_cap + t];
-        rr.v = d.rest_vol[t];
-#pragma unroll
-        for (int i = 0; i < 7; ++i) rr.pl[i] = d.plastic[(size_t)i * d.tet_cap + t];
-    }
-    const int k = live ? (int)count : 0;
-    const int corners = live ? 4 * (int)(tl.end - tl.begin) : 0;
-    const long long c0 = 4 * tl.begin;
-    // 1. the tile's nodes once each, and its tables
-    for (int j = threadIdx.x; j < k; j += kTiledTile) {
-        const uint32_t n = d.node_tab[base + j];
-        su[j] = d.disp[n];
-        sc[j] = d.disp_c[n];
-        s_start[j] = d.inv_start[base + j];
-        s_slot[j] = d.part_slot[base + j];
-    }
-    for (int i = threadIdx.x; i < corners; i += kTiledTile) s_inv[i] = d.inv[c0 + i];
-    if (threadIdx.x == 0) s_start[k] = (uint16_t)corners;
-    __syncthreads();
-    // 2. each tet from its corners in shared memory
-    float4 un[4], cn[4];
-    if (mine) {
-        un[0] = su[l.x], un[1] = su[l.y], un[2] = su[l.z], un[3] = su[l.w];
-        cn[0] = sc[l.x], cn[1] = sc[l.y], cn[2] = sc[l.z], cn[3] = sc[l.w];
-    }
-    __syncthreads();  // every tet holds its corners: the forces may overwrite them
-    double diss = 0.0, energy = 0.0;
-    if (mine) {
-        const TetElementRefs r{d.index,     d.slot, d.rest_inv, d.rest_vol, d.plastic,
-                               d.plastic_c, d.disp, d.disp_c,   d.slots,    d.tet_cap};
-        float4 fc[4];
-        tet_element_f32_eval<true, RegRows>(r, rr, t, m.mat, un, cn, diss, energy, fc);
-        sf[threadIdx.x] = fc[0];
-        sf[kTiledTile + threadIdx.x] = fc[1];
-        sf[2 * kTiledTile + threadIdx.x] = fc[2];
-        sf[3 * kTiledTile + threadIdx.x] = fc[3];
-    }
-    __syncthreads();
-    // 3. per node of the tile, its corners' forces in ascending tet order
-    for (int j = threadIdx.x; j < k; j += kTiledTile) {
-        const int b = s_start[j], e = s_start[j + 1];
-        float4 f = sf[s_inv[b]];
-        for (int q = b + 1; q < e; ++q) {
-            const float4 h = sf[s_inv[q]];
-            f.x += h.x;
-            f.y += h.y;
-            f.z += h.z;
-        }
-        d.slots[s_slot[j]] = make_float4(f.x, f.y, f.z, 0.0f);
-    }
-    block_sum2(diss, energy, scratch);  // valid in thread 0
-    if (live && threadIdx.x == 0) {
-        d.e_diss[tl.part] += diss;
-        d.e_strain[tl.part] = energy;
-    }
-}
+// A tet's own rows, loaded into registers before the tile's corners arrive (so their
+// latency runs alongside the wait), handed to tet_element_f32_eval as its `Rows`.
+struct RegRows {
+    float dm[9], v, pl[7];
+    __device__ __forceinline__ float inv(int k, long long) const { return dm[k]; }
+    __device__ __forceinline__ float vol(long long) const { return v; }
+    __device__ __forceinline__ float plastic(int i, long long) const { return pl[i]; }
+};
 
 // ---- the staged form: a persistent block walks its tiles, and while it computes one,
 // the next one's node gather and tables are already on their way into the other of two
@@ -511,22 +386,23 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
 }  // namespace
 
 void launch_pool_tiled_element_pass(const PoolDevice& d, int sub, cudaStream_t stream) {
-    if (!d.n_etiles) return;
-    if (d.tab_kcap <= 0) {  // no stage size known: the one-block-per-tile form
-        pool_elements_tiled<<<d.n_etiles, kTiledTile, 0, stream>>>(d, sub, sm_count() * (1024 / kTiledTile));
-        return;
-    }
-    // the persistent staged form: as many blocks as fit with two stages of kcap nodes
-    static int cached_kcap = -1, per_sm = 1;
+    if (!d.n_etiles || d.tab_kcap <= 0) return;  // no tables: nothing to step
+    // a persistent grid of as many blocks as fit with two stages of kcap nodes.  The
+    // kernel's dynamic shared-memory ceiling only ever grows (under a lock), so a pool
+    // with smaller stages, in this thread or another, never lowers it under a launch.
+    static std::mutex lock;
+    static size_t ceiling = 0;
     const size_t dyn = 2 * TiledStage::bytes(d.tab_kcap);
-    if (cached_kcap != d.tab_kcap) {
-        cudaFuncSetAttribute(pool_elements_tiled_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        int n = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pool_elements_tiled_ring, kTiledTile, dyn);
-        per_sm = n > 0 ? n : 1;
-        cached_kcap = d.tab_kcap;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> hold(lock);
+        if (dyn > ceiling) {
+            cudaFuncSetAttribute(pool_elements_tiled_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            ceiling = dyn;
+        }
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pool_elements_tiled_ring, kTiledTile, dyn);
     }
-    const int grid = std::min(d.n_etiles, per_sm * sm_count());
+    const int grid = std::min(d.n_etiles, std::max(per_sm, 1) * sm_count());
     pool_elements_tiled_ring<<<grid, kTiledTile, dyn, stream>>>(d, sub, d.tab_kcap);
 }
 

@@ -152,8 +152,19 @@ def test_tile_sizes_and_autotune_leave_results_unchanged(fem):
     assert pool.status(i)[0] == 100  # tuning rolled its trial steps back
     pool.run(200)
     p, v = pool.readback(i)
-    assert np.array_equal(p, base[0]) and np.array_equal(v, base[1])
-    assert np.allclose(pool.energy(i), base[2], rtol=1e-12, atol=0.0)
+    # the same 300 steps with no tuning in between: 100 in the pool's first schedule,
+    # 200 in the one the autotuner picked (the tiled schedule has its own association,
+    # so this, not the graph schedule's bits, is what tuning must leave unchanged)
+    ref = fem.TetPool(50000, 15000, max_meshes=2)
+    j = ref.admit(steps=300, ramp_steps=150, **MATS[0], **m)
+    ref.run(100)
+    ref.set_schedule(best["tile"], {n: c for c, n in fem.POOL_MODE_NAMES.items()}[best["mode"]])
+    ref.run(200)
+    pr, vr = ref.readback(j)
+    assert np.array_equal(p, pr) and np.array_equal(v, vr)
+    assert np.allclose(pool.energy(i), ref.energy(j), rtol=1e-12, atol=0.0)
+    if best["mode"] != "graph-tiled":
+        assert np.array_equal(p, base[0]) and np.array_equal(v, base[1])
 
 
 def test_admission_against_capacity(fem):
