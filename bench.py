@@ -522,17 +522,19 @@ def plain_sequential(F, W, built, steps, mode):
     return units / (total_ms / 1e3), total_ms
 
 
-def pool_drift(F, W, specs, steps=2000):
+def pool_drift(F, W, specs, tune, steps=2000):
     """Drift of the batched FP32-compensated step against FP64 on a sample of the
     batch (workloads.drift_sample: the largest mesh and the smallest plate of each
-    clamped face and load kind), over the 1,000-step load ramp plus 1,000 steps.  The
-    FP64 side is the plain single-mesh FP64 GPU step, which is bit-identical to the FP64
-    oracle (tests/test_tet_gpu.py, tests/test_pool_gpu.py)."""
+    clamped face and load kind), over the 1,000-step load ramp plus 1,000 steps, in the
+    schedule and tile the line reports (`tune`).  The FP64 side is the plain single-mesh
+    FP64 GPU step, which is bit-identical to the FP64 oracle (tests/test_tet_gpu.py,
+    tests/test_pool_gpu.py)."""
     picks = W.drift_sample(specs)
     built = [W.build(specs[i]) for i in picks]
     T = sum(b.spec.tets for b in built)
     N = sum(b.spec.nodes for b in built)
-    pool = F.TetPool(T, N + len(built) + 1, max_meshes=len(built) + 1)
+    pool = F.TetPool(T, N + len(built) + 1, max_meshes=len(built) + 1, tile=tune["tile"])
+    pool.set_schedule(tune["tile"], {v: k for k, v in F.POOL_MODE_NAMES.items()}[tune["mode"]])
     mu, kappa = W.YOUNGS / (2 * (1 + W.POISSON)), W.YOUNGS / (3 * (1 - 2 * W.POISSON))
     ids, refs = [], []
     for b in built:
@@ -570,7 +572,8 @@ def pool_drift(F, W, specs, steps=2000):
                      "energy_terms_vs_work": float(np.abs(np.asarray(e[:4]) - np.asarray(e64[:4])).max()
                                                    / abs(e64[0]))})
     pool.close()
-    return {"meshes": picks, "steps": steps, "reference": "FP64 GPU step, bit-identical to the FP64 oracle",
+    return {"meshes": picks, "steps": steps, "schedule": f"{tune['tile']}:{tune['mode']}",
+            "reference": "FP64 GPU step, bit-identical to the FP64 oracle",
             "max_rel_displacement_error": max(r["displacement"] for r in rows),
             "max_rel_von_mises_error": max(r["von_mises"] for r in rows),
             "max_rel_plastic_strain_error": max(r["plastic_strain"] for r in rows),
@@ -662,7 +665,7 @@ def run_pool(args, wl, rank, world, barrier, dist, local):
                        "every mesh's positions and velocities (femstep_pool_readback_many), destroy.  `value` is "
                        "the second such job in the process, with the pinned staging and device memory the first "
                        "one left in the library's caches, as in a serving process; `cold_value` is the first"}
-    drift = None if args.no_drift else pool_drift(F, W, specs)
+    drift = None if args.no_drift else pool_drift(F, W, specs, tune)
     element_kernel = {"graph": "pool_elements", "graph-staged": "pool_elements_ring",
                       "persistent": "pool_persistent", "graph-tiled": "pool_elements_tiled_ring"}[tune["mode"]]
     peak, peak_kind = measured_peak()
