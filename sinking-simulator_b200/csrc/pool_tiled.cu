@@ -318,8 +318,8 @@ __global__ void __launch_bounds__(kTiledTile, 1024 / kTiledTile) pool_elements_t
             if (lane == 1) prefetch_l2(d.part_slot + ob);
             if (lane == 2) prefetch_l2(d.inv_start + ob);
         }
-        // this tile, as its fill recorded it (the barrier that ended the tile before, or
-        // the one below for the first, has made it visible)
+        // this tile, as its fill recorded it: visible after the barriers of the tile before
+        // (its wait), or, for the first tile, after this one
         if (it == 0) __syncthreads();
         const TiledInfo& ti = info[it & 1];
         const PoolMesh& m = d.meshes[ti.mesh];
