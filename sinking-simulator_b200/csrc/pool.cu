@@ -492,7 +492,7 @@ __global__ void pool_admit_omega(PoolDevice d, const PoolAdmit* adm, int G, long
         for (int c = 0; c < 3; ++c)
             for (int r = 0; r < 3; ++r) gr[c + 1][r] = (double)d.rest_inv[(size_t)(r * 3 + c) * d.tet_cap + t];
         for (int r = 0; r < 3; ++r) gr[0][r] = -(gr[1][r] + gr[2][r] + gr[3][r]);
-        const double v = tet_omega2_one(gr, a.lambda, a.mu, a.density);
+        const double v = tet_omega2_one<true>(gr, a.lambda, a.mu, a.density);
         atomicMax(w2 + g, (unsigned long long)__double_as_longlong(v > 0.0 ? v : 0.0));
     }
 }

@@ -157,7 +157,8 @@ struct PoolAdmit {
 // uploaded: zero the plastic state and the energy partials, form the FP64 rest state
 // (Dm^-1, volumes, lumped masses), start the nodes at rest, and, for the meshes that
 // want it, set the time step to 0.9 x the FP64 element bound, 2 / sqrt(max omega^2)
-// over its tets (tet_omega2_one, the single-mesh handle's bound).
+// over its tets (tet_omega2_one, the single-mesh handle's bound, normalising its iterate
+// by a reciprocal: within rounding of the single-mesh value).
 // `adm` (device) holds the G records; `w2` is G scratch words.  Four launches per
 // group, whatever its size.
 void launch_pool_admit(const PoolDevice& d, const PoolAdmit* adm, int G, long long tets, long long nodes,
