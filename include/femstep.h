@@ -190,7 +190,9 @@ typedef struct femstep_pool femstep_pool;
                                        writes one force partial per (tile, node); the node pass sums a
                                        node's partials in tile order.  Same bits alone or in the mix;
                                        the per-tile association differs from the other schedules' in
-                                       rounding */
+                                       rounding.  Its tables are allocated at first use (about 21 B
+                                       per tet and 4 B per node of capacity, beyond the pool's own)
+                                       and rebuilt whenever the set of meshes changes */
 
 /* A pool holding up to `tet_capacity` tets and `node_capacity` nodes (each mesh also
    takes one spare node slot) of at most `max_meshes` meshes; tile = threads per block

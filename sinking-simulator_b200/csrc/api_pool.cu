@@ -234,6 +234,7 @@ struct femstep_pool {
         uint32_t *node_tab = nullptr, *part_slot = nullptr;
         uint16_t* inv_start = nullptr;
         size_t entries_cap = 0;
+        size_t fixed_bytes = 0;       // the per-capacity arrays, allocated at first use
         void* scan_tmp = nullptr;
         size_t scan_bytes = 0;
         uint32_t* h_total = nullptr;  // pinned: [0] last tile's offset, [1] its span, [2] the largest count
@@ -354,6 +355,7 @@ int ensure_tiled(femstep_pool* p) {
         if (e == cudaSuccess) e = fs::device_alloc((void**)&t.part_off, (size_t)(p->node_cap + 2) * 4);
         if (e == cudaSuccess) e = fs::device_alloc((void**)&t.lidx, (size_t)p->tet_cap * sizeof(ushort4));
         if (e == cudaSuccess) e = fs::device_alloc((void**)&t.inv, (size_t)p->tet_cap * 4 * sizeof(uint16_t));
+        t.fixed_bytes = (size_t)p->part_cap * 12 + 4 + (size_t)(p->node_cap + 2) * 4 + (size_t)p->tet_cap * 16;
         size_t reduce_bytes = 0;
         if (e == cudaSuccess)
             e = cub::DeviceScan::ExclusiveSum(nullptr, t.scan_bytes, t.span, t.off, (int)p->part_cap, p->stream);
@@ -1503,7 +1505,8 @@ int femstep_pool_info(femstep_pool* p, long long out[8]) {
     out[3] = p->tile;
     out[4] = p->mode;
     out[5] = p->launches;
-    out[6] = (long long)p->arena.bytes();
+    // the pool's own arrays, and the tiled schedule's tables where they were built
+    out[6] = (long long)(p->arena.bytes() + p->tiled.fixed_bytes + p->tiled.entries_cap * 10);
     out[7] = (long long)p->staging.count();
     return FEMSTEP_OK;
 }
