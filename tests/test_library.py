@@ -23,6 +23,22 @@ def test_library_exports_every_declared_symbol(fem):
         assert hasattr(fem.lib, name), name
 
 
+def test_binding_constants_match_the_header(fem):
+    """The status codes and the pool's schedule codes the Python binding passes through
+    the C ABI are the header's own values."""
+    text = open(HEADER).read()
+    defines = {k: int(v) for k, v in re.findall(r"#define\s+(FEMSTEP_[A-Z0-9_]+)\s+(-?\d+)", text)}
+    pairs = {"FEMSTEP_POOL_AUTO": fem.POOL_AUTO, "FEMSTEP_POOL_GRAPH": fem.POOL_GRAPH,
+             "FEMSTEP_POOL_PERSISTENT": fem.POOL_PERSISTENT, "FEMSTEP_POOL_GRAPH_STAGED": fem.POOL_GRAPH_STAGED,
+             "FEMSTEP_POOL_GRAPH_TILED": fem.POOL_GRAPH_TILED, "FEMSTEP_OK": fem.OK, "FEMSTEP_SKIP": fem.SKIP,
+             "FEMSTEP_EINVAL": fem.EINVAL, "FEMSTEP_ENOMEM": fem.ENOMEM, "FEMSTEP_ECUDA": fem.ECUDA,
+             "FEMSTEP_ESTATE": fem.ESTATE, "FEMSTEP_ETIMEOUT": fem.ETIMEOUT}
+    for name, value in pairs.items():
+        assert defines.get(name) == value, (name, defines.get(name), value)
+    assert set(fem.POOL_MODE_NAMES) == {fem.POOL_GRAPH, fem.POOL_PERSISTENT, fem.POOL_GRAPH_STAGED,
+                                        fem.POOL_GRAPH_TILED}
+
+
 def _has_gpu(fem):
     buf = C.create_string_buffer(64)
     return fem.lib.femstep_device_name(buf, 64) == 0
